@@ -1,0 +1,328 @@
+#!/usr/bin/env python
+"""Benchmark of the path-trace pass on the procedural city (config 1).
+
+Workload: 1,984,402 triangles (4,000 seeded boxes and UV spheres, 4,002 units), 200 emissive quads under a light
+tree, a 90,000-lux sun and a baked gradient sky; 1280 x 720, 1 spp, max depth 4; the camera on a seeded Catmull-Rom
+spline of 240 frames. A step is one frame: one wave of 921,600 paths through every bounce, closest-hit and shadow
+rays. `value` counts every ray traced (closest + shadow) per second of device time, all ranks together.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torchrun, one rank per GPU; each rank renders its own frames of the spline (no collective on the
+data path: weak scaling), and the time is the max over ranks. `--impl reference` times the reference algorithm's
+CPU restatement (the oracle) on the host's cores over a bounded sample of each frame's pixels: the reference's own
+WGSL pass needs a graphics stack that neither this machine nor the GPU box has.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+FRAMES = 240
+WIDTH, HEIGHT, DEPTH, SPP = 1280, 720, 4, 1
+WORKLOAD = "procedural city 1984402 tris / 4002 units, 1280x720, 1 spp, depth 4, sun + sky + 400 emitter tris"
+METRIC = "Mrays/s (closest + shadow rays, city 720p 1 spp depth 4)"
+# Algorithmic bytes a walk reads: a node record, a triangle's leaf record, the part of a unit record the walk reads.
+NODE_BYTES, LEAF_BYTES, UNIT_BYTES = 32, 48, 64
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per extend launch from the committed ncu summary of this workload, if there is one."""
+    p = ROOT / "profiles" / "extend_city720p.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("dram_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi's clocks and throttle reasons of one GPU every 200 ms while it runs."""
+
+    QUERY = ("index,uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            cmd = ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "200"]
+            if self.uuid:
+                cmd += ["-i", self.uuid]
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 10:
+                self.rows.append(f)
+
+    def stop(self):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=5)
+        sm = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        mx = [float(r[3]) for r in self.rows if r[3].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[6 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def city_scene():
+    from threert_b200 import prep, scenes
+    t = time.perf_counter()
+    d = scenes.city(width=WIDTH, height=HEIGHT, max_depth=DEPTH)
+    P = prep.prepare(d)
+    log(f"city: {P.info['n_tris']} tris, {P.info['n_units']} units, prep {time.perf_counter() - t:.1f} s")
+    return P
+
+
+def frame_params(P, frame: int):
+    from threert_b200 import prep, scenes
+    cam = scenes.city_camera(frame % FRAMES, FRAMES, 1, WIDTH, HEIGHT)
+    return prep.set_camera(P.params, cam)
+
+
+def cpu_sample(P, frames, budget_s: float, threads: int = 0):
+    """The oracle over a sample of pixels of the given frames, about `budget_s` of work; rays/s, and what it was."""
+    import oracle
+    O = oracle.Oracle(P)
+    rng = np.random.default_rng(12345)
+    n_pix = WIDTH * HEIGHT
+    # Calibrate on a small sample, then size the sample to the budget.
+    cal = rng.choice(n_pix, 2048, replace=False).astype(np.uint32)
+    t = time.perf_counter()
+    _, st = O.render(frame_params(P, frames[0]), SPP, pixels=cal, threads=threads)
+    dt = max(time.perf_counter() - t, 1e-3)
+    px_per_s = len(cal) / dt
+    per_frame = int(max(2048, min(n_pix, px_per_s * budget_s / len(frames))))
+    rays, secs = 0, 0.0
+    for f in frames:
+        px = rng.choice(n_pix, per_frame, replace=False).astype(np.uint32)
+        t = time.perf_counter()
+        _, st = O.render(frame_params(P, f), SPP, pixels=px, threads=threads)
+        secs += time.perf_counter() - t
+        rays += st["closest_rays"] + st["shadow_rays"]
+    cores = threads if threads > 0 else oracle.hardware_threads()
+    return rays / secs, cores, f"{per_frame} random pixels x {len(frames)} frames ({per_frame * len(frames)} paths)"
+
+
+def cpu_model():
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def run_reference(args, rank, world):
+    """The reference algorithm on the host's cores (its CPU restatement): rank 0 alone."""
+    if rank != 0:
+        return
+    P = city_scene()
+    steps = max(1, args.steps)
+    warm = max(0, args.warmup)
+    # Whole run about 100 s: warm-up frames get a small sample, timed frames share the rest.
+    if warm:
+        cpu_sample(P, list(range(warm)), 5.0)
+    value, cores, sample = cpu_sample(P, [warm + i for i in range(steps)], 90.0)
+    mrays = value / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": mrays, "unit": "Mrays/s", "n_gpus": args.gpus,
+            "steps": steps, "warmup": warm, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "frames": FRAMES, "cpu": cpu_model()},
+            "cpu_baseline": {"value": mrays, "unit": "Mrays/s", "cores": cores, "kind": "port",
+                             "sample": sample + " of the city frames; the reference's WGSL pass needs a graphics "
+                                       "stack this box does not have, so its C++ restatement stands in"},
+            "e2e": {"value": mrays, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=120)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--binary", action="store_true", help="walk the reference's binary trees")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_
+        dist = dist_
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    from threert_b200 import Gpu
+    from threert_b200 import _native as N
+
+    P = city_scene()
+    gpu = Gpu(local)
+    name, sms = gpu.device_info()
+    S = gpu.upload(P)
+    flags = N.TRT_RENDER_BINARY if args.binary else 0
+    frames = [(rank + world * (args.warmup + i)) % FRAMES for i in range(args.steps)]
+    warm_frames = [(rank + world * i) % FRAMES for i in range(args.warmup)]
+    params = {f: frame_params(P, f) for f in set(frames + warm_frames)}
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    for f in warm_frames:
+        S.render_raw(params[f], SPP, flags=flags, read=False, stats=False)
+    gpu.synchronize()
+
+    # Timed: K frames, device time on the pass's own stream.
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        pass
+    S.reset_totals()
+    S.set_profiling(True)
+    clocks = ClockSampler(uuid)
+    barrier()
+    gpu.synchronize()
+    clocks.start()
+    gpu.timer_start()
+    for f in frames:
+        S.render_raw(params[f], SPP, flags=flags, read=False, stats=False)
+    ms = gpu.timer_stop()
+    clk = clocks.stop()
+    barrier()
+    tot = S.totals()
+    S.set_profiling(False)
+    rays = tot["closest_rays"] + tot["shadow_rays"]
+    launches = tot["launches"]
+    ext_avg_ms = tot["extend_ms"] / max(1, tot["extend_launches"])
+
+    # End to end through the C ABI: each frame's Params from the host, its accum read back into pinned memory.
+    acc = torch.empty((WIDTH * HEIGHT, N.PIXEL_FLOATS), dtype=torch.float32, pin_memory=True)
+    acc_ptr = C.cast(acc.data_ptr(), C.POINTER(C.c_float))
+    L = N.lib()
+    pinned = {f: torch.from_numpy(params[f].astype(np.uint32).view(np.int32)).pin_memory() for f in frames}
+    barrier()
+    gpu.synchronize()
+    gpu.timer_start()
+    for f in frames:
+        p = C.cast(pinned[f].data_ptr(), C.POINTER(C.c_uint32))
+        gpu._check(L.trt_render(S.handle, p, 0, SPP, flags, acc_ptr, None), "trt_render")
+    e2e_ms = gpu.timer_stop()
+    barrier()
+
+    # The walks' reads over the same frames, untimed (a counting walk).
+    S.reset_totals()
+    for f in frames:
+        S.render_raw(params[f], SPP, flags=flags | N.TRT_RENDER_COUNT, read=False, stats=False)
+    cnt = S.totals()
+    ext_bytes = (cnt["node_visits"] * NODE_BYTES + cnt["tri_tests"] * LEAF_BYTES + cnt["unit_entries"] * UNIT_BYTES)
+    ext_bytes_per_launch = ext_bytes / max(1, cnt["extend_launches"])
+
+    if dist:
+        t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e2e_ms = float(t[0]), float(t[1])
+        r = torch.tensor([float(rays)], dtype=torch.float64, device="cuda")
+        dist.all_reduce(r, op=dist.ReduceOp.SUM)
+        rays_all = float(r[0])
+    else:
+        rays_all = float(rays)
+
+    peak, peak_kind = measured_peaks()
+    achieved = ext_bytes_per_launch / (ext_avg_ms * 1e-3) / 1e9 if ext_avg_ms > 0 else None
+    traffic = profile_traffic()
+    line = {
+        "metric": METRIC, "value": rays_all / (ms * 1e-3) / 1e6, "unit": "Mrays/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "frames_per_rank": args.steps, "walk": "binary" if args.binary else "wide",
+                   "l2": "inputs larger than L2: 221 MB of scene buffers, each step a new camera along the spline",
+                   "device": name, "sms": sms, "parallelism": f"replicas x{world}, frames split across ranks"},
+        "e2e": {"value": rays_all / (e2e_ms * 1e-3) / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": 624,
+                "d2h_bytes_per_step": WIDTH * HEIGHT * 80},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                     "kernel": "k_extend (closest-hit walk)", "peak_kind": f"{peak_kind} hbm_gbs",
+                     "bytes_per_launch": ext_bytes_per_launch, "launch_ms": ext_avg_ms,
+                     "bytes_per_ray": ext_bytes / max(1, tot["closest_rays"])},
+        "clocks": clk,
+        "rays_per_path": rays / max(1, tot["paths"]),
+        "paths_per_s": tot["paths"] * world / (ms * 1e-3),
+        "stage_ms_per_step": {"extend": tot["extend_ms"] / args.steps, "shadow": tot["shadow_ms"] / args.steps,
+                              "shade": tot["shade_ms"] / args.steps},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, cores, sample = cpu_sample(P, frames[:4], 20.0)
+        line["cpu_baseline"] = {"value": v / 1e6, "unit": "Mrays/s", "cores": cores, "kind": "port",
+                                "sample": sample + f"; host CPU: {cpu_model()}"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    S.close()
+    gpu.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

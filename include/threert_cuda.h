@@ -1,0 +1,127 @@
+/* threert_b200: the B200 path-trace pass behind a C ABI.
+ *
+ * The drop-in for ThreeRT's offline path-trace pass under software traversal: the buffers `Gpu::render` uploads
+ * (renderer/src/gpu.rs:4116-4236, upload at gpu.rs:2613) go in as plain pointers and byte counts, the per-sample
+ * dispatch loop of renderer/shaders/pathtrace.wgsl `main` (gpu.rs:4174-4196) runs as a wavefront of sm_100a kernels,
+ * and the 80-byte `Pixel` records of `accum` (renderer/shaders/records.wgsl `Pixel`; gpu.rs:4211-4232 reads them)
+ * come back. Every function returns 0 on success and a nonzero TRT_E* code otherwise; `trt_last_error` has the
+ * message (the reference returns anyhow::Result, gpu.rs:4116).
+ *
+ * Threading: one context per host thread; a context owns one CUDA stream, and every call on a context and its
+ * scenes is ordered on that stream.
+ */
+#ifndef THREERT_CUDA_H
+#define THREERT_CUDA_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    TRT_OK = 0,
+    TRT_EINVAL = 1,    /* a bad argument: sizes, offsets, counts past their buffers */
+    TRT_ECUDA = 2,     /* a CUDA call failed (out of device memory, no device) */
+    TRT_EGUARD = 3,    /* a traversal gave up at its iteration limit: the scene's trees are not trees */
+};
+
+#define TRT_PARAMS_WORDS 156 /* Params: 39 vec4s, 624 bytes (gpu.rs:127-186) */
+#define TRT_PIXEL_FLOATS 20  /* Pixel: color, albedo, normal, emit, spec (records.wgsl) */
+
+typedef struct trt_ctx trt_ctx;
+typedef struct trt_scene trt_scene;
+
+typedef struct {
+    int device;          /* CUDA device ordinal */
+    uint32_t flags;      /* 0 */
+} trt_options;
+
+/* The scene's buffers as the reference binds them (pathtrace.wgsl:141-268): vertices (binding 1), leaves (2), nodes
+ * (3), tables (4), words (5), the environment texels (9, RGBA16F, env_w x env_h). Copied to the device; the library
+ * owns the copies. Replaces `Gpu::upload` (gpu.rs:2613). */
+typedef struct {
+    const void* vertices; uint64_t vertices_bytes;
+    const void* leaves;   uint64_t leaves_bytes;
+    const void* nodes;    uint64_t nodes_bytes;
+    const void* tables;   uint64_t tables_bytes;
+    const void* words;    uint64_t words_bytes;
+    const uint16_t* env_half; uint32_t env_w, env_h;
+} trt_scene_desc;
+
+/* What one render did (gpu.rs:4197 trace_ms and the ray counts the reference does not keep). */
+typedef struct {
+    uint64_t closest_rays;   /* extend rays traced (camera + bounce) */
+    uint64_t shadow_rays;    /* shadow / any-hit rays traced */
+    uint64_t paths;          /* pixels x samples */
+    float device_ms;         /* device time of the call, CUDA events on the context's stream */
+    uint32_t launches;       /* kernels launched */
+    uint32_t guard_trips;    /* traversals stopped at the iteration limit (pathtrace.wgsl's loop guard) */
+} trt_stats;
+
+/* Cumulative counters of a scene since `trt_scene_reset_totals` (reads them with one synchronisation). */
+typedef struct {
+    uint64_t closest_rays, shadow_rays, paths, renders, launches;
+    /* Filled by renders (and traces) with TRT_RENDER_COUNT, for the closest-hit walks and the shadow walks: node
+     * records read (a binary walk reads a node and, at an interior node, both children), triangles tested, unit
+     * records entered. */
+    uint64_t node_visits, tri_tests, unit_entries;
+    uint64_t shadow_node_visits, shadow_tri_tests, shadow_unit_entries;
+    double extend_ms, shadow_ms, shade_ms;          /* with trt_scene_set_profiling on: per-stage device time */
+    uint64_t extend_launches, shadow_launches;
+    uint64_t guard_trips;
+} trt_totals;
+
+/* One ray for trt_trace: origin, tmax, direction, mode (0 closest, 1 shadow casters, 2 any surface). */
+typedef struct { float o[3]; float tmax; float d[3]; uint32_t mode; } trt_ray;
+typedef struct { float t; uint32_t tri; float u; float v; uint32_t inst; uint32_t part; } trt_hit;
+
+/* Render flags. */
+#define TRT_RENDER_ACCUMULATE 1u /* add to accum instead of clearing it first (resume at first_sample) */
+#define TRT_RENDER_COUNT      2u /* also count node visits, triangle tests and unit entries (a slower walk) */
+#define TRT_RENDER_BINARY     4u /* walk the reference's binary trees instead of the wide BVH */
+
+int trt_create(const trt_options* opts, trt_ctx** out);
+void trt_destroy(trt_ctx* ctx);
+const char* trt_last_error(const trt_ctx* ctx);
+/* The library's version and the device it runs on (name, SM count). */
+int trt_device_info(const trt_ctx* ctx, char* name, size_t name_len, int* sm_count);
+
+/* Uploads a scene (gpu.rs:2613 Gpu::upload) and builds its wide BVH on the device. */
+int trt_scene_upload(trt_ctx* ctx, const trt_scene_desc* desc, trt_scene** out);
+void trt_scene_free(trt_scene* scene);
+/* Overwrites bytes [offset, offset + bytes) of one of the scene's buffers (0 vertices, 1 leaves, 2 nodes, 3 tables,
+ * 4 words) from host memory: in-place record edits and refits (gpu.rs:4028 write_nodes). A change to nodes or leaves
+ * rebuilds the wide BVH. */
+int trt_scene_update(trt_scene* scene, uint32_t which, uint64_t offset, const void* src, uint64_t bytes);
+
+/* Renders samples [first_sample, first_sample + spp) at Params' size (gpu.rs:4116 Gpu::render; its per-dispatch
+ * `size.z` is the sample index). Without TRT_RENDER_ACCUMULATE the scene's accum is cleared first, as the reference
+ * clears it (gpu.rs:4170). accum_host: NULL, or w * h * 20 floats to copy the result to. stats: NULL (no
+ * synchronisation), or filled after the call completes. */
+int trt_render(trt_scene* scene, const uint32_t params[TRT_PARAMS_WORDS], uint32_t first_sample, uint32_t spp,
+               uint32_t flags, float* accum_host, trt_stats* stats);
+/* The scene's accum on the device (w * h Pixel records) for zero-copy consumers (a denoiser). */
+int trt_accum_device_ptr(trt_scene* scene, void** ptr, uint64_t* bytes);
+/* Copies the accum to host memory. */
+int trt_accum_read(trt_scene* scene, float* accum_host, uint64_t bytes);
+
+/* Casts rays against the scene (trace_units.wgsl:44-135's query) from host arrays: parity and cost tests. */
+int trt_trace(trt_scene* scene, const uint32_t params[TRT_PARAMS_WORDS], const trt_ray* rays, uint64_t n, uint32_t flags,
+              trt_hit* hits);
+
+int trt_scene_totals(trt_scene* scene, trt_totals* out);
+void trt_scene_reset_totals(trt_scene* scene);
+/* 1: record per-stage CUDA events (extend_ms, shadow_ms in the totals). */
+void trt_scene_set_profiling(trt_scene* scene, int on);
+
+/* Device-time brackets on the context's stream: start records an event, stop records one, synchronises and returns
+ * the milliseconds between them. */
+int trt_timer_start(trt_ctx* ctx);
+int trt_timer_stop(trt_ctx* ctx, float* ms);
+int trt_synchronize(trt_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,140 @@
+"""Test infrastructure, not product code: the CPU oracle of the path-trace pass.
+
+A C++ restatement of the reference's offline kernel (oracle.cpp, built by the Makefile beside it into
+liboracle.so) with ctypes bindings. Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use it, as
+the checker or as the timed CPU baseline; the product never calls it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "liboracle.so"
+
+
+class _Scene(C.Structure):
+    _fields_ = [("vertices", C.c_void_p), ("n_vertex_vec4", C.c_uint64), ("leaves", C.c_void_p),
+                ("n_leaf_vec4", C.c_uint64), ("nodes", C.c_void_p), ("n_nodes", C.c_uint64), ("tables", C.c_void_p),
+                ("n_table_vec4", C.c_uint64), ("words", C.c_void_p), ("n_words", C.c_uint64),
+                ("env_half", C.c_void_p), ("env_w", C.c_uint32), ("env_h", C.c_uint32)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("closest_rays", C.c_uint64), ("shadow_rays", C.c_uint64), ("node_visits", C.c_uint64),
+                ("tri_tests", C.c_uint64), ("unit_entries", C.c_uint64)]
+
+
+def build(force: bool = False) -> Path:
+    """Builds liboracle.so with make (g++)."""
+    if force or not LIB_PATH.exists() or any(
+            p.stat().st_mtime > LIB_PATH.stat().st_mtime for p in (HERE / "oracle.cpp", HERE / "oracle.h")):
+        subprocess.run(["make", "-s", "-C", str(HERE), "-B" if force else "liboracle.so"], check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        L = C.CDLL(str(LIB_PATH))
+        P = C.POINTER
+        L.orc_render.argtypes = [P(_Scene), P(C.c_uint32), C.c_uint32, C.c_uint32, P(C.c_float), C.c_int, P(Stats)]
+        L.orc_render_pixels.argtypes = [P(_Scene), P(C.c_uint32), C.c_uint32, C.c_uint32, P(C.c_uint32), C.c_uint64,
+                                        P(C.c_float), C.c_int, P(Stats)]
+        L.orc_trace.argtypes = [P(_Scene), P(C.c_uint32), C.c_void_p, C.c_uint64, C.c_void_p, C.c_int, P(Stats)]
+        L.orc_trace_brute.argtypes = [P(_Scene), P(C.c_uint32), C.c_void_p, C.c_uint64, C.c_void_p, C.c_int]
+        L.orc_intersect.argtypes = [P(_Scene), P(C.c_uint32), C.c_void_p, C.c_void_p, C.c_uint64, P(C.c_float)]
+        L.orc_rng4.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, P(C.c_float)]
+        L.orc_rng4.restype = None
+        L.orc_sobol_directions.argtypes = [P(C.c_uint32)]
+        L.orc_sobol_directions.restype = None
+        L.orc_hash_hp.argtypes = [C.c_uint32]
+        L.orc_hash_hp.restype = C.c_uint32
+        L.orc_hardware_threads.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+class Oracle:
+    """The oracle over one prepared scene (threert_b200.prep.Prepared: the buffers the GPU pass takes)."""
+
+    def __init__(self, prepared):
+        self.p = prepared
+        self._keep = [np.ascontiguousarray(a) for a in (prepared.vertices, prepared.leaves, prepared.nodes,
+                                                         prepared.tables, prepared.words, prepared.env_half)]
+        v, l, n, t, w, e = self._keep
+        self.scene = _Scene(v.ctypes.data, v.size // 4, l.ctypes.data, l.size // 4, n.ctypes.data, n.size // 8,
+                            t.ctypes.data, t.size // 4, w.ctypes.data, w.size, e.ctypes.data, prepared.env_w,
+                            prepared.env_h)
+
+    def render(self, params, spp: int, first_sample: int = 0, pixels=None, threads: int = 0, accum=None):
+        """accum (w * h, 20) float32 after `spp` samples (added to `accum` if given), and the walk's counts."""
+        L = lib()
+        p = np.ascontiguousarray(params, dtype=np.uint32)
+        w, h = int(p[16]), int(p[17])
+        acc = np.zeros((w * h, 20), np.float32) if accum is None else accum
+        st = Stats()
+        if pixels is None:
+            L.orc_render(C.byref(self.scene), p.ctypes.data_as(C.POINTER(C.c_uint32)), first_sample, spp,
+                         acc.ctypes.data_as(C.POINTER(C.c_float)), threads, C.byref(st))
+        else:
+            px = np.ascontiguousarray(pixels, dtype=np.uint32)
+            L.orc_render_pixels(C.byref(self.scene), p.ctypes.data_as(C.POINTER(C.c_uint32)), first_sample, spp,
+                                px.ctypes.data_as(C.POINTER(C.c_uint32)), len(px),
+                                acc.ctypes.data_as(C.POINTER(C.c_float)), threads, C.byref(st))
+        return acc, {f[0]: getattr(st, f[0]) for f in Stats._fields_}
+
+    def trace(self, params, rays, brute: bool = False, threads: int = 0):
+        from threert_b200.gpu import HIT_DTYPE, RAY_DTYPE
+        L = lib()
+        r = np.ascontiguousarray(rays, dtype=RAY_DTYPE)
+        hits = np.zeros(len(r), HIT_DTYPE)
+        p = np.ascontiguousarray(params, dtype=np.uint32)
+        st = Stats()
+        if brute:
+            L.orc_trace_brute(C.byref(self.scene), p.ctypes.data_as(C.POINTER(C.c_uint32)), r.ctypes.data, len(r),
+                              hits.ctypes.data, threads)
+        else:
+            L.orc_trace(C.byref(self.scene), p.ctypes.data_as(C.POINTER(C.c_uint32)), r.ctypes.data, len(r),
+                        hits.ctypes.data, threads, C.byref(st))
+        return hits, {f[0]: getattr(st, f[0]) for f in Stats._fields_}
+
+
+    def intersect(self, params, rays, hits):
+        """The t of each hit's own triangle along its ray (inf where it misses or names none)."""
+        from threert_b200.gpu import HIT_DTYPE, RAY_DTYPE
+        r = np.ascontiguousarray(rays, dtype=RAY_DTYPE)
+        h = np.ascontiguousarray(hits, dtype=HIT_DTYPE)
+        t = np.zeros(len(r), np.float32)
+        p = np.ascontiguousarray(params, dtype=np.uint32)
+        lib().orc_intersect(C.byref(self.scene), p.ctypes.data_as(C.POINTER(C.c_uint32)), r.ctypes.data, h.ctypes.data,
+                            len(r), t.ctypes.data_as(C.POINTER(C.c_float)))
+        return t
+
+
+def rng4(pixel_seed: int, index: int, dim: int) -> np.ndarray:
+    out = (C.c_float * 4)()
+    lib().orc_rng4(pixel_seed, index, dim, out)
+    return np.array(out[:], np.float32)
+
+
+def sobol_directions() -> np.ndarray:
+    out = (C.c_uint32 * 96)()
+    lib().orc_sobol_directions(out)
+    return np.array(out[:], np.uint32).reshape(3, 32)
+
+
+def hash_hp(x: int) -> int:
+    return int(lib().orc_hash_hp(x))
+
+
+def hardware_threads() -> int:
+    return int(lib().orc_hardware_threads())

@@ -1,0 +1,998 @@
+// The path-trace pass as a wavefront of sm_100a kernels, and the C ABI around it (include/threert_cuda.h).
+//
+// The reference runs one megakernel invocation per pixel per sample (renderer/shaders/pathtrace.wgsl:4105-4558,
+// dispatched per sample by renderer/src/gpu.rs:4174-4196). Here a wave is every pixel for K samples at once, and each
+// path vertex is four kernels over compacted queues:
+//   extend  - closest hit of every live path's ray (persistent threads fetching warps of rays);
+//   shade   - surface, emission with its MIS weight, the vertex's light samples (sun, emitter, sky) as shadow rays
+//             with their unoccluded contributions, the BSDF sample and Russian roulette; live paths go to the next
+//             queue (warp-aggregated appends);
+//   shadow  - any-hit of every shadow ray, a visibility bit per light slot;
+//   resolve - the vertex's direct light from the visible slots, in the reference's order and with its clamp, then
+//             the finished paths' last fixes.
+// Every random number is keyed by (pixel, sample, vertex, decision) (sample.wgsl), so nothing a path draws depends on
+// how the wave is scheduled, and a path's floating-point sums are taken in the megakernel's order.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "shade.cuh"
+#include "threert_cuda.h"
+#include "wide_bvh.cuh"
+
+namespace trt {
+
+// ---- path state -----------------------------------------------------------------------------------------------------
+
+constexpr uint32_t F_SPECULAR_BOUNCE = 1u, F_STRAIGHT = 2u, F_MIRROR = 4u, F_DONE = 8u;
+constexpr uint32_t MAX_DIR_LIGHTS = 4u;
+constexpr uint32_t SLOT_EMIT = MAX_DIR_LIGHTS, SLOT_ENV = MAX_DIR_LIGHTS + 1, N_SLOTS = MAX_DIR_LIGHTS + 2;
+constexpr uint32_t MAX_DEPTH = 64u;            // counters are kept for this many vertices
+
+struct PathBufs {
+    float4* o;        // origin, w: last_pdf
+    float4* d;        // direction, w: flags (bits)
+    float4* thr;      // throughput, w: pixel (bits)
+    float4* rad;      // radiance, w: sample (bits)
+    float4* alb;      // first-hit albedo
+    float4* nrm;      // first-hit normal
+    float4* mis_x;    // the last light-sampling vertex's point
+    float4* mis_n;    // and normal
+    float4* nee;      // N_SLOTS contributions a path (slot-major: nee[slot * n + p])
+    float4* nee_thr;  // throughput at the light samples, w: slot mask | clamp << 8 (bits)
+    uint32_t* vis;    // visible slots (bits)
+    uint32_t n;       // slots
+};
+struct Queues {
+    uint32_t* q[2];       // path queues (extend inputs), alternating by depth
+    float4* hit_a;        // t, u, v, tri (bits) per queue position
+    uint2* hit_b;         // inst, part
+    float4* so;           // shadow rays: origin, tmax
+    float4* sd;           // direction, mode (bits)
+    uint32_t* sp;         // path << 3 | slot
+    uint32_t* cnt;        // per depth: [queue size, shadow count, extend fetch, shadow fetch]
+    unsigned long long* totals;  // cumulative: closest, shadow, paths, nodes, tris, units, guard trips
+    uint32_t shadow_cap;
+};
+// Cumulative counters: rays, paths, guard trips, and (TRT_RENDER_COUNT) the walks' reads by stage: node records
+// read, triangles tested, unit records entered, for the extend (closest) and the shadow walks.
+enum { T_CLOSEST = 0, T_SHADOW, T_PATHS, T_GUARD, T_E_NODES, T_E_TRIS, T_E_UNITS, T_S_NODES, T_S_TRIS, T_S_UNITS, T_COUNT };
+
+// Warp-aggregated append: one atomic per warp for the lanes whose `want` is set; returns each lane's slot.
+__device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool want) {
+    unsigned mask = __ballot_sync(0xffffffffu, want);
+    if (mask == 0) return 0;
+    int lane = threadIdx.x & 31;
+    int leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    return base + (uint32_t)__popc(mask & ((1u << lane) - 1u));
+}
+// Persistent-thread work fetch: a warp takes 32 consecutive items.
+__device__ __forceinline__ uint32_t warp_fetch(uint32_t* counter) {
+    uint32_t base = 0;
+    if ((threadIdx.x & 31) == 0) base = atomicAdd(counter, 32u);
+    return __shfl_sync(0xffffffffu, base, 0) + (threadIdx.x & 31);
+}
+__device__ __forceinline__ void warp_add64(unsigned long long* p, unsigned long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(p, v);
+}
+
+// The slot -> pixel map: 8 x 4 tiles in rows, so a warp's paths start from one tile.
+__device__ __forceinline__ bool slot_pixel(uint32_t idx, uint32_t w, uint32_t h, uint32_t& gx, uint32_t& gy) {
+    uint32_t tiles_x = (w + 7u) / 8u;
+    uint32_t t = idx / 32u, within = idx % 32u;
+    gx = (t % tiles_x) * 8u + (within % 8u);
+    gy = (t / tiles_x) * 4u + (within / 8u);
+    return gx < w && gy < h;
+}
+
+// pathtrace.wgsl:4002-4026 camera_ray
+__device__ void camera_ray(const Params& P, uint32_t gx, uint32_t gy, const float cam[4], V3& o, V3& d) {
+    float w = (float)P.w[P_SIZE], h = (float)P.w[P_SIZE + 1];
+    float ndcx = ((float)gx + cam[0]) / w * 2.0f - 1.0f;
+    float ndcy = 1.0f - ((float)gy + cam[1]) / h * 2.0f;
+    V3 fwd = pv(P, P_CAM_FWD), right = pv(P, P_CAM_RIGHT), up = pv(P, P_CAM_UP);
+    float tanf_ = pf(P, P_CAM_POS + 3), aspect = pf(P, P_CAM_FWD + 3);
+    d = normalize(fwd + right * (ndcx * tanf_ * aspect) + up * (ndcy * tanf_));
+    o = pv(P, P_CAM_POS);
+    if (pf(P, P_CAM_RIGHT + 3) > 0.0f) {
+        V3 focus = o + d * (pf(P, P_CAM_UP + 3) / dot(d, fwd));
+        float r = sqrtf(cam[2]) * pf(P, P_CAM_RIGHT + 3);
+        float phi = 2.0f * PI * cam[3];
+        o = o + right * (r * cosf(phi)) + up * (r * sinf(phi));
+        d = normalize(focus - o);
+    }
+}
+
+__global__ void k_raygen(Params P, PathBufs B, Queues Q, uint32_t first_sample, uint32_t n_idx, uint32_t K) {
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t w = P.w[P_SIZE], h = P.w[P_SIZE + 1];
+    bool valid = false;
+    uint32_t gx = 0, gy = 0;
+    if (p < n_idx * K) valid = slot_pixel(p % n_idx, w, h, gx, gy);
+    uint32_t at = warp_append(&Q.cnt[0], valid);
+    if (!valid) return;
+    uint32_t sample = first_sample + p / n_idx;
+    Rng R{sample, pixel_seed(gx, gy, P.w[P_SIZE + 3]), 0u};
+    float cam[4];
+    R.rng4(R.dim(D_CAMERA), cam);
+    V3 o, d;
+    camera_ray(P, gx, gy, cam, o, d);
+    B.o[p] = f4(o, 0.0f);
+    B.d[p] = f4(d, bf(F_SPECULAR_BOUNCE | F_STRAIGHT));
+    B.thr[p] = f4(v3(1.0f), bf(gy * w + gx));
+    B.rad[p] = f4(v3(0.0f), bf(sample));
+    B.alb[p] = f4(v3(0.0f), 0.0f);
+    B.nrm[p] = f4(v3(0.0f), 0.0f);
+    B.mis_x[p] = f4(v3(0.0f), 0.0f);
+    B.mis_n[p] = f4(v3(0.0f), 0.0f);
+    B.nee_thr[p] = f4(v3(0.0f), bf(0u));
+    Q.q[0][at] = p;
+}
+
+struct Walk {
+    const DScene S;
+    const WideView W;
+    uint32_t top, n_units;
+};
+
+template <bool COUNT, bool WIDE>
+__device__ __forceinline__ Hit walk(const Walk& wk, const Sections& X, V3 o, V3 d, float tmax, uint32_t mode,
+                                    WalkCount* wc, bool* guard) {
+    if (WIDE) return trace_wide<COUNT>(wk.S, wk.W, X, o, d, tmax, mode, wc, guard);
+    return trace_binary<COUNT>(wk.S, X, wk.top, wk.n_units, o, d, tmax, mode, wc, guard);
+}
+
+template <bool COUNT, bool WIDE>
+__global__ void __launch_bounds__(128) k_extend(Params P, Walk wk, PathBufs B, Queues Q, uint32_t depth) {
+    Sections X(P);
+    uint32_t* cnt = Q.cnt + depth * 4u;
+    const uint32_t* queue = Q.q[depth & 1u];
+    uint32_t n = *(volatile uint32_t*)&cnt[0];
+    WalkCount wc{0, 0, 0};
+    unsigned long long guard_trips = 0;
+    for (;;) {
+        uint32_t i = warp_fetch(&cnt[2]);
+        if (__shfl_sync(0xffffffffu, i, 0) >= n) break;
+        if (i < n) {
+            uint32_t p = queue[i];
+            float4 o = B.o[p], d = B.d[p];
+            bool guard = false;
+            Hit h = walk<COUNT, WIDE>(wk, X, xyz(o), xyz(d), INF, TRACE_CLOSEST, &wc, &guard);
+            if (guard) guard_trips++;
+            Q.hit_a[i] = make_float4(h.t, h.u, h.v, bf(h.tri));
+            Q.hit_b[i] = make_uint2(h.inst, h.part);
+        }
+    }
+    if (COUNT) {
+        warp_add64(&Q.totals[T_E_NODES], wc.nodes);
+        warp_add64(&Q.totals[T_E_TRIS], wc.tris);
+        warp_add64(&Q.totals[T_E_UNITS], wc.units);
+    }
+    warp_add64(&Q.totals[T_GUARD], guard_trips);
+}
+
+template <bool COUNT, bool WIDE>
+__global__ void __launch_bounds__(128) k_shadow(Params P, Walk wk, PathBufs B, Queues Q, uint32_t depth) {
+    Sections X(P);
+    uint32_t* cnt = Q.cnt + depth * 4u;
+    uint32_t n = min(*(volatile uint32_t*)&cnt[1], Q.shadow_cap);
+    WalkCount wc{0, 0, 0};
+    unsigned long long guard_trips = 0;
+    for (;;) {
+        uint32_t i = warp_fetch(&cnt[3]);
+        if (__shfl_sync(0xffffffffu, i, 0) >= n) break;
+        if (i < n) {
+            float4 o = Q.so[i], d = Q.sd[i];
+            bool guard = false;
+            Hit h = walk<COUNT, WIDE>(wk, X, xyz(o), xyz(d), o.w, bu(d.w), &wc, &guard);
+            if (guard) guard_trips++;
+            if (h.tri == MISS) {
+                uint32_t sp = Q.sp[i];
+                atomicOr(&B.vis[sp >> 3], 1u << (sp & 7u));
+            }
+        }
+    }
+    if (COUNT) {
+        warp_add64(&Q.totals[T_S_NODES], wc.nodes);
+        warp_add64(&Q.totals[T_S_TRIS], wc.tris);
+        warp_add64(&Q.totals[T_S_UNITS], wc.units);
+    }
+    warp_add64(&Q.totals[T_GUARD], guard_trips);
+}
+
+__device__ __forceinline__ void push_shadow(const Queues& Q, uint32_t* cnt, uint32_t p, uint32_t slot, V3 o, V3 d,
+                                            float tmax, uint32_t mode) {
+    uint32_t at = atomicAdd(&cnt[1], 1u);
+    if (at >= Q.shadow_cap) return;
+    Q.so[at] = f4(o, tmax);
+    Q.sd[at] = f4(d, bf(mode));
+    Q.sp[at] = (p << 3) | slot;
+}
+
+// One path vertex: pathtrace.wgsl:4176-4477 from the hit on (the trace itself is k_extend's).
+__global__ void __launch_bounds__(128) k_shade(Params P, DScene S, PathBufs B, Queues Q, uint32_t depth) {
+    Sections X(P);
+    uint32_t* cnt = Q.cnt + depth * 4u;
+    const uint32_t* queue = Q.q[depth & 1u];
+    uint32_t n = cnt[0];
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    bool live = false;
+    uint32_t p = 0;
+    if (i < n) {
+        p = queue[i];
+        float4 o4 = B.o[p], d4 = B.d[p], thr4 = B.thr[p], rad4 = B.rad[p];
+        V3 o = xyz(o4), d = xyz(d4), thr = xyz(thr4), radiance = xyz(rad4);
+        float last_pdf = o4.w;
+        uint32_t flags = bu(d4.w);
+        uint32_t pix = bu(thr4.w), sample = bu(rad4.w);
+        uint32_t w = P.w[P_SIZE];
+        Rng R{sample, pixel_seed(pix % w, pix / w, P.w[P_SIZE + 3]), depth};
+        float clamp_v = pf(P, P_MISC);
+        uint32_t last = P.w[P_COUNTS + 2];
+        bool straight = (flags & F_STRAIGHT) != 0;
+        float4 ha = Q.hit_a[i];
+        uint2 hb = Q.hit_b[i];
+        Hit hit{ha.x, bu(ha.w), ha.y, ha.z, hb.x, hb.y};
+        uint32_t nee_mask = 0, vis = 0;
+        if (hit.tri == MISS) {
+            V3 c = thr * sky_mis(S, X, P, d, depth > 0u ? last_pdf : 0.0f);
+            if (depth > 1u && !straight) {
+                float lum = luminance(c);
+                if (lum > clamp_v) c = c * (clamp_v / lum);
+            }
+            radiance = radiance + c;
+            flags |= F_DONE;
+        } else {
+            Surface s = surface(S, X, o, d, hit);
+            if (depth == 0u) {
+                V3 albedo = s.card ? s.emissive / fmaxf(fmaxf(s.emissive.x, fmaxf(s.emissive.y, s.emissive.z)), 1e-6f) : s.base;
+                B.alb[p] = f4(albedo, 0.0f);
+                B.nrm[p] = f4(s.n, 0.0f);
+            }
+            if (any_gt0(s.emissive) && (s.front || !s.card)) {
+                float wgt = 1.0f;
+                if (depth > 0u && (flags & F_SPECULAR_BOUNCE) == 0u)
+                    wgt = emit_mis(S, X, P, hit, d, last_pdf, xyz(B.mis_x[p]), xyz(B.mis_n[p]));
+                V3 c = thr * s.emissive * wgt;
+                if (depth > 1u && !straight) {
+                    float lum = luminance(c);
+                    if (lum > clamp_v) c = c * (clamp_v / lum);
+                }
+                radiance = radiance + c;
+            }
+            if (s.card || depth == last) {
+                flags |= F_DONE;
+            } else {
+                V3 v = -d;
+                float nov = fmaxf(dot(s.n, v), 1e-4f);
+                Lobes lb = lobes(S, X, P, s, nov);
+                // direct_light (pathtrace.wgsl:2444-2546): each light's sample and its contribution if unoccluded.
+                V3 oo = offset_origin(s.p, s.ng);
+                uint32_t nd = min(P.w[P_COUNTS2], MAX_DIR_LIGHTS);
+                for (uint32_t li = 0; li < nd; ++li) {
+                    uint32_t b = X.t_lights + li * 5u;
+                    float4 dir = tab(S, b + 1);
+                    float cos_max = dir.w;
+                    V3 to_light = -xyz(dir);
+                    float u[2];
+                    R.rng2(rng_sub(R.dim(D_SUN), li), u);
+                    float cos_t = 1.0f - u[0] * (1.0f - cos_max);
+                    float sin_t = sqrtf(fmaxf(0.0f, 1.0f - cos_t * cos_t));
+                    float phi = 2.0f * PI * u[1];
+                    Mat3 tb = basis(to_light);
+                    V3 l = mul(tb, V3{sin_t * cosf(phi), sin_t * sinf(phi), cos_t});
+                    V3 color = xyz(tab(S, b + 2));
+                    if (all_le0(color)) continue;
+                    V3 f = eval_bsdf_k(s, lb, v, l, tab(S, b + 4).y);
+                    if (any_gt0(f)) {
+                        float pdf_l = 1.0f / (2.0f * PI * (1.0f - cos_max));
+                        float wgt = light_mis(pdf_l, s, lb, v, l);
+                        B.nee[li * B.n + p] = f4(color * f * wgt * 1.0f, 0.0f);
+                        nee_mask |= 1u << li;
+                        if (tab(S, b + 3).w >= 0.5f) push_shadow(Q, cnt, p, li, oo, l, INF, TRACE_SHADOW);
+                        else vis |= 1u << li;
+                    }
+                }
+                V3 ne = s.n;
+                B.mis_x[p] = f4(oo, 0.0f);
+                B.mis_n[p] = f4(ne, 0.0f);
+                if (emitters_on(S, X, P)) {
+                    ES es;
+                    bool lt_on = pf(P, P_LTREE + 3) > 0.5f;
+                    bool seen_directly = depth == 0u || (depth == 1u && (flags & F_MIRROR) != 0u);
+                    if (lt_on) es = sample_emitter_ris(S, X, P, R, oo, ne, depth == 0u ? (uint32_t)pf(P, P_LTREE + 3) : 1u, s, lb, v, R.dim(D_EMIT));
+                    else if (seen_directly) es = sample_emitter_ris(S, X, P, R, oo, ne, depth == 0u ? EMIT_RIS_M : EMIT_RIS_M / 2u, s, lb, v, R.dim(D_EMIT));
+                    else if (pf(P, P_LIGHT_LOD + 3) > 0.0f) es = sample_emitter_ris(S, X, P, R, oo, ne, 2u, s, lb, v, R.dim(D_EMIT));
+                    else es = sample_emitter(S, X, P, R, oo, ne, R.dim(D_EMIT));
+                    if (es.pdf_w > 0.0f) {
+                        V3 f = eval_bsdf_k(s, lb, v, es.l, 1.0f);
+                        if (any_gt0(f)) {
+                            float wgt = light_mis(es.pdf_w, s, lb, v, es.l) * 1.0f;
+                            B.nee[SLOT_EMIT * B.n + p] = f4(es.le * f * wgt * es.w, 0.0f);
+                            nee_mask |= 1u << SLOT_EMIT;
+                            push_shadow(Q, cnt, p, SLOT_EMIT, oo, es.l, es.dist * 0.999f, TRACE_ANY);
+                        }
+                    }
+                }
+                bool env_sampled = P.w[P_COUNTS2 + 1] != 0u && (pf(P, P_ENV) > 0.5f || luminance(pv(P, P_SKY)) > 0.0f);
+                if (env_sampled) {
+                    V3 l = sample_env(S, P, R, R.dim(D_ENV));
+                    V3 f = eval_bsdf_k(s, lb, v, l, 1.0f);
+                    if (any_gt0(f)) {
+                        float pdf_e = env_pdf(S, P, l);
+                        if (pdf_e > 0.0f) {
+                            B.nee[SLOT_ENV * B.n + p] = f4(env_radiance(S, P, l) * f * light_mis(pdf_e, s, lb, v, l) / pdf_e * 1.0f, 0.0f);
+                            nee_mask |= 1u << SLOT_ENV;
+                            push_shadow(Q, cnt, p, SLOT_ENV, oo, l, INF, TRACE_SHADOW);
+                        }
+                    }
+                }
+                bool clamp_dl = depth > 0u && !straight;
+                B.nee_thr[p] = f4(thr, bf(nee_mask | (clamp_dl ? 0x100u : 0u)));
+                // sample_bsdf (pathtrace.wgsl:1848-1887, no coat, no glass)
+                Mat3 tbn = basis(s.n);
+                float r4[4];
+                R.rng4(R.dim(D_BSDF), r4);
+                bool sampled_spec = r4[1] < lb.p_spec;
+                V3 l;
+                if (sampled_spec) {
+                    V3 hv = sample_vndf(v, tbn, s.roughness * s.roughness, r4[2], r4[3]);
+                    l = reflect(-v, hv);
+                } else {
+                    float rr = sqrtf(r4[2]);
+                    float phi = 2.0f * PI * r4[3];
+                    l = mul(tbn, V3{rr * cosf(phi), rr * sinf(phi), sqrtf(fmaxf(0.0f, 1.0f - rr * rr))});
+                }
+                float pdf = pdf_bsdf(s, lb, v, l);
+                V3 wgt = eval_bsdf_k(s, lb, v, l, 1.0f) / fmaxf(pdf, 1e-20f);
+                if (pdf <= 0.0f || all_le0(wgt)) {
+                    flags |= F_DONE;
+                } else {
+                    thr = thr * wgt;
+                    bool mirror = (depth == 0u || (flags & F_MIRROR) != 0u) && s.roughness < MIRROR_ROUGHNESS && sampled_spec;
+                    flags &= ~(F_SPECULAR_BOUNCE | F_STRAIGHT | F_MIRROR);
+                    if (mirror) flags |= F_MIRROR;
+                    if (depth >= P.w[P_COUNTS + 3]) {
+                        float q = fminf(fmaxf(thr.x, fmaxf(thr.y, thr.z)), 0.95f);
+                        if (R.rng1(R.dim(D_RR)) > q) flags |= F_DONE;
+                        else thr = thr / q;
+                    }
+                    if ((flags & F_DONE) == 0u) {
+                        o = offset_origin(s.p, dot(l, s.ng) < 0.0f ? -s.ng : s.ng);
+                        d = l;
+                        last_pdf = pdf;
+                        live = true;
+                    }
+                }
+            }
+        }
+        B.vis[p] = vis;
+        if (nee_mask == 0u) B.nee_thr[p] = f4(v3(0.0f), bf(0u));
+        B.o[p] = f4(o, last_pdf);
+        B.d[p] = f4(d, bf(flags));
+        B.thr[p] = f4(thr, bf(pix));
+        B.rad[p] = f4(radiance, bf(sample));
+    }
+    uint32_t at = warp_append(&Q.cnt[(depth + 1u) * 4u], live);
+    if (live && depth + 1u < MAX_DEPTH) Q.q[(depth + 1u) & 1u][at] = p;
+}
+
+// The vertex's direct light from its visible slots (pathtrace.wgsl:4398-4403), and a finished path's last fixes
+// (4494-4497).
+__global__ void k_resolve(PathBufs B, Queues Q, uint32_t depth, float clamp_v) {
+    uint32_t n = Q.cnt[depth * 4u];
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t p = Q.q[depth & 1u][i];
+    float4 nt = B.nee_thr[p];
+    uint32_t m = bu(nt.w);
+    float4 rad4 = B.rad[p];
+    V3 radiance = xyz(rad4);
+    if (m & 0xffu) {
+        uint32_t vis = B.vis[p] & m;
+        V3 sum = v3(0.0f);
+        for (uint32_t k = 0; k < N_SLOTS; ++k)
+            if (vis & (1u << k)) sum = sum + xyz(B.nee[k * B.n + p]);
+        V3 dl = xyz(nt) * sum;
+        if (m & 0x100u) {
+            float lum = luminance(dl);
+            if (lum > clamp_v) dl = dl * (clamp_v / lum);
+        }
+        radiance = radiance + dl;
+    }
+    uint32_t flags = bu(B.d[p].w);
+    if (flags & F_DONE) {
+        if (non_finite3(radiance)) radiance = v3(0.0f);
+        float4 a = B.alb[p], nn = B.nrm[p];
+        if (non_finite3(xyz(a))) B.alb[p] = f4(v3(0.0f), 0.0f);
+        if (non_finite3(xyz(nn))) B.nrm[p] = f4(V3{0.0f, 1.0f, 0.0f}, 0.0f);
+    }
+    B.rad[p] = f4(radiance, rad4.w);
+}
+
+// accum += each sample's path, in sample order (pathtrace.wgsl:4541-4557).
+__global__ void k_accumulate(Params P, PathBufs B, float4* accum, uint32_t n_idx, uint32_t K) {
+    uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t w = P.w[P_SIZE], h = P.w[P_SIZE + 1];
+    uint32_t gx, gy;
+    if (idx >= n_idx || !slot_pixel(idx, w, h, gx, gy)) return;
+    uint32_t pix = gy * w + gx;
+    float4 c = accum[pix * 5], a = accum[pix * 5 + 1], nn = accum[pix * 5 + 2];
+    for (uint32_t k = 0; k < K; ++k) {
+        uint32_t p = k * n_idx + idx;
+        V3 r = xyz(B.rad[p]), al = xyz(B.alb[p]), nm = xyz(B.nrm[p]);
+        c.x += r.x; c.y += r.y; c.z += r.z; c.w += 1.0f;
+        float lum = luminance(r);
+        a.x += al.x; a.y += al.y; a.z += al.z; a.w += lum;
+        nn.x += nm.x; nn.y += nm.y; nn.z += nm.z; nn.w += lum * lum;
+    }
+    accum[pix * 5] = c;
+    accum[pix * 5 + 1] = a;
+    accum[pix * 5 + 2] = nn;
+}
+
+// Per-wave counts into the cumulative totals.
+__global__ void k_tally(Queues Q, uint32_t depths, uint32_t paths) {
+    if (threadIdx.x != 0) return;
+    unsigned long long c = 0, s = 0;
+    for (uint32_t d = 0; d < depths; ++d) {
+        c += Q.cnt[d * 4u];
+        s += min(Q.cnt[d * 4u + 1], Q.shadow_cap);
+    }
+    atomicAdd(&Q.totals[T_CLOSEST], c);
+    atomicAdd(&Q.totals[T_SHADOW], s);
+    atomicAdd(&Q.totals[T_PATHS], (unsigned long long)paths);
+}
+
+template <bool COUNT, bool WIDE>
+__global__ void k_trace(Params P, Walk wk, const trt_ray* rays, uint64_t n, trt_hit* hits, unsigned long long* totals) {
+    Sections X(P);
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    WalkCount wc{0, 0, 0};
+    if (i < n) {
+        trt_ray r = rays[i];
+        bool guard = false;
+        Hit h = walk<COUNT, WIDE>(wk, X, V3{r.o[0], r.o[1], r.o[2]}, V3{r.d[0], r.d[1], r.d[2]}, r.tmax, r.mode, &wc, &guard);
+        hits[i] = trt_hit{h.t, h.tri, h.u, h.v, h.inst, h.part};
+    }
+    if (COUNT) {
+        warp_add64(&totals[T_E_NODES], wc.nodes);
+        warp_add64(&totals[T_E_TRIS], wc.tris);
+        warp_add64(&totals[T_E_UNITS], wc.units);
+    }
+}
+
+// The Joe-Kuo direction numbers of Sobol dimensions 1-3, bit-reversed (the recurrence of the primitive polynomials
+// x + 1, x^2 + x + 1, x^3 + x + 1 with initial numbers 1; 1, 3; 1, 3, 1).
+void sobol_directions(uint32_t out[3][16]) {
+    const int s_[3] = {1, 2, 3};
+    const uint32_t a_[3] = {0, 1, 1};
+    const uint32_t m0[3][3] = {{1, 0, 0}, {1, 3, 0}, {1, 3, 1}};
+    for (int k = 0; k < 3; ++k) {
+        uint32_t m[32];
+        int s = s_[k];
+        for (int i = 0; i < 32; ++i) {
+            if (i < s) {
+                m[i] = m0[k][i];
+            } else {
+                uint32_t v = m[i - s] ^ (m[i - s] << s);
+                for (int j = 1; j < s; ++j) v ^= ((a_[k] >> (s - 1 - j)) & 1u) * (m[i - j] << j);
+                m[i] = v;
+            }
+        }
+        for (int i = 0; i < 16; ++i) {
+            uint32_t x = m[i] << (31 - i), r = 0;
+            for (int b = 0; b < 32; ++b) r |= ((x >> b) & 1u) << (31 - b);
+            out[k][i] = r;
+        }
+    }
+}
+
+}  // namespace trt
+
+using namespace trt;
+
+// ---- host side ------------------------------------------------------------------------------------------------------
+
+struct trt_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int sm_count = 0;
+    char name[256] = {0};
+    std::string err;
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+};
+
+struct trt_scene {
+    trt_ctx* ctx = nullptr;
+    void* buf[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    uint64_t bytes[5] = {0, 0, 0, 0, 0};
+    ushort4* env = nullptr;
+    uint32_t env_w = 1, env_h = 1;
+    WideBvh wide;
+    float4* accum = nullptr;
+    uint32_t accum_w = 0, accum_h = 0;
+    // work buffers
+    void* work = nullptr;
+    uint64_t work_bytes = 0;
+    uint32_t slots = 0;
+    PathBufs B{};
+    Queues Q{};
+    unsigned long long* totals = nullptr;
+    int profiling = 0;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_extend, ev_shadow, ev_shade, ev_free;
+    double extend_ms = 0, shadow_ms = 0, shade_ms = 0;
+    uint64_t extend_launches = 0, shadow_launches = 0, renders = 0, launches = 0;
+};
+
+namespace {
+
+std::mutex g_sobol_mu;
+
+int fail(trt_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+int cuda_fail(trt_ctx* c, cudaError_t e, const char* what) {
+    return fail(c, TRT_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define TRT_CUDA(ctx, call)                                         \
+    do {                                                            \
+        cudaError_t e_ = (call);                                    \
+        if (e_ != cudaSuccess) return cuda_fail((ctx), e_, #call);  \
+    } while (0)
+
+DScene scene_view(const trt_scene* s) {
+    DScene S;
+    S.vertices = (const float4*)s->buf[0];
+    S.leaves = (const float4*)s->buf[1];
+    S.nodes = (const uint4*)s->buf[2];
+    S.tables = (const uint4*)s->buf[3];
+    S.words = (const uint32_t*)s->buf[4];
+    S.env = s->env;
+    S.env_w = s->env_w;
+    S.env_h = s->env_h;
+    S.n_nodes = s->bytes[2] / 32;
+    S.n_tris = s->bytes[1] / 48;
+    S.n_table_vec4 = s->bytes[3] / 16;
+    S.n_words = s->bytes[4] / 4;
+    return S;
+}
+
+// Checks that what Params names lies inside the uploaded buffers (the reference trusts its own prep; a C ABI does not).
+int check_params(trt_scene* s, const uint32_t* P) {
+    uint64_t tv = s->bytes[3] / 16, wn = s->bytes[4] / 4;
+    for (int k = 0; k < 12; ++k)
+        if (P[P_TABLE_FIRST + k] > tv) return fail(s->ctx, TRT_EINVAL, "Params.table_first names a vec4 past the tables");
+    for (int k = 0; k < 5; ++k)
+        if (P[P_WORD_FIRST + k] > wn) return fail(s->ctx, TRT_EINVAL, "Params.word_first names a word past the words");
+    uint32_t w = P[P_SIZE], h = P[P_SIZE + 1];
+    if (w == 0 || h == 0 || (uint64_t)w * h > (1ull << 26)) return fail(s->ctx, TRT_EINVAL, "Params.size: 1 to 2^26 pixels");
+    if (P[P_COUNTS + 2] >= MAX_DEPTH - 1) return fail(s->ctx, TRT_EINVAL, "Params.counts.z (max bounces) must be below 63");
+    if (P[P_COUNTS2] > MAX_DIR_LIGHTS) return fail(s->ctx, TRT_EINVAL, "more than 4 directional lights");
+    if (P[P_COUNTS] != P[P_COUNTS2]) return fail(s->ctx, TRT_EINVAL, "local lights are not part of this pass");
+    uint32_t top = P[P_MOTION + 2], units = P[P_MOTION + 3];
+    if (units > 0 && (uint64_t)top >= s->bytes[2] / 32) return fail(s->ctx, TRT_EINVAL, "Params.motion.z names a node past the nodes");
+    if (P[P_ENV] == 0x3f800000u && ((uint32_t)bf(P[P_ENV + 1]) != s->env_w || (uint32_t)bf(P[P_ENV + 2]) != s->env_h))
+        return fail(s->ctx, TRT_EINVAL, "Params.env's size is not the uploaded environment's");
+    return TRT_OK;
+}
+
+int ensure_work(trt_scene* s, uint32_t slots, uint32_t shadow_slots) {
+    uint32_t shadow_cap = slots * shadow_slots;
+    uint64_t need = 0;
+    auto add = [&](uint64_t b) { uint64_t at = need; need += (b + 255) / 256 * 256; return at; };
+    uint64_t o_o = add(16ull * slots), o_d = add(16ull * slots), o_thr = add(16ull * slots), o_rad = add(16ull * slots),
+             o_alb = add(16ull * slots), o_nrm = add(16ull * slots), o_mx = add(16ull * slots), o_mn = add(16ull * slots),
+             o_nee = add(16ull * slots * N_SLOTS), o_nt = add(16ull * slots), o_vis = add(4ull * slots),
+             o_q0 = add(4ull * slots), o_q1 = add(4ull * slots), o_ha = add(16ull * slots), o_hb = add(8ull * slots),
+             o_so = add(16ull * shadow_cap), o_sd = add(16ull * shadow_cap), o_sp = add(4ull * shadow_cap),
+             o_cnt = add(4ull * (MAX_DEPTH * 4 + 4));
+    if (s->work && s->slots >= slots && s->Q.shadow_cap >= shadow_cap) return TRT_OK;
+    if (s->work) cudaFree(s->work);
+    s->work = nullptr;
+    TRT_CUDA(s->ctx, cudaMalloc(&s->work, need));
+    s->work_bytes = need;
+    char* b = (char*)s->work;
+    s->slots = slots;
+    s->B = PathBufs{(float4*)(b + o_o), (float4*)(b + o_d), (float4*)(b + o_thr), (float4*)(b + o_rad),
+                    (float4*)(b + o_alb), (float4*)(b + o_nrm), (float4*)(b + o_mx), (float4*)(b + o_mn),
+                    (float4*)(b + o_nee), (float4*)(b + o_nt), (uint32_t*)(b + o_vis), slots};
+    s->Q.q[0] = (uint32_t*)(b + o_q0);
+    s->Q.q[1] = (uint32_t*)(b + o_q1);
+    s->Q.hit_a = (float4*)(b + o_ha);
+    s->Q.hit_b = (uint2*)(b + o_hb);
+    s->Q.so = (float4*)(b + o_so);
+    s->Q.sd = (float4*)(b + o_sd);
+    s->Q.sp = (uint32_t*)(b + o_sp);
+    s->Q.cnt = (uint32_t*)(b + o_cnt);
+    s->Q.totals = s->totals;
+    s->Q.shadow_cap = shadow_cap;
+    return TRT_OK;
+}
+
+std::pair<cudaEvent_t, cudaEvent_t> take_events(trt_scene* s) {
+    if (!s->ev_free.empty()) {
+        auto e = s->ev_free.back();
+        s->ev_free.pop_back();
+        return e;
+    }
+    std::pair<cudaEvent_t, cudaEvent_t> e{nullptr, nullptr};
+    cudaEventCreate(&e.first);
+    cudaEventCreate(&e.second);
+    return e;
+}
+
+int grid_for(const void* fn, int block, int sm_count) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, 0);
+    return std::max(1, per_sm) * sm_count;
+}
+
+template <bool COUNT, bool WIDE>
+int render_waves(trt_scene* s, const Params& P, uint32_t first_sample, uint32_t spp) {
+    trt_ctx* c = s->ctx;
+    cudaStream_t st = c->stream;
+    uint32_t w = P.w[P_SIZE], h = P.w[P_SIZE + 1];
+    uint32_t n_idx = ((w + 7u) / 8u) * ((h + 3u) / 4u) * 32u;
+    // Samples a wave: enough paths to fill the GPU (about two million), at most spp.
+    uint32_t K = std::max(1u, std::min(spp, (2u << 20) / std::max(1u, n_idx)));
+    uint32_t n_dir = P.w[P_COUNTS2];
+    int rc = ensure_work(s, n_idx * K, n_dir + 2u);
+    if (rc) return rc;
+    DScene S = scene_view(s);
+    Walk wk{S, s->wide.view(), P.w[P_MOTION + 2], P.w[P_MOTION + 3]};
+    uint32_t last = P.w[P_COUNTS + 2];
+    const int blk = 128;
+    int g_ext = grid_for((const void*)k_extend<COUNT, WIDE>, blk, c->sm_count);
+    int g_sha = grid_for((const void*)k_shadow<COUNT, WIDE>, blk, c->sm_count);
+    std::vector<uint32_t> host_cnt(MAX_DEPTH * 4 + 4, 0);
+    for (uint32_t s0 = 0; s0 < spp; s0 += K) {
+        uint32_t k = std::min(K, spp - s0);
+        TRT_CUDA(c, cudaMemcpyAsync(s->Q.cnt, host_cnt.data(), host_cnt.size() * 4, cudaMemcpyHostToDevice, st));
+        uint32_t n = n_idx * k;
+        k_raygen<<<(n + blk - 1) / blk, blk, 0, st>>>(P, s->B, s->Q, first_sample + s0, n_idx, k);
+        s->launches++;
+        for (uint32_t depth = 0; depth <= last; ++depth) {
+            std::pair<cudaEvent_t, cudaEvent_t> e{};
+            if (s->profiling) { e = take_events(s); cudaEventRecord(e.first, st); }
+            k_extend<COUNT, WIDE><<<g_ext, blk, 0, st>>>(P, wk, s->B, s->Q, depth);
+            if (s->profiling) { cudaEventRecord(e.second, st); s->ev_extend.push_back(e); }
+            if (s->profiling) { e = take_events(s); cudaEventRecord(e.first, st); }
+            k_shade<<<(n + blk - 1) / blk, blk, 0, st>>>(P, S, s->B, s->Q, depth);
+            if (s->profiling) { cudaEventRecord(e.second, st); s->ev_shade.push_back(e); }
+            if (s->profiling) { e = take_events(s); cudaEventRecord(e.first, st); }
+            k_shadow<COUNT, WIDE><<<g_sha, blk, 0, st>>>(P, wk, s->B, s->Q, depth);
+            if (s->profiling) { cudaEventRecord(e.second, st); s->ev_shadow.push_back(e); }
+            k_resolve<<<(n + blk - 1) / blk, blk, 0, st>>>(s->B, s->Q, depth, bf(P.w[P_MISC]));
+            s->launches += 4;
+            s->extend_launches++;
+            s->shadow_launches++;
+        }
+        k_accumulate<<<(n_idx + blk - 1) / blk, blk, 0, st>>>(P, s->B, s->accum, n_idx, k);
+        k_tally<<<1, 32, 0, st>>>(s->Q, last + 1, w * h * k);
+        s->launches += 2;
+    }
+    TRT_CUDA(c, cudaGetLastError());
+    return TRT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int trt_create(const trt_options* opts, trt_ctx** out) {
+    if (!out) return TRT_EINVAL;
+    *out = nullptr;
+    auto* c = new trt_ctx();
+    c->device = opts ? opts->device : 0;
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device);
+    cudaDeviceProp prop;
+    if (e == cudaSuccess) e = cudaGetDeviceProperties(&prop, c->device);
+    if (e == cudaSuccess) {
+        std::snprintf(c->name, sizeof(c->name), "%s", prop.name);
+        if (prop.major < 10) e = cudaErrorNoKernelImageForDevice;
+    }
+    if (e == cudaSuccess) {
+        std::lock_guard<std::mutex> lk(g_sobol_mu);
+        uint32_t t[3][16];
+        sobol_directions(t);
+        e = cudaMemcpyToSymbol(c_sobol, t, sizeof(t));
+    }
+    if (e == cudaSuccess) e = cudaEventCreate(&c->t0);
+    if (e == cudaSuccess) e = cudaEventCreate(&c->t1);
+    if (e != cudaSuccess) {
+        // (No context to hold the message: the caller gets the code.)
+        std::fprintf(stderr, "trt_create: %s\n", cudaGetErrorString(e));
+        if (c->stream) cudaStreamDestroy(c->stream);
+        delete c;
+        return TRT_ECUDA;
+    }
+    *out = c;
+    return TRT_OK;
+}
+
+void trt_destroy(trt_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->t0) cudaEventDestroy(c->t0);
+    if (c->t1) cudaEventDestroy(c->t1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+const char* trt_last_error(const trt_ctx* c) { return c ? c->err.c_str() : "no context"; }
+
+int trt_device_info(const trt_ctx* c, char* name, size_t name_len, int* sm_count) {
+    if (!c) return TRT_EINVAL;
+    if (name && name_len) std::snprintf(name, name_len, "%s", c->name);
+    if (sm_count) *sm_count = c->sm_count;
+    return TRT_OK;
+}
+
+int trt_scene_upload(trt_ctx* c, const trt_scene_desc* d, trt_scene** out) {
+    if (!c || !d || !out) return TRT_EINVAL;
+    *out = nullptr;
+    cudaSetDevice(c->device);
+    const void* src[5] = {d->vertices, d->leaves, d->nodes, d->tables, d->words};
+    const uint64_t n[5] = {d->vertices_bytes, d->leaves_bytes, d->nodes_bytes, d->tables_bytes, d->words_bytes};
+    const uint64_t unit[5] = {48, 48, 32, 16, 4};
+    for (int k = 0; k < 5; ++k)
+        if (!src[k] || n[k] == 0 || n[k] % unit[k] != 0)
+            return fail(c, TRT_EINVAL, "scene buffer " + std::to_string(k) + ": no data, or not whole records");
+    if (!d->env_half || d->env_w == 0 || d->env_h == 0) return fail(c, TRT_EINVAL, "no environment texels");
+    auto* s = new trt_scene();
+    s->ctx = c;
+    auto cleanup = [&](int rc) { trt_scene_free(s); return rc; };
+    for (int k = 0; k < 5; ++k) {
+        cudaError_t e = cudaMalloc(&s->buf[k], n[k]);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(s->buf[k], src[k], n[k], cudaMemcpyHostToDevice, c->stream);
+        if (e != cudaSuccess) return cleanup(cuda_fail(c, e, "scene upload"));
+        s->bytes[k] = n[k];
+    }
+    s->env_w = d->env_w;
+    s->env_h = d->env_h;
+    uint64_t eb = 8ull * d->env_w * d->env_h;
+    cudaError_t e = cudaMalloc(&s->env, eb);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(s->env, d->env_half, eb, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMalloc(&s->totals, sizeof(unsigned long long) * T_COUNT);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->totals, 0, sizeof(unsigned long long) * T_COUNT, c->stream);
+    if (e != cudaSuccess) return cleanup(cuda_fail(c, e, "scene upload"));
+    s->Q.totals = s->totals;
+    int rc = s->wide.build(c, scene_view(s), d, c->stream);
+    if (rc) return cleanup(rc);
+    e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cleanup(cuda_fail(c, e, "scene upload"));
+    *out = s;
+    return TRT_OK;
+}
+
+void trt_scene_free(trt_scene* s) {
+    if (!s) return;
+    cudaSetDevice(s->ctx->device);
+    cudaStreamSynchronize(s->ctx->stream);
+    for (void* b : s->buf)
+        if (b) cudaFree(b);
+    if (s->env) cudaFree(s->env);
+    if (s->accum) cudaFree(s->accum);
+    if (s->work) cudaFree(s->work);
+    if (s->totals) cudaFree(s->totals);
+    s->wide.release();
+    for (auto* v : {&s->ev_extend, &s->ev_shadow, &s->ev_shade, &s->ev_free})
+        for (auto& e : *v) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
+    delete s;
+}
+
+int trt_scene_update(trt_scene* s, uint32_t which, uint64_t offset, const void* src, uint64_t bytes) {
+    if (!s) return TRT_EINVAL;
+    trt_ctx* c = s->ctx;
+    if (which > 4 || !src || offset + bytes > s->bytes[which] || offset + bytes < offset)
+        return fail(c, TRT_EINVAL, "trt_scene_update: the range is not inside the buffer");
+    cudaSetDevice(c->device);
+    TRT_CUDA(c, cudaMemcpyAsync((char*)s->buf[which] + offset, src, bytes, cudaMemcpyHostToDevice, c->stream));
+    if (which == 1 || which == 2 || which == 3) {
+        int rc = s->wide.refit(c, scene_view(s), c->stream);
+        if (rc) return rc;
+    }
+    return TRT_OK;
+}
+
+int trt_render(trt_scene* s, const uint32_t params[TRT_PARAMS_WORDS], uint32_t first_sample, uint32_t spp,
+               uint32_t flags, float* accum_host, trt_stats* stats) {
+    if (!s || !params) return TRT_EINVAL;
+    trt_ctx* c = s->ctx;
+    cudaSetDevice(c->device);
+    int rc = check_params(s, params);
+    if (rc) return rc;
+    Params P;
+    std::memcpy(P.w, params, sizeof(P.w));
+    uint32_t w = P.w[P_SIZE], h = P.w[P_SIZE + 1];
+    if (!s->accum || s->accum_w != w || s->accum_h != h) {
+        if (s->accum) cudaFree(s->accum);
+        s->accum = nullptr;
+        TRT_CUDA(c, cudaMalloc(&s->accum, 80ull * w * h));
+        s->accum_w = w;
+        s->accum_h = h;
+        flags &= ~TRT_RENDER_ACCUMULATE;
+    }
+    if (!(flags & TRT_RENDER_ACCUMULATE)) TRT_CUDA(c, cudaMemsetAsync(s->accum, 0, 80ull * w * h, c->stream));
+    unsigned long long before[T_COUNT] = {0};
+    if (stats) {
+        TRT_CUDA(c, cudaMemcpyAsync(before, s->totals, sizeof(before), cudaMemcpyDeviceToHost, c->stream));
+        TRT_CUDA(c, cudaEventRecord(c->t0, c->stream));
+    }
+    uint64_t launches0 = s->launches;
+    bool count = (flags & TRT_RENDER_COUNT) != 0, binary = (flags & TRT_RENDER_BINARY) != 0 || !s->wide.ready();
+    if (spp > 0) {
+        if (count) rc = binary ? render_waves<true, false>(s, P, first_sample, spp) : render_waves<true, true>(s, P, first_sample, spp);
+        else rc = binary ? render_waves<false, false>(s, P, first_sample, spp) : render_waves<false, true>(s, P, first_sample, spp);
+        if (rc) return rc;
+    }
+    s->renders++;
+    if (accum_host)
+        TRT_CUDA(c, cudaMemcpyAsync(accum_host, s->accum, 80ull * w * h, cudaMemcpyDeviceToHost, c->stream));
+    if (stats) {
+        unsigned long long after[T_COUNT];
+        TRT_CUDA(c, cudaEventRecord(c->t1, c->stream));
+        TRT_CUDA(c, cudaMemcpyAsync(after, s->totals, sizeof(after), cudaMemcpyDeviceToHost, c->stream));
+        TRT_CUDA(c, cudaStreamSynchronize(c->stream));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, c->t0, c->t1);
+        stats->closest_rays = after[T_CLOSEST] - before[T_CLOSEST];
+        stats->shadow_rays = after[T_SHADOW] - before[T_SHADOW];
+        stats->paths = after[T_PATHS] - before[T_PATHS];
+        stats->guard_trips = (uint32_t)(after[T_GUARD] - before[T_GUARD]);
+        stats->device_ms = ms;
+        stats->launches = (uint32_t)(s->launches - launches0);
+        if (stats->guard_trips) return fail(c, TRT_EGUARD, "a traversal stopped at its iteration limit");
+    } else if (accum_host) {
+        TRT_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
+    return TRT_OK;
+}
+
+int trt_accum_device_ptr(trt_scene* s, void** ptr, uint64_t* bytes) {
+    if (!s || !ptr) return TRT_EINVAL;
+    *ptr = s->accum;
+    if (bytes) *bytes = 80ull * s->accum_w * s->accum_h;
+    return TRT_OK;
+}
+
+int trt_accum_read(trt_scene* s, float* accum_host, uint64_t bytes) {
+    if (!s || !accum_host) return TRT_EINVAL;
+    trt_ctx* c = s->ctx;
+    if (bytes != 80ull * s->accum_w * s->accum_h) return fail(c, TRT_EINVAL, "trt_accum_read: wrong size");
+    cudaSetDevice(c->device);
+    TRT_CUDA(c, cudaMemcpyAsync(accum_host, s->accum, bytes, cudaMemcpyDeviceToHost, c->stream));
+    TRT_CUDA(c, cudaStreamSynchronize(c->stream));
+    return TRT_OK;
+}
+
+int trt_trace(trt_scene* s, const uint32_t params[TRT_PARAMS_WORDS], const trt_ray* rays, uint64_t n, uint32_t flags,
+              trt_hit* hits) {
+    if (!s || !params || (!rays && n) || (!hits && n)) return TRT_EINVAL;
+    trt_ctx* c = s->ctx;
+    cudaSetDevice(c->device);
+    int rc = check_params(s, params);
+    if (rc) return rc;
+    if (n == 0) return TRT_OK;
+    Params P;
+    std::memcpy(P.w, params, sizeof(P.w));
+    trt_ray* dr = nullptr;
+    trt_hit* dh = nullptr;
+    TRT_CUDA(c, cudaMalloc(&dr, sizeof(trt_ray) * n));
+    cudaError_t e = cudaMalloc(&dh, sizeof(trt_hit) * n);
+    if (e != cudaSuccess) { cudaFree(dr); return cuda_fail(c, e, "trt_trace"); }
+    e = cudaMemcpyAsync(dr, rays, sizeof(trt_ray) * n, cudaMemcpyHostToDevice, c->stream);
+    DScene S = scene_view(s);
+    Walk wk{S, s->wide.view(), P.w[P_MOTION + 2], P.w[P_MOTION + 3]};
+    bool binary = (flags & TRT_RENDER_BINARY) != 0 || !s->wide.ready();
+    bool count = (flags & TRT_RENDER_COUNT) != 0;
+    unsigned grid = (unsigned)((n + 127) / 128);
+    if (e == cudaSuccess) {
+        if (count) {
+            if (binary) k_trace<true, false><<<grid, 128, 0, c->stream>>>(P, wk, dr, n, dh, s->totals);
+            else k_trace<true, true><<<grid, 128, 0, c->stream>>>(P, wk, dr, n, dh, s->totals);
+        } else {
+            if (binary) k_trace<false, false><<<grid, 128, 0, c->stream>>>(P, wk, dr, n, dh, s->totals);
+            else k_trace<false, true><<<grid, 128, 0, c->stream>>>(P, wk, dr, n, dh, s->totals);
+        }
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hits, dh, sizeof(trt_hit) * n, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(dr);
+    cudaFree(dh);
+    if (e != cudaSuccess) return cuda_fail(c, e, "trt_trace");
+    return TRT_OK;
+}
+
+int trt_scene_totals(trt_scene* s, trt_totals* out) {
+    if (!s || !out) return TRT_EINVAL;
+    trt_ctx* c = s->ctx;
+    cudaSetDevice(c->device);
+    unsigned long long t[T_COUNT];
+    TRT_CUDA(c, cudaMemcpyAsync(t, s->totals, sizeof(t), cudaMemcpyDeviceToHost, c->stream));
+    TRT_CUDA(c, cudaStreamSynchronize(c->stream));
+    auto drain = [&](std::vector<std::pair<cudaEvent_t, cudaEvent_t>>& v, double& acc) {
+        for (auto& e : v) {
+            float ms = 0;
+            if (cudaEventElapsedTime(&ms, e.first, e.second) == cudaSuccess) acc += ms;
+            s->ev_free.push_back(e);
+        }
+        v.clear();
+    };
+    drain(s->ev_extend, s->extend_ms);
+    drain(s->ev_shadow, s->shadow_ms);
+    drain(s->ev_shade, s->shade_ms);
+    out->closest_rays = t[T_CLOSEST];
+    out->shadow_rays = t[T_SHADOW];
+    out->paths = t[T_PATHS];
+    out->node_visits = t[T_E_NODES];
+    out->tri_tests = t[T_E_TRIS];
+    out->unit_entries = t[T_E_UNITS];
+    out->shadow_node_visits = t[T_S_NODES];
+    out->shadow_tri_tests = t[T_S_TRIS];
+    out->shadow_unit_entries = t[T_S_UNITS];
+    out->guard_trips = t[T_GUARD];
+    out->renders = s->renders;
+    out->launches = s->launches;
+    out->extend_ms = s->extend_ms;
+    out->shadow_ms = s->shadow_ms;
+    out->shade_ms = s->shade_ms;
+    out->extend_launches = s->extend_launches;
+    out->shadow_launches = s->shadow_launches;
+    return TRT_OK;
+}
+
+void trt_scene_reset_totals(trt_scene* s) {
+    if (!s) return;
+    cudaSetDevice(s->ctx->device);
+    cudaStreamSynchronize(s->ctx->stream);
+    cudaMemsetAsync(s->totals, 0, sizeof(unsigned long long) * T_COUNT, s->ctx->stream);
+    cudaStreamSynchronize(s->ctx->stream);
+    for (auto* v : {&s->ev_extend, &s->ev_shadow, &s->ev_shade}) {
+        for (auto& e : *v) s->ev_free.push_back(e);
+        v->clear();
+    }
+    s->extend_ms = s->shadow_ms = s->shade_ms = 0;
+    s->extend_launches = s->shadow_launches = s->renders = s->launches = 0;
+}
+
+void trt_scene_set_profiling(trt_scene* s, int on) {
+    if (s) s->profiling = on;
+}
+
+int trt_timer_start(trt_ctx* c) {
+    if (!c) return TRT_EINVAL;
+    TRT_CUDA(c, cudaEventRecord(c->t0, c->stream));
+    return TRT_OK;
+}
+
+int trt_timer_stop(trt_ctx* c, float* ms) {
+    if (!c || !ms) return TRT_EINVAL;
+    TRT_CUDA(c, cudaEventRecord(c->t1, c->stream));
+    TRT_CUDA(c, cudaEventSynchronize(c->t1));
+    TRT_CUDA(c, cudaEventElapsedTime(ms, c->t0, c->t1));
+    return TRT_OK;
+}
+
+int trt_synchronize(trt_ctx* c) {
+    if (!c) return TRT_EINVAL;
+    TRT_CUDA(c, cudaStreamSynchronize(c->stream));
+    return TRT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,166 @@
+"""The pass from Python, shaped as the reference's host interface.
+
+`Gpu.render` mirrors renderer/src/gpu.rs:4116 `Gpu::render(scene, ..., base: Params, spp, timings) -> Result<Frame>`:
+it uploads the prepared buffers, runs `spp` samples (Params `size.z` is the sample index), reads `accum` back and
+converts each 80-byte `Pixel` to a `Frame` (gpu.rs:4211-4232). Errors raise `RenderError` (the reference's
+anyhow::Err), among them a traversal that hit its loop guard (gpu.rs:4199-4205).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import time
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native as N
+from .prep import Prepared
+
+
+class RenderError(RuntimeError):
+    pass
+
+
+@dataclass
+class Frame:
+    """gpu.rs:2059-2076 Frame (without the live-only emission / specular split and the translucent overlay)."""
+    width: int
+    height: int
+    color: np.ndarray      # (h, w, 3)
+    albedo: np.ndarray
+    normal: np.ndarray
+    variance: np.ndarray   # (h, w): variance of the per-pixel mean luminance
+    samples: int
+
+
+def frame_of(accum: np.ndarray, width: int, height: int, spp: int) -> Frame:
+    """gpu.rs:4219-4232: each Pixel over its sample count (at least 1), non-finite values as 0."""
+    px = np.asarray(accum, np.float32).reshape(-1, N.PIXEL_FLOATS)
+    c = np.maximum(px[:, 3:4], 1.0)
+    p = np.where(np.isfinite(px), px, 0.0)
+    mean = p[:, 7] / c[:, 0]
+    var = np.maximum(p[:, 11] / c[:, 0] - mean * mean, 0.0) / c[:, 0]
+    shape3 = (height, width, 3)
+    return Frame(width, height, (p[:, 0:3] / c).reshape(shape3), (p[:, 4:7] / c).reshape(shape3),
+                 (p[:, 8:11] / c).reshape(shape3), var.reshape(height, width), spp)
+
+
+RAY_DTYPE = np.dtype([("o", np.float32, 3), ("tmax", np.float32), ("d", np.float32, 3), ("mode", np.uint32)])
+HIT_DTYPE = np.dtype([("t", np.float32), ("tri", np.uint32), ("u", np.float32), ("v", np.float32),
+                      ("inst", np.uint32), ("part", np.uint32)])
+
+
+class Scene:
+    """A scene resident on the device (trt_scene)."""
+
+    def __init__(self, gpu: "Gpu", prepared: Prepared):
+        self.gpu = gpu
+        self.prepared = prepared
+        self.handle = C.c_void_p()
+        L = N.lib()
+        arrs = [prepared.vertices, prepared.leaves, prepared.nodes, prepared.tables, prepared.words, prepared.env_half]
+        arrs = [np.ascontiguousarray(a) for a in arrs]
+        d = N.SceneDesc(arrs[0].ctypes.data, arrs[0].nbytes, arrs[1].ctypes.data, arrs[1].nbytes,
+                        arrs[2].ctypes.data, arrs[2].nbytes, arrs[3].ctypes.data, arrs[3].nbytes,
+                        arrs[4].ctypes.data, arrs[4].nbytes, arrs[5].ctypes.data, prepared.env_w, prepared.env_h)
+        gpu._check(L.trt_scene_upload(gpu.ctx, C.byref(d), C.byref(self.handle)), "trt_scene_upload")
+
+    def close(self):
+        if self.handle:
+            N.lib().trt_scene_free(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def render_raw(self, params: np.ndarray, spp: int, first_sample: int = 0, flags: int = 0, read: bool = True,
+                   stats: bool = True):
+        """Runs the pass; returns (accum as (w*h, 20) float32 or None, Stats or None)."""
+        L = N.lib()
+        p = np.ascontiguousarray(params, dtype=np.uint32)
+        w, h = int(p[16]), int(p[17])
+        acc = np.empty((w * h, N.PIXEL_FLOATS), np.float32) if read else None
+        st = N.Stats() if stats else None
+        rc = L.trt_render(self.handle, p.ctypes.data_as(C.POINTER(C.c_uint32)), first_sample, spp, flags,
+                          acc.ctypes.data_as(C.POINTER(C.c_float)) if read else None, C.byref(st) if stats else None)
+        self.gpu._check(rc, "trt_render")
+        return acc, st
+
+    def trace(self, params: np.ndarray, rays: np.ndarray, flags: int = 0) -> np.ndarray:
+        L = N.lib()
+        rays = np.ascontiguousarray(rays, dtype=RAY_DTYPE)
+        hits = np.zeros(len(rays), HIT_DTYPE)
+        p = np.ascontiguousarray(params, dtype=np.uint32)
+        rc = L.trt_trace(self.handle, p.ctypes.data_as(C.POINTER(C.c_uint32)),
+                         rays.ctypes.data_as(C.POINTER(N.Ray)), len(rays), flags,
+                         hits.ctypes.data_as(C.POINTER(N.Hit)))
+        self.gpu._check(rc, "trt_trace")
+        return hits
+
+    def totals(self) -> dict:
+        t = N.Totals()
+        self.gpu._check(N.lib().trt_scene_totals(self.handle, C.byref(t)), "trt_scene_totals")
+        return {f[0]: getattr(t, f[0]) for f in N.Totals._fields_}
+
+    def reset_totals(self):
+        N.lib().trt_scene_reset_totals(self.handle)
+
+    def set_profiling(self, on: bool):
+        N.lib().trt_scene_set_profiling(self.handle, 1 if on else 0)
+
+
+class Gpu:
+    """One device context (trt_ctx): a CUDA stream and the scenes uploaded through it."""
+
+    def __init__(self, device: int = 0):
+        L = N.lib()
+        self.ctx = C.c_void_p()
+        rc = L.trt_create(C.byref(N.Options(device, 0)), C.byref(self.ctx))
+        if rc != 0:
+            raise RenderError(f"trt_create failed ({N.ERRORS.get(rc, rc)}): no sm_100 device {device}?")
+
+    def _check(self, rc: int, what: str):
+        if rc != 0:
+            msg = N.lib().trt_last_error(self.ctx).decode()
+            raise RenderError(f"{what}: {N.ERRORS.get(rc, rc)}: {msg}")
+
+    def device_info(self) -> tuple[str, int]:
+        name = C.create_string_buffer(256)
+        sms = C.c_int()
+        self._check(N.lib().trt_device_info(self.ctx, name, 256, C.byref(sms)), "trt_device_info")
+        return name.value.decode(), sms.value
+
+    def upload(self, prepared: Prepared) -> Scene:
+        return Scene(self, prepared)
+
+    def render(self, prepared: Prepared | Scene, base: np.ndarray, spp: int, timings: list | None = None,
+               first_sample: int = 0, flags: int = 0) -> Frame:
+        """gpu.rs:4116 Gpu::render: upload (unless given a resident Scene), `spp` samples, readback, Frame."""
+        t0 = time.perf_counter()
+        scene = prepared if isinstance(prepared, Scene) else self.upload(prepared)
+        if timings is not None and not isinstance(prepared, Scene):
+            timings.append(("upload_ms", (time.perf_counter() - t0) * 1e3))
+        acc, st = scene.render_raw(base, spp, first_sample=first_sample, flags=flags)
+        if timings is not None:
+            timings.append(("trace_ms", float(st.device_ms)))
+        w, h = int(base[16]), int(base[17])
+        return frame_of(acc, w, h, spp)
+
+    def timer_start(self):
+        self._check(N.lib().trt_timer_start(self.ctx), "trt_timer_start")
+
+    def timer_stop(self) -> float:
+        ms = C.c_float()
+        self._check(N.lib().trt_timer_stop(self.ctx, C.byref(ms)), "trt_timer_stop")
+        return float(ms.value)
+
+    def synchronize(self):
+        self._check(N.lib().trt_synchronize(self.ctx), "trt_synchronize")
+
+    def close(self):
+        if self.ctx:
+            N.lib().trt_destroy(self.ctx)
+            self.ctx = C.c_void_p()
