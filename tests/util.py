@@ -52,6 +52,9 @@ def random_rays(P, n, seed=0, modes=(0, 1, 2), spread=1.0):
     r["o"][:k] = cam + rng.normal(0, spread, (k, 3))
     r["o"][k:] = lo + (hi - lo) * rng.random((n - k, 3))
     d = rng.normal(0, 1, (n, 3))
+    # Half the rays aimed at points inside the scene's bounds, half in any direction.
+    aim = rng.random(n) < 0.5
+    d[aim] = lo + (hi - lo) * rng.random((aim.sum(), 3)) - r["o"][aim]
     r["d"] = d / np.linalg.norm(d, axis=1, keepdims=True)
     r["tmax"] = np.where(rng.random(n) < 0.2, rng.uniform(0.1, 50.0, n), 3.0e38).astype(np.float32)
     r["mode"] = rng.choice(modes, n)

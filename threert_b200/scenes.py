@@ -145,20 +145,21 @@ def catmull_rom(points: np.ndarray, t: float) -> np.ndarray:
 
 
 def city_camera_path(seed: int, extent: float = 500.0, keys: int = 12) -> np.ndarray:
+    """Key points of the camera's loop over the city: 0.25 to 0.75 of the way out, 3 to 9 % of the extent up."""
     rng = np.random.default_rng(seed ^ 0xC0FFEE)
     ang = np.sort(rng.uniform(0, 2 * math.pi, keys))
     rad = rng.uniform(0.25, 0.75, keys) * extent
-    hgt = rng.uniform(15.0, 45.0, keys)
+    hgt = rng.uniform(0.03, 0.09, keys) * extent
     return np.stack([np.cos(ang) * rad, hgt, np.sin(ang) * rad], -1)
 
 
-def city_camera(frame: int, frames: int, seed: int, width: int, height: int) -> Camera:
-    pts = city_camera_path(seed)
+def city_camera(frame: int, frames: int, seed: int, width: int, height: int, extent: float = 500.0) -> Camera:
+    pts = city_camera_path(seed, extent)
     t = frame / frames
     p = catmull_rom(pts, t)
     q = catmull_rom(pts, t + 0.5 / frames)
-    look = q + (q - p) / max(np.linalg.norm(q - p), 1e-6) * 50.0
-    look[1] = p[1] - 12.0
+    look = q + (q - p) / max(np.linalg.norm(q - p), 1e-6) * (0.1 * extent)
+    look[1] = p[1] - 0.024 * extent
     return Camera.look_at(tuple(p), tuple(look), 60.0, width, height)
 
 
@@ -226,7 +227,7 @@ def city(n_objects: int = 4000, width: int = 1280, height: int = 720, max_depth:
     sun = DirLight(direction=tuple(-np.asarray(to_sun)), color=(1.0, 0.96, 0.9), intensity=90000.0)
     sky = Sky("gradient", zenith=(1200.0, 2000.0, 4000.0), horizon=(5250.0, 5950.0, 7000.0), ground=(600.0, 600.0, 600.0),
               width=sky_size[0], height=sky_size[1])
-    cam = city_camera(frame, frames, seed, width, height)
+    cam = city_camera(frame, frames, seed, width, height, extent)
     return SceneDescription(meshes, materials, instances, cam, lights=[sun], sky=sky,
                             preset=Preset(max_bounces=max_depth, rr_depth=3, clamp_indirect=1.0e9), seed=0x5EED)
 
