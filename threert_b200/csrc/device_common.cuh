@@ -7,6 +7,7 @@
 // rounds exactly as the C++ restatement does.
 #pragma once
 #include <cstdint>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 namespace trt {
@@ -86,29 +87,19 @@ __device__ __forceinline__ bool non_finite3(V3 v) {
 }
 __device__ __forceinline__ V3 xyz(float4 a) { return {a.x, a.y, a.z}; }
 __device__ __forceinline__ float4 f4(V3 a, float w) { return make_float4(a.x, a.y, a.z, w); }
-__device__ __forceinline__ float half_to_float(uint32_t h) {
-    uint32_t s = (h & 0x8000u) << 16, e = (h >> 10) & 0x1fu, m = h & 0x3ffu;
-    if (e == 0) {
-        if (m == 0) return bf(s);
-        float f = (float)m * (1.0f / 16777216.0f);
-        return s ? -f : f;
-    }
-    if (e == 31) return bf(s | 0x7f800000u | (m << 13));
-    return bf(s | ((e + 112u) << 23) | (m << 13));
-}
+// An IEEE binary16 value (the low 16 bits of h) as f32: the conversion is exact, one cvt instruction.
+__device__ __forceinline__ float half_to_float(uint32_t h) { return __half2float(__ushort_as_half((unsigned short)h)); }
 
 // ---- sampler (sample.wgsl) ---------------------------------------------------------------------------------------
 
-// Sobol dimensions 1-3, bit-reversed direction numbers: the first 16 of each, which a 16-bit index reaches. Filled at
-// start-up from the Joe-Kuo recurrence (sobol_directions in pathtrace.cu).
-__constant__ uint32_t c_sobol[3][16];
+// Sobol dimensions 1-3 of a 16-bit bit-reversed index: the XOR of the direction numbers of its set bits (sample.wgsl
+// sobol_d1..d3), by bytes. g_sobol_bytes[d][0][b] is the XOR of directions 0-7 selected by bits 7..0 of b (the index's
+// bits 31..24), [d][1][b] of directions 8-15 (bits 23..16): the same XOR in two loads. Filled at start-up from the
+// Joe-Kuo recurrence (sobol_directions in pathtrace.cu).
+__device__ uint32_t g_sobol_bytes[3][2][256];
 
 __device__ __forceinline__ uint32_t sobol_dim(uint32_t x, int dim) {
-    uint32_t r = 0;
-#pragma unroll
-    for (int i = 0; i < 16; ++i)
-        if (x & (0x80000000u >> i)) r ^= c_sobol[dim - 1][i];
-    return r;
+    return __ldg(&g_sobol_bytes[dim - 1][0][x >> 24]) ^ __ldg(&g_sobol_bytes[dim - 1][1][(x >> 16) & 255u]);
 }
 __device__ __forceinline__ uint32_t owen_rev(uint32_t n, uint32_t seed) {
     n ^= n * 0x3d20adeau;

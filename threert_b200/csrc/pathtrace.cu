@@ -55,10 +55,17 @@ struct Queues {
     float4* so;           // shadow rays: origin, tmax
     float4* sd;           // direction, mode (bits)
     uint32_t* sp;         // path << 3 | slot
-    uint32_t* cnt;        // per depth: [queue size, shadow count, extend fetch, shadow fetch]
-    unsigned long long* totals;  // cumulative: closest, shadow, paths, nodes, tris, units, guard trips
-    uint32_t shadow_cap;
+    uint32_t* cnt;        // per depth, CNT_STRIDE words: queue size, -, extend fetch, shadow fetch, then the shadow
+                          // rays of each light class (sun, emitter, sky)
+    unsigned long long* totals;
+    uint32_t shadow_cap;  // the three classes' regions together
+    uint32_t class_base[3], class_cap[3];  // each class's region of so / sd / sp
 };
+// Counter words a depth: [0] paths in the extend queue, [2] extend fetch, [3] shadow fetch, [4 + c] shadow rays of
+// light class c. Shadow rays are queued by class, so a warp of the shadow walk holds rays toward one kind of light
+// (the sun's are nearly parallel).
+constexpr uint32_t CNT_STRIDE = 8u;
+constexpr uint32_t CLASS_SUN = 0u, CLASS_EMIT = 1u, CLASS_ENV = 2u;
 // Cumulative counters: rays, paths, guard trips, and (TRT_RENDER_COUNT) the walks' reads by stage: node records
 // read, triangles tested, unit records entered, for the extend (closest) and the shadow walks.
 enum { T_CLOSEST = 0, T_SHADOW, T_PATHS, T_GUARD, T_E_NODES, T_E_TRIS, T_E_UNITS, T_S_NODES, T_S_TRIS, T_S_UNITS, T_COUNT };
@@ -72,6 +79,16 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool want) {
     uint32_t base = 0;
     if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
     base = __shfl_sync(0xffffffffu, base, leader);
+    return base + (uint32_t)__popc(mask & ((1u << lane) - 1u));
+}
+// The same for lanes in divergent code: the lanes that are here together take consecutive slots.
+__device__ __forceinline__ uint32_t warp_append_active(uint32_t* counter) {
+    unsigned mask = __activemask();
+    int lane = threadIdx.x & 31;
+    int leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
+    base = __shfl_sync(mask, base, leader);
     return base + (uint32_t)__popc(mask & ((1u << lane) - 1u));
 }
 // Persistent-thread work fetch: a warp takes 32 consecutive items.
@@ -155,7 +172,7 @@ __device__ __forceinline__ Hit walk(const Walk& wk, const Sections& X, V3 o, V3 
 template <bool COUNT, bool WIDE>
 __global__ void __launch_bounds__(128) k_extend(Params P, Walk wk, PathBufs B, Queues Q, uint32_t depth) {
     Sections X(P);
-    uint32_t* cnt = Q.cnt + depth * 4u;
+    uint32_t* cnt = Q.cnt + depth * CNT_STRIDE;
     const uint32_t* queue = Q.q[depth & 1u];
     uint32_t n = *(volatile uint32_t*)&cnt[0];
     WalkCount wc{0, 0, 0};
@@ -184,14 +201,20 @@ __global__ void __launch_bounds__(128) k_extend(Params P, Walk wk, PathBufs B, Q
 template <bool COUNT, bool WIDE>
 __global__ void __launch_bounds__(128) k_shadow(Params P, Walk wk, PathBufs B, Queues Q, uint32_t depth) {
     Sections X(P);
-    uint32_t* cnt = Q.cnt + depth * 4u;
-    uint32_t n = min(*(volatile uint32_t*)&cnt[1], Q.shadow_cap);
+    uint32_t* cnt = Q.cnt + depth * CNT_STRIDE;
+    uint32_t n0 = min(*(volatile uint32_t*)&cnt[4], Q.class_cap[0]);
+    uint32_t n1 = min(*(volatile uint32_t*)&cnt[5], Q.class_cap[1]);
+    uint32_t n2 = min(*(volatile uint32_t*)&cnt[6], Q.class_cap[2]);
+    uint32_t n = n0 + n1 + n2;
     WalkCount wc{0, 0, 0};
     unsigned long long guard_trips = 0;
     for (;;) {
-        uint32_t i = warp_fetch(&cnt[3]);
-        if (__shfl_sync(0xffffffffu, i, 0) >= n) break;
-        if (i < n) {
+        uint32_t j = warp_fetch(&cnt[3]);
+        if (__shfl_sync(0xffffffffu, j, 0) >= n) break;
+        if (j < n) {
+            // The classes' regions one after another: the j-th ray of the three.
+            uint32_t i = j < n0 ? Q.class_base[0] + j
+                                : (j < n0 + n1 ? Q.class_base[1] + (j - n0) : Q.class_base[2] + (j - n0 - n1));
             float4 o = Q.so[i], d = Q.sd[i];
             bool guard = false;
             Hit h = walk<COUNT, WIDE>(wk, X, xyz(o), xyz(d), o.w, bu(d.w), &wc, &guard);
@@ -210,10 +233,11 @@ __global__ void __launch_bounds__(128) k_shadow(Params P, Walk wk, PathBufs B, Q
     warp_add64(&Q.totals[T_GUARD], guard_trips);
 }
 
-__device__ __forceinline__ void push_shadow(const Queues& Q, uint32_t* cnt, uint32_t p, uint32_t slot, V3 o, V3 d,
-                                            float tmax, uint32_t mode) {
-    uint32_t at = atomicAdd(&cnt[1], 1u);
-    if (at >= Q.shadow_cap) return;
+__device__ __forceinline__ void push_shadow(const Queues& Q, uint32_t* cnt, uint32_t cls, uint32_t p, uint32_t slot, V3 o,
+                                            V3 d, float tmax, uint32_t mode) {
+    uint32_t at = warp_append_active(&cnt[4 + cls]);
+    if (at >= Q.class_cap[cls]) return;
+    at += Q.class_base[cls];
     Q.so[at] = f4(o, tmax);
     Q.sd[at] = f4(d, bf(mode));
     Q.sp[at] = (p << 3) | slot;
@@ -222,7 +246,7 @@ __device__ __forceinline__ void push_shadow(const Queues& Q, uint32_t* cnt, uint
 // One path vertex: pathtrace.wgsl:4176-4477 from the hit on (the trace itself is k_extend's).
 __global__ void __launch_bounds__(128) k_shade(Params P, DScene S, PathBufs B, Queues Q, uint32_t depth) {
     Sections X(P);
-    uint32_t* cnt = Q.cnt + depth * 4u;
+    uint32_t* cnt = Q.cnt + depth * CNT_STRIDE;
     const uint32_t* queue = Q.q[depth & 1u];
     uint32_t n = cnt[0];
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -299,7 +323,7 @@ __global__ void __launch_bounds__(128) k_shade(Params P, DScene S, PathBufs B, Q
                         float wgt = light_mis(pdf_l, s, lb, v, l);
                         B.nee[li * B.n + p] = f4(color * f * wgt * 1.0f, 0.0f);
                         nee_mask |= 1u << li;
-                        if (tab(S, b + 3).w >= 0.5f) push_shadow(Q, cnt, p, li, oo, l, INF, TRACE_SHADOW);
+                        if (tab(S, b + 3).w >= 0.5f) push_shadow(Q, cnt, CLASS_SUN, p, li, oo, l, INF, TRACE_SHADOW);
                         else vis |= 1u << li;
                     }
                 }
@@ -320,7 +344,7 @@ __global__ void __launch_bounds__(128) k_shade(Params P, DScene S, PathBufs B, Q
                             float wgt = light_mis(es.pdf_w, s, lb, v, es.l) * 1.0f;
                             B.nee[SLOT_EMIT * B.n + p] = f4(es.le * f * wgt * es.w, 0.0f);
                             nee_mask |= 1u << SLOT_EMIT;
-                            push_shadow(Q, cnt, p, SLOT_EMIT, oo, es.l, es.dist * 0.999f, TRACE_ANY);
+                            push_shadow(Q, cnt, CLASS_EMIT, p, SLOT_EMIT, oo, es.l, es.dist * 0.999f, TRACE_ANY);
                         }
                     }
                 }
@@ -333,7 +357,7 @@ __global__ void __launch_bounds__(128) k_shade(Params P, DScene S, PathBufs B, Q
                         if (pdf_e > 0.0f) {
                             B.nee[SLOT_ENV * B.n + p] = f4(env_radiance(S, P, l) * f * light_mis(pdf_e, s, lb, v, l) / pdf_e * 1.0f, 0.0f);
                             nee_mask |= 1u << SLOT_ENV;
-                            push_shadow(Q, cnt, p, SLOT_ENV, oo, l, INF, TRACE_SHADOW);
+                            push_shadow(Q, cnt, CLASS_ENV, p, SLOT_ENV, oo, l, INF, TRACE_SHADOW);
                         }
                     }
                 }
@@ -383,14 +407,14 @@ __global__ void __launch_bounds__(128) k_shade(Params P, DScene S, PathBufs B, Q
         B.thr[p] = f4(thr, bf(pix));
         B.rad[p] = f4(radiance, bf(sample));
     }
-    uint32_t at = warp_append(&Q.cnt[(depth + 1u) * 4u], live);
+    uint32_t at = warp_append(&Q.cnt[(depth + 1u) * CNT_STRIDE], live);
     if (live && depth + 1u < MAX_DEPTH) Q.q[(depth + 1u) & 1u][at] = p;
 }
 
 // The vertex's direct light from its visible slots (pathtrace.wgsl:4398-4403), and a finished path's last fixes
 // (4494-4497).
 __global__ void k_resolve(PathBufs B, Queues Q, uint32_t depth, float clamp_v) {
-    uint32_t n = Q.cnt[depth * 4u];
+    uint32_t n = Q.cnt[depth * CNT_STRIDE];
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     uint32_t p = Q.q[depth & 1u][i];
@@ -446,8 +470,8 @@ __global__ void k_tally(Queues Q, uint32_t depths, uint32_t paths) {
     if (threadIdx.x != 0) return;
     unsigned long long c = 0, s = 0;
     for (uint32_t d = 0; d < depths; ++d) {
-        c += Q.cnt[d * 4u];
-        s += min(Q.cnt[d * 4u + 1], Q.shadow_cap);
+        c += Q.cnt[d * CNT_STRIDE];
+        for (uint32_t k = 0; k < 3; ++k) s += min(Q.cnt[d * CNT_STRIDE + 4 + k], Q.class_cap[k]);
     }
     atomicAdd(&Q.totals[T_CLOSEST], c);
     atomicAdd(&Q.totals[T_SHADOW], s);
@@ -519,13 +543,14 @@ struct trt_scene {
     uint64_t bytes[5] = {0, 0, 0, 0, 0};
     ushort4* env = nullptr;
     uint32_t env_w = 1, env_h = 1;
+    std::vector<uint8_t> host[5];  // host copies of the buffers the wide BVH is built from
     WideBvh wide;
     float4* accum = nullptr;
     uint32_t accum_w = 0, accum_h = 0;
     // work buffers
     void* work = nullptr;
     uint64_t work_bytes = 0;
-    uint32_t slots = 0;
+    uint32_t slots = 0, shadow_alloc = 0;
     PathBufs B{};
     Queues Q{};
     unsigned long long* totals = nullptr;
@@ -588,36 +613,45 @@ int check_params(trt_scene* s, const uint32_t* P) {
     return TRT_OK;
 }
 
-int ensure_work(trt_scene* s, uint32_t slots, uint32_t shadow_slots) {
-    uint32_t shadow_cap = slots * shadow_slots;
-    uint64_t need = 0;
-    auto add = [&](uint64_t b) { uint64_t at = need; need += (b + 255) / 256 * 256; return at; };
-    uint64_t o_o = add(16ull * slots), o_d = add(16ull * slots), o_thr = add(16ull * slots), o_rad = add(16ull * slots),
-             o_alb = add(16ull * slots), o_nrm = add(16ull * slots), o_mx = add(16ull * slots), o_mn = add(16ull * slots),
-             o_nee = add(16ull * slots * N_SLOTS), o_nt = add(16ull * slots), o_vis = add(4ull * slots),
-             o_q0 = add(4ull * slots), o_q1 = add(4ull * slots), o_ha = add(16ull * slots), o_hb = add(8ull * slots),
-             o_so = add(16ull * shadow_cap), o_sd = add(16ull * shadow_cap), o_sp = add(4ull * shadow_cap),
-             o_cnt = add(4ull * (MAX_DEPTH * 4 + 4));
-    if (s->work && s->slots >= slots && s->Q.shadow_cap >= shadow_cap) return TRT_OK;
-    if (s->work) cudaFree(s->work);
-    s->work = nullptr;
-    TRT_CUDA(s->ctx, cudaMalloc(&s->work, need));
-    s->work_bytes = need;
-    char* b = (char*)s->work;
-    s->slots = slots;
-    s->B = PathBufs{(float4*)(b + o_o), (float4*)(b + o_d), (float4*)(b + o_thr), (float4*)(b + o_rad),
-                    (float4*)(b + o_alb), (float4*)(b + o_nrm), (float4*)(b + o_mx), (float4*)(b + o_mn),
-                    (float4*)(b + o_nee), (float4*)(b + o_nt), (uint32_t*)(b + o_vis), slots};
-    s->Q.q[0] = (uint32_t*)(b + o_q0);
-    s->Q.q[1] = (uint32_t*)(b + o_q1);
-    s->Q.hit_a = (float4*)(b + o_ha);
-    s->Q.hit_b = (uint2*)(b + o_hb);
-    s->Q.so = (float4*)(b + o_so);
-    s->Q.sd = (float4*)(b + o_sd);
-    s->Q.sp = (uint32_t*)(b + o_sp);
-    s->Q.cnt = (uint32_t*)(b + o_cnt);
-    s->Q.totals = s->totals;
+int ensure_work(trt_scene* s, uint32_t slots, uint32_t n_dir) {
+    // Shadow-ray regions: a ray a sun a path, one toward an emitter, one toward the sky.
+    uint32_t caps[3] = {slots * std::max(1u, n_dir), slots, slots};
+    uint32_t shadow_cap = caps[0] + caps[1] + caps[2];
+    if (!s->work || s->slots < slots || s->shadow_alloc < shadow_cap) {
+        uint64_t need = 0;
+        auto add = [&](uint64_t b) { uint64_t at = need; need += (b + 255) / 256 * 256; return at; };
+        uint64_t o_o = add(16ull * slots), o_d = add(16ull * slots), o_thr = add(16ull * slots),
+                 o_rad = add(16ull * slots), o_alb = add(16ull * slots), o_nrm = add(16ull * slots),
+                 o_mx = add(16ull * slots), o_mn = add(16ull * slots), o_nee = add(16ull * slots * N_SLOTS),
+                 o_nt = add(16ull * slots), o_vis = add(4ull * slots), o_q0 = add(4ull * slots), o_q1 = add(4ull * slots),
+                 o_ha = add(16ull * slots), o_hb = add(8ull * slots), o_so = add(16ull * shadow_cap),
+                 o_sd = add(16ull * shadow_cap), o_sp = add(4ull * shadow_cap),
+                 o_cnt = add(4ull * (MAX_DEPTH * CNT_STRIDE + CNT_STRIDE));
+        if (s->work) cudaFree(s->work);
+        s->work = nullptr;
+        TRT_CUDA(s->ctx, cudaMalloc(&s->work, need));
+        s->work_bytes = need;
+        char* b = (char*)s->work;
+        s->slots = slots;
+        s->shadow_alloc = shadow_cap;
+        s->B = PathBufs{(float4*)(b + o_o), (float4*)(b + o_d), (float4*)(b + o_thr), (float4*)(b + o_rad),
+                        (float4*)(b + o_alb), (float4*)(b + o_nrm), (float4*)(b + o_mx), (float4*)(b + o_mn),
+                        (float4*)(b + o_nee), (float4*)(b + o_nt), (uint32_t*)(b + o_vis), slots};
+        s->Q.q[0] = (uint32_t*)(b + o_q0);
+        s->Q.q[1] = (uint32_t*)(b + o_q1);
+        s->Q.hit_a = (float4*)(b + o_ha);
+        s->Q.hit_b = (uint2*)(b + o_hb);
+        s->Q.so = (float4*)(b + o_so);
+        s->Q.sd = (float4*)(b + o_sd);
+        s->Q.sp = (uint32_t*)(b + o_sp);
+        s->Q.cnt = (uint32_t*)(b + o_cnt);
+        s->Q.totals = s->totals;
+    }
     s->Q.shadow_cap = shadow_cap;
+    s->Q.class_base[0] = 0;
+    s->Q.class_base[1] = caps[0];
+    s->Q.class_base[2] = caps[0] + caps[1];
+    for (int k = 0; k < 3; ++k) s->Q.class_cap[k] = caps[k];
     return TRT_OK;
 }
 
@@ -648,7 +682,7 @@ int render_waves(trt_scene* s, const Params& P, uint32_t first_sample, uint32_t 
     // Samples a wave: enough paths to fill the GPU (about two million), at most spp.
     uint32_t K = std::max(1u, std::min(spp, (2u << 20) / std::max(1u, n_idx)));
     uint32_t n_dir = P.w[P_COUNTS2];
-    int rc = ensure_work(s, n_idx * K, n_dir + 2u);
+    int rc = ensure_work(s, n_idx * K, n_dir);
     if (rc) return rc;
     DScene S = scene_view(s);
     Walk wk{S, s->wide.view(), P.w[P_MOTION + 2], P.w[P_MOTION + 3]};
@@ -656,7 +690,7 @@ int render_waves(trt_scene* s, const Params& P, uint32_t first_sample, uint32_t 
     const int blk = 128;
     int g_ext = grid_for((const void*)k_extend<COUNT, WIDE>, blk, c->sm_count);
     int g_sha = grid_for((const void*)k_shadow<COUNT, WIDE>, blk, c->sm_count);
-    std::vector<uint32_t> host_cnt(MAX_DEPTH * 4 + 4, 0);
+    std::vector<uint32_t> host_cnt(MAX_DEPTH * CNT_STRIDE + CNT_STRIDE, 0);
     for (uint32_t s0 = 0; s0 < spp; s0 += K) {
         uint32_t k = std::min(K, spp - s0);
         TRT_CUDA(c, cudaMemcpyAsync(s->Q.cnt, host_cnt.data(), host_cnt.size() * 4, cudaMemcpyHostToDevice, st));
@@ -707,9 +741,17 @@ int trt_create(const trt_options* opts, trt_ctx** out) {
     }
     if (e == cudaSuccess) {
         std::lock_guard<std::mutex> lk(g_sobol_mu);
-        uint32_t t[3][16];
+        uint32_t t[3][16], bytes[3][2][256];
         sobol_directions(t);
-        e = cudaMemcpyToSymbol(c_sobol, t, sizeof(t));
+        for (int d = 0; d < 3; ++d)
+            for (int half = 0; half < 2; ++half)
+                for (uint32_t b = 0; b < 256; ++b) {
+                    uint32_t r = 0;
+                    for (int i = 0; i < 8; ++i)
+                        if (b & (0x80u >> i)) r ^= t[d][half * 8 + i];
+                    bytes[d][half][b] = r;
+                }
+        e = cudaMemcpyToSymbol(g_sobol_bytes, bytes, sizeof(bytes));
     }
     if (e == cudaSuccess) e = cudaEventCreate(&c->t0);
     if (e == cudaSuccess) e = cudaEventCreate(&c->t1);
@@ -761,6 +803,7 @@ int trt_scene_upload(trt_ctx* c, const trt_scene_desc* d, trt_scene** out) {
         if (e == cudaSuccess) e = cudaMemcpyAsync(s->buf[k], src[k], n[k], cudaMemcpyHostToDevice, c->stream);
         if (e != cudaSuccess) return cleanup(cuda_fail(c, e, "scene upload"));
         s->bytes[k] = n[k];
+        if (k >= 1 && k <= 3) s->host[k].assign((const uint8_t*)src[k], (const uint8_t*)src[k] + n[k]);
     }
     s->env_w = d->env_w;
     s->env_h = d->env_h;
@@ -771,8 +814,6 @@ int trt_scene_upload(trt_ctx* c, const trt_scene_desc* d, trt_scene** out) {
     if (e == cudaSuccess) e = cudaMemsetAsync(s->totals, 0, sizeof(unsigned long long) * T_COUNT, c->stream);
     if (e != cudaSuccess) return cleanup(cuda_fail(c, e, "scene upload"));
     s->Q.totals = s->totals;
-    int rc = s->wide.build(c, scene_view(s), d, c->stream);
-    if (rc) return cleanup(rc);
     e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return cleanup(cuda_fail(c, e, "scene upload"));
     *out = s;
@@ -802,9 +843,9 @@ int trt_scene_update(trt_scene* s, uint32_t which, uint64_t offset, const void* 
         return fail(c, TRT_EINVAL, "trt_scene_update: the range is not inside the buffer");
     cudaSetDevice(c->device);
     TRT_CUDA(c, cudaMemcpyAsync((char*)s->buf[which] + offset, src, bytes, cudaMemcpyHostToDevice, c->stream));
-    if (which == 1 || which == 2 || which == 3) {
-        int rc = s->wide.refit(c, scene_view(s), c->stream);
-        if (rc) return rc;
+    if (which >= 1 && which <= 3) {
+        std::memcpy(s->host[which].data() + offset, src, bytes);
+        s->wide.invalidate();  // rebuilt from the edited buffers at the next render
     }
     return TRT_OK;
 }
@@ -834,7 +875,8 @@ int trt_render(trt_scene* s, const uint32_t params[TRT_PARAMS_WORDS], uint32_t f
         TRT_CUDA(c, cudaEventRecord(c->t0, c->stream));
     }
     uint64_t launches0 = s->launches;
-    bool count = (flags & TRT_RENDER_COUNT) != 0, binary = (flags & TRT_RENDER_BINARY) != 0 || !s->wide.ready();
+    bool count = (flags & TRT_RENDER_COUNT) != 0, binary = (flags & TRT_RENDER_BINARY) != 0;
+    if (!binary && s->wide.ensure(params, s->host, c->stream) != 0) return fail(c, TRT_EINVAL, s->wide.error);
     if (spp > 0) {
         if (count) rc = binary ? render_waves<true, false>(s, P, first_sample, spp) : render_waves<true, true>(s, P, first_sample, spp);
         else rc = binary ? render_waves<false, false>(s, P, first_sample, spp) : render_waves<false, true>(s, P, first_sample, spp);
@@ -896,10 +938,15 @@ int trt_trace(trt_scene* s, const uint32_t params[TRT_PARAMS_WORDS], const trt_r
     cudaError_t e = cudaMalloc(&dh, sizeof(trt_hit) * n);
     if (e != cudaSuccess) { cudaFree(dr); return cuda_fail(c, e, "trt_trace"); }
     e = cudaMemcpyAsync(dr, rays, sizeof(trt_ray) * n, cudaMemcpyHostToDevice, c->stream);
+    bool binary = (flags & TRT_RENDER_BINARY) != 0;
+    bool count = (flags & TRT_RENDER_COUNT) != 0;
+    if (e == cudaSuccess && !binary && s->wide.ensure(params, s->host, c->stream) != 0) {
+        cudaFree(dr);
+        cudaFree(dh);
+        return fail(c, TRT_EINVAL, s->wide.error);
+    }
     DScene S = scene_view(s);
     Walk wk{S, s->wide.view(), P.w[P_MOTION + 2], P.w[P_MOTION + 3]};
-    bool binary = (flags & TRT_RENDER_BINARY) != 0 || !s->wide.ready();
-    bool count = (flags & TRT_RENDER_COUNT) != 0;
     unsigned grid = (unsigned)((n + 127) / 128);
     if (e == cudaSuccess) {
         if (count) {

@@ -1,36 +1,214 @@
-// The wide BVH: the reference's binary trees collapsed to 8-wide nodes with quantised child boxes (declared here;
-// built in wide_bvh.cu).
+// The wide BVH: the reference's binary trees (the units' top tree and every mesh tree) collapsed into 8-wide nodes
+// whose child boxes are quantised to 8 bits against the node's origin, each node five 16-byte loads. It is built from
+// the uploaded buffers (wide_bvh.cu) and walked by `trace_wide`; the triangle test is the reference's own
+// Moller-Trumbore on the same unit-space ray (pathtrace.wgsl:742-761), so every hit and its t are the reference's.
+//
+// Node (80 bytes):
+//   [0, 12)  origin xyz (f32)                     [12, 15) exponent byte a axis (the scale 2^(e - 127))
+//   [15]     interior mask: bit i, slot i is a wide node
+//   [16, 20) first interior child's node index   [20, 24) first leaf item of the node
+//   [24, 32) items of each leaf slot (0: interior or empty): a leaf slot's items follow the lower slots' in order
+//   [32, 80) q_lo x[8], q_lo y[8], q_lo z[8], q_hi x[8], q_hi y[8], q_hi z[8]: slot i's box is
+//            origin + q * scale, widened by a step on every side; an empty slot has q_lo > q_hi.
+// Leaf items: in a mesh tree, triangles (a copy of the reference's leaf record, three vec4s, with the reference's
+// triangle index in the third's w); in the top tree, unit records (bit 31: the unit casts shadows).
 #pragma once
-#include "traverse.cuh"
+#include <string>
+#include <vector>
 
-struct trt_ctx;
-struct trt_scene_desc_s;
+#include "traverse.cuh"
 
 namespace trt {
 
 struct WideView {
-    const uint4* nodes;   // 5 uint4s a node
-    uint32_t top_root;    // the top tree's root node
-    uint32_t valid;
+    const uint4* nodes;        // 5 uint4 a node
+    const float4* tris;        // 3 float4 a triangle: (v0, section), (e1, rank), (e2, reference index)
+    const uint32_t* units;     // the top tree's leaf items: unit record | shadow bit << 31
+    const uint32_t* unit_root; // a unit record's mesh tree root (wide node index)
+    uint32_t top_root;         // the top tree's root (wide node index)
+    uint32_t n_nodes, n_tris, n_units, n_records;
 };
+
+constexpr uint32_t WIDE_UNIT_BIT = 0x80000000u;
+constexpr int WIDE_STACK = 64;
 
 struct WideBvh {
     uint4* nodes = nullptr;
-    uint64_t n_nodes = 0;
-    uint32_t top_root = 0;
+    float4* tris = nullptr;
+    uint32_t* units = nullptr;
+    uint32_t* unit_root = nullptr;
+    WideView v{};
     bool built = false;
+    uint32_t key[6] = {0, 0, 0, 0, 0, 0};  // the Params words the build read (it is redone when they change)
+    double build_ms = 0.0;
     bool ready() const { return built; }
-    WideView view() const { return WideView{nodes, top_root, built ? 1u : 0u}; }
-    int build(trt_ctx*, const DScene&, const void*, cudaStream_t) { built = false; return 0; }
-    int refit(trt_ctx*, const DScene&, cudaStream_t) { return 0; }
-    void release() {}
+    WideView view() const { return v; }
+    std::string error;
+    // Builds (or keeps) the wide trees for the scene as `params` lays it out, from host copies of the scene's nodes,
+    // leaves and tables (host[2], host[1], host[3]). 0, or 1 with `error` set.
+    int ensure(const uint32_t* params, const std::vector<uint8_t>* host, cudaStream_t st);
+    void release();
+    void invalidate() { built = false; }
 };
 
+__device__ __forceinline__ float byte_f(uint32_t w, int k) { return (float)((w >> (8 * k)) & 0xffu); }
+
+struct WideRay {
+    V3 o, d, inv;
+};
+
+// The eight child boxes of node `nd` against the ray: each slot's entry t (INF: missed, or past tmax).
+__device__ __forceinline__ void wide_children(const uint4 nd[5], const WideRay& r, float tmax, float tn[8]) {
+    float ox = bf(nd[0].x), oy = bf(nd[0].y), oz = bf(nd[0].z);
+    uint32_t eb = nd[0].w;
+    float sx = bf((eb & 0xffu) << 23) * r.inv.x, sy = bf(((eb >> 8) & 0xffu) << 23) * r.inv.y,
+          sz = bf(((eb >> 16) & 0xffu) << 23) * r.inv.z;
+    float bx = (ox - r.o.x) * r.inv.x, by = (oy - r.o.y) * r.inv.y, bz = (oz - r.o.z) * r.inv.z;
+    const uint32_t lox[2] = {nd[2].x, nd[2].y}, loy[2] = {nd[2].z, nd[2].w}, loz[2] = {nd[3].x, nd[3].y};
+    const uint32_t hix[2] = {nd[3].z, nd[3].w}, hiy[2] = {nd[4].x, nd[4].y}, hiz[2] = {nd[4].z, nd[4].w};
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        int h = i >> 2, k = i & 3;
+        float x0 = fmaf(byte_f(lox[h], k), sx, bx), x1 = fmaf(byte_f(hix[h], k), sx, bx);
+        float y0 = fmaf(byte_f(loy[h], k), sy, by), y1 = fmaf(byte_f(hiy[h], k), sy, by);
+        float z0 = fmaf(byte_f(loz[h], k), sz, bz), z1 = fmaf(byte_f(hiz[h], k), sz, bz);
+        float tnear = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), 0.0f));
+        float tfar = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), tmax));
+        // (An empty slot's q_lo > q_hi gives an empty interval on every axis whatever the ray's signs.)
+        bool empty = ((lox[h] >> (8 * k)) & 0xffu) > ((hix[h] >> (8 * k)) & 0xffu);
+        tn[i] = (tnear <= tfar && !empty) ? tnear : INF;
+    }
+}
+
+// The walk over both levels: the top tree's hit leaves are units, entered (the ray in the unit's space, as
+// trace_units.wgsl:86-105) when popped; a unit's walk ends when the stack is back to where it was entered. Entries
+// carry the t they were hit at and are skipped once a closer hit is known.
 template <bool COUNT>
-__device__ __forceinline__ Hit trace_wide(const DScene& S, const WideView& W, const Sections& X, V3 o, V3 d, float tmax,
-                                          uint32_t mode, WalkCount* wc, bool* guard) {
-    (void)W;
-    return trace_binary<COUNT>(S, X, 0u, 0u, o, d, tmax, mode, wc, guard);
+__device__ Hit trace_wide(const DScene& S, const WideView& W, const Sections& X, V3 o, V3 d, float tmax, uint32_t mode,
+                          WalkCount* wc, bool* guard) {
+    Hit hit{tmax, MISS, 0.0f, 0.0f, NO_INST, 0u};
+    if (W.n_units == 0) return hit;
+    V3 inv_d = safe_inv(d);
+    WideRay r{o, d, inv_d};
+    uint32_t stack_ref[WIDE_STACK];
+    float stack_t[WIDE_STACK];
+    int sp = 0;
+    uint32_t cur = W.top_root;  // the node to open next (NO_INST: pop)
+    uint32_t rec = NO_INST;
+    int base = 0;
+    for (uint32_t iter = 0;; ++iter) {
+        if (iter >= WALK_GUARD) { *guard = true; break; }
+        if (cur != NO_INST) {
+            if (cur >= W.n_nodes) { *guard = true; break; }
+            const uint4* np = W.nodes + 5ull * cur;
+            uint4 nd[5];
+#pragma unroll
+            for (int k = 0; k < 5; ++k) nd[k] = __ldg(np + k);
+            if (COUNT) wc->nodes++;
+            float tn[8];
+            wide_children(nd, r, hit.t, tn);
+            uint32_t imask = nd[0].w >> 24;
+            uint32_t child_base = nd[1].x, leaf_base = nd[1].y;
+            uint64_t counts = ((uint64_t)nd[1].w << 32) | nd[1].z;
+            uint64_t prefix = counts * 0x0101010101010101ull;  // byte i: the items of slots 0..i
+            int sp0 = sp;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                if (tn[i] == INF) continue;
+                if (imask & (1u << i)) {
+                    if (sp < WIDE_STACK) {
+                        stack_ref[sp] = child_base + (uint32_t)__popc(imask & ((1u << i) - 1u));
+                        stack_t[sp] = tn[i];
+                        sp++;
+                    }
+                    continue;
+                }
+                uint32_t cnt = (uint32_t)(counts >> (8 * i)) & 0xffu;
+                uint32_t off = (uint32_t)(prefix >> (8 * i)) & 0xffu;
+                uint32_t item = leaf_base + off - cnt;
+                if (rec == NO_INST) {
+                    // Top-tree leaves: units, entered in the order of their t.
+                    for (uint32_t k = 0; k < cnt; ++k) {
+                        if (item + k >= W.n_units) { *guard = true; return hit; }
+                        uint32_t u = __ldg(W.units + item + k);
+                        if (mode == TRACE_SHADOW && !(u & WIDE_UNIT_BIT)) continue;
+                        if (sp < WIDE_STACK) { stack_ref[sp] = u | WIDE_UNIT_BIT; stack_t[sp] = tn[i]; sp++; }
+                    }
+                    if (COUNT) wc->units += cnt;
+                } else {
+                    for (uint32_t k = 0; k < cnt; ++k) {
+                        uint32_t ti = item + k;
+                        if (ti >= W.n_tris) { *guard = true; return hit; }
+                        const float4* tp = W.tris + 3ull * ti;
+                        float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+                        if (COUNT) wc->tris++;
+                        // pathtrace.wgsl:742-761 intersect_tri, on the copy of the reference's leaf record.
+                        V3 v0 = xyz(a), e1 = xyz(b), e2 = xyz(c);
+                        V3 pv = cross(r.d, e2);
+                        float det = dot(e1, pv);
+                        if (fabsf(det) < 1e-12f) continue;
+                        float inv = 1.0f / det;
+                        V3 tv = r.o - v0;
+                        float u = dot(tv, pv) * inv;
+                        if (u < 0.0f || u > 1.0f) continue;
+                        V3 qv = cross(tv, e1);
+                        float v = dot(r.d, qv) * inv;
+                        if (v < 0.0f || u + v > 1.0f) continue;
+                        float t = dot(e2, qv) * inv;
+                        if (t <= 0.0f || t >= hit.t) continue;
+                        hit = Hit{t, bu(c.w), u, v, rec, bu(a.w)};
+                        if (mode != TRACE_CLOSEST) return hit;
+                    }
+                }
+            }
+            // This node's entries, the nearest last (on top).
+            for (int x = sp0 + 1; x < sp; ++x) {
+                uint32_t er = stack_ref[x];
+                float et = stack_t[x];
+                int y = x - 1;
+                while (y >= sp0 && stack_t[y] < et) {
+                    stack_ref[y + 1] = stack_ref[y];
+                    stack_t[y + 1] = stack_t[y];
+                    --y;
+                }
+                stack_ref[y + 1] = er;
+                stack_t[y + 1] = et;
+            }
+        }
+        // Pop: the nearest pending entry still in front of the closest hit.
+        for (;;) {
+            if (rec != NO_INST && sp == base) {
+                rec = NO_INST;
+                r = WideRay{o, d, inv_d};
+            }
+            if (sp == 0) return hit;
+            --sp;
+            if (stack_t[sp] < hit.t) break;
+        }
+        uint32_t e = stack_ref[sp];
+        if (e & WIDE_UNIT_BIT) {
+            uint32_t u = e & ~WIDE_UNIT_BIT;
+            uint32_t b = X.t_instances + u * 10u;
+            if (u >= W.n_records || (uint64_t)b + 10u > S.n_table_vec4) { *guard = true; break; }
+            float4 m0 = tab(S, b), m1 = tab(S, b + 1), m2 = tab(S, b + 2);
+            float4 n0 = tab(S, b + 3), n1 = tab(S, b + 4), n2 = tab(S, b + 5);
+            rec = u;
+            V3 ro = o - V3{m0.w, m1.w, m2.w};
+            V3 rd = d;
+            V3 rinv = inv_d;
+            if ((bu(n1.w) & UNIT_SHIFTED) == 0) {
+                ro = proc_dir(n0, n1, n2, ro);
+                rd = proc_dir(n0, n1, n2, d);
+                rinv = safe_inv(rd);
+            }
+            r = WideRay{ro, rd, rinv};
+            base = sp;
+            cur = __ldg(W.unit_root + u);
+        } else {
+            cur = e;
+        }
+    }
+    return hit;
 }
 
 }  // namespace trt
