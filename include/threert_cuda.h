@@ -82,6 +82,7 @@ typedef struct { float t; uint32_t tri; float u; float v; uint32_t inst; uint32_
 #define TRT_RENDER_BINARY     4u /* walk the reference's binary trees instead of the wide BVH */
 
 int trt_create(const trt_options* opts, trt_ctx** out);
+/* Frees the context and every scene still uploaded through it (their handles are then invalid). */
 void trt_destroy(trt_ctx* ctx);
 const char* trt_last_error(const trt_ctx* ctx);
 /* The library's version and the device it runs on (name, SM count). */

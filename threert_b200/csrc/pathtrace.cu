@@ -18,6 +18,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -531,6 +532,7 @@ using namespace trt;
 struct trt_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
+    std::vector<trt_scene*> scenes;  // live scenes, freed by trt_destroy
     int sm_count = 0;
     char name[256] = {0};
     std::string err;
@@ -769,6 +771,7 @@ int trt_create(const trt_options* opts, trt_ctx** out) {
 void trt_destroy(trt_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
+    while (!c->scenes.empty()) trt_scene_free(c->scenes.back());
     if (c->t0) cudaEventDestroy(c->t0);
     if (c->t1) cudaEventDestroy(c->t1);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -816,12 +819,15 @@ int trt_scene_upload(trt_ctx* c, const trt_scene_desc* d, trt_scene** out) {
     s->Q.totals = s->totals;
     e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return cleanup(cuda_fail(c, e, "scene upload"));
+    c->scenes.push_back(s);
     *out = s;
     return TRT_OK;
 }
 
 void trt_scene_free(trt_scene* s) {
     if (!s) return;
+    auto& live = s->ctx->scenes;
+    live.erase(std::remove(live.begin(), live.end(), s), live.end());
     cudaSetDevice(s->ctx->device);
     cudaStreamSynchronize(s->ctx->stream);
     for (void* b : s->buf)

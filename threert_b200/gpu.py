@@ -66,9 +66,10 @@ class Scene:
         gpu._check(L.trt_scene_upload(gpu.ctx, C.byref(d), C.byref(self.handle)), "trt_scene_upload")
 
     def close(self):
-        if self.handle:
+        # (A closed Gpu has freed its scenes with its context.)
+        if self.handle and self.gpu.ctx:
             N.lib().trt_scene_free(self.handle)
-            self.handle = C.c_void_p()
+        self.handle = C.c_void_p()
 
     def __del__(self):
         try:
@@ -140,12 +141,17 @@ class Gpu:
                first_sample: int = 0, flags: int = 0) -> Frame:
         """gpu.rs:4116 Gpu::render: upload (unless given a resident Scene), `spp` samples, readback, Frame."""
         t0 = time.perf_counter()
-        scene = prepared if isinstance(prepared, Scene) else self.upload(prepared)
-        if timings is not None and not isinstance(prepared, Scene):
-            timings.append(("upload_ms", (time.perf_counter() - t0) * 1e3))
-        acc, st = scene.render_raw(base, spp, first_sample=first_sample, flags=flags)
-        if timings is not None:
-            timings.append(("trace_ms", float(st.device_ms)))
+        resident = isinstance(prepared, Scene)
+        scene = prepared if resident else self.upload(prepared)
+        try:
+            if timings is not None and not resident:
+                timings.append(("upload_ms", (time.perf_counter() - t0) * 1e3))
+            acc, st = scene.render_raw(base, spp, first_sample=first_sample, flags=flags)
+            if timings is not None:
+                timings.append(("trace_ms", float(st.device_ms)))
+        finally:
+            if not resident:
+                scene.close()
         w, h = int(base[16]), int(base[17])
         return frame_of(acc, w, h, spp)
 
@@ -162,5 +168,5 @@ class Gpu:
 
     def close(self):
         if self.ctx:
-            N.lib().trt_destroy(self.ctx)
+            N.lib().trt_destroy(self.ctx)  # frees the scenes still uploaded through it
             self.ctx = C.c_void_p()
