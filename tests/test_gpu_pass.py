@@ -58,7 +58,7 @@ def test_render_matches_the_oracle(gpu, make, spp):
     w, h = P.width, P.height
     acc_g = gpu.upload(P).render_raw(P.params, spp)[0]
     acc_o, st = oracle.Oracle(P).render(P.params, spp)
-    assert st["tri_tests"] > w * h and st["shadow_rays"] > w * h  # the camera sees the scene
+    assert st["tri_tests"] > w * h and st["shadow_rays"] > w * h // 4  # the camera sees the scene
     frac, mean_err = image_parity(acc_g, acc_o, w, h, spp)
     assert frac >= 0.99, frac
     assert mean_err <= 0.01, mean_err

@@ -35,7 +35,7 @@ struct Builder {
 
     // Quantises the child boxes of one wide node (wide_bvh.cuh's layout) and writes its header.
     void encode(WNode& W, const std::vector<const BinNode*>& ch, const std::vector<bool>& interior, uint32_t child_base,
-                uint32_t leaf_base, const std::vector<uint32_t>& counts) {
+                uint32_t leaf_base, const std::vector<uint32_t>& counts, float tree_pad) {
         std::memset(&W, 0, sizeof(W));
         float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
         for (const BinNode* c : ch)
@@ -47,7 +47,7 @@ struct Builder {
             float mag = std::max(std::fabs(lo[k]), std::fabs(hi[k]));
             // A step's margin on every side is added per child; this pad keeps the widened boxes inside 0..255 and
             // gives flat boxes a width of some 2^-16 of their coordinates.
-            float pad = ext * (1.0f / 253.0f) + mag * (1.0f / 65536.0f) + 1e-20f;
+            float pad = ext * (1.0f / 253.0f) + mag * (1.0f / 65536.0f) + tree_pad + 1e-20f;
             origin[k] = lo[k] - pad;
             float range = (hi[k] + pad) - origin[k];
             int e;
@@ -87,6 +87,17 @@ struct Builder {
     template <class Leaf>
     uint32_t collapse(uint32_t root, Leaf&& leaf, uint32_t max_leaf_items) {
         if (root >= n_nodes) { error = "a tree's root is past the nodes"; return UINT32_MAX; }
+        // A slab test rounds with the distance to the box: a box far from the ray's origin but small (a few
+        // millimetres of a 10 m mesh seen from 1 km) needs more margin than its own size gives, so every box of a
+        // tree is widened by at least 2^-14 of the tree's extent.
+        float tree_pad;
+        {
+            const BinNode& r0 = nodes[root];
+            float ext = 0.0f;
+            for (int k = 0; k < 3; ++k) ext = std::max(ext, r0.bmax[k] - r0.bmin[k]);
+            tree_pad = std::isfinite(ext) ? ext * (1.0f / 16384.0f) : 0.0f;
+        }
+        const float pad_of_tree = tree_pad;  // (a nested collapse of a unit's mesh tree has its own)
         uint32_t wroot = (uint32_t)out.size();
         out.emplace_back();
         std::vector<std::pair<uint32_t, uint32_t>> work{{root, wroot}};
@@ -144,7 +155,7 @@ struct Builder {
                 }
             }
             if (leaf_base == UINT32_MAX) leaf_base = 0;
-            encode(out[w], cp, interior, child_base, leaf_base, counts);
+            encode(out[w], cp, interior, child_base, leaf_base, counts, pad_of_tree);
 
         }
         return wroot;

@@ -51,33 +51,64 @@ struct WideBvh {
     void invalidate() { built = false; }
 };
 
-__device__ __forceinline__ float byte_f(uint32_t w, int k) { return (float)((w >> (8 * k)) & 0xffu); }
-
 struct WideRay {
     V3 o, d, inv;
+    uint32_t neg;  // bit k: the direction's axis k is negative (its near planes are the boxes' high sides)
 };
+__device__ __forceinline__ WideRay wide_ray(V3 o, V3 d, V3 inv) {
+    return WideRay{o, d, inv, (inv.x < 0.0f ? 1u : 0u) | (inv.y < 0.0f ? 2u : 0u) | (inv.z < 0.0f ? 4u : 0u)};
+}
+
+// Byte k of w as the float 1 + q / 256, exactly: q in the mantissa's top eight bits.
+__device__ __forceinline__ float q_float(uint32_t w, int k) {
+    uint32_t m = k >= 2 ? (w >> (8 * k - 15)) : (w << (15 - 8 * k));
+    return bf((m & 0x007f8000u) | 0x3f800000u);
+}
 
 // The eight child boxes of node `nd` against the ray: each slot's entry t (INF: missed, or past tmax).
+// A slot's plane at q steps is origin + q 2^e = (origin - 2^(e+8)) + (1 + q/256) 2^(e+8): one FMA of the bit-built
+// float. The near and far planes of each axis are picked once by the ray's signs; an empty slot (q_lo > q_hi) has
+// its near plane past its far one on every axis, so it misses whatever the signs.
 __device__ __forceinline__ void wide_children(const uint4 nd[5], const WideRay& r, float tmax, float tn[8]) {
-    float ox = bf(nd[0].x), oy = bf(nd[0].y), oz = bf(nd[0].z);
     uint32_t eb = nd[0].w;
-    float sx = bf((eb & 0xffu) << 23) * r.inv.x, sy = bf(((eb >> 8) & 0xffu) << 23) * r.inv.y,
-          sz = bf(((eb >> 16) & 0xffu) << 23) * r.inv.z;
-    float bx = (ox - r.o.x) * r.inv.x, by = (oy - r.o.y) * r.inv.y, bz = (oz - r.o.z) * r.inv.z;
-    const uint32_t lox[2] = {nd[2].x, nd[2].y}, loy[2] = {nd[2].z, nd[2].w}, loz[2] = {nd[3].x, nd[3].y};
-    const uint32_t hix[2] = {nd[3].z, nd[3].w}, hiy[2] = {nd[4].x, nd[4].y}, hiz[2] = {nd[4].z, nd[4].w};
+    float s8x = bf(((eb & 0xffu) + 8u) << 23), s8y = bf((((eb >> 8) & 0xffu) + 8u) << 23),
+          s8z = bf((((eb >> 16) & 0xffu) + 8u) << 23);
+    float Sx = s8x * r.inv.x, Sy = s8y * r.inv.y, Sz = s8z * r.inv.z;
+    float Bx = ((bf(nd[0].x) - r.o.x) - s8x) * r.inv.x, By = ((bf(nd[0].y) - r.o.y) - s8y) * r.inv.y,
+          Bz = ((bf(nd[0].z) - r.o.z) - s8z) * r.inv.z;
+    // q_lo x: nd[2].x,y; y: nd[2].z,w; z: nd[3].x,y. q_hi x: nd[3].z,w; y: nd[4].x,y; z: nd[4].z,w.
+    bool nx = r.neg & 1u, ny = r.neg & 2u, nz = r.neg & 4u;
+    uint32_t nearx[2] = {nx ? nd[3].z : nd[2].x, nx ? nd[3].w : nd[2].y};
+    uint32_t farx[2] = {nx ? nd[2].x : nd[3].z, nx ? nd[2].y : nd[3].w};
+    uint32_t neary[2] = {ny ? nd[4].x : nd[2].z, ny ? nd[4].y : nd[2].w};
+    uint32_t fary[2] = {ny ? nd[2].z : nd[4].x, ny ? nd[2].w : nd[4].y};
+    uint32_t nearz[2] = {nz ? nd[4].z : nd[3].x, nz ? nd[4].w : nd[3].y};
+    uint32_t farz[2] = {nz ? nd[3].x : nd[4].z, nz ? nd[3].y : nd[4].w};
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
         int h = i >> 2, k = i & 3;
-        float x0 = fmaf(byte_f(lox[h], k), sx, bx), x1 = fmaf(byte_f(hix[h], k), sx, bx);
-        float y0 = fmaf(byte_f(loy[h], k), sy, by), y1 = fmaf(byte_f(hiy[h], k), sy, by);
-        float z0 = fmaf(byte_f(loz[h], k), sz, bz), z1 = fmaf(byte_f(hiz[h], k), sz, bz);
-        float tnear = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), 0.0f));
-        float tfar = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), tmax));
-        // (An empty slot's q_lo > q_hi gives an empty interval on every axis whatever the ray's signs.)
-        bool empty = ((lox[h] >> (8 * k)) & 0xffu) > ((hix[h] >> (8 * k)) & 0xffu);
-        tn[i] = (tnear <= tfar && !empty) ? tnear : INF;
+        float x0 = fmaf(q_float(nearx[h], k), Sx, Bx), x1 = fmaf(q_float(farx[h], k), Sx, Bx);
+        float y0 = fmaf(q_float(neary[h], k), Sy, By), y1 = fmaf(q_float(fary[h], k), Sy, By);
+        float z0 = fmaf(q_float(nearz[h], k), Sz, Bz), z1 = fmaf(q_float(farz[h], k), Sz, Bz);
+        float tnear = fmaxf(fmaxf(x0, y0), fmaxf(z0, 0.0f));
+        float tfar = fminf(fminf(x1, y1), fminf(z1, tmax));
+        tn[i] = tnear <= tfar ? tnear : INF;
     }
+}
+
+// Ascending sort of eight keys (a sorting network of 19 compare-exchanges).
+__device__ __forceinline__ void cas(uint32_t& a, uint32_t& b) {
+    uint32_t lo = min(a, b), hi = max(a, b);
+    a = lo;
+    b = hi;
+}
+__device__ __forceinline__ void sort8(uint32_t k[8]) {
+    cas(k[0], k[2]); cas(k[1], k[3]); cas(k[4], k[6]); cas(k[5], k[7]);
+    cas(k[0], k[4]); cas(k[1], k[5]); cas(k[2], k[6]); cas(k[3], k[7]);
+    cas(k[0], k[1]); cas(k[2], k[3]); cas(k[4], k[5]); cas(k[6], k[7]);
+    cas(k[2], k[4]); cas(k[3], k[5]);
+    cas(k[1], k[4]); cas(k[3], k[6]);
+    cas(k[1], k[2]); cas(k[3], k[4]); cas(k[5], k[6]);
 }
 
 // The walk over both levels: the top tree's hit leaves are units, entered (the ray in the unit's space, as
@@ -89,7 +120,7 @@ __device__ Hit trace_wide(const DScene& S, const WideView& W, const Sections& X,
     Hit hit{tmax, MISS, 0.0f, 0.0f, NO_INST, 0u};
     if (W.n_units == 0) return hit;
     V3 inv_d = safe_inv(d);
-    WideRay r{o, d, inv_d};
+    WideRay r = wide_ray(o, d, inv_d);
     uint32_t stack_ref[WIDE_STACK];
     float stack_t[WIDE_STACK];
     int sp = 0;
@@ -111,75 +142,74 @@ __device__ Hit trace_wide(const DScene& S, const WideView& W, const Sections& X,
             uint32_t child_base = nd[1].x, leaf_base = nd[1].y;
             uint64_t counts = ((uint64_t)nd[1].w << 32) | nd[1].z;
             uint64_t prefix = counts * 0x0101010101010101ull;  // byte i: the items of slots 0..i
-            int sp0 = sp;
+            // The hit slots by their entry t (t >= 0, so its bits order as the floats), the slot in the low bits.
+            uint32_t key[8];
 #pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                if (tn[i] == INF) continue;
-                if (imask & (1u << i)) {
-                    if (sp < WIDE_STACK) {
-                        stack_ref[sp] = child_base + (uint32_t)__popc(imask & ((1u << i) - 1u));
-                        stack_t[sp] = tn[i];
-                        sp++;
-                    }
-                    continue;
-                }
+            for (int i = 0; i < 8; ++i) key[i] = tn[i] == INF ? 0xffffffffu : ((bu(tn[i]) & ~7u) | (uint32_t)i);
+            sort8(key);
+            // Leaves first, nearest first: their hits cull the farther entries. Then the other entries, farthest
+            // first, so the nearest is on top.
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                if (key[j] == 0xffffffffu) break;
+                uint32_t i = key[j] & 7u;
+                if (imask & (1u << i)) continue;
+                if (bf(key[j] & ~7u) >= hit.t) break;
                 uint32_t cnt = (uint32_t)(counts >> (8 * i)) & 0xffu;
-                uint32_t off = (uint32_t)(prefix >> (8 * i)) & 0xffu;
-                uint32_t item = leaf_base + off - cnt;
+                uint32_t item = leaf_base + ((uint32_t)(prefix >> (8 * i)) & 0xffu) - cnt;
                 if (rec == NO_INST) {
-                    // Top-tree leaves: units, entered in the order of their t.
+                    if (COUNT) wc->units += cnt;
+                    continue;  // units are entries, pushed below
+                }
+                for (uint32_t k = 0; k < cnt; ++k) {
+                    uint32_t ti = item + k;
+                    if (ti >= W.n_tris) { *guard = true; return hit; }
+                    const float4* tp = W.tris + 3ull * ti;
+                    float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+                    if (COUNT) wc->tris++;
+                    // pathtrace.wgsl:742-761 intersect_tri, on the copy of the reference's leaf record.
+                    V3 v0 = xyz(a), e1 = xyz(b), e2 = xyz(c);
+                    V3 pv = cross(r.d, e2);
+                    float det = dot(e1, pv);
+                    if (fabsf(det) < 1e-12f) continue;
+                    float inv = 1.0f / det;
+                    V3 tv = r.o - v0;
+                    float u = dot(tv, pv) * inv;
+                    if (u < 0.0f || u > 1.0f) continue;
+                    V3 qv = cross(tv, e1);
+                    float v = dot(r.d, qv) * inv;
+                    if (v < 0.0f || u + v > 1.0f) continue;
+                    float t = dot(e2, qv) * inv;
+                    if (t <= 0.0f || t >= hit.t) continue;
+                    hit = Hit{t, bu(c.w), u, v, rec, bu(a.w)};
+                    if (mode != TRACE_CLOSEST) return hit;
+                }
+            }
+#pragma unroll
+            for (int j = 7; j >= 0; --j) {
+                if (key[j] == 0xffffffffu) continue;
+                float t = bf(key[j] & ~7u);
+                if (t >= hit.t) continue;
+                uint32_t i = key[j] & 7u;
+                if (imask & (1u << i)) {
+                    if (sp < WIDE_STACK) { stack_ref[sp] = child_base + (uint32_t)__popc(imask & ((1u << i) - 1u)); stack_t[sp] = t; sp++; }
+                } else if (rec == NO_INST) {
+                    uint32_t cnt = (uint32_t)(counts >> (8 * i)) & 0xffu;
+                    uint32_t item = leaf_base + ((uint32_t)(prefix >> (8 * i)) & 0xffu) - cnt;
                     for (uint32_t k = 0; k < cnt; ++k) {
                         if (item + k >= W.n_units) { *guard = true; return hit; }
                         uint32_t u = __ldg(W.units + item + k);
                         if (mode == TRACE_SHADOW && !(u & WIDE_UNIT_BIT)) continue;
-                        if (sp < WIDE_STACK) { stack_ref[sp] = u | WIDE_UNIT_BIT; stack_t[sp] = tn[i]; sp++; }
-                    }
-                    if (COUNT) wc->units += cnt;
-                } else {
-                    for (uint32_t k = 0; k < cnt; ++k) {
-                        uint32_t ti = item + k;
-                        if (ti >= W.n_tris) { *guard = true; return hit; }
-                        const float4* tp = W.tris + 3ull * ti;
-                        float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
-                        if (COUNT) wc->tris++;
-                        // pathtrace.wgsl:742-761 intersect_tri, on the copy of the reference's leaf record.
-                        V3 v0 = xyz(a), e1 = xyz(b), e2 = xyz(c);
-                        V3 pv = cross(r.d, e2);
-                        float det = dot(e1, pv);
-                        if (fabsf(det) < 1e-12f) continue;
-                        float inv = 1.0f / det;
-                        V3 tv = r.o - v0;
-                        float u = dot(tv, pv) * inv;
-                        if (u < 0.0f || u > 1.0f) continue;
-                        V3 qv = cross(tv, e1);
-                        float v = dot(r.d, qv) * inv;
-                        if (v < 0.0f || u + v > 1.0f) continue;
-                        float t = dot(e2, qv) * inv;
-                        if (t <= 0.0f || t >= hit.t) continue;
-                        hit = Hit{t, bu(c.w), u, v, rec, bu(a.w)};
-                        if (mode != TRACE_CLOSEST) return hit;
+                        if (sp < WIDE_STACK) { stack_ref[sp] = u | WIDE_UNIT_BIT; stack_t[sp] = t; sp++; }
                     }
                 }
-            }
-            // This node's entries, the nearest last (on top).
-            for (int x = sp0 + 1; x < sp; ++x) {
-                uint32_t er = stack_ref[x];
-                float et = stack_t[x];
-                int y = x - 1;
-                while (y >= sp0 && stack_t[y] < et) {
-                    stack_ref[y + 1] = stack_ref[y];
-                    stack_t[y + 1] = stack_t[y];
-                    --y;
-                }
-                stack_ref[y + 1] = er;
-                stack_t[y + 1] = et;
             }
         }
         // Pop: the nearest pending entry still in front of the closest hit.
         for (;;) {
             if (rec != NO_INST && sp == base) {
                 rec = NO_INST;
-                r = WideRay{o, d, inv_d};
+                r = wide_ray(o, d, inv_d);
             }
             if (sp == 0) return hit;
             --sp;
@@ -201,7 +231,7 @@ __device__ Hit trace_wide(const DScene& S, const WideView& W, const Sections& X,
                 rd = proc_dir(n0, n1, n2, d);
                 rinv = safe_inv(rd);
             }
-            r = WideRay{ro, rd, rinv};
+            r = wide_ray(ro, rd, rinv);
             base = sp;
             cur = __ldg(W.unit_root + u);
         } else {
