@@ -171,7 +171,7 @@ __device__ __forceinline__ Hit walk(const Walk& wk, const Sections& X, V3 o, V3 
 }
 
 template <bool COUNT, bool WIDE>
-__global__ void __launch_bounds__(128) k_extend(Params P, Walk wk, PathBufs B, Queues Q, uint32_t depth) {
+__global__ void __launch_bounds__(128, 6) k_extend(Params P, Walk wk, PathBufs B, Queues Q, uint32_t depth) {
     Sections X(P);
     uint32_t* cnt = Q.cnt + depth * CNT_STRIDE;
     const uint32_t* queue = Q.q[depth & 1u];
@@ -200,7 +200,7 @@ __global__ void __launch_bounds__(128) k_extend(Params P, Walk wk, PathBufs B, Q
 }
 
 template <bool COUNT, bool WIDE>
-__global__ void __launch_bounds__(128) k_shadow(Params P, Walk wk, PathBufs B, Queues Q, uint32_t depth) {
+__global__ void __launch_bounds__(128, 6) k_shadow(Params P, Walk wk, PathBufs B, Queues Q, uint32_t depth) {
     Sections X(P);
     uint32_t* cnt = Q.cnt + depth * CNT_STRIDE;
     uint32_t n0 = min(*(volatile uint32_t*)&cnt[4], Q.class_cap[0]);
@@ -245,7 +245,7 @@ __device__ __forceinline__ void push_shadow(const Queues& Q, uint32_t* cnt, uint
 }
 
 // One path vertex: pathtrace.wgsl:4176-4477 from the hit on (the trace itself is k_extend's).
-__global__ void __launch_bounds__(128) k_shade(Params P, DScene S, PathBufs B, Queues Q, uint32_t depth) {
+__global__ void __launch_bounds__(128, 4) k_shade(Params P, DScene S, PathBufs B, Queues Q, uint32_t depth) {
     Sections X(P);
     uint32_t* cnt = Q.cnt + depth * CNT_STRIDE;
     const uint32_t* queue = Q.q[depth & 1u];
@@ -332,13 +332,16 @@ __global__ void __launch_bounds__(128) k_shade(Params P, DScene S, PathBufs B, Q
                 B.mis_x[p] = f4(oo, 0.0f);
                 B.mis_n[p] = f4(ne, 0.0f);
                 if (emitters_on(S, X, P)) {
-                    ES es;
+                    // The candidates pathtrace.wgsl:2513 resamples: the tree's count at camera hits (one deeper),
+                    // 6 / 3 without a tree where the camera sees the point, 2 with light LOD; else one CDF draw.
                     bool lt_on = pf(P, P_LTREE + 3) > 0.5f;
                     bool seen_directly = depth == 0u || (depth == 1u && (flags & F_MIRROR) != 0u);
-                    if (lt_on) es = sample_emitter_ris(S, X, P, R, oo, ne, depth == 0u ? (uint32_t)pf(P, P_LTREE + 3) : 1u, s, lb, v, R.dim(D_EMIT));
-                    else if (seen_directly) es = sample_emitter_ris(S, X, P, R, oo, ne, depth == 0u ? EMIT_RIS_M : EMIT_RIS_M / 2u, s, lb, v, R.dim(D_EMIT));
-                    else if (pf(P, P_LIGHT_LOD + 3) > 0.0f) es = sample_emitter_ris(S, X, P, R, oo, ne, 2u, s, lb, v, R.dim(D_EMIT));
-                    else es = sample_emitter(S, X, P, R, oo, ne, R.dim(D_EMIT));
+                    uint32_t m = 0;
+                    if (lt_on) m = depth == 0u ? (uint32_t)pf(P, P_LTREE + 3) : 1u;
+                    else if (seen_directly) m = depth == 0u ? EMIT_RIS_M : EMIT_RIS_M / 2u;
+                    else if (pf(P, P_LIGHT_LOD + 3) > 0.0f) m = 2u;
+                    ES es = m > 0u ? sample_emitter_ris(S, X, P, R, oo, ne, m, s, lb, v, R.dim(D_EMIT))
+                                   : sample_emitter(S, X, P, R, oo, ne, R.dim(D_EMIT));
                     if (es.pdf_w > 0.0f) {
                         V3 f = eval_bsdf_k(s, lb, v, es.l, 1.0f);
                         if (any_gt0(f)) {
