@@ -39,7 +39,8 @@ struct Builder {
         std::memset(&W, 0, sizeof(W));
         float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
         for (const BinNode* c : ch)
-            for (int k = 0; k < 3; ++k) { lo[k] = std::min(lo[k], c->bmin[k]); hi[k] = std::max(hi[k], c->bmax[k]); }
+            if (c)
+                for (int k = 0; k < 3; ++k) { lo[k] = std::min(lo[k], c->bmin[k]); hi[k] = std::max(hi[k], c->bmax[k]); }
         float origin[3];
         int ex[3];
         for (int k = 0; k < 3; ++k) {
@@ -59,6 +60,7 @@ struct Builder {
         for (int i = 0; i < 8; ++i)
             for (int k = 0; k < 3; ++k) { qlo[k][i] = 255; qhi[k][i] = 0; }
         for (size_t i = 0; i < ch.size(); ++i) {
+            if (!ch[i]) continue;
             for (int k = 0; k < 3; ++k) {
                 float s = std::ldexp(1.0f, ex[k]);
                 double a = std::floor((double)(ch[i]->bmin[k] - origin[k]) / s) - 1.0;
@@ -75,11 +77,41 @@ struct Builder {
         W.w[4] = child_base;
         W.w[5] = leaf_base;
         uint8_t cnt[8] = {0};
-        for (size_t i = 0; i < ch.size(); ++i) cnt[i] = interior[i] ? 0 : (uint8_t)counts[i];
+        for (size_t i = 0; i < ch.size(); ++i) cnt[i] = (interior[i] || !ch[i]) ? 0 : (uint8_t)counts[i];
         std::memcpy(&W.w[6], cnt, 8);
         uint8_t* q = reinterpret_cast<uint8_t*>(&W.w[8]);
         for (int k = 0; k < 3; ++k) std::memcpy(q + 8 * k, qlo[k], 8);
         for (int k = 0; k < 3; ++k) std::memcpy(q + 24 + 8 * k, qhi[k], 8);
+    }
+
+    // The children in slots by octant: slot s (bit k set: the upper half along axis k) takes the child whose centre
+    // lies most that way from the node's centre, so that a walk visiting slots in the order k ^ (the ray's sign bits)
+    // meets them nearly front to back without sorting. Greedy assignment by score; unused slots are empty (index
+    // UINT32_MAX).
+    std::vector<uint32_t> octant_slots(const std::vector<uint32_t>& ch) {
+        float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (uint32_t c : ch)
+            for (int k = 0; k < 3; ++k) { lo[k] = std::min(lo[k], nodes[c].bmin[k]); hi[k] = std::max(hi[k], nodes[c].bmax[k]); }
+        struct Cand { float score; int child, slot; };
+        std::vector<Cand> cands;
+        for (size_t j = 0; j < ch.size(); ++j) {
+            float v[3];
+            for (int k = 0; k < 3; ++k) {
+                float e = std::max(hi[k] - lo[k], 1e-30f);
+                v[k] = ((nodes[ch[j]].bmin[k] + nodes[ch[j]].bmax[k]) - (lo[k] + hi[k])) / e;
+            }
+            for (int sl = 0; sl < 8; ++sl) {
+                float sc = 0.0f;
+                for (int k = 0; k < 3; ++k) sc += (sl >> k & 1) ? v[k] : -v[k];
+                cands.push_back({sc, (int)j, sl});
+            }
+        }
+        std::stable_sort(cands.begin(), cands.end(), [](const Cand& a, const Cand& b) { return a.score > b.score; });
+        std::vector<uint32_t> slots(8, UINT32_MAX);
+        std::vector<bool> placed(ch.size(), false);
+        for (const Cand& c : cands)
+            if (!placed[c.child] && slots[c.slot] == UINT32_MAX) { slots[c.slot] = ch[c.child]; placed[c.child] = true; }
+        return slots;
     }
 
     // Collapses the binary tree rooted at `root` (child indices from `root`); `leaf(node, items)` appends a binary
@@ -129,20 +161,23 @@ struct Builder {
                     ch.insert(ch.begin() + best + 1, cl + 1);
                 }
             }
+            ch = octant_slots(ch);
             std::vector<const BinNode*> cp;
             std::vector<bool> interior;
             std::vector<uint32_t> counts;
             uint32_t n_interior = 0;
             for (uint32_t c : ch) {
-                cp.push_back(&nodes[c]);
-                interior.push_back(nodes[c].count == 0);
-                if (nodes[c].count == 0) n_interior++;
+                cp.push_back(c == UINT32_MAX ? nullptr : &nodes[c]);
+                interior.push_back(c != UINT32_MAX && nodes[c].count == 0);
+                if (c != UINT32_MAX && nodes[c].count == 0) n_interior++;
             }
             uint32_t child_base = (uint32_t)out.size();
             out.resize(out.size() + n_interior);
             uint32_t leaf_base = UINT32_MAX, k = 0;
             for (size_t i = 0; i < ch.size(); ++i) {
-                if (interior[i]) {
+                if (ch[i] == UINT32_MAX) {
+                    counts.push_back(0);
+                } else if (interior[i]) {
                     work.push_back({ch[i], child_base + k++});
                     counts.push_back(0);
                 } else {

@@ -65,11 +65,21 @@ __device__ __forceinline__ float q_float(uint32_t w, int k) {
     return bf((m & 0x007f8000u) | 0x3f800000u);
 }
 
-// The eight child boxes of node `nd` against the ray: each slot's entry t (INF: missed, or past tmax).
-// A slot's plane at q steps is origin + q 2^e = (origin - 2^(e+8)) + (1 + q/256) 2^(e+8): one FMA of the bit-built
-// float. The near and far planes of each axis are picked once by the ray's signs; an empty slot (q_lo > q_hi) has
-// its near plane past its far one on every axis, so it misses whatever the signs.
-__device__ __forceinline__ void wide_children(const uint4 nd[5], const WideRay& r, float tmax, float tn[8]) {
+// Visit order: slot i is visited k-th for i = k ^ oct. A node's byte arrays (one byte a slot, slots 0-3 in the low word)
+// are put in that order with one byte permute a word: oct bit 0 swaps neighbouring bytes, bit 1 byte pairs, bit 2 the
+// two words.
+__device__ __forceinline__ void visit_order(uint32_t oct, uint32_t a, uint32_t b, uint32_t& x, uint32_t& y) {
+    const uint32_t sel = (oct & 3u) == 0u ? 0x3210u : ((oct & 3u) == 1u ? 0x2301u : ((oct & 3u) == 2u ? 0x1032u : 0x0123u));
+    uint32_t pa = __byte_perm(a, 0u, sel), pb = __byte_perm(b, 0u, sel);
+    x = (oct & 4u) ? pb : pa;
+    y = (oct & 4u) ? pa : pb;
+}
+
+// The eight child boxes of node `nd` against the ray, in visit order: tv[k] is the entry t of slot k ^ r.neg (INF:
+// missed, or past tmax). A slot's plane at q steps is origin + q 2^e = (origin - 2^(e+8)) + (1 + q/256) 2^(e+8): one
+// FMA of the bit-built float. The near and far planes of each axis are picked once by the ray's signs; an empty slot
+// (q_lo > q_hi) has its near plane past its far one on every axis, so it misses whatever the signs.
+__device__ __forceinline__ void wide_children(const uint4 nd[5], const WideRay& r, float tmax, float tv[8]) {
     uint32_t eb = nd[0].w;
     float s8x = bf(((eb & 0xffu) + 8u) << 23), s8y = bf((((eb >> 8) & 0xffu) + 8u) << 23),
           s8z = bf((((eb >> 16) & 0xffu) + 8u) << 23);
@@ -78,37 +88,23 @@ __device__ __forceinline__ void wide_children(const uint4 nd[5], const WideRay& 
           Bz = ((bf(nd[0].z) - r.o.z) - s8z) * r.inv.z;
     // q_lo x: nd[2].x,y; y: nd[2].z,w; z: nd[3].x,y. q_hi x: nd[3].z,w; y: nd[4].x,y; z: nd[4].z,w.
     bool nx = r.neg & 1u, ny = r.neg & 2u, nz = r.neg & 4u;
-    uint32_t nearx[2] = {nx ? nd[3].z : nd[2].x, nx ? nd[3].w : nd[2].y};
-    uint32_t farx[2] = {nx ? nd[2].x : nd[3].z, nx ? nd[2].y : nd[3].w};
-    uint32_t neary[2] = {ny ? nd[4].x : nd[2].z, ny ? nd[4].y : nd[2].w};
-    uint32_t fary[2] = {ny ? nd[2].z : nd[4].x, ny ? nd[2].w : nd[4].y};
-    uint32_t nearz[2] = {nz ? nd[4].z : nd[3].x, nz ? nd[4].w : nd[3].y};
-    uint32_t farz[2] = {nz ? nd[3].x : nd[4].z, nz ? nd[3].y : nd[4].w};
+    uint32_t nearx[2], farx[2], neary[2], fary[2], nearz[2], farz[2];
+    visit_order(r.neg, nx ? nd[3].z : nd[2].x, nx ? nd[3].w : nd[2].y, nearx[0], nearx[1]);
+    visit_order(r.neg, nx ? nd[2].x : nd[3].z, nx ? nd[2].y : nd[3].w, farx[0], farx[1]);
+    visit_order(r.neg, ny ? nd[4].x : nd[2].z, ny ? nd[4].y : nd[2].w, neary[0], neary[1]);
+    visit_order(r.neg, ny ? nd[2].z : nd[4].x, ny ? nd[2].w : nd[4].y, fary[0], fary[1]);
+    visit_order(r.neg, nz ? nd[4].z : nd[3].x, nz ? nd[4].w : nd[3].y, nearz[0], nearz[1]);
+    visit_order(r.neg, nz ? nd[3].x : nd[4].z, nz ? nd[3].y : nd[4].w, farz[0], farz[1]);
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        int h = i >> 2, k = i & 3;
-        float x0 = fmaf(q_float(nearx[h], k), Sx, Bx), x1 = fmaf(q_float(farx[h], k), Sx, Bx);
-        float y0 = fmaf(q_float(neary[h], k), Sy, By), y1 = fmaf(q_float(fary[h], k), Sy, By);
-        float z0 = fmaf(q_float(nearz[h], k), Sz, Bz), z1 = fmaf(q_float(farz[h], k), Sz, Bz);
+    for (int k = 0; k < 8; ++k) {
+        int h = k >> 2, j = k & 3;
+        float x0 = fmaf(q_float(nearx[h], j), Sx, Bx), x1 = fmaf(q_float(farx[h], j), Sx, Bx);
+        float y0 = fmaf(q_float(neary[h], j), Sy, By), y1 = fmaf(q_float(fary[h], j), Sy, By);
+        float z0 = fmaf(q_float(nearz[h], j), Sz, Bz), z1 = fmaf(q_float(farz[h], j), Sz, Bz);
         float tnear = fmaxf(fmaxf(x0, y0), fmaxf(z0, 0.0f));
         float tfar = fminf(fminf(x1, y1), fminf(z1, tmax));
-        tn[i] = tnear <= tfar ? tnear : INF;
+        tv[k] = tnear <= tfar ? tnear : INF;
     }
-}
-
-// Ascending sort of eight keys (a sorting network of 19 compare-exchanges).
-__device__ __forceinline__ void cas(uint32_t& a, uint32_t& b) {
-    uint32_t lo = min(a, b), hi = max(a, b);
-    a = lo;
-    b = hi;
-}
-__device__ __forceinline__ void sort8(uint32_t k[8]) {
-    cas(k[0], k[2]); cas(k[1], k[3]); cas(k[4], k[6]); cas(k[5], k[7]);
-    cas(k[0], k[4]); cas(k[1], k[5]); cas(k[2], k[6]); cas(k[3], k[7]);
-    cas(k[0], k[1]); cas(k[2], k[3]); cas(k[4], k[5]); cas(k[6], k[7]);
-    cas(k[2], k[4]); cas(k[3], k[5]);
-    cas(k[1], k[4]); cas(k[3], k[6]);
-    cas(k[1], k[2]); cas(k[3], k[4]); cas(k[5], k[6]);
 }
 
 // The walk over both levels: the top tree's hit leaves are units, entered (the ray in the unit's space, as
@@ -142,27 +138,20 @@ __device__ Hit trace_wide(const DScene& S, const WideView& W, const Sections& X,
             uint32_t child_base = nd[1].x, leaf_base = nd[1].y;
             uint64_t counts = ((uint64_t)nd[1].w << 32) | nd[1].z;
             uint64_t prefix = counts * 0x0101010101010101ull;  // byte i: the items of slots 0..i
-            // The hit slots by their entry t (t >= 0, so its bits order as the floats), the slot in the low bits.
-            uint32_t key[8];
+            // Slots in the order k ^ (the ray's signs): the builder put children by octant, so this order is
+            // nearly front to back. Leaves first (their hits cull the farther entries), then the other entries
+            // pushed farthest first, so the nearest is on top.
+            uint32_t oct = r.neg;
 #pragma unroll
-            for (int i = 0; i < 8; ++i) key[i] = tn[i] == INF ? 0xffffffffu : ((bu(tn[i]) & ~7u) | (uint32_t)i);
-            sort8(key);
-            // Leaves first, nearest first: their hits cull the farther entries. Then the other entries, farthest
-            // first, so the nearest is on top.
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                if (key[j] == 0xffffffffu) break;
-                uint32_t i = key[j] & 7u;
+            for (int k = 0; k < 8; ++k) {
+                uint32_t i = (uint32_t)k ^ oct;
+                if (tn[k] >= hit.t) continue;
                 if (imask & (1u << i)) continue;
-                if (bf(key[j] & ~7u) >= hit.t) break;
                 uint32_t cnt = (uint32_t)(counts >> (8 * i)) & 0xffu;
+                if (cnt == 0 || rec == NO_INST) continue;  // (top-tree leaves are units: entries, below)
                 uint32_t item = leaf_base + ((uint32_t)(prefix >> (8 * i)) & 0xffu) - cnt;
-                if (rec == NO_INST) {
-                    if (COUNT) wc->units += cnt;
-                    continue;  // units are entries, pushed below
-                }
-                for (uint32_t k = 0; k < cnt; ++k) {
-                    uint32_t ti = item + k;
+                for (uint32_t q = 0; q < cnt; ++q) {
+                    uint32_t ti = item + q;
                     if (ti >= W.n_tris) { *guard = true; return hit; }
                     const float4* tp = W.tris + 3ull * ti;
                     float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
@@ -186,19 +175,19 @@ __device__ Hit trace_wide(const DScene& S, const WideView& W, const Sections& X,
                 }
             }
 #pragma unroll
-            for (int j = 7; j >= 0; --j) {
-                if (key[j] == 0xffffffffu) continue;
-                float t = bf(key[j] & ~7u);
+            for (int k = 7; k >= 0; --k) {
+                uint32_t i = (uint32_t)k ^ oct;
+                float t = tn[k];
                 if (t >= hit.t) continue;
-                uint32_t i = key[j] & 7u;
                 if (imask & (1u << i)) {
                     if (sp < WIDE_STACK) { stack_ref[sp] = child_base + (uint32_t)__popc(imask & ((1u << i) - 1u)); stack_t[sp] = t; sp++; }
                 } else if (rec == NO_INST) {
                     uint32_t cnt = (uint32_t)(counts >> (8 * i)) & 0xffu;
                     uint32_t item = leaf_base + ((uint32_t)(prefix >> (8 * i)) & 0xffu) - cnt;
-                    for (uint32_t k = 0; k < cnt; ++k) {
-                        if (item + k >= W.n_units) { *guard = true; return hit; }
-                        uint32_t u = __ldg(W.units + item + k);
+                    if (COUNT) wc->units += cnt;
+                    for (uint32_t q = 0; q < cnt; ++q) {
+                        if (item + q >= W.n_units) { *guard = true; return hit; }
+                        uint32_t u = __ldg(W.units + item + q);
                         if (mode == TRACE_SHADOW && !(u & WIDE_UNIT_BIT)) continue;
                         if (sp < WIDE_STACK) { stack_ref[sp] = u | WIDE_UNIT_BIT; stack_t[sp] = t; sp++; }
                     }
