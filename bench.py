@@ -193,7 +193,8 @@ def main():
     ap.add_argument("--steps", type=int, default=120)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--binary", action="store_true", help="walk the reference's binary trees")
+    ap.add_argument("--walk", default="binary", choices=["binary", "wide"],
+                    help="the reference's binary trees (fastest measured here) or the 8-wide quantised BVH")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -219,7 +220,7 @@ def main():
     gpu = Gpu(local)
     name, sms = gpu.device_info()
     S = gpu.upload(P)
-    flags = N.TRT_RENDER_BINARY if args.binary else 0
+    flags = N.TRT_RENDER_WIDE if args.walk == "wide" else 0
     frames = [(rank + world * (args.warmup + i)) % FRAMES for i in range(args.steps)]
     warm_frames = [(rank + world * i) % FRAMES for i in range(args.warmup)]
     params = {f: frame_params(P, f) for f in set(frames + warm_frames)}
@@ -295,7 +296,7 @@ def main():
         "metric": METRIC, "value": rays_all / (ms * 1e-3) / 1e6, "unit": "Mrays/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "frames_per_rank": args.steps, "walk": "binary" if args.binary else "wide",
+        "config": {"workload": WORKLOAD, "frames_per_rank": args.steps, "walk": args.walk,
                    "l2": "inputs larger than L2: 221 MB of scene buffers, each step a new camera along the spline",
                    "device": name, "sms": sms, "parallelism": f"replicas x{world}, frames split across ranks"},
         "e2e": {"value": rays_all / (e2e_ms * 1e-3) / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": 624,

@@ -79,7 +79,7 @@ typedef struct { float t; uint32_t tri; float u; float v; uint32_t inst; uint32_
 /* Render flags. */
 #define TRT_RENDER_ACCUMULATE 1u /* add to accum instead of clearing it first (resume at first_sample) */
 #define TRT_RENDER_COUNT      2u /* also count node visits, triangle tests and unit entries (a slower walk) */
-#define TRT_RENDER_BINARY     4u /* walk the reference's binary trees instead of the wide BVH */
+#define TRT_RENDER_WIDE       4u /* walk the 8-wide quantised BVH instead of the reference's binary trees */
 
 int trt_create(const trt_options* opts, trt_ctx** out);
 /* Frees the context and every scene still uploaded through it (their handles are then invalid). */
@@ -88,12 +88,12 @@ const char* trt_last_error(const trt_ctx* ctx);
 /* The library's version and the device it runs on (name, SM count). */
 int trt_device_info(const trt_ctx* ctx, char* name, size_t name_len, int* sm_count);
 
-/* Uploads a scene (gpu.rs:2613 Gpu::upload) and builds its wide BVH on the device. */
+/* Uploads a scene (gpu.rs:2613 Gpu::upload). Its wide BVH is built from the uploaded trees at the first render or
+ * trace that asks for it (TRT_RENDER_WIDE), and again after an update to the nodes, leaves or tables. */
 int trt_scene_upload(trt_ctx* ctx, const trt_scene_desc* desc, trt_scene** out);
 void trt_scene_free(trt_scene* scene);
 /* Overwrites bytes [offset, offset + bytes) of one of the scene's buffers (0 vertices, 1 leaves, 2 nodes, 3 tables,
- * 4 words) from host memory: in-place record edits and refits (gpu.rs:4028 write_nodes). A change to nodes or leaves
- * rebuilds the wide BVH. */
+ * 4 words) from host memory: in-place record edits and refits (gpu.rs:4028 write_nodes). */
 int trt_scene_update(trt_scene* scene, uint32_t which, uint64_t offset, const void* src, uint64_t bytes);
 
 /* Renders samples [first_sample, first_sample + spp) at Params' size (gpu.rs:4116 Gpu::render; its per-dispatch

@@ -37,7 +37,7 @@ def trace_parity(gpu, P, flags, n=20000):
 
 
 @pytest.mark.parametrize("make", [small_city, scaled_units_scene, scenes.cornell])
-@pytest.mark.parametrize("flags", [N.TRT_RENDER_BINARY, 0])
+@pytest.mark.parametrize("flags", [0, N.TRT_RENDER_WIDE])
 def test_trace_matches_the_oracle(gpu, make, flags):
     assert trace_parity(gpu, prep.prepare(make()), flags) > 500
 
@@ -51,12 +51,13 @@ def image_parity(acc_g, acc_o, w, h, spp):
     return ok.mean(), np.abs(mg / np.maximum(mo, 1e-12) - 1).max()
 
 
+@pytest.mark.parametrize("flags", [0, N.TRT_RENDER_WIDE])
 @pytest.mark.parametrize("make,spp", [(lambda: scenes.cornell(64, 64), 16), (small_city, 4),
                                       (scaled_units_scene, 4)])
-def test_render_matches_the_oracle(gpu, make, spp):
+def test_render_matches_the_oracle(gpu, make, spp, flags):
     P = prep.prepare(make())
     w, h = P.width, P.height
-    acc_g = gpu.upload(P).render_raw(P.params, spp)[0]
+    acc_g = gpu.upload(P).render_raw(P.params, spp, flags=flags)[0]
     acc_o, st = oracle.Oracle(P).render(P.params, spp)
     assert st["tri_tests"] > w * h and st["shadow_rays"] > w * h // 4  # the camera sees the scene
     frac, mean_err = image_parity(acc_g, acc_o, w, h, spp)
@@ -128,4 +129,4 @@ def test_a_cycle_in_the_tree_trips_the_guard(gpu):
     P.nodes[top, 7] = 0
     S = gpu.upload(P)
     with pytest.raises(RenderError, match="TRT_EGUARD"):
-        S.render_raw(P.params, 1, flags=N.TRT_RENDER_BINARY)
+        S.render_raw(P.params, 1)

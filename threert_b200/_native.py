@@ -18,7 +18,7 @@ PIXEL_FLOATS = 20
 
 TRT_RENDER_ACCUMULATE = 1
 TRT_RENDER_COUNT = 2
-TRT_RENDER_BINARY = 4
+TRT_RENDER_WIDE = 4
 
 ERRORS = {1: "TRT_EINVAL", 2: "TRT_ECUDA", 3: "TRT_EGUARD"}
 

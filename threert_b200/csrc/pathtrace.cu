@@ -884,7 +884,7 @@ int trt_render(trt_scene* s, const uint32_t params[TRT_PARAMS_WORDS], uint32_t f
         TRT_CUDA(c, cudaEventRecord(c->t0, c->stream));
     }
     uint64_t launches0 = s->launches;
-    bool count = (flags & TRT_RENDER_COUNT) != 0, binary = (flags & TRT_RENDER_BINARY) != 0;
+    bool count = (flags & TRT_RENDER_COUNT) != 0, binary = (flags & TRT_RENDER_WIDE) == 0;
     if (!binary && s->wide.ensure(params, s->host, c->stream) != 0) return fail(c, TRT_EINVAL, s->wide.error);
     if (spp > 0) {
         if (count) rc = binary ? render_waves<true, false>(s, P, first_sample, spp) : render_waves<true, true>(s, P, first_sample, spp);
@@ -947,7 +947,7 @@ int trt_trace(trt_scene* s, const uint32_t params[TRT_PARAMS_WORDS], const trt_r
     cudaError_t e = cudaMalloc(&dh, sizeof(trt_hit) * n);
     if (e != cudaSuccess) { cudaFree(dr); return cuda_fail(c, e, "trt_trace"); }
     e = cudaMemcpyAsync(dr, rays, sizeof(trt_ray) * n, cudaMemcpyHostToDevice, c->stream);
-    bool binary = (flags & TRT_RENDER_BINARY) != 0;
+    bool binary = (flags & TRT_RENDER_WIDE) == 0;
     bool count = (flags & TRT_RENDER_COUNT) != 0;
     if (e == cudaSuccess && !binary && s->wide.ensure(params, s->host, c->stream) != 0) {
         cudaFree(dr);

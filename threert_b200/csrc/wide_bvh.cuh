@@ -59,11 +59,8 @@ __device__ __forceinline__ WideRay wide_ray(V3 o, V3 d, V3 inv) {
     return WideRay{o, d, inv, (inv.x < 0.0f ? 1u : 0u) | (inv.y < 0.0f ? 2u : 0u) | (inv.z < 0.0f ? 4u : 0u)};
 }
 
-// Byte k of w as the float 1 + q / 256, exactly: q in the mantissa's top eight bits.
-__device__ __forceinline__ float q_float(uint32_t w, int k) {
-    uint32_t m = k >= 2 ? (w >> (8 * k - 15)) : (w << (15 - 8 * k));
-    return bf((m & 0x007f8000u) | 0x3f800000u);
-}
+// Byte k of w as a float (the conversion runs beside the walk's integer work, which keeps the ALU pipe busy).
+__device__ __forceinline__ float q_float(uint32_t w, int k) { return __uint2float_rn((w >> (8 * k)) & 0xffu); }
 
 // Visit order: slot i is visited k-th for i = k ^ oct. A node's byte arrays (one byte a slot, slots 0-3 in the low word)
 // are put in that order with one byte permute a word: oct bit 0 swaps neighbouring bytes, bit 1 byte pairs, bit 2 the
@@ -76,16 +73,14 @@ __device__ __forceinline__ void visit_order(uint32_t oct, uint32_t a, uint32_t b
 }
 
 // The eight child boxes of node `nd` against the ray, in visit order: tv[k] is the entry t of slot k ^ r.neg (INF:
-// missed, or past tmax). A slot's plane at q steps is origin + q 2^e = (origin - 2^(e+8)) + (1 + q/256) 2^(e+8): one
-// FMA of the bit-built float. The near and far planes of each axis are picked once by the ray's signs; an empty slot
-// (q_lo > q_hi) has its near plane past its far one on every axis, so it misses whatever the signs.
+// missed, or past tmax). A slot's plane at q steps is origin + q 2^e: t = q (2^e / d) + (origin - o) / d, one FMA.
+// The near and far planes of each axis are picked once by the ray's signs; an empty slot (q_lo > q_hi) has its near
+// plane past its far one on every axis, so it misses whatever the signs.
 __device__ __forceinline__ void wide_children(const uint4 nd[5], const WideRay& r, float tmax, float tv[8]) {
     uint32_t eb = nd[0].w;
-    float s8x = bf(((eb & 0xffu) + 8u) << 23), s8y = bf((((eb >> 8) & 0xffu) + 8u) << 23),
-          s8z = bf((((eb >> 16) & 0xffu) + 8u) << 23);
-    float Sx = s8x * r.inv.x, Sy = s8y * r.inv.y, Sz = s8z * r.inv.z;
-    float Bx = ((bf(nd[0].x) - r.o.x) - s8x) * r.inv.x, By = ((bf(nd[0].y) - r.o.y) - s8y) * r.inv.y,
-          Bz = ((bf(nd[0].z) - r.o.z) - s8z) * r.inv.z;
+    float Sx = bf((eb & 0xffu) << 23) * r.inv.x, Sy = bf(((eb >> 8) & 0xffu) << 23) * r.inv.y,
+          Sz = bf(((eb >> 16) & 0xffu) << 23) * r.inv.z;
+    float Bx = (bf(nd[0].x) - r.o.x) * r.inv.x, By = (bf(nd[0].y) - r.o.y) * r.inv.y, Bz = (bf(nd[0].z) - r.o.z) * r.inv.z;
     // q_lo x: nd[2].x,y; y: nd[2].z,w; z: nd[3].x,y. q_hi x: nd[3].z,w; y: nd[4].x,y; z: nd[4].z,w.
     bool nx = r.neg & 1u, ny = r.neg & 2u, nz = r.neg & 4u;
     uint32_t nearx[2], farx[2], neary[2], fary[2], nearz[2], farz[2];
@@ -107,6 +102,21 @@ __device__ __forceinline__ void wide_children(const uint4 nd[5], const WideRay& 
     }
 }
 
+// Ascending sort of eight keys (a sorting network of 19 compare-exchanges).
+__device__ __forceinline__ void cas(uint32_t& a, uint32_t& b) {
+    uint32_t lo = min(a, b), hi = max(a, b);
+    a = lo;
+    b = hi;
+}
+__device__ __forceinline__ void sort8(uint32_t k[8]) {
+    cas(k[0], k[2]); cas(k[1], k[3]); cas(k[4], k[6]); cas(k[5], k[7]);
+    cas(k[0], k[4]); cas(k[1], k[5]); cas(k[2], k[6]); cas(k[3], k[7]);
+    cas(k[0], k[1]); cas(k[2], k[3]); cas(k[4], k[5]); cas(k[6], k[7]);
+    cas(k[2], k[4]); cas(k[3], k[5]);
+    cas(k[1], k[4]); cas(k[3], k[6]);
+    cas(k[1], k[2]); cas(k[3], k[4]); cas(k[5], k[6]);
+}
+
 // The walk over both levels: the top tree's hit leaves are units, entered (the ray in the unit's space, as
 // trace_units.wgsl:86-105) when popped; a unit's walk ends when the stack is back to where it was entered. Entries
 // carry the t they were hit at and are skipped once a closer hit is known.
@@ -120,6 +130,14 @@ __device__ Hit trace_wide(const DScene& S, const WideView& W, const Sections& X,
     uint32_t stack_ref[WIDE_STACK];
     float stack_t[WIDE_STACK];
     int sp = 0;
+#define STACK_PUSH(ref, tt)                                   \
+    do {                                                      \
+        if (sp < WIDE_STACK) {                                \
+            stack_ref[sp] = (ref);                            \
+            stack_t[sp] = (tt);                               \
+            sp++;                                             \
+        }                                                     \
+    } while (0)
     uint32_t cur = W.top_root;  // the node to open next (NO_INST: pop)
     uint32_t rec = NO_INST;
     int base = 0;
@@ -138,15 +156,36 @@ __device__ Hit trace_wide(const DScene& S, const WideView& W, const Sections& X,
             uint32_t child_base = nd[1].x, leaf_base = nd[1].y;
             uint64_t counts = ((uint64_t)nd[1].w << 32) | nd[1].z;
             uint64_t prefix = counts * 0x0101010101010101ull;  // byte i: the items of slots 0..i
-            // Slots in the order k ^ (the ray's signs): the builder put children by octant, so this order is
-            // nearly front to back. Leaves first (their hits cull the farther entries), then the other entries
-            // pushed farthest first, so the nearest is on top.
+            // The visit order: for closest hits the hit slots sorted by their entry t; for any-hit rays (shadow
+            // rays stop at the first hit, whichever) the octant order k ^ (the ray's signs), nearly front to back
+            // as the builder put children by octant. order[j]: visit index of the j-th slot to visit (9: none).
             uint32_t oct = r.neg;
+            uint32_t key[8];
 #pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                uint32_t i = (uint32_t)k ^ oct;
-                if (tn[k] >= hit.t) continue;
+            for (int k = 0; k < 8; ++k) key[k] = tn[k] >= hit.t ? 0xffffffffu : ((bu(tn[k]) & ~7u) | (uint32_t)k);
+            if (mode == TRACE_CLOSEST) {
+                uint32_t hits = 0;
+#pragma unroll
+                for (int k = 0; k < 8; ++k) hits += key[k] != 0xffffffffu;
+                if (hits > 1) sort8(key);
+                else if (hits == 1) {
+                    // (One hit: move it first.)
+                    uint32_t m = key[0];
+#pragma unroll
+                    for (int k = 1; k < 8; ++k) m = min(m, key[k]);
+                    key[0] = m;
+#pragma unroll
+                    for (int k = 1; k < 8; ++k) key[k] = 0xffffffffu;
+                }
+            }
+            // Leaves first (their hits cull the farther entries), then the other entries pushed farthest first,
+            // so the nearest is on top.
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                if (key[j] == 0xffffffffu) continue;
+                uint32_t i = (key[j] & 7u) ^ oct;
                 if (imask & (1u << i)) continue;
+                if (bf(key[j] & ~7u) >= hit.t) continue;
                 uint32_t cnt = (uint32_t)(counts >> (8 * i)) & 0xffu;
                 if (cnt == 0 || rec == NO_INST) continue;  // (top-tree leaves are units: entries, below)
                 uint32_t item = leaf_base + ((uint32_t)(prefix >> (8 * i)) & 0xffu) - cnt;
@@ -175,12 +214,13 @@ __device__ Hit trace_wide(const DScene& S, const WideView& W, const Sections& X,
                 }
             }
 #pragma unroll
-            for (int k = 7; k >= 0; --k) {
-                uint32_t i = (uint32_t)k ^ oct;
-                float t = tn[k];
+            for (int j = 7; j >= 0; --j) {
+                if (key[j] == 0xffffffffu) continue;
+                float t = bf(key[j] & ~7u);
                 if (t >= hit.t) continue;
+                uint32_t i = (key[j] & 7u) ^ oct;
                 if (imask & (1u << i)) {
-                    if (sp < WIDE_STACK) { stack_ref[sp] = child_base + (uint32_t)__popc(imask & ((1u << i) - 1u)); stack_t[sp] = t; sp++; }
+                    STACK_PUSH(child_base + (uint32_t)__popc(imask & ((1u << i) - 1u)), t);
                 } else if (rec == NO_INST) {
                     uint32_t cnt = (uint32_t)(counts >> (8 * i)) & 0xffu;
                     uint32_t item = leaf_base + ((uint32_t)(prefix >> (8 * i)) & 0xffu) - cnt;
@@ -189,7 +229,7 @@ __device__ Hit trace_wide(const DScene& S, const WideView& W, const Sections& X,
                         if (item + q >= W.n_units) { *guard = true; return hit; }
                         uint32_t u = __ldg(W.units + item + q);
                         if (mode == TRACE_SHADOW && !(u & WIDE_UNIT_BIT)) continue;
-                        if (sp < WIDE_STACK) { stack_ref[sp] = u | WIDE_UNIT_BIT; stack_t[sp] = t; sp++; }
+                        STACK_PUSH(u | WIDE_UNIT_BIT, t);
                     }
                 }
             }
@@ -228,6 +268,7 @@ __device__ Hit trace_wide(const DScene& S, const WideView& W, const Sections& X,
         }
     }
     return hit;
+#undef STACK_PUSH
 }
 
 }  // namespace trt
