@@ -111,6 +111,21 @@ int trt_accum_read(trt_scene* scene, float* accum_host, uint64_t bytes);
 int trt_trace(trt_scene* scene, const uint32_t params[TRT_PARAMS_WORDS], const trt_ray* rays, uint64_t n, uint32_t flags,
               trt_hit* hits);
 
+/* The render without allocations, for callers that cannot call cudaMalloc: code inside a CUDA graph capture, or a
+ * process whose device memory all belongs to one pool (an engine's caching allocator, a hard memory budget). It has
+ * no counterpart in the reference. The caller owns every buffer: `dev` holds DEVICE pointers to the scene's buffers
+ * (laid out as for trt_scene_upload), `accum_device` w * h Pixel records, `stream` a cudaStream_t (NULL: the legacy
+ * default stream); the call is asynchronous on that stream. The wave's working state lives in one file-scope device
+ * array of 32 MiB (31.5 MiB used) that every GPU loading the library holds until the process exits; it allocates
+ * nothing: no cudaMalloc, no cudaFree, no allocating library routine. Limits: images of at most 65,536 path slots
+ * (8 x 4 pixel tiles: 256 x 256), at most 4 directional lights, the binary walk; larger sizes are refused with
+ * TRT_EINVAL and a message in `err` (err_len bytes, may be NULL). The first call on a device sets it up (the array's
+ * device address, the sampler's tables): make that first call before any stream capture. Every call shares the
+ * array, so calls whose work overlaps on the GPU race: run them on one stream, or one at a time. Flags:
+ * TRT_RENDER_ACCUMULATE alone. */
+int trt_render_noalloc(const trt_scene_desc* dev, const uint32_t params[TRT_PARAMS_WORDS], uint32_t first_sample,
+                       uint32_t spp, uint32_t flags, float* accum_device, void* stream, char* err, size_t err_len);
+
 int trt_scene_totals(trt_scene* scene, trt_totals* out);
 void trt_scene_reset_totals(trt_scene* scene);
 /* 1: record per-stage CUDA events (extend_ms, shadow_ms in the totals). */

@@ -132,6 +132,8 @@ SIGNATURES = [
     ("trt_accum_device_ptr", C.c_int, [C.c_void_p, P(C.c_void_p), P(u64)]),
     ("trt_accum_read", C.c_int, [C.c_void_p, P(f32), u64]),
     ("trt_trace", C.c_int, [C.c_void_p, P(u32), P(Ray), u64, u32, P(Hit)]),
+    ("trt_render_noalloc", C.c_int, [P(SceneDesc), P(u32), u32, u32, u32, C.c_void_p, C.c_void_p, C.c_char_p,
+                                     C.c_size_t]),
     ("trt_scene_totals", C.c_int, [C.c_void_p, P(Totals)]),
     ("trt_scene_reset_totals", None, [C.c_void_p]),
     ("trt_scene_set_profiling", None, [C.c_void_p, C.c_int]),

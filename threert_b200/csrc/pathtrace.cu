@@ -728,6 +728,64 @@ int render_waves(trt_scene* s, const Params& P, uint32_t first_sample, uint32_t 
 
 }  // namespace
 
+// ---- the render without allocations --------------------------------------------------------------------------------
+//
+// For callers that cannot call cudaMalloc: code running inside a CUDA graph being captured, or under a memory pool
+// that owns all of a device's memory (an engine's caching allocator, a process with a hard device-memory budget).
+// They own the scene's buffers and the accum themselves; the wave's working state lives in this file-scope array,
+// which every GPU that loads the library holds until the process exits.
+
+// The largest wave the array holds: 65,536 path slots (a 256 x 256 image, one sample a wave) with up to 4 suns.
+constexpr uint32_t NOALLOC_SLOTS = 65536u;
+constexpr uint32_t NOALLOC_SHADOW = NOALLOC_SLOTS * (MAX_DIR_LIGHTS + 2u);
+constexpr uint64_t na_round(uint64_t b) { return (b + 255u) / 256u * 256u; }
+constexpr uint64_t NOALLOC_BYTES =
+    8 * na_round(16ull * NOALLOC_SLOTS) + na_round(16ull * NOALLOC_SLOTS * N_SLOTS) + na_round(16ull * NOALLOC_SLOTS) +
+    na_round(4ull * NOALLOC_SLOTS) + 2 * na_round(4ull * NOALLOC_SLOTS) + na_round(16ull * NOALLOC_SLOTS) +
+    na_round(8ull * NOALLOC_SLOTS) + 2 * na_round(16ull * NOALLOC_SHADOW) + na_round(4ull * NOALLOC_SHADOW) +
+    na_round(4ull * (MAX_DEPTH * CNT_STRIDE + CNT_STRIDE)) + na_round(8ull * T_COUNT);
+static_assert(NOALLOC_BYTES < (32ull << 20), "the no-allocation scratch stays under 32 MiB");
+
+static __device__ __align__(256) uint8_t g_noalloc_scratch[NOALLOC_BYTES];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+uint8_t* g_noalloc_ptr[256] = {nullptr};  // the array's device address, per device ordinal
+
+int na_fail(char* err, size_t err_len, int code, const std::string& msg) {
+    if (err && err_len) std::snprintf(err, err_len, "%s", msg.c_str());
+    return code;
+}
+
+// Once per device, with it current: the array's device address (in host code its name is only a stand-in for it)
+// and the sampler's tables.
+int noalloc_setup(int dev, char* err, size_t err_len) {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (dev < 0 || dev >= 256) return na_fail(err, err_len, TRT_EINVAL, "device ordinal out of range");
+    if (g_noalloc_ptr[dev]) return TRT_OK;
+    void* ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess) return na_fail(err, err_len, TRT_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    uint32_t t[3][16], bytes[3][2][256];
+    sobol_directions(t);
+    for (int d = 0; d < 3; ++d)
+        for (int half = 0; half < 2; ++half)
+            for (uint32_t b = 0; b < 256; ++b) {
+                uint32_t r = 0;
+                for (int i = 0; i < 8; ++i)
+                    if (b & (0x80u >> i)) r ^= t[d][half * 8 + i];
+                bytes[d][half][b] = r;
+            }
+    e = cudaMemcpyToSymbol(g_sobol_bytes, bytes, sizeof(bytes));
+    if (e != cudaSuccess) return na_fail(err, err_len, TRT_ECUDA, std::string("sampler tables: ") + cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = (uint8_t*)ptr;
+    return TRT_OK;
+}
+
+}  // namespace
+
+
 extern "C" {
 
 int trt_create(const trt_options* opts, trt_ctx** out) {
@@ -1048,6 +1106,126 @@ int trt_timer_stop(trt_ctx* c, float* ms) {
 int trt_synchronize(trt_ctx* c) {
     if (!c) return TRT_EINVAL;
     TRT_CUDA(c, cudaStreamSynchronize(c->stream));
+    return TRT_OK;
+}
+
+int trt_render_noalloc(const trt_scene_desc* dev, const uint32_t params[TRT_PARAMS_WORDS], uint32_t first_sample,
+                       uint32_t spp, uint32_t flags, float* accum_device, void* stream, char* err, size_t err_len) {
+    if (err && err_len) err[0] = 0;
+    if (!dev || !params || !accum_device) return na_fail(err, err_len, TRT_EINVAL, "a null argument");
+    if (flags & ~TRT_RENDER_ACCUMULATE) return na_fail(err, err_len, TRT_EINVAL, "only TRT_RENDER_ACCUMULATE is taken here");
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return na_fail(err, err_len, TRT_ECUDA, cudaGetErrorString(e));
+    int rc = noalloc_setup(device, err, err_len);
+    if (rc) return rc;
+    Params P;
+    std::memcpy(P.w, params, sizeof(P.w));
+    // The same checks as trt_render's, against the caller's buffers.
+    const uint64_t nb[5] = {dev->vertices_bytes, dev->leaves_bytes, dev->nodes_bytes, dev->tables_bytes, dev->words_bytes};
+    const void* ptrs[5] = {dev->vertices, dev->leaves, dev->nodes, dev->tables, dev->words};
+    const uint64_t unit[5] = {48, 48, 32, 16, 4};
+    for (int k = 0; k < 5; ++k)
+        if (!ptrs[k] || nb[k] == 0 || nb[k] % unit[k] != 0)
+            return na_fail(err, err_len, TRT_EINVAL, "scene buffer " + std::to_string(k) + ": no data, or not whole records");
+    if (!dev->env_half || dev->env_w == 0 || dev->env_h == 0) return na_fail(err, err_len, TRT_EINVAL, "no environment texels");
+    for (int k = 0; k < 12; ++k)
+        if (P.w[P_TABLE_FIRST + k] > nb[3] / 16) return na_fail(err, err_len, TRT_EINVAL, "Params.table_first names a vec4 past the tables");
+    for (int k = 0; k < 5; ++k)
+        if (P.w[P_WORD_FIRST + k] > nb[4] / 4) return na_fail(err, err_len, TRT_EINVAL, "Params.word_first names a word past the words");
+    uint32_t w = P.w[P_SIZE], h = P.w[P_SIZE + 1];
+    if (w == 0 || h == 0) return na_fail(err, err_len, TRT_EINVAL, "Params.size: an empty image");
+    uint32_t n_idx = ((w + 7u) / 8u) * ((h + 3u) / 4u) * 32u;
+    if (n_idx > NOALLOC_SLOTS)
+        return na_fail(err, err_len, TRT_EINVAL, "image too large for the no-allocation render: " + std::to_string(w) + " x " +
+                       std::to_string(h) + " needs " + std::to_string(n_idx) + " path slots (8 x 4 tiles), the most is " +
+                       std::to_string(NOALLOC_SLOTS) + " (256 x 256)");
+    if (P.w[P_COUNTS + 2] >= MAX_DEPTH - 1) return na_fail(err, err_len, TRT_EINVAL, "Params.counts.z (max bounces) must be below 63");
+    if (P.w[P_COUNTS2] > MAX_DIR_LIGHTS) return na_fail(err, err_len, TRT_EINVAL, "more than 4 directional lights");
+    if (P.w[P_COUNTS] != P.w[P_COUNTS2]) return na_fail(err, err_len, TRT_EINVAL, "local lights are not part of this pass");
+    if (P.w[P_MOTION + 3] > 0 && (uint64_t)P.w[P_MOTION + 2] >= nb[2] / 32)
+        return na_fail(err, err_len, TRT_EINVAL, "Params.motion.z names a node past the nodes");
+    if (P.w[P_ENV] == 0x3f800000u && ((uint32_t)bf(P.w[P_ENV + 1]) != dev->env_w || (uint32_t)bf(P.w[P_ENV + 2]) != dev->env_h))
+        return na_fail(err, err_len, TRT_EINVAL, "Params.env's size is not the environment's");
+    cudaStream_t st = (cudaStream_t)stream;
+    uint32_t K = std::max(1u, std::min(spp, NOALLOC_SLOTS / n_idx));
+    uint32_t slots = n_idx * K;
+    // The array's parts, as ensure_work lays out an allocation.
+    uint8_t* b = g_noalloc_ptr[device];
+    uint64_t at = 0;
+    auto take = [&](uint64_t bytes) { uint8_t* p = b + at; at += na_round(bytes); return p; };
+    PathBufs B;
+    B.o = (float4*)take(16ull * NOALLOC_SLOTS);
+    B.d = (float4*)take(16ull * NOALLOC_SLOTS);
+    B.thr = (float4*)take(16ull * NOALLOC_SLOTS);
+    B.rad = (float4*)take(16ull * NOALLOC_SLOTS);
+    B.alb = (float4*)take(16ull * NOALLOC_SLOTS);
+    B.nrm = (float4*)take(16ull * NOALLOC_SLOTS);
+    B.mis_x = (float4*)take(16ull * NOALLOC_SLOTS);
+    B.mis_n = (float4*)take(16ull * NOALLOC_SLOTS);
+    B.nee = (float4*)take(16ull * NOALLOC_SLOTS * N_SLOTS);
+    B.nee_thr = (float4*)take(16ull * NOALLOC_SLOTS);
+    B.vis = (uint32_t*)take(4ull * NOALLOC_SLOTS);
+    B.n = NOALLOC_SLOTS;
+    Queues Q;
+    Q.q[0] = (uint32_t*)take(4ull * NOALLOC_SLOTS);
+    Q.q[1] = (uint32_t*)take(4ull * NOALLOC_SLOTS);
+    Q.hit_a = (float4*)take(16ull * NOALLOC_SLOTS);
+    Q.hit_b = (uint2*)take(8ull * NOALLOC_SLOTS);
+    Q.so = (float4*)take(16ull * NOALLOC_SHADOW);
+    Q.sd = (float4*)take(16ull * NOALLOC_SHADOW);
+    Q.sp = (uint32_t*)take(4ull * NOALLOC_SHADOW);
+    uint64_t cnt_bytes = 4ull * (MAX_DEPTH * CNT_STRIDE + CNT_STRIDE);
+    Q.cnt = (uint32_t*)take(cnt_bytes);
+    Q.totals = (unsigned long long*)take(8ull * T_COUNT);
+    uint32_t n_dir = P.w[P_COUNTS2];
+    uint32_t caps[3] = {slots * std::max(1u, n_dir), slots, slots};
+    Q.shadow_cap = caps[0] + caps[1] + caps[2];
+    Q.class_base[0] = 0;
+    Q.class_base[1] = caps[0];
+    Q.class_base[2] = caps[0] + caps[1];
+    for (int k = 0; k < 3; ++k) Q.class_cap[k] = caps[k];
+    DScene S;
+    S.vertices = (const float4*)dev->vertices;
+    S.leaves = (const float4*)dev->leaves;
+    S.nodes = (const uint4*)dev->nodes;
+    S.tables = (const uint4*)dev->tables;
+    S.words = (const uint32_t*)dev->words;
+    S.env = (const ushort4*)dev->env_half;
+    S.env_w = dev->env_w;
+    S.env_h = dev->env_h;
+    S.n_nodes = nb[2] / 32;
+    S.n_tris = nb[1] / 48;
+    S.n_table_vec4 = nb[3] / 16;
+    S.n_words = nb[4] / 4;
+    Walk wk{S, WideView{}, P.w[P_MOTION + 2], P.w[P_MOTION + 3]};
+    int sms = 0;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) return na_fail(err, err_len, TRT_ECUDA, cudaGetErrorString(e));
+    const int blk = 128;
+    int g_ext = grid_for((const void*)k_extend<false, false>, blk, sms);
+    int g_sha = grid_for((const void*)k_shadow<false, false>, blk, sms);
+    uint32_t last = P.w[P_COUNTS + 2];
+    // What must start at zero: the accum (unless accumulating), the totals, each wave's counters.
+    if (!(flags & TRT_RENDER_ACCUMULATE)) e = cudaMemsetAsync(accum_device, 0, 80ull * w * h, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(Q.totals, 0, 8ull * T_COUNT, st);
+    for (uint32_t s0 = 0; s0 < spp && e == cudaSuccess; s0 += K) {
+        uint32_t k = std::min(K, spp - s0);
+        e = cudaMemsetAsync(Q.cnt, 0, cnt_bytes, st);
+        if (e != cudaSuccess) break;
+        uint32_t n = n_idx * k;
+        k_raygen<<<(n + blk - 1) / blk, blk, 0, st>>>(P, B, Q, first_sample + s0, n_idx, k);
+        for (uint32_t depth = 0; depth <= last; ++depth) {
+            k_extend<false, false><<<g_ext, blk, 0, st>>>(P, wk, B, Q, depth);
+            k_shade<<<(n + blk - 1) / blk, blk, 0, st>>>(P, S, B, Q, depth);
+            k_shadow<false, false><<<g_sha, blk, 0, st>>>(P, wk, B, Q, depth);
+            k_resolve<<<(n + blk - 1) / blk, blk, 0, st>>>(B, Q, depth, bf(P.w[P_MISC]));
+        }
+        k_accumulate<<<(n_idx + blk - 1) / blk, blk, 0, st>>>(P, B, (float4*)accum_device, n_idx, k);
+        k_tally<<<1, 32, 0, st>>>(Q, last + 1, w * h * k);
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) return na_fail(err, err_len, TRT_ECUDA, cudaGetErrorString(e));
     return TRT_OK;
 }
 
