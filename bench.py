@@ -44,6 +44,26 @@ def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
+def rank_frames(rank: int, world: int, warmup: int, steps: int, frames: int = FRAMES):
+    """The frames of the spline a rank renders: warm-up frames, then timed frames, interleaved across ranks so that
+    the ranks' timed frames are disjoint (weak scaling: every rank renders `steps` frames)."""
+    warm = [(rank + world * i) % frames for i in range(warmup)]
+    timed = [(rank + world * (warmup + i)) % frames for i in range(steps)]
+    return warm, timed
+
+
+def reduce_over_ranks(dist, ms: float, e2e_ms: float, rays: float, device=None):
+    """The job's time is the slowest rank's (max), its rays every rank's (sum)."""
+    if dist is None:
+        return ms, e2e_ms, rays
+    import torch
+    t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    r = torch.tensor([rays], dtype=torch.float64, device=device)
+    dist.all_reduce(r, op=dist.ReduceOp.SUM)
+    return float(t[0]), float(t[1]), float(r[0])
+
+
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -221,8 +241,7 @@ def main():
     name, sms = gpu.device_info()
     S = gpu.upload(P)
     flags = N.TRT_RENDER_WIDE if args.walk == "wide" else 0
-    frames = [(rank + world * (args.warmup + i)) % FRAMES for i in range(args.steps)]
-    warm_frames = [(rank + world * i) % FRAMES for i in range(args.warmup)]
+    warm_frames, frames = rank_frames(rank, world, args.warmup, args.steps)
     params = {f: frame_params(P, f) for f in set(frames + warm_frames)}
 
     def barrier():
@@ -279,15 +298,7 @@ def main():
     ext_bytes = (cnt["node_visits"] * NODE_BYTES + cnt["tri_tests"] * LEAF_BYTES + cnt["unit_entries"] * UNIT_BYTES)
     ext_bytes_per_launch = ext_bytes / max(1, cnt["extend_launches"])
 
-    if dist:
-        t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_ms = float(t[0]), float(t[1])
-        r = torch.tensor([float(rays)], dtype=torch.float64, device="cuda")
-        dist.all_reduce(r, op=dist.ReduceOp.SUM)
-        rays_all = float(r[0])
-    else:
-        rays_all = float(rays)
+    ms, e2e_ms, rays_all = reduce_over_ranks(dist, ms, e2e_ms, float(rays), device="cuda")
 
     peak, peak_kind = measured_peaks()
     achieved = ext_bytes_per_launch / (ext_avg_ms * 1e-3) / 1e9 if ext_avg_ms > 0 else None
