@@ -215,6 +215,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--walk", default="binary", choices=["binary", "wide"],
                     help="the reference's binary trees (fastest measured here) or the 8-wide quantised BVH")
+    ap.add_argument("--sort", default="hits",
+                    help="coherence sorts on the device: 'none', or a comma list of rays, hits, shadows "
+                         "(hits by material is the pass's default; the other two measured slower here)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -241,6 +244,10 @@ def main():
     name, sms = gpu.device_info()
     S = gpu.upload(P)
     flags = N.TRT_RENDER_WIDE if args.walk == "wide" else 0
+    sorts = [] if args.sort == "none" else args.sort.split(",")
+    if "hits" not in sorts:
+        flags |= N.TRT_RENDER_UNSORTED_HITS
+    flags |= (N.TRT_RENDER_SORT_RAYS if "rays" in sorts else 0) | (N.TRT_RENDER_SORT_SHADOWS if "shadows" in sorts else 0)
     warm_frames, frames = rank_frames(rank, world, args.warmup, args.steps)
     params = {f: frame_params(P, f) for f in set(frames + warm_frames)}
 
@@ -307,7 +314,7 @@ def main():
         "metric": METRIC, "value": rays_all / (ms * 1e-3) / 1e6, "unit": "Mrays/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "frames_per_rank": args.steps, "walk": args.walk,
+        "config": {"workload": WORKLOAD, "frames_per_rank": args.steps, "walk": args.walk, "sort": args.sort,
                    "l2": "inputs larger than L2: 221 MB of scene buffers, each step a new camera along the spline",
                    "device": name, "sms": sms, "parallelism": f"replicas x{world}, frames split across ranks"},
         "e2e": {"value": rays_all / (e2e_ms * 1e-3) / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": 624,
@@ -322,7 +329,7 @@ def main():
         "rays_per_path": rays / max(1, tot["paths"]),
         "paths_per_s": tot["paths"] * world / (ms * 1e-3),
         "stage_ms_per_step": {"extend": tot["extend_ms"] / args.steps, "shadow": tot["shadow_ms"] / args.steps,
-                              "shade": tot["shade_ms"] / args.steps},
+                              "shade": tot["shade_ms"] / args.steps, "sort": tot["sort_ms"] / args.steps},
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         v, cores, sample = cpu_sample(P, frames[:4], 20.0)

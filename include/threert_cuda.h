@@ -70,6 +70,7 @@ typedef struct {
     double extend_ms, shadow_ms, shade_ms;          /* with trt_scene_set_profiling on: per-stage device time */
     uint64_t extend_launches, shadow_launches;
     uint64_t guard_trips;
+    double sort_ms;                                 /* with profiling on: the coherence sorts' device time */
 } trt_totals;
 
 /* One ray for trt_trace: origin, tmax, direction, mode (0 closest, 1 shadow casters, 2 any surface). */
@@ -80,6 +81,13 @@ typedef struct { float t; uint32_t tri; float u; float v; uint32_t inst; uint32_
 #define TRT_RENDER_ACCUMULATE 1u /* add to accum instead of clearing it first (resume at first_sample) */
 #define TRT_RENDER_COUNT      2u /* also count node visits, triangle tests and unit entries (a slower walk) */
 #define TRT_RENDER_WIDE       4u /* walk the 8-wide quantised BVH instead of the reference's binary trees */
+/* Coherence sorts on the device, per depth; the image does not depend on them, bit for bit. Hits are sorted by
+ * material before shading unless this flag is given (the sort pays for itself on the city scene): */
+#define TRT_RENDER_UNSORTED_HITS 16u
+/* Optional, measured slower on the city scene: secondary rays by (queue chunk, direction octant) before the
+ * closest-hit walk, shadow rays by (position chunk, direction octant) in each light class before the shadow walk. */
+#define TRT_RENDER_SORT_RAYS      8u
+#define TRT_RENDER_SORT_SHADOWS  32u
 
 int trt_create(const trt_options* opts, trt_ctx** out);
 /* Frees the context and every scene still uploaded through it (their handles are then invalid). */

@@ -96,6 +96,22 @@ def test_resume_by_sample_range(gpu):
     assert np.array_equal(a8, a44)
 
 
+SORTS = N.TRT_RENDER_SORT_RAYS | N.TRT_RENDER_SORT_SHADOWS
+
+
+@pytest.mark.parametrize("walk", [0, N.TRT_RENDER_WIDE])
+@pytest.mark.parametrize("sorts", [N.TRT_RENDER_SORT_RAYS, N.TRT_RENDER_SORT_SHADOWS, SORTS])
+@pytest.mark.parametrize("make,spp", [(small_city, 3), (lambda: scenes.cornell(64, 64), 8)])
+def test_sorted_queues_render_the_same_image(gpu, make, spp, sorts, walk):
+    """A path's state, hit and random numbers are its own, so the coherence sorts change no bit of the image."""
+    P = prep.prepare(make())
+    S = gpu.upload(P)
+    plain, st0 = S.render_raw(P.params, spp, flags=walk | N.TRT_RENDER_UNSORTED_HITS)
+    got, st1 = S.render_raw(P.params, spp, flags=walk | sorts)  # hits sorted by material, the default
+    assert np.array_equal(plain, got)
+    assert (st0.closest_rays, st0.shadow_rays, st0.paths) == (st1.closest_rays, st1.shadow_rays, st1.paths)
+
+
 def test_counts_match_the_oracles_rays(gpu):
     P = prep.prepare(small_city())
     S = gpu.upload(P)

@@ -19,6 +19,9 @@ PIXEL_FLOATS = 20
 TRT_RENDER_ACCUMULATE = 1
 TRT_RENDER_COUNT = 2
 TRT_RENDER_WIDE = 4
+TRT_RENDER_SORT_RAYS = 8
+TRT_RENDER_UNSORTED_HITS = 16
+TRT_RENDER_SORT_SHADOWS = 32
 
 ERRORS = {1: "TRT_EINVAL", 2: "TRT_ECUDA", 3: "TRT_EGUARD"}
 
@@ -96,7 +99,7 @@ class Totals(C.Structure):
                 ("node_visits", u64), ("tri_tests", u64), ("unit_entries", u64), ("shadow_node_visits", u64),
                 ("shadow_tri_tests", u64), ("shadow_unit_entries", u64), ("extend_ms", C.c_double),
                 ("shadow_ms", C.c_double), ("shade_ms", C.c_double), ("extend_launches", u64),
-                ("shadow_launches", u64), ("guard_trips", u64)]
+                ("shadow_launches", u64), ("guard_trips", u64), ("sort_ms", C.c_double)]
 
 
 class Ray(C.Structure):

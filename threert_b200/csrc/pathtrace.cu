@@ -51,7 +51,8 @@ struct PathBufs {
 };
 struct Queues {
     uint32_t* q[2];       // path queues (extend inputs), alternating by depth
-    float4* hit_a;        // t, u, v, tri (bits) per queue position
+    uint32_t* qx;         // a depth's queue sorted (a third buffer, so the two above stay the raw queues)
+    float4* hit_a;        // t, u, v, tri (bits) per path
     uint2* hit_b;         // inst, part
     float4* so;           // shadow rays: origin, tmax
     float4* sd;           // direction, mode (bits)
@@ -59,6 +60,11 @@ struct Queues {
     uint32_t* cnt;        // per depth, CNT_STRIDE words: queue size, -, extend fetch, shadow fetch, then the shadow
                           // rays of each light class (sun, emitter, sky)
     unsigned long long* totals;
+    uint2* sort_kr;       // the coherence sort: each item's key and its rank among the key's items
+    uint32_t* sort_hist;  // SORT_BINS counts (zero between sorts)
+    uint32_t* sort_start; // SORT_BINS starts
+    uint32_t* sort_done;  // blocks of the count kernel that have finished (zero between sorts)
+    uint32_t* perm;       // the shadow rays' order after their sort: perm[j] is the j-th ray's slot in so / sd / sp
     uint32_t shadow_cap;  // the three classes' regions together
     uint32_t class_base[3], class_cap[3];  // each class's region of so / sd / sp
 };
@@ -171,10 +177,10 @@ __device__ __forceinline__ Hit walk(const Walk& wk, const Sections& X, V3 o, V3 
 }
 
 template <bool COUNT, bool WIDE>
-__global__ void __launch_bounds__(128, 6) k_extend(Params P, Walk wk, PathBufs B, Queues Q, uint32_t depth) {
+__global__ void __launch_bounds__(128, 6) k_extend(Params P, Walk wk, PathBufs B, Queues Q, uint32_t depth,
+                                                   const uint32_t* __restrict__ queue) {
     Sections X(P);
     uint32_t* cnt = Q.cnt + depth * CNT_STRIDE;
-    const uint32_t* queue = Q.q[depth & 1u];
     uint32_t n = *(volatile uint32_t*)&cnt[0];
     WalkCount wc{0, 0, 0};
     unsigned long long guard_trips = 0;
@@ -187,8 +193,8 @@ __global__ void __launch_bounds__(128, 6) k_extend(Params P, Walk wk, PathBufs B
             bool guard = false;
             Hit h = walk<COUNT, WIDE>(wk, X, xyz(o), xyz(d), INF, TRACE_CLOSEST, &wc, &guard);
             if (guard) guard_trips++;
-            Q.hit_a[i] = make_float4(h.t, h.u, h.v, bf(h.tri));
-            Q.hit_b[i] = make_uint2(h.inst, h.part);
+            Q.hit_a[p] = make_float4(h.t, h.u, h.v, bf(h.tri));
+            Q.hit_b[p] = make_uint2(h.inst, h.part);
         }
     }
     if (COUNT) {
@@ -199,8 +205,14 @@ __global__ void __launch_bounds__(128, 6) k_extend(Params P, Walk wk, PathBufs B
     warp_add64(&Q.totals[T_GUARD], guard_trips);
 }
 
+// The j-th shadow ray of a depth, counting the classes' regions one after another.
+__device__ __forceinline__ uint32_t shadow_slot(const Queues& Q, uint32_t j, uint32_t n0, uint32_t n1) {
+    return j < n0 ? Q.class_base[0] + j : (j < n0 + n1 ? Q.class_base[1] + (j - n0) : Q.class_base[2] + (j - n0 - n1));
+}
+
 template <bool COUNT, bool WIDE>
-__global__ void __launch_bounds__(128, 6) k_shadow(Params P, Walk wk, PathBufs B, Queues Q, uint32_t depth) {
+__global__ void __launch_bounds__(128, 6) k_shadow(Params P, Walk wk, PathBufs B, Queues Q, uint32_t depth,
+                                                   const uint32_t* __restrict__ perm) {
     Sections X(P);
     uint32_t* cnt = Q.cnt + depth * CNT_STRIDE;
     uint32_t n0 = min(*(volatile uint32_t*)&cnt[4], Q.class_cap[0]);
@@ -213,9 +225,8 @@ __global__ void __launch_bounds__(128, 6) k_shadow(Params P, Walk wk, PathBufs B
         uint32_t j = warp_fetch(&cnt[3]);
         if (__shfl_sync(0xffffffffu, j, 0) >= n) break;
         if (j < n) {
-            // The classes' regions one after another: the j-th ray of the three.
-            uint32_t i = j < n0 ? Q.class_base[0] + j
-                                : (j < n0 + n1 ? Q.class_base[1] + (j - n0) : Q.class_base[2] + (j - n0 - n1));
+            // The classes' regions one after another: the j-th ray of the three (or of their sorted order).
+            uint32_t i = perm ? perm[j] : shadow_slot(Q, j, n0, n1);
             float4 o = Q.so[i], d = Q.sd[i];
             bool guard = false;
             Hit h = walk<COUNT, WIDE>(wk, X, xyz(o), xyz(d), o.w, bu(d.w), &wc, &guard);
@@ -245,10 +256,10 @@ __device__ __forceinline__ void push_shadow(const Queues& Q, uint32_t* cnt, uint
 }
 
 // One path vertex: pathtrace.wgsl:4176-4477 from the hit on (the trace itself is k_extend's).
-__global__ void __launch_bounds__(128, 4) k_shade(Params P, DScene S, PathBufs B, Queues Q, uint32_t depth) {
+__global__ void __launch_bounds__(128, 4) k_shade(Params P, DScene S, PathBufs B, Queues Q, uint32_t depth,
+                                                  const uint32_t* __restrict__ queue, uint32_t* __restrict__ next) {
     Sections X(P);
     uint32_t* cnt = Q.cnt + depth * CNT_STRIDE;
-    const uint32_t* queue = Q.q[depth & 1u];
     uint32_t n = cnt[0];
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     bool live = false;
@@ -265,8 +276,8 @@ __global__ void __launch_bounds__(128, 4) k_shade(Params P, DScene S, PathBufs B
         float clamp_v = pf(P, P_MISC);
         uint32_t last = P.w[P_COUNTS + 2];
         bool straight = (flags & F_STRAIGHT) != 0;
-        float4 ha = Q.hit_a[i];
-        uint2 hb = Q.hit_b[i];
+        float4 ha = Q.hit_a[p];
+        uint2 hb = Q.hit_b[p];
         Hit hit{ha.x, bu(ha.w), ha.y, ha.z, hb.x, hb.y};
         uint32_t nee_mask = 0, vis = 0;
         if (hit.tri == MISS) {
@@ -412,16 +423,16 @@ __global__ void __launch_bounds__(128, 4) k_shade(Params P, DScene S, PathBufs B
         B.rad[p] = f4(radiance, bf(sample));
     }
     uint32_t at = warp_append(&Q.cnt[(depth + 1u) * CNT_STRIDE], live);
-    if (live && depth + 1u < MAX_DEPTH) Q.q[(depth + 1u) & 1u][at] = p;
+    if (live && depth + 1u < MAX_DEPTH) next[at] = p;
 }
 
 // The vertex's direct light from its visible slots (pathtrace.wgsl:4398-4403), and a finished path's last fixes
 // (4494-4497).
-__global__ void k_resolve(PathBufs B, Queues Q, uint32_t depth, float clamp_v) {
+__global__ void k_resolve(PathBufs B, Queues Q, uint32_t depth, float clamp_v, const uint32_t* __restrict__ queue) {
     uint32_t n = Q.cnt[depth * CNT_STRIDE];
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    uint32_t p = Q.q[depth & 1u][i];
+    uint32_t p = queue[i];
     float4 nt = B.nee_thr[p];
     uint32_t m = bu(nt.w);
     float4 rad4 = B.rad[p];
@@ -446,6 +457,136 @@ __global__ void k_resolve(PathBufs B, Queues Q, uint32_t depth, float clamp_v) {
         if (non_finite3(xyz(nn))) B.nrm[p] = f4(V3{0.0f, 1.0f, 0.0f}, 0.0f);
     }
     B.rad[p] = f4(radiance, rad4.w);
+}
+
+// ---- coherence sorts ----
+// A counting sort of a depth's queue by a 12-bit key, on the device (no count reaches the host): each block counts
+// its items' keys in shared memory and takes its range of each key with one global atomic; the last block to finish
+// turns the global counts into starts (and zeroes them for the next sort); k_sort_scatter moves each item to its key's
+// start plus its rank. Order within a key is the blocks' arrival order and may differ run to run: nothing depends on
+// it, since a path's state, hit and random numbers belong to the path, not to its queue position.
+//   SORT_RAYS: the extend queue by (queue chunk, direction octant): a warp's rays start near one another (the chunk)
+//     and point the same way, so they walk the same nodes in the same order.
+//   SORT_HITS (on unless TRT_RENDER_UNSORTED_HITS): the shade queue by material, misses first: a warp then reads one
+//     material record and takes one set of branches, and the next depth's queue, appended in this order, starts its
+//     rays from one mesh.
+//   SORT_SHADOWS: the shadow rays by (position chunk, direction octant) in each light class.
+constexpr uint32_t SORT_BINS = 4096u, SORT_THREADS = 256u, SORT_PER_THREAD = 8u;
+constexpr uint32_t SORT_ITEMS = SORT_THREADS * SORT_PER_THREAD;
+enum : uint32_t { SORT_RAYS = 0u, SORT_HITS = 1u, SORT_SHADOWS = 2u };
+
+__device__ __forceinline__ uint32_t octant(float4 d) {
+    return (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
+}
+
+// The items a sort orders: the depth's queue, or its shadow rays (n0, n1: the first two classes' counts).
+template <uint32_t KIND>
+__device__ __forceinline__ uint32_t sort_count(const Queues& Q, uint32_t depth, uint32_t& n0, uint32_t& n1) {
+    const uint32_t* cnt = Q.cnt + depth * CNT_STRIDE;
+    if (KIND != SORT_SHADOWS) return *(volatile const uint32_t*)&cnt[0];
+    n0 = min(*(volatile const uint32_t*)&cnt[4], Q.class_cap[0]);
+    n1 = min(*(volatile const uint32_t*)&cnt[5], Q.class_cap[1]);
+    return n0 + n1 + min(*(volatile const uint32_t*)&cnt[6], Q.class_cap[2]);
+}
+template <uint32_t KIND>
+__device__ __forceinline__ uint32_t sort_item(const Queues& Q, const uint32_t* in, uint32_t j, uint32_t n0, uint32_t n1) {
+    return KIND == SORT_SHADOWS ? shadow_slot(Q, j, n0, n1) : in[j];
+}
+template <uint32_t KIND>
+__device__ __forceinline__ uint32_t sort_key(const DScene& S, const Sections& X, const PathBufs& B, const Queues& Q,
+                                             uint32_t j, uint32_t item, uint32_t shift) {
+    if (KIND == SORT_RAYS) return ((j >> shift) << 3) | octant(B.d[item]);
+    if (KIND == SORT_SHADOWS) return ((j >> shift) << 3) | octant(Q.sd[item]);
+    if (bu(Q.hit_a[item].w) == MISS) return 0u;
+    uint2 hb = Q.hit_b[item];
+    uint32_t mat = 0;
+    if (hb.x != NO_INST) {
+        uint32_t rows = tabu(S, X.t_instances + hb.x * 10u + 6u).w;
+        mat = __ldg(S.words + X.w_rows + (rows + hb.y) * 4u) & ROW_MATERIAL;
+    }
+    return 1u + mat % (SORT_BINS - 1u);
+}
+
+template <uint32_t KIND>
+__global__ void __launch_bounds__(SORT_THREADS) k_sort_count(Params P, DScene S, PathBufs B, Queues Q,
+                                                            const uint32_t* __restrict__ in, uint32_t depth,
+                                                            uint32_t shift) {
+    __shared__ uint32_t h[SORT_BINS];
+    __shared__ uint32_t warp_sums[SORT_THREADS / 32u];
+    __shared__ bool last;
+    Sections X(P);
+    uint32_t n0 = 0, n1 = 0;
+    uint32_t n = sort_count<KIND>(Q, depth, n0, n1);
+    uint32_t base = blockIdx.x * SORT_ITEMS, tid = threadIdx.x;
+    if (base < n) {
+        for (uint32_t b = tid; b < SORT_BINS; b += SORT_THREADS) h[b] = 0u;
+        __syncthreads();
+        uint32_t key[SORT_PER_THREAD], loc[SORT_PER_THREAD];
+        // The keys first, then the counts: the items' loads overlap instead of waiting behind each atomic.
+#pragma unroll
+        for (uint32_t k = 0; k < SORT_PER_THREAD; ++k) {
+            uint32_t j = base + k * SORT_THREADS + tid;
+            key[k] = j < n ? sort_key<KIND>(S, X, B, Q, j, sort_item<KIND>(Q, in, j, n0, n1), shift) & (SORT_BINS - 1u) : 0u;
+        }
+#pragma unroll
+        for (uint32_t k = 0; k < SORT_PER_THREAD; ++k) {
+            uint32_t j = base + k * SORT_THREADS + tid;
+            loc[k] = j < n ? atomicAdd(&h[key[k]], 1u) : 0u;
+        }
+        __syncthreads();
+        for (uint32_t b = tid; b < SORT_BINS; b += SORT_THREADS) {
+            uint32_t c = h[b];
+            if (c) h[b] = atomicAdd(&Q.sort_hist[b], c);
+        }
+        __syncthreads();
+#pragma unroll
+        for (uint32_t k = 0; k < SORT_PER_THREAD; ++k) {
+            uint32_t j = base + k * SORT_THREADS + tid;
+            if (j < n) Q.sort_kr[j] = make_uint2(key[k], h[key[k]] + loc[k]);
+        }
+    }
+    // The last block to finish: the counts into starts, by one exclusive scan of SORT_BINS.
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) last = atomicAdd(Q.sort_done, 1u) == gridDim.x - 1u;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    constexpr uint32_t PER = SORT_BINS / SORT_THREADS;
+    uint32_t v[PER], sum = 0;
+#pragma unroll
+    for (uint32_t k = 0; k < PER; ++k) {
+        v[k] = *(volatile uint32_t*)&Q.sort_hist[tid * PER + k];
+        sum += v[k];
+    }
+    uint32_t lane = tid & 31u, warp = tid >> 5;
+    uint32_t incl = sum;
+#pragma unroll
+    for (uint32_t o = 1; o < 32; o <<= 1) {
+        uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31u) warp_sums[warp] = incl;
+    __syncthreads();
+    uint32_t run = incl - sum;
+    for (uint32_t w = 0; w < warp; ++w) run += warp_sums[w];
+#pragma unroll
+    for (uint32_t k = 0; k < PER; ++k) {
+        Q.sort_start[tid * PER + k] = run;
+        Q.sort_hist[tid * PER + k] = 0u;
+        run += v[k];
+    }
+    if (tid == 0) *Q.sort_done = 0u;
+}
+
+template <uint32_t KIND>
+__global__ void k_sort_scatter(Queues Q, const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint32_t depth) {
+    uint32_t n0 = 0, n1 = 0;
+    uint32_t n = sort_count<KIND>(Q, depth, n0, n1);
+    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    uint2 kr = Q.sort_kr[j];
+    out[Q.sort_start[kr.x] + kr.y] = sort_item<KIND>(Q, in, j, n0, n1);
 }
 
 // accum += each sample's path, in sample order (pathtrace.wgsl:4541-4557).
@@ -560,8 +701,8 @@ struct trt_scene {
     Queues Q{};
     unsigned long long* totals = nullptr;
     int profiling = 0;
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_extend, ev_shadow, ev_shade, ev_free;
-    double extend_ms = 0, shadow_ms = 0, shade_ms = 0;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_extend, ev_shadow, ev_shade, ev_sort, ev_free;
+    double extend_ms = 0, shadow_ms = 0, shade_ms = 0, sort_ms = 0;
     uint64_t extend_launches = 0, shadow_launches = 0, renders = 0, launches = 0;
 };
 
@@ -631,7 +772,9 @@ int ensure_work(trt_scene* s, uint32_t slots, uint32_t n_dir) {
                  o_nt = add(16ull * slots), o_vis = add(4ull * slots), o_q0 = add(4ull * slots), o_q1 = add(4ull * slots),
                  o_ha = add(16ull * slots), o_hb = add(8ull * slots), o_so = add(16ull * shadow_cap),
                  o_sd = add(16ull * shadow_cap), o_sp = add(4ull * shadow_cap),
-                 o_cnt = add(4ull * (MAX_DEPTH * CNT_STRIDE + CNT_STRIDE));
+                 o_cnt = add(4ull * (MAX_DEPTH * CNT_STRIDE + CNT_STRIDE)), o_qx = add(4ull * slots),
+                 o_kr = add(8ull * std::max(slots, shadow_cap)), o_hist = add(4ull * SORT_BINS),
+                 o_start = add(4ull * SORT_BINS), o_done = add(4ull), o_perm = add(4ull * shadow_cap);
         if (s->work) cudaFree(s->work);
         s->work = nullptr;
         TRT_CUDA(s->ctx, cudaMalloc(&s->work, need));
@@ -650,7 +793,16 @@ int ensure_work(trt_scene* s, uint32_t slots, uint32_t n_dir) {
         s->Q.sd = (float4*)(b + o_sd);
         s->Q.sp = (uint32_t*)(b + o_sp);
         s->Q.cnt = (uint32_t*)(b + o_cnt);
+        s->Q.qx = (uint32_t*)(b + o_qx);
+        s->Q.sort_kr = (uint2*)(b + o_kr);
+        s->Q.sort_hist = (uint32_t*)(b + o_hist);
+        s->Q.sort_start = (uint32_t*)(b + o_start);
+        s->Q.sort_done = (uint32_t*)(b + o_done);
+        s->Q.perm = (uint32_t*)(b + o_perm);
         s->Q.totals = s->totals;
+        // The sort's counts and its finished-block count start at zero (each sort leaves them so).
+        TRT_CUDA(s->ctx, cudaMemsetAsync(b + o_hist, 0, o_start - o_hist, s->ctx->stream));
+        TRT_CUDA(s->ctx, cudaMemsetAsync(b + o_done, 0, 4, s->ctx->stream));
     }
     s->Q.shadow_cap = shadow_cap;
     s->Q.class_base[0] = 0;
@@ -678,8 +830,24 @@ int grid_for(const void* fn, int block, int sm_count) {
     return std::max(1, per_sm) * sm_count;
 }
 
+// The smallest shift that maps positions below `cap` onto at most SORT_BINS / 8 chunks.
+uint32_t chunk_shift(uint32_t cap) {
+    uint32_t sh = 0;
+    while (cap > 0 && ((cap - 1u) >> sh) >= SORT_BINS / 8u) ++sh;
+    return sh;
+}
+
+template <uint32_t KIND>
+void launch_sort(trt_scene* s, const Params& P, const DScene& S, const uint32_t* in, uint32_t* out, uint32_t depth,
+                 uint32_t cap, cudaStream_t st) {
+    uint32_t shift = chunk_shift(cap);
+    k_sort_count<KIND><<<(cap + SORT_ITEMS - 1u) / SORT_ITEMS, SORT_THREADS, 0, st>>>(P, S, s->B, s->Q, in, depth, shift);
+    k_sort_scatter<KIND><<<(cap + 255u) / 256u, 256, 0, st>>>(s->Q, in, out, depth);
+    s->launches += 2;
+}
+
 template <bool COUNT, bool WIDE>
-int render_waves(trt_scene* s, const Params& P, uint32_t first_sample, uint32_t spp) {
+int render_waves(trt_scene* s, const Params& P, uint32_t first_sample, uint32_t spp, uint32_t flags) {
     trt_ctx* c = s->ctx;
     cudaStream_t st = c->stream;
     uint32_t w = P.w[P_SIZE], h = P.w[P_SIZE + 1];
@@ -692,10 +860,17 @@ int render_waves(trt_scene* s, const Params& P, uint32_t first_sample, uint32_t 
     DScene S = scene_view(s);
     Walk wk{S, s->wide.view(), P.w[P_MOTION + 2], P.w[P_MOTION + 3]};
     uint32_t last = P.w[P_COUNTS + 2];
+    bool sort_rays = (flags & TRT_RENDER_SORT_RAYS) != 0, sort_hits = (flags & TRT_RENDER_UNSORTED_HITS) == 0;
+    bool sort_shadows = (flags & TRT_RENDER_SORT_SHADOWS) != 0;
     const int blk = 128;
     int g_ext = grid_for((const void*)k_extend<COUNT, WIDE>, blk, c->sm_count);
     int g_sha = grid_for((const void*)k_shadow<COUNT, WIDE>, blk, c->sm_count);
     std::vector<uint32_t> host_cnt(MAX_DEPTH * CNT_STRIDE + CNT_STRIDE, 0);
+    auto mark = [&](std::vector<std::pair<cudaEvent_t, cudaEvent_t>>& v, bool begin) {
+        if (!s->profiling) return;
+        if (begin) { v.push_back(take_events(s)); cudaEventRecord(v.back().first, st); }
+        else cudaEventRecord(v.back().second, st);
+    };
     for (uint32_t s0 = 0; s0 < spp; s0 += K) {
         uint32_t k = std::min(K, spp - s0);
         TRT_CUDA(c, cudaMemcpyAsync(s->Q.cnt, host_cnt.data(), host_cnt.size() * 4, cudaMemcpyHostToDevice, st));
@@ -703,17 +878,40 @@ int render_waves(trt_scene* s, const Params& P, uint32_t first_sample, uint32_t 
         k_raygen<<<(n + blk - 1) / blk, blk, 0, st>>>(P, s->B, s->Q, first_sample + s0, n_idx, k);
         s->launches++;
         for (uint32_t depth = 0; depth <= last; ++depth) {
-            std::pair<cudaEvent_t, cudaEvent_t> e{};
-            if (s->profiling) { e = take_events(s); cudaEventRecord(e.first, st); }
-            k_extend<COUNT, WIDE><<<g_ext, blk, 0, st>>>(P, wk, s->B, s->Q, depth);
-            if (s->profiling) { cudaEventRecord(e.second, st); s->ev_extend.push_back(e); }
-            if (s->profiling) { e = take_events(s); cudaEventRecord(e.first, st); }
-            k_shade<<<(n + blk - 1) / blk, blk, 0, st>>>(P, S, s->B, s->Q, depth);
-            if (s->profiling) { cudaEventRecord(e.second, st); s->ev_shade.push_back(e); }
-            if (s->profiling) { e = take_events(s); cudaEventRecord(e.first, st); }
-            k_shadow<COUNT, WIDE><<<g_sha, blk, 0, st>>>(P, wk, s->B, s->Q, depth);
-            if (s->profiling) { cudaEventRecord(e.second, st); s->ev_shadow.push_back(e); }
-            k_resolve<<<(n + blk - 1) / blk, blk, 0, st>>>(s->B, s->Q, depth, bf(P.w[P_MISC]));
+            // The depth's queue (raw), the order extend walks it in, the order shade takes the hits in.
+            uint32_t* raw = s->Q.q[depth & 1u];
+            uint32_t* next = s->Q.q[(depth + 1u) & 1u];
+            uint32_t* ext_q = raw;
+            if (sort_rays && depth > 0u) {
+                mark(s->ev_sort, true);
+                launch_sort<SORT_RAYS>(s, P, S, raw, s->Q.qx, depth, n, st);
+                mark(s->ev_sort, false);
+                ext_q = s->Q.qx;
+            }
+            mark(s->ev_extend, true);
+            k_extend<COUNT, WIDE><<<g_ext, blk, 0, st>>>(P, wk, s->B, s->Q, depth, ext_q);
+            mark(s->ev_extend, false);
+            uint32_t* shade_q = ext_q;
+            if (sort_hits) {
+                shade_q = ext_q == raw ? s->Q.qx : raw;
+                mark(s->ev_sort, true);
+                launch_sort<SORT_HITS>(s, P, S, ext_q, shade_q, depth, n, st);
+                mark(s->ev_sort, false);
+            }
+            mark(s->ev_shade, true);
+            k_shade<<<(n + blk - 1) / blk, blk, 0, st>>>(P, S, s->B, s->Q, depth, shade_q, next);
+            mark(s->ev_shade, false);
+            const uint32_t* perm = nullptr;
+            if (sort_shadows) {
+                mark(s->ev_sort, true);
+                launch_sort<SORT_SHADOWS>(s, P, S, nullptr, s->Q.perm, depth, s->Q.shadow_cap, st);
+                mark(s->ev_sort, false);
+                perm = s->Q.perm;
+            }
+            mark(s->ev_shadow, true);
+            k_shadow<COUNT, WIDE><<<g_sha, blk, 0, st>>>(P, wk, s->B, s->Q, depth, perm);
+            mark(s->ev_shadow, false);
+            k_resolve<<<(n + blk - 1) / blk, blk, 0, st>>>(s->B, s->Q, depth, bf(P.w[P_MISC]), shade_q);
             s->launches += 4;
             s->extend_launches++;
             s->shadow_launches++;
@@ -898,7 +1096,7 @@ void trt_scene_free(trt_scene* s) {
     if (s->work) cudaFree(s->work);
     if (s->totals) cudaFree(s->totals);
     s->wide.release();
-    for (auto* v : {&s->ev_extend, &s->ev_shadow, &s->ev_shade, &s->ev_free})
+    for (auto* v : {&s->ev_extend, &s->ev_shadow, &s->ev_shade, &s->ev_sort, &s->ev_free})
         for (auto& e : *v) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
     delete s;
 }
@@ -945,8 +1143,8 @@ int trt_render(trt_scene* s, const uint32_t params[TRT_PARAMS_WORDS], uint32_t f
     bool count = (flags & TRT_RENDER_COUNT) != 0, binary = (flags & TRT_RENDER_WIDE) == 0;
     if (!binary && s->wide.ensure(params, s->host, c->stream) != 0) return fail(c, TRT_EINVAL, s->wide.error);
     if (spp > 0) {
-        if (count) rc = binary ? render_waves<true, false>(s, P, first_sample, spp) : render_waves<true, true>(s, P, first_sample, spp);
-        else rc = binary ? render_waves<false, false>(s, P, first_sample, spp) : render_waves<false, true>(s, P, first_sample, spp);
+        if (count) rc = binary ? render_waves<true, false>(s, P, first_sample, spp, flags) : render_waves<true, true>(s, P, first_sample, spp, flags);
+        else rc = binary ? render_waves<false, false>(s, P, first_sample, spp, flags) : render_waves<false, true>(s, P, first_sample, spp, flags);
         if (rc) return rc;
     }
     s->renders++;
@@ -1051,6 +1249,7 @@ int trt_scene_totals(trt_scene* s, trt_totals* out) {
     drain(s->ev_extend, s->extend_ms);
     drain(s->ev_shadow, s->shadow_ms);
     drain(s->ev_shade, s->shade_ms);
+    drain(s->ev_sort, s->sort_ms);
     out->closest_rays = t[T_CLOSEST];
     out->shadow_rays = t[T_SHADOW];
     out->paths = t[T_PATHS];
@@ -1066,6 +1265,7 @@ int trt_scene_totals(trt_scene* s, trt_totals* out) {
     out->extend_ms = s->extend_ms;
     out->shadow_ms = s->shadow_ms;
     out->shade_ms = s->shade_ms;
+    out->sort_ms = s->sort_ms;
     out->extend_launches = s->extend_launches;
     out->shadow_launches = s->shadow_launches;
     return TRT_OK;
@@ -1077,11 +1277,11 @@ void trt_scene_reset_totals(trt_scene* s) {
     cudaStreamSynchronize(s->ctx->stream);
     cudaMemsetAsync(s->totals, 0, sizeof(unsigned long long) * T_COUNT, s->ctx->stream);
     cudaStreamSynchronize(s->ctx->stream);
-    for (auto* v : {&s->ev_extend, &s->ev_shadow, &s->ev_shade}) {
+    for (auto* v : {&s->ev_extend, &s->ev_shadow, &s->ev_shade, &s->ev_sort}) {
         for (auto& e : *v) s->ev_free.push_back(e);
         v->clear();
     }
-    s->extend_ms = s->shadow_ms = s->shade_ms = 0;
+    s->extend_ms = s->shadow_ms = s->shade_ms = s->sort_ms = 0;
     s->extend_launches = s->shadow_launches = s->renders = s->launches = 0;
 }
 
@@ -1113,7 +1313,8 @@ int trt_render_noalloc(const trt_scene_desc* dev, const uint32_t params[TRT_PARA
                        uint32_t spp, uint32_t flags, float* accum_device, void* stream, char* err, size_t err_len) {
     if (err && err_len) err[0] = 0;
     if (!dev || !params || !accum_device) return na_fail(err, err_len, TRT_EINVAL, "a null argument");
-    if (flags & ~TRT_RENDER_ACCUMULATE) return na_fail(err, err_len, TRT_EINVAL, "only TRT_RENDER_ACCUMULATE is taken here");
+    if (flags & ~(TRT_RENDER_ACCUMULATE | TRT_RENDER_UNSORTED_HITS))
+        return na_fail(err, err_len, TRT_EINVAL, "only TRT_RENDER_ACCUMULATE is taken here (its hits are shaded unsorted)");
     int device = 0;
     cudaError_t e = cudaGetDevice(&device);
     if (e != cudaSuccess) return na_fail(err, err_len, TRT_ECUDA, cudaGetErrorString(e));
@@ -1216,10 +1417,11 @@ int trt_render_noalloc(const trt_scene_desc* dev, const uint32_t params[TRT_PARA
         uint32_t n = n_idx * k;
         k_raygen<<<(n + blk - 1) / blk, blk, 0, st>>>(P, B, Q, first_sample + s0, n_idx, k);
         for (uint32_t depth = 0; depth <= last; ++depth) {
-            k_extend<false, false><<<g_ext, blk, 0, st>>>(P, wk, B, Q, depth);
-            k_shade<<<(n + blk - 1) / blk, blk, 0, st>>>(P, S, B, Q, depth);
-            k_shadow<false, false><<<g_sha, blk, 0, st>>>(P, wk, B, Q, depth);
-            k_resolve<<<(n + blk - 1) / blk, blk, 0, st>>>(B, Q, depth, bf(P.w[P_MISC]));
+            uint32_t* queue = Q.q[depth & 1u];
+            k_extend<false, false><<<g_ext, blk, 0, st>>>(P, wk, B, Q, depth, queue);
+            k_shade<<<(n + blk - 1) / blk, blk, 0, st>>>(P, S, B, Q, depth, queue, Q.q[(depth + 1u) & 1u]);
+            k_shadow<false, false><<<g_sha, blk, 0, st>>>(P, wk, B, Q, depth, nullptr);
+            k_resolve<<<(n + blk - 1) / blk, blk, 0, st>>>(B, Q, depth, bf(P.w[P_MISC]), queue);
         }
         k_accumulate<<<(n_idx + blk - 1) / blk, blk, 0, st>>>(P, B, (float4*)accum_device, n_idx, k);
         k_tally<<<1, 32, 0, st>>>(Q, last + 1, w * h * k);
