@@ -104,6 +104,57 @@ void trt_scene_free(trt_scene* scene);
  * 4 words) from host memory: in-place record edits and refits (gpu.rs:4028 write_nodes). */
 int trt_scene_update(trt_scene* scene, uint32_t which, uint64_t offset, const void* src, uint64_t bytes);
 
+/* Copies bytes [offset, offset + bytes) of one of the scene's buffers (numbered as for trt_scene_update) to host
+ * memory: what a deformation wrote, for checks. */
+int trt_scene_read(trt_scene* scene, uint32_t which, uint64_t offset, void* dst, uint64_t bytes);
+
+/* ---- Scenes that move: the per-frame deformation, on the device ----
+ * The reference poses skinned meshes with two shaders (renderer/shaders/skin.wgsl, leaf_gather.wgsl), refits their
+ * mesh trees on the CPU (units.rs:251-275 refit, live/edits.rs:2395-2450) and builds the top tree on the CPU
+ * (units.rs:303-326 top_tree through Kept::top, units.rs:771-830; written by gpu.rs:4014 Gpu::retop). Here all of it
+ * runs on the scene's stream: skinning, leaf gather, a bottom-up refit of each deforming mesh's tree, the units' world
+ * boxes (units.rs:288-300 UnitBox::new) and the top tree built again over all units by the same binned SAH
+ * (units.rs:140-224 build_sah), laid out as that build lays it out.
+ *
+ * The units are the instances 0 .. Params.motion.w - 1 (one a top-tree leaf, as trt_prep_build lays scenes out) and
+ * the top tree's 2 * units - 1 nodes start at Params.motion.z. A unit's world box comes from its record in the tables
+ * (its world rows and its tree's root, n0.w) and its tree's root box: move units by writing their records
+ * (trt_scene_update, trt_prep_unit_records) before trt_deform. */
+
+/* A corner of a skinned model (skin.wgsl Corner): position, w the bits of its first two palette indices (16 bits
+ * each, low first); normal, w the other two; tangent, w the bits of TRT_CORNER_* flags; the four weights. */
+typedef struct { float p[4], n[4], t[4], w[4]; } trt_corner;
+#define TRT_CORNER_NORMAL  1u
+#define TRT_CORNER_TANGENT 2u
+
+/* A mesh that deforms (skin.wgsl and leaf_gather.wgsl Job, with its tree): its vertices among the scene's and the
+ * corner of the first (one corner a vertex, in the vertices' order), the first matrix of its palette, its triangles
+ * (leaves; indices in the words' Indices section, counted from first_vertex), its tree's root node and node count. */
+typedef struct {
+    uint32_t first_vertex, n_vertices, first_corner, palette;
+    uint32_t first_tri, n_tris, root, n_nodes;
+} trt_deform_mesh;
+
+typedef struct {
+    const trt_corner* corners;
+    uint64_t n_corners;
+    const trt_deform_mesh* meshes;
+    uint32_t n_meshes;
+} trt_deform_desc;
+
+/* Device times of one deformation (filled when stats is given: the call then waits for it) and the errors the device
+ * found (a tree that is not one, a top tree that came out deeper than TOP_DEPTH). */
+typedef struct { float device_ms, skin_ms, gather_ms, refit_ms, top_ms; uint32_t errors; } trt_deform_stats;
+
+/* Uploads the skinned models' corners and the deforming meshes, checks each mesh's tree (on the host copy taken at
+ * upload) and links every node to its parent. Again replaces what was set up. */
+int trt_deform_setup(trt_scene* scene, const trt_deform_desc* desc);
+/* One frame: palette_rows holds n_matrices matrices of 3 rows (x, y, z, translation) each; every mesh's palette
+ * indices must fall inside it. Asynchronous unless stats is given. After it the scene walks the binary trees only
+ * (the wide BVH is built from host copies the deformation does not update). flags: 0. */
+int trt_deform(trt_scene* scene, const uint32_t params[TRT_PARAMS_WORDS], const float* palette_rows,
+               uint32_t n_matrices, uint32_t flags, trt_deform_stats* stats);
+
 /* Renders samples [first_sample, first_sample + spp) at Params' size (gpu.rs:4116 Gpu::render; its per-dispatch
  * `size.z` is the sample index). Without TRT_RENDER_ACCUMULATE the scene's accum is cleared first, as the reference
  * clears it (gpu.rs:4170). accum_host: NULL, or w * h * 20 floats to copy the result to. stats: NULL (no

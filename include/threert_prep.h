@@ -27,6 +27,8 @@ typedef struct {
     const float* uvs;        /* n_tris * 6, or NULL: zeros */
     const uint32_t* sections;/* n_tris section indices, or NULL: all in section 0 */
     uint32_t n_sections;     /* at least 1 */
+    uint32_t like;           /* 1 + an earlier mesh this one repeats (its own vertices, leaves and tree, copied from
+                              * that mesh's instead of built: the fields above are then not read); 0: none */
 } trt_mesh_spec;
 
 /* A metal-rough material (scene.rs:480-491 GpuMaterial's fields the pass reads). */
@@ -132,6 +134,16 @@ uint32_t trt_prep_bvh(const float* tris, uint32_t n_tris, uint32_t max_depth, ui
 /* bvh.rs:246-285 check_tree over a tree's nodes with leaves of at most max_leaf items among n_items. 0 if it holds. */
 int trt_prep_check_tree(const uint32_t* nodes, uint32_t n_nodes, uint32_t max_depth, uint32_t max_leaf,
                         uint32_t n_items, uint32_t* depth);
+/* Unit records for instances placed anew (scene.rs:239-247 Instance::gpu with units.rs:329-342 unit_record), to write
+ * over the tables' instance section with trt_scene_update before trt_deform: worlds n * 12 floats (3x4 row-major),
+ * info n * 4 words (first triangle, object, first vertex, rows' first), roots n tree roots, cast_shadow n flags;
+ * out n * 40 words. 0 on success. */
+int trt_prep_unit_records(uint32_t n, const float* worlds, const uint32_t* info, const uint32_t* roots,
+                          const uint32_t* cast_shadow, uint32_t* out);
+/* The top tree over n units (units.rs:303-326 top_tree over units.rs:288-300 UnitBox::new of each unit's model-space
+ * box, local_boxes n * 6 floats lo then hi, under its world rows): (2n - 1) * 8 words of nodes, a leaf's
+ * left_or_first its unit's index. What trt_deform builds on the device. 0 on success; *depth the tree's depth. */
+int trt_prep_units_top(uint32_t n, const float* worlds, const float* local_boxes, uint32_t* nodes, uint32_t* depth);
 /* lib.rs:1041-1083 specular_albedo (f64), for the energy table's tests. */
 void trt_prep_specular_albedo(double mu, double alpha, uint32_t nr, uint32_t nphi, double out[2]);
 

@@ -31,7 +31,7 @@ class Stats(C.Structure):
 def build(force: bool = False) -> Path:
     """Builds liboracle.so with make (g++)."""
     if force or not LIB_PATH.exists() or any(
-            p.stat().st_mtime > LIB_PATH.stat().st_mtime for p in (HERE / "oracle.cpp", HERE / "oracle.h")):
+            p.stat().st_mtime > LIB_PATH.stat().st_mtime for p in (HERE / "oracle.cpp", HERE / "deform.cpp", HERE / "oracle.h")):
         subprocess.run(["make", "-s", "-C", str(HERE), "-B" if force else "liboracle.so"], check=True)
     return LIB_PATH
 
@@ -59,6 +59,9 @@ def lib():
         L.orc_hash_hp.argtypes = [C.c_uint32]
         L.orc_hash_hp.restype = C.c_uint32
         L.orc_hardware_threads.restype = C.c_int
+        L.orc_skin.argtypes = [P(C.c_uint32), C.c_uint32, P(C.c_float), P(C.c_float), P(C.c_float)]
+        L.orc_leaf_gather.argtypes = [P(C.c_uint32), C.c_uint32, P(C.c_float), P(C.c_uint32), C.c_uint32, P(C.c_float)]
+        L.orc_refit.argtypes = [P(C.c_uint32), C.c_uint32, P(C.c_float), P(C.c_uint32), C.c_uint32, P(C.c_uint32)]
         _lib = L
     return _lib
 
@@ -138,3 +141,23 @@ def hash_hp(x: int) -> int:
 
 def hardware_threads() -> int:
     return int(lib().orc_hardware_threads())
+
+
+def _p(a, t):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+def deform(jobs, corners, palette, vertices, leaves, nodes, words, w_indices: int):
+    """skin.wgsl, leaf_gather.wgsl and units.rs refit over the jobs: new (vertices, leaves, nodes) arrays."""
+    j = np.ascontiguousarray(jobs, np.uint32).reshape(-1, 8)
+    c = np.ascontiguousarray(corners, np.float32).reshape(-1, 16)
+    pal = np.ascontiguousarray(palette, np.float32).reshape(-1, 12)
+    v = np.array(vertices, np.float32, copy=True, order="C")
+    lv = np.array(leaves, np.float32, copy=True, order="C")
+    nd = np.array(nodes, np.uint32, copy=True, order="C")
+    w = np.ascontiguousarray(words, np.uint32)
+    L = lib()
+    L.orc_skin(_p(j, C.c_uint32), len(j), _p(c, C.c_float), _p(pal, C.c_float), _p(v, C.c_float))
+    L.orc_leaf_gather(_p(j, C.c_uint32), len(j), _p(v, C.c_float), _p(w, C.c_uint32), w_indices, _p(lv, C.c_float))
+    L.orc_refit(_p(j, C.c_uint32), len(j), _p(v, C.c_float), _p(w, C.c_uint32), w_indices, _p(nd, C.c_uint32))
+    return v, lv, nd

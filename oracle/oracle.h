@@ -60,6 +60,16 @@ int orc_trace_brute(const orc_scene* s, const uint32_t* params, const orc_ray* r
 /* The t of one named triangle (of instance which[i].inst) along each ray, in the unit's space as the walk tests it. */
 int orc_intersect(const orc_scene* s, const uint32_t* params, const orc_ray* rays, const orc_hit* which, uint64_t n,
                   float* t_out);
+/* The per-frame deformation (deform.cpp), one job a mesh: 8 words (first vertex, vertices, first corner, palette's
+ * first matrix, first triangle, triangles, tree root, tree nodes). Corners: 16 floats each (skin.wgsl Corner); palette:
+ * 12 floats a matrix (three rows). skin.wgsl main over each job's vertices, in place: */
+int orc_skin(const uint32_t* jobs, uint32_t n_jobs, const float* corners, const float* palette, float* vertices);
+/* leaf_gather.wgsl main over each job's triangles, in place (w_indices: the Indices section's first word): */
+int orc_leaf_gather(const uint32_t* jobs, uint32_t n_jobs, const float* vertices, const uint32_t* words,
+                    uint32_t w_indices, float* leaves);
+/* units.rs:251-275 refit of each job's tree from the vertices, in place: */
+int orc_refit(const uint32_t* jobs, uint32_t n_jobs, const float* vertices, const uint32_t* words, uint32_t w_indices,
+              uint32_t* nodes);
 /* sample.wgsl rng4 for a pixel seed, an index and a dimension id (tests pin the sampler with it). */
 void orc_rng4(uint32_t pixel_seed, uint32_t index, uint32_t dim, float out[4]);
 /* The Sobol direction numbers (3 dimensions x 32, bit-reversed) the sampler's tables hold. */

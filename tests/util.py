@@ -65,3 +65,12 @@ def region_mean(acc, w, h, spp, region):
     f = frame_of(acc, w, h, spp)
     px = scenes.region_pixels(w, h, region)
     return f.color.reshape(-1, 3)[px].mean(0)
+
+
+def small_crowd(n=160, groups=3, width=64, height=36, max_depth=3):
+    """Config 2 small enough for the oracle: a lighter humanoid (30 capsules of 8 x 9 quads), n walkers in `groups`
+    pose groups, a small ground, 12 lamps."""
+    from threert_b200 import crowd
+    body = crowd.humanoid(segments=8, hemi_rings=3, body_rings=4)
+    return crowd.crowd(n=n, groups=groups, width=width, height=height, max_depth=max_depth, extent=12.0,
+                       ground_segments=12, n_emitters=12, body=body, sky_size=(64, 32))

@@ -28,7 +28,7 @@ ERRORS = {1: "TRT_EINVAL", 2: "TRT_ECUDA", 3: "TRT_EGUARD"}
 
 class MeshSpec(C.Structure):
     _fields_ = [("n_tris", u32), ("positions", P(f32)), ("normals", P(f32)), ("uvs", P(f32)),
-                ("sections", P(u32)), ("n_sections", u32)]
+                ("sections", P(u32)), ("n_sections", u32), ("like", u32)]
 
 
 class MaterialSpec(C.Structure):
@@ -110,6 +110,27 @@ class Hit(C.Structure):
     _fields_ = [("t", f32), ("tri", u32), ("u", f32), ("v", f32), ("inst", u32), ("part", u32)]
 
 
+class Corner(C.Structure):
+    _fields_ = [("p", f32 * 4), ("n", f32 * 4), ("t", f32 * 4), ("w", f32 * 4)]
+
+
+class DeformMesh(C.Structure):
+    _fields_ = [("first_vertex", u32), ("n_vertices", u32), ("first_corner", u32), ("palette", u32),
+                ("first_tri", u32), ("n_tris", u32), ("root", u32), ("n_nodes", u32)]
+
+
+class DeformDesc(C.Structure):
+    _fields_ = [("corners", C.c_void_p), ("n_corners", u64), ("meshes", P(DeformMesh)), ("n_meshes", u32)]
+
+
+class DeformStats(C.Structure):
+    _fields_ = [("device_ms", f32), ("skin_ms", f32), ("gather_ms", f32), ("refit_ms", f32), ("top_ms", f32),
+                ("errors", u32)]
+
+
+TRT_CORNER_NORMAL = 1
+TRT_CORNER_TANGENT = 2
+
 # Every function the C headers declare, with its signature: (name, restype, argtypes).
 SIGNATURES = [
     # threert_prep.h
@@ -123,6 +144,8 @@ SIGNATURES = [
     ("trt_prep_bvh", u32, [P(f32), u32, u32, P(u32), u32, P(u32), P(u32)]),
     ("trt_prep_check_tree", C.c_int, [P(u32), u32, u32, u32, u32, P(u32)]),
     ("trt_prep_specular_albedo", None, [C.c_double, C.c_double, u32, u32, P(C.c_double)]),
+    ("trt_prep_unit_records", C.c_int, [u32, P(f32), P(u32), P(u32), P(u32), P(u32)]),
+    ("trt_prep_units_top", C.c_int, [u32, P(f32), P(f32), P(u32), P(u32)]),
     # threert_cuda.h
     ("trt_create", C.c_int, [P(Options), P(C.c_void_p)]),
     ("trt_destroy", None, [C.c_void_p]),
@@ -131,6 +154,9 @@ SIGNATURES = [
     ("trt_scene_upload", C.c_int, [C.c_void_p, P(SceneDesc), P(C.c_void_p)]),
     ("trt_scene_free", None, [C.c_void_p]),
     ("trt_scene_update", C.c_int, [C.c_void_p, u32, u64, C.c_void_p, u64]),
+    ("trt_scene_read", C.c_int, [C.c_void_p, u32, u64, C.c_void_p, u64]),
+    ("trt_deform_setup", C.c_int, [C.c_void_p, P(DeformDesc)]),
+    ("trt_deform", C.c_int, [C.c_void_p, P(u32), P(f32), u32, u32, P(DeformStats)]),
     ("trt_render", C.c_int, [C.c_void_p, P(u32), u32, u32, u32, P(f32), P(Stats)]),
     ("trt_accum_device_ptr", C.c_int, [C.c_void_p, P(C.c_void_p), P(u64)]),
     ("trt_accum_read", C.c_int, [C.c_void_p, P(f32), u64]),

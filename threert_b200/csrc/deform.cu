@@ -1,0 +1,651 @@
+// The per-frame deformation of a resident scene, on the device: skin (renderer/shaders/skin.wgsl), leaf gather
+// (renderer/shaders/leaf_gather.wgsl), the deforming meshes' trees refit bottom-up (units.rs:251-275 refit), the units'
+// world boxes (units.rs:288-300 UnitBox::new) and the top tree built again (units.rs:140-224 build_sah under
+// units.rs:303-326 top_tree). The reference does the last three on the CPU each frame; here every stage is a kernel
+// and nothing but the palette crosses PCIe.
+//
+// Arithmetic is in source order under -fmad=false, so each stage rounds as its C++ restatement does: skinned vertices,
+// leaves and refit boxes are bit-exact against the oracle, and the top tree is the one trt_prep_build's build_sah makes
+// over the same boxes, node for node.
+#include "deform.h"
+
+#include <algorithm>
+#include <cstring>
+
+#include "device_common.cuh"
+
+namespace trt {
+
+constexpr uint32_t NONE = 0xffffffffu;
+constexpr uint32_t TOP_DEPTH = 19u;                 // units.rs:30-37: leaves at most TOP_DEPTH - 1 deep
+constexpr uint32_t TOP_MAX_DEPTH = TOP_DEPTH - 1u;  // build_sah's max_depth
+constexpr uint32_t TOP_LEVELS = TOP_MAX_DEPTH + 1u; // levels 0 .. TOP_MAX_DEPTH
+constexpr uint32_t MAX_UNITS = 1u << TOP_MAX_DEPTH;
+constexpr uint32_t TOP_BINS = 32u;                  // units.rs:121
+constexpr uint32_t REFIT_CLIMB = 64u;               // a mesh tree is less deep than the walk's 64-entry stack
+// Error bits the kernels record.
+constexpr uint32_t E_TREE = 1u, E_DEPTH = 2u, E_ROOT = 4u, E_INDEX = 8u;
+
+struct DMesh { uint32_t first_vertex, n_vertices, first_corner, palette, first_tri, n_tris, root, n_nodes; };
+static_assert(sizeof(DMesh) == sizeof(trt_deform_mesh), "DMesh mirrors trt_deform_mesh");
+
+// glam's Vec3A::min / max (SSE minps / maxps): the first operand where it is smaller (larger), else the second.
+__host__ __device__ __forceinline__ float gmin(float a, float b) { return a < b ? a : b; }
+__host__ __device__ __forceinline__ float gmax(float a, float b) { return a > b ? a : b; }
+__device__ __forceinline__ bool finite1(float v) { return (bu(v) & 0x7f800000u) != 0x7f800000u; }
+
+// ---- skin.wgsl ----------------------------------------------------------------------------------------------------
+
+__device__ __forceinline__ float4 add4(float4 a, float4 b) { return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
+__device__ __forceinline__ float4 mul4(float4 a, float s) { return make_float4(a.x * s, a.y * s, a.z * s, a.w * s); }
+__device__ __forceinline__ float dot4(float4 a, float4 b) { return a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w; }
+// skin.wgsl unit: v / |v| where |v| is positive and finite, else zero.
+__device__ __forceinline__ V3 unit3(V3 v) {
+    float l = sqrtf(dot(v, v));
+    if (l > 0.0f && finite1(l)) return V3{v.x / l, v.y / l, v.z / l};
+    return v3(0.0f);
+}
+
+// skin.wgsl:66-90 place, and main's writes (skin.wgsl:92-113): one thread a vertex, blockIdx.y a mesh.
+__global__ void k_skin(const DMesh* __restrict__ meshes, uint32_t n_meshes, const float4* __restrict__ corners,
+                       const float4* __restrict__ palette, float4* vertices) {
+    for (uint32_t m = blockIdx.y; m < n_meshes; m += gridDim.y) {
+        DMesh M = meshes[m];
+        for (uint32_t local = blockIdx.x * blockDim.x + threadIdx.x; local < M.n_vertices; local += gridDim.x * blockDim.x) {
+            const float4* c = corners + 4ull * (M.first_corner + local);
+            float4 cp = c[0], cn = c[1], ct = c[2], cw = c[3];
+            uint32_t a = bu(cp.w), b = bu(cn.w), flags = bu(ct.w);
+            uint32_t j0 = (M.palette + (a & 0xffffu)) * 3u, j1 = (M.palette + (a >> 16)) * 3u;
+            uint32_t j2 = (M.palette + (b & 0xffffu)) * 3u, j3 = (M.palette + (b >> 16)) * 3u;
+            float4 r0 = add4(add4(add4(mul4(palette[j0], cw.x), mul4(palette[j1], cw.y)), mul4(palette[j2], cw.z)), mul4(palette[j3], cw.w));
+            float4 r1 = add4(add4(add4(mul4(palette[j0 + 1], cw.x), mul4(palette[j1 + 1], cw.y)), mul4(palette[j2 + 1], cw.z)), mul4(palette[j3 + 1], cw.w));
+            float4 r2 = add4(add4(add4(mul4(palette[j0 + 2], cw.x), mul4(palette[j1 + 2], cw.y)), mul4(palette[j2 + 2], cw.z)), mul4(palette[j3 + 2], cw.w));
+            float4 p = make_float4(cp.x, cp.y, cp.z, 1.0f);
+            V3 R0 = xyz(r0), R1 = xyz(r1), R2 = xyz(r2), N = xyz(cn), T = xyz(ct);
+            V3 c12 = cross(R1, R2);
+            V3 n = V3{dot(c12, N), dot(cross(R2, R0), N), dot(cross(R0, R1), N)};
+            if (dot(R0, c12) < 0.0f) n = -n;
+            V3 pos = V3{dot4(r0, p), dot4(r1, p), dot4(r2, p)};
+            if (!(finite1(pos.x) && finite1(pos.y) && finite1(pos.z))) pos = v3(0.0f);
+            uint64_t k = 3ull * (M.first_vertex + local);
+            vertices[k] = f4(pos, vertices[k].w);
+            if (flags & TRT_CORNER_NORMAL) vertices[k + 1] = f4(unit3(n), vertices[k + 1].w);
+            if (flags & TRT_CORNER_TANGENT) vertices[k + 2] = f4(unit3(V3{dot(R0, T), dot(R1, T), dot(R2, T)}), vertices[k + 2].w);
+        }
+    }
+}
+
+// ---- leaf_gather.wgsl ---------------------------------------------------------------------------------------------
+
+// Corner c of triangle t through its index; an index past the mesh's vertices is recorded and read as its first.
+__device__ __forceinline__ V3 corner(const float4* vertices, const uint32_t* words, uint32_t w_indices, const DMesh& M,
+                                     uint32_t t, uint32_t c, uint32_t* err) {
+    uint32_t i = words[w_indices + t * 3u + c];
+    if (i >= M.n_vertices) { atomicOr(err, E_INDEX); i = 0u; }
+    return xyz(vertices[3ull * (M.first_vertex + i)]);
+}
+
+// leaf_gather.wgsl:31-52: each triangle of a mesh again from its vertices: (v0, keep w), (e1, keep w), (e2, 0).
+__global__ void k_gather(const DMesh* __restrict__ meshes, uint32_t n_meshes, const float4* __restrict__ vertices,
+                         const uint32_t* __restrict__ words, uint32_t w_indices, float4* leaves, uint32_t* err) {
+    for (uint32_t m = blockIdx.y; m < n_meshes; m += gridDim.y) {
+        DMesh M = meshes[m];
+        for (uint32_t local = blockIdx.x * blockDim.x + threadIdx.x; local < M.n_tris; local += gridDim.x * blockDim.x) {
+            uint32_t t = M.first_tri + local;
+            V3 p0 = corner(vertices, words, w_indices, M, t, 0, err);
+            V3 p1 = corner(vertices, words, w_indices, M, t, 1, err);
+            V3 p2 = corner(vertices, words, w_indices, M, t, 2, err);
+            uint64_t k = 3ull * t;
+            leaves[k] = f4(p0, leaves[k].w);
+            leaves[k + 1] = f4(p1 - p0, leaves[k + 1].w);
+            leaves[k + 2] = f4(p2 - p0, 0.0f);
+        }
+    }
+}
+
+// ---- refit (units.rs:251-275) -------------------------------------------------------------------------------------
+//
+// The reference refits a tree from its last node back to its root, one node after another. Here each leaf's thread
+// takes its box from its triangles' corners, then climbs: at each parent the first child's thread to arrive stops
+// (atomic counter) and the second, which sees both children's boxes, writes the parent's and goes on. The counter
+// is put back to zero by the thread that used it, so it is zero for the next frame.
+
+__device__ __forceinline__ void store_box(uint4* nodes, uint32_t i, V3 lo, V3 hi, uint32_t lf, uint32_t count) {
+    nodes[2ull * i] = make_uint4(bu(lo.x), bu(lo.y), bu(lo.z), lf);
+    nodes[2ull * i + 1] = make_uint4(bu(hi.x), bu(hi.y), bu(hi.z), count);
+}
+
+__global__ void k_refit(const DMesh* __restrict__ meshes, uint32_t n_meshes, const float4* __restrict__ vertices,
+                        const uint32_t* __restrict__ words, uint32_t w_indices, uint4* nodes,
+                        const uint32_t* __restrict__ parent, uint32_t* arrivals, uint32_t* err) {
+    for (uint32_t m = blockIdx.y; m < n_meshes; m += gridDim.y) {
+        DMesh M = meshes[m];
+        for (uint32_t local = blockIdx.x * blockDim.x + threadIdx.x; local < M.n_nodes; local += gridDim.x * blockDim.x) {
+            uint32_t i = M.root + local;
+            uint4 a = __ldcg(nodes + 2ull * i), b = __ldcg(nodes + 2ull * i + 1);
+            if (b.w == 0u) continue;  // interior: its box comes from its children
+            V3 lo = v3(__uint_as_float(0x7f800000u)), hi = v3(__uint_as_float(0xff800000u));
+            for (uint32_t k = a.w; k < a.w + b.w; ++k) {
+                uint32_t t = M.first_tri + k;
+                for (uint32_t c = 0; c < 3; ++c) {
+                    V3 v = corner(vertices, words, w_indices, M, t, c, err);
+                    if (finite1(v.x) && finite1(v.y) && finite1(v.z)) {
+                        lo = V3{gmin(lo.x, v.x), gmin(lo.y, v.y), gmin(lo.z, v.z)};
+                        hi = V3{gmax(hi.x, v.x), gmax(hi.y, v.y), gmax(hi.z, v.z)};
+                    }
+                }
+            }
+            if (lo.x > hi.x) { lo = v3(0.0f); hi = v3(0.0f); }  // a leaf of nothing finite: a point
+            store_box(nodes, i, lo, hi, a.w, b.w);
+            uint32_t cur = i;
+            for (uint32_t climb = 0;; ++climb) {
+                uint32_t par = parent[cur];
+                if (par == NONE) break;
+                if (climb >= REFIT_CLIMB) { atomicOr(err, E_TREE); break; }
+                __threadfence();
+                if (atomicAdd(&arrivals[par], 1u) == 0u) break;  // the sibling's thread finishes the parent
+                arrivals[par] = 0u;
+                __threadfence();
+                uint4 pa = __ldcg(nodes + 2ull * par), pb = __ldcg(nodes + 2ull * par + 1);
+                uint32_t l = M.root + pa.w;
+                uint4 la = __ldcg(nodes + 2ull * l), lb = __ldcg(nodes + 2ull * l + 1);
+                uint4 ra = __ldcg(nodes + 2ull * l + 2), rb = __ldcg(nodes + 2ull * l + 3);
+                V3 plo = V3{gmin(__uint_as_float(la.x), __uint_as_float(ra.x)), gmin(__uint_as_float(la.y), __uint_as_float(ra.y)),
+                            gmin(__uint_as_float(la.z), __uint_as_float(ra.z))};
+                V3 phi = V3{gmax(__uint_as_float(lb.x), __uint_as_float(rb.x)), gmax(__uint_as_float(lb.y), __uint_as_float(rb.y)),
+                            gmax(__uint_as_float(lb.z), __uint_as_float(rb.z))};
+                store_box(nodes, par, plo, phi, pa.w, pb.w);
+                cur = par;
+            }
+        }
+    }
+}
+
+// Parent links of the deforming meshes' nodes (once, at setup): parent[root + left + {0,1}] = the interior node.
+__global__ void k_parents(const DMesh* __restrict__ meshes, uint32_t n_meshes, const uint4* __restrict__ nodes,
+                          uint32_t* parent) {
+    for (uint32_t m = blockIdx.y; m < n_meshes; m += gridDim.y) {
+        DMesh M = meshes[m];
+        for (uint32_t local = blockIdx.x * blockDim.x + threadIdx.x; local < M.n_nodes; local += gridDim.x * blockDim.x) {
+            uint32_t i = M.root + local;
+            uint4 a = nodes[2ull * i], b = nodes[2ull * i + 1];
+            if (local == 0) parent[i] = NONE;
+            if (b.w == 0u) {
+                parent[M.root + a.w] = i;
+                parent[M.root + a.w + 1] = i;
+            }
+        }
+    }
+}
+
+// ---- the top tree ---------------------------------------------------------------------------------------------------
+
+struct TopBuild {
+    float4* box;      // 2 a unit: lo, hi
+    float4* centre;   // a unit's box centre
+    uint32_t* order[2];
+    uint4* tasks[2];  // a level's nodes: (start, end, final index, interior nodes before it in preorder)
+    uint32_t* cnt;    // nodes a level, TOP_LEVELS + 1
+    uint32_t* err;
+    uint4* nodes;
+    uint32_t top_first, n_units;
+};
+
+// units.rs:288-300 UnitBox::new of each unit's tree root box under its world rows, its centre, and the build's start.
+__global__ void k_unit_boxes(const uint4* __restrict__ tables, uint32_t t_instances, uint64_t n_nodes, TopBuild T) {
+    uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u == 0) {
+        T.tasks[0][0] = make_uint4(0u, T.n_units, 0u, 0u);
+        T.cnt[0] = 1u;
+        for (uint32_t l = 1; l <= TOP_LEVELS; ++l) T.cnt[l] = 0u;
+    }
+    if (u >= T.n_units) return;
+    T.order[0][u] = u;
+    uint32_t b = t_instances + u * 10u;
+    uint4 m0 = tables[b], m1 = tables[b + 1], m2 = tables[b + 2], n0 = tables[b + 3];
+    uint32_t root = n0.w;
+    V3 lo = v3(0.0f), hi = v3(0.0f);
+    if (root < n_nodes) {
+        uint4 na = T.nodes[2ull * root], nb = T.nodes[2ull * root + 1];
+        lo = V3{__uint_as_float(na.x), __uint_as_float(na.y), __uint_as_float(na.z)};
+        hi = V3{__uint_as_float(nb.x), __uint_as_float(nb.y), __uint_as_float(nb.z)};
+    } else {
+        atomicOr(T.err, E_ROOT);
+    }
+    float w[3][4] = {{__uint_as_float(m0.x), __uint_as_float(m0.y), __uint_as_float(m0.z), __uint_as_float(m0.w)},
+                     {__uint_as_float(m1.x), __uint_as_float(m1.y), __uint_as_float(m1.z), __uint_as_float(m1.w)},
+                     {__uint_as_float(m2.x), __uint_as_float(m2.y), __uint_as_float(m2.z), __uint_as_float(m2.w)}};
+    V3 a = v3(__uint_as_float(0x7f800000u)), bb = v3(__uint_as_float(0xff800000u));
+    for (int c = 0; c < 8; ++c) {
+        V3 q = V3{(c & 1) == 0 ? lo.x : hi.x, (c & 2) == 0 ? lo.y : hi.y, (c & 4) == 0 ? lo.z : hi.z};
+        // glam's Mat4 * point: x_axis * x + y_axis * y + z_axis * z + w_axis
+        V3 p = V3{w[0][0] * q.x + w[0][1] * q.y + w[0][2] * q.z + w[0][3], w[1][0] * q.x + w[1][1] * q.y + w[1][2] * q.z + w[1][3],
+                  w[2][0] * q.x + w[2][1] * q.y + w[2][2] * q.z + w[2][3]};
+        a = V3{gmin(a.x, p.x), gmin(a.y, p.y), gmin(a.z, p.z)};
+        bb = V3{gmax(bb.x, p.x), gmax(bb.y, p.y), gmax(bb.z, p.z)};
+    }
+    V3 e = bb - a;
+    V3 m = V3{gmax(fabsf(a.x), fabsf(bb.x)), gmax(fabsf(a.y), fabsf(bb.y)), gmax(fabsf(a.z), fabsf(bb.z))};
+    float pad = gmax(e.x, gmax(e.y, e.z)) * 1e-4f + gmax(m.x, gmax(m.y, m.z)) * 1e-5f + 1e-6f;
+    V3 blo = a - v3(pad), bhi = bb + v3(pad);
+    T.box[2ull * u] = f4(blo, 0.0f);
+    T.box[2ull * u + 1] = f4(bhi, 0.0f);
+    T.centre[u] = f4((blo + bhi) * 0.5f, 0.0f);
+}
+
+// Atomic min / max of floats in shared memory, by their bits (non-negative floats order as ints, negative ones in
+// reverse as unsigned).
+__device__ __forceinline__ void atomic_min_f(float* a, float v) {
+    if (__float_as_int(v) >= 0) atomicMin((int*)a, __float_as_int(v));
+    else atomicMax((unsigned*)a, __float_as_uint(v));
+}
+__device__ __forceinline__ void atomic_max_f(float* a, float v) {
+    if (__float_as_int(v) >= 0) atomicMax((int*)a, __float_as_int(v));
+    else atomicMin((unsigned*)a, __float_as_uint(v));
+}
+__device__ __forceinline__ float area3(V3 lo, V3 hi) {
+    V3 e = V3{gmax(hi.x - lo.x, 0.0f), gmax(hi.y - lo.y, 0.0f), gmax(hi.z - lo.z, 0.0f)};
+    return 2.0f * (e.x * e.y + e.y * e.z + e.z * e.x);
+}
+__device__ __forceinline__ float comp(float4 v, uint32_t axis) { return axis == 0 ? v.x : (axis == 1 ? v.y : v.z); }
+__device__ __forceinline__ float comp3(V3 v, uint32_t axis) { return axis == 0 ? v.x : (axis == 1 ? v.y : v.z); }
+// Rust's `f as usize` for the bin (non-negative here), saturating, NaN to 0, then at most TOP_BINS - 1.
+__device__ __forceinline__ uint32_t bin_of(float c, float clo, float scale) {
+    float f = (c - clo) * scale;
+    if (!(f > 0.0f)) return 0u;
+    return f >= (float)TOP_BINS ? TOP_BINS - 1u : min((uint32_t)f, TOP_BINS - 1u);
+}
+// f32::total_cmp's key.
+__device__ __forceinline__ int32_t total_key(float f) {
+    int32_t b = __float_as_int(f);
+    return b ^ (int32_t)(((uint32_t)(b >> 31)) >> 1);
+}
+
+constexpr uint32_t TOP_WARPS = 8u;
+
+// One level of the build: a warp a node. It takes the node's boxes (order[level & 1][start, end)), picks the split
+// build_sah picks (the cheapest binned split along the centres' axes among those the depth allows, else the median
+// along the widest axis), writes the node where build_sah's depth-first layout puts it and hands its two children to
+// the next level with their items partitioned into order[(level + 1) & 1]. In that layout a node's children sit at
+// 1 + 2 * I and 2 + 2 * I, where I counts the interior nodes before it in preorder: a left child's I is its parent's
+// plus one, a right child's its parent's plus the left side's item count (a subtree of k items has k - 1 interior
+// nodes), so each node's place is known when it is made.
+__global__ void __launch_bounds__(TOP_WARPS * 32) k_top_level(TopBuild T, uint32_t level) {
+    __shared__ float s_lo[TOP_WARPS][3][3][TOP_BINS], s_hi[TOP_WARPS][3][3][TOP_BINS];
+    __shared__ uint32_t s_n[TOP_WARPS][3][TOP_BINS];
+    uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+    uint32_t n_tasks = T.cnt[level];
+    const uint32_t* order = T.order[level & 1u];
+    uint32_t* out = T.order[(level + 1u) & 1u];
+    const uint4* tasks = T.tasks[level & 1u];
+    for (uint32_t ti = blockIdx.x * TOP_WARPS + wib; ti < n_tasks; ti += gridDim.x * TOP_WARPS) {
+        uint4 task = tasks[ti];
+        uint32_t start = task.x, end = task.y, fin = task.z, pre = task.w, count = end - start;
+        V3 lo = v3(__uint_as_float(0x7f800000u)), hi = v3(__uint_as_float(0xff800000u)), clo = lo, chi = hi;
+        for (uint32_t j = start + lane; j < end; j += 32u) {
+            uint32_t k = order[j];
+            float4 bl = T.box[2ull * k], bh = T.box[2ull * k + 1], c = T.centre[k];
+            lo = V3{gmin(lo.x, bl.x), gmin(lo.y, bl.y), gmin(lo.z, bl.z)};
+            hi = V3{gmax(hi.x, bh.x), gmax(hi.y, bh.y), gmax(hi.z, bh.z)};
+            clo = V3{gmin(clo.x, c.x), gmin(clo.y, c.y), gmin(clo.z, c.z)};
+            chi = V3{gmax(chi.x, c.x), gmax(chi.y, c.y), gmax(chi.z, c.z)};
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            lo = V3{gmin(lo.x, __shfl_xor_sync(~0u, lo.x, o)), gmin(lo.y, __shfl_xor_sync(~0u, lo.y, o)), gmin(lo.z, __shfl_xor_sync(~0u, lo.z, o))};
+            hi = V3{gmax(hi.x, __shfl_xor_sync(~0u, hi.x, o)), gmax(hi.y, __shfl_xor_sync(~0u, hi.y, o)), gmax(hi.z, __shfl_xor_sync(~0u, hi.z, o))};
+            clo = V3{gmin(clo.x, __shfl_xor_sync(~0u, clo.x, o)), gmin(clo.y, __shfl_xor_sync(~0u, clo.y, o)), gmin(clo.z, __shfl_xor_sync(~0u, clo.z, o))};
+            chi = V3{gmax(chi.x, __shfl_xor_sync(~0u, chi.x, o)), gmax(chi.y, __shfl_xor_sync(~0u, chi.y, o)), gmax(chi.z, __shfl_xor_sync(~0u, chi.z, o))};
+        }
+        if (fin >= 2u * T.n_units - 1u || count == 0 || end > T.n_units) {  // (a build of n leaves has 2n - 1 nodes)
+            if (lane == 0) atomicOr(T.err, E_TREE);
+            continue;
+        }
+        uint32_t node = T.top_first + fin;
+        if (count == 1) {
+            if (lane == 0) store_box(T.nodes, node, lo, hi, order[start], 1u);
+            continue;
+        }
+        if (level >= TOP_MAX_DEPTH || count > MAX_UNITS) {
+            if (lane == 0) atomicOr(T.err, E_DEPTH);
+            continue;
+        }
+        uint32_t room = 1u << (TOP_MAX_DEPTH - level - 1u);
+        V3 ext = chi - clo;
+        float scale[3] = {(float)TOP_BINS / ext.x, (float)TOP_BINS / ext.y, (float)TOP_BINS / ext.z};
+        bool use[3] = {ext.x > 0.0f, ext.y > 0.0f, ext.z > 0.0f};
+        for (uint32_t i = lane; i < 3u * TOP_BINS; i += 32u) {
+            uint32_t ax = i / TOP_BINS, bn = i % TOP_BINS;
+            for (int q = 0; q < 3; ++q) {
+                s_lo[wib][ax][q][bn] = __uint_as_float(0x7f800000u);
+                s_hi[wib][ax][q][bn] = __uint_as_float(0xff800000u);
+            }
+            s_n[wib][ax][bn] = 0u;
+        }
+        __syncwarp();
+        for (uint32_t j = start + lane; j < end; j += 32u) {
+            uint32_t k = order[j];
+            float4 bl = T.box[2ull * k], bh = T.box[2ull * k + 1], c = T.centre[k];
+            for (uint32_t ax = 0; ax < 3; ++ax) {
+                if (!use[ax]) continue;
+                uint32_t bn = bin_of(comp(c, ax), comp3(clo, ax), scale[ax]);
+                atomic_min_f(&s_lo[wib][ax][0][bn], bl.x);
+                atomic_min_f(&s_lo[wib][ax][1][bn], bl.y);
+                atomic_min_f(&s_lo[wib][ax][2][bn], bl.z);
+                atomic_max_f(&s_hi[wib][ax][0][bn], bh.x);
+                atomic_max_f(&s_hi[wib][ax][1][bn], bh.y);
+                atomic_max_f(&s_hi[wib][ax][2][bn], bh.z);
+                atomicAdd(&s_n[wib][ax][bn], 1u);
+            }
+        }
+        __syncwarp();
+        // build_sah's sweep, as written: right sides from the last bin back, left sides forward, the first cheapest.
+        float best_cost = __uint_as_float(0x7f800000u);
+        uint32_t best_axis = 0, best_split = 0, best_left = 0;
+        if (lane == 0) {
+            for (uint32_t ax = 0; ax < 3; ++ax) {
+                if (!use[ax]) continue;
+                float right[TOP_BINS];
+                V3 alo = v3(__uint_as_float(0x7f800000u)), ahi = v3(__uint_as_float(0xff800000u));
+                right[0] = 0.0f;
+                for (uint32_t i = TOP_BINS - 1u; i >= 1u; --i) {
+                    alo = V3{gmin(alo.x, s_lo[wib][ax][0][i]), gmin(alo.y, s_lo[wib][ax][1][i]), gmin(alo.z, s_lo[wib][ax][2][i])};
+                    ahi = V3{gmax(ahi.x, s_hi[wib][ax][0][i]), gmax(ahi.y, s_hi[wib][ax][1][i]), gmax(ahi.z, s_hi[wib][ax][2][i])};
+                    right[i] = area3(alo, ahi);
+                }
+                alo = v3(__uint_as_float(0x7f800000u));
+                ahi = v3(__uint_as_float(0xff800000u));
+                uint32_t nl = 0;
+                for (uint32_t i = 1; i < TOP_BINS; ++i) {
+                    alo = V3{gmin(alo.x, s_lo[wib][ax][0][i - 1]), gmin(alo.y, s_lo[wib][ax][1][i - 1]), gmin(alo.z, s_lo[wib][ax][2][i - 1])};
+                    ahi = V3{gmax(ahi.x, s_hi[wib][ax][0][i - 1]), gmax(ahi.y, s_hi[wib][ax][1][i - 1]), gmax(ahi.z, s_hi[wib][ax][2][i - 1])};
+                    nl += s_n[wib][ax][i - 1];
+                    uint32_t nr = count - nl;
+                    if (nl == 0 || nr == 0 || nl > room || nr > room) continue;
+                    float cost = area3(alo, ahi) * (float)nl + right[i] * (float)nr;
+                    if (cost < best_cost) { best_cost = cost; best_axis = ax; best_split = i; best_left = nl; }
+                }
+            }
+        }
+        best_cost = __shfl_sync(~0u, best_cost, 0);
+        best_axis = __shfl_sync(~0u, best_axis, 0);
+        best_split = __shfl_sync(~0u, best_split, 0);
+        best_left = __shfl_sync(~0u, best_left, 0);
+        bool binned = finite1(best_cost);
+        uint32_t med_axis = (ext.x >= ext.y && ext.x >= ext.z) ? 0u : (ext.y >= ext.z ? 1u : 2u);
+        uint32_t mid = binned ? best_left : count / 2u;
+        // Partition, left side first (stable: the order inside a side does not change the tree).
+        uint32_t nl_run = 0, nr_run = 0;
+        for (uint32_t base = start; base < end; base += 32u) {
+            uint32_t j = base + lane;
+            bool valid = j < end, left = false;
+            uint32_t k = valid ? order[j] : 0u;
+            if (valid) {
+                if (binned) {
+                    left = bin_of(comp(T.centre[k], best_axis), comp3(clo, best_axis), scale[best_axis]) < best_split;
+                } else {
+                    // the median by (centre along the axis, total order; then the unit's index): its rank among all
+                    int32_t kk = total_key(comp(T.centre[k], med_axis));
+                    uint32_t rank = 0;
+                    for (uint32_t q = start; q < end; ++q) {
+                        uint32_t o = order[q];
+                        int32_t ko = total_key(comp(T.centre[o], med_axis));
+                        rank += (ko < kk || (ko == kk && o < k)) ? 1u : 0u;
+                    }
+                    left = rank < count / 2u;
+                }
+            }
+            unsigned lm = __ballot_sync(~0u, valid && left), rm = __ballot_sync(~0u, valid && !left);
+            unsigned below = (1u << lane) - 1u;
+            if (valid) {
+                if (left) out[start + nl_run + __popc(lm & below)] = k;
+                else out[start + mid + nr_run + __popc(rm & below)] = k;
+            }
+            nl_run += __popc(lm);
+            nr_run += __popc(rm);
+        }
+        if (lane == 0) {
+            if (nl_run != mid) atomicOr(T.err, E_TREE);
+            store_box(T.nodes, node, lo, hi, 1u + 2u * pre, 0u);
+            uint32_t at = atomicAdd(&T.cnt[level + 1u], 2u);
+            uint4* next = T.tasks[(level + 1u) & 1u];
+            next[at] = make_uint4(start, start + mid, 1u + 2u * pre, pre + 1u);
+            next[at + 1] = make_uint4(start + mid, end, 2u + 2u * pre, pre + mid);
+        }
+    }
+}
+
+}  // namespace trt
+
+// ---- host ----------------------------------------------------------------------------------------------------------
+
+namespace trt {
+
+struct DeformState {
+    DMesh* meshes = nullptr;
+    float4* corners = nullptr;
+    uint32_t* parent = nullptr;    // a word a node of the whole node buffer
+    uint32_t* arrivals = nullptr;  // likewise, zero between frames
+    uint32_t* err = nullptr;
+    float4* palette = nullptr;
+    uint32_t palette_cap = 0;
+    void* top = nullptr;           // the top build's scratch
+    uint32_t top_units = 0;
+    TopBuild T{};
+    std::vector<DMesh> host_meshes;
+    std::vector<uint32_t> max_bone;  // per mesh: the largest palette index its corners name
+    uint32_t max_vertices = 0, max_tris = 0, max_nodes = 0;
+    cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+};
+
+namespace {
+
+int cuda_err(std::string& err, cudaError_t e, const char* what) {
+    err = std::string(what) + ": " + cudaGetErrorString(e);
+    return TRT_ECUDA;
+}
+#define DF_CUDA(call)                                              \
+    do {                                                           \
+        cudaError_t e_ = (call);                                   \
+        if (e_ != cudaSuccess) return cuda_err(err, e_, #call);    \
+    } while (0)
+
+// Reads node i of the host copy.
+void host_node(const std::vector<uint8_t>& nodes, uint64_t i, uint32_t w[8]) { std::memcpy(w, nodes.data() + 32 * i, 32); }
+
+int ensure_top(DeformState* st, uint32_t n_units, std::string& err) {
+    if (st->top && st->top_units >= n_units) return TRT_OK;
+    if (st->top) cudaFree(st->top);
+    st->top = nullptr;
+    uint64_t need = 0;
+    auto add = [&](uint64_t b) { uint64_t at = need; need += (b + 255) / 256 * 256; return at; };
+    uint64_t o_box = add(32ull * n_units), o_c = add(16ull * n_units), o_o0 = add(4ull * n_units),
+             o_o1 = add(4ull * n_units), o_t0 = add(16ull * n_units), o_t1 = add(16ull * n_units),
+             o_cnt = add(4ull * (TOP_LEVELS + 1));
+    DF_CUDA(cudaMalloc(&st->top, need));
+    char* b = (char*)st->top;
+    st->T.box = (float4*)(b + o_box);
+    st->T.centre = (float4*)(b + o_c);
+    st->T.order[0] = (uint32_t*)(b + o_o0);
+    st->T.order[1] = (uint32_t*)(b + o_o1);
+    st->T.tasks[0] = (uint4*)(b + o_t0);
+    st->T.tasks[1] = (uint4*)(b + o_t1);
+    st->T.cnt = (uint32_t*)(b + o_cnt);
+    st->top_units = n_units;
+    return TRT_OK;
+}
+
+dim3 mesh_grid(uint32_t per_mesh, uint32_t n_meshes) {
+    uint32_t x = std::max(1u, std::min((per_mesh + 255u) / 256u, 1024u));
+    uint32_t y = std::max(1u, std::min(n_meshes, 65535u));
+    return dim3(x, y);
+}
+
+}  // namespace
+
+void deform_free(DeformState* st) {
+    if (!st) return;
+    for (void* p : {(void*)st->meshes, (void*)st->corners, (void*)st->parent, (void*)st->arrivals, (void*)st->err,
+                    (void*)st->palette, st->top})
+        if (p) cudaFree(p);
+    for (auto& e : st->ev)
+        if (e) cudaEventDestroy(e);
+    delete st;
+}
+
+int deform_setup(DeformState** out, const SceneBuffers& sb, const trt_deform_desc* d, std::string& err) {
+    if (!d || (d->n_meshes && !d->meshes) || (d->n_corners && !d->corners)) { err = "trt_deform_setup: a null array"; return TRT_EINVAL; }
+    const uint64_t n_vertices = sb.bytes[0] / 48, n_tris = sb.bytes[1] / 48, n_nodes = sb.bytes[2] / 32;
+    const std::vector<uint8_t>& hn = sb.host[2];
+    if (hn.size() != sb.bytes[2]) { err = "trt_deform_setup: the scene's node copy is missing"; return TRT_EINVAL; }
+    std::vector<uint32_t> refs(n_nodes, 0);
+    auto* st = new DeformState();
+    auto fail = [&](const std::string& m) { deform_free(st); err = "trt_deform_setup: " + m; return TRT_EINVAL; };
+    st->host_meshes.assign((const DMesh*)d->meshes, (const DMesh*)d->meshes + d->n_meshes);
+    st->max_bone.assign(d->n_meshes, 0);
+    for (uint32_t m = 0; m < d->n_meshes; ++m) {
+        const DMesh& M = st->host_meshes[m];
+        std::string at = "mesh " + std::to_string(m) + ": ";
+        if ((uint64_t)M.first_vertex + M.n_vertices > n_vertices) return fail(at + "vertices past the scene's");
+        if ((uint64_t)M.first_corner + M.n_vertices > d->n_corners) return fail(at + "corners past the corners given");
+        if ((uint64_t)M.first_tri + M.n_tris > n_tris) return fail(at + "triangles past the scene's");
+        if (M.n_nodes == 0 || (uint64_t)M.root + M.n_nodes > n_nodes) return fail(at + "nodes past the scene's");
+        // The tree: children after their parent and inside the tree, each node a child once; leaves' triangles
+        // inside the mesh.
+        for (uint32_t k = 0; k < M.n_nodes; ++k) {
+            uint32_t w[8];
+            host_node(hn, M.root + k, w);
+            if (w[7] == 0) {
+                if (w[3] <= k || (uint64_t)w[3] + 1 >= M.n_nodes) return fail(at + "a node's children are not after it in its tree");
+                refs[M.root + w[3]]++;
+                refs[M.root + w[3] + 1]++;
+            } else if ((uint64_t)w[3] + w[7] > M.n_tris) {
+                return fail(at + "a leaf's triangles are past the mesh's");
+            }
+        }
+        for (uint32_t k = 0; k < M.n_nodes; ++k)
+            if (refs[M.root + k] != (k == 0 ? 0u : 1u)) return fail(at + "a node is not the child of one node");
+        for (uint32_t v = 0; v < M.n_vertices; ++v) {
+            const trt_corner& c = d->corners[M.first_corner + v];
+            uint32_t a, b;
+            std::memcpy(&a, &c.p[3], 4);
+            std::memcpy(&b, &c.n[3], 4);
+            st->max_bone[m] = std::max({st->max_bone[m], a & 0xffffu, a >> 16, b & 0xffffu, b >> 16});
+        }
+        st->max_vertices = std::max(st->max_vertices, M.n_vertices);
+        st->max_tris = std::max(st->max_tris, M.n_tris);
+        st->max_nodes = std::max(st->max_nodes, M.n_nodes);
+    }
+    cudaError_t e = cudaSuccess;
+    if (d->n_meshes) e = cudaMalloc(&st->meshes, sizeof(DMesh) * d->n_meshes);
+    if (e == cudaSuccess && d->n_meshes) e = cudaMemcpyAsync(st->meshes, d->meshes, sizeof(DMesh) * d->n_meshes, cudaMemcpyHostToDevice, sb.stream);
+    if (e == cudaSuccess && d->n_corners) e = cudaMalloc(&st->corners, sizeof(trt_corner) * d->n_corners);
+    if (e == cudaSuccess && d->n_corners) e = cudaMemcpyAsync(st->corners, d->corners, sizeof(trt_corner) * d->n_corners, cudaMemcpyHostToDevice, sb.stream);
+    if (e == cudaSuccess) e = cudaMalloc(&st->parent, 4 * std::max<uint64_t>(n_nodes, 1));
+    if (e == cudaSuccess) e = cudaMalloc(&st->arrivals, 4 * std::max<uint64_t>(n_nodes, 1));
+    if (e == cudaSuccess) e = cudaMemsetAsync(st->arrivals, 0, 4 * std::max<uint64_t>(n_nodes, 1), sb.stream);
+    if (e == cudaSuccess) e = cudaMalloc(&st->err, 4);
+    if (e == cudaSuccess) e = cudaMemsetAsync(st->err, 0, 4, sb.stream);
+    for (auto& ev : st->ev)
+        if (e == cudaSuccess) e = cudaEventCreate(&ev);
+    if (e == cudaSuccess && d->n_meshes) {
+        k_parents<<<mesh_grid(st->max_nodes, d->n_meshes), 256, 0, sb.stream>>>(st->meshes, d->n_meshes,
+                                                                               (const uint4*)sb.buf[2], st->parent);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(sb.stream);
+    if (e != cudaSuccess) {
+        deform_free(st);
+        return cuda_err(err, e, "trt_deform_setup");
+    }
+    *out = st;
+    return TRT_OK;
+}
+
+int deform_run(DeformState* st, const SceneBuffers& sb, const uint32_t* P, const float* palette_rows,
+               uint32_t n_matrices, uint32_t flags, trt_deform_stats* stats, std::string& err) {
+    if (flags != 0) { err = "trt_deform: flags must be 0"; return TRT_EINVAL; }
+    uint32_t n_meshes = (uint32_t)st->host_meshes.size();
+    for (uint32_t m = 0; m < n_meshes; ++m)
+        if ((uint64_t)st->host_meshes[m].palette + st->max_bone[m] >= n_matrices) {
+            err = "trt_deform: mesh " + std::to_string(m) + "'s palette indices reach past the matrices given";
+            return TRT_EINVAL;
+        }
+    if (n_meshes && !palette_rows) { err = "trt_deform: no palette"; return TRT_EINVAL; }
+    const uint64_t n_nodes = sb.bytes[2] / 32;
+    uint32_t t_instances = P[P_TABLE_FIRST + 7], w_indices = P[P_WORD_FIRST + 4];
+    uint32_t top = P[P_MOTION + 2], n_units = P[P_MOTION + 3];
+    if (n_units == 0 || n_units > MAX_UNITS) { err = "trt_deform: Params.motion.w (units) must be 1 to 2^18"; return TRT_EINVAL; }
+    if ((uint64_t)top + 2ull * n_units - 1 > n_nodes) { err = "trt_deform: the top tree's nodes reach past the node buffer"; return TRT_EINVAL; }
+    if ((uint64_t)t_instances + 10ull * n_units > sb.bytes[3] / 16) { err = "trt_deform: the units' records reach past the tables"; return TRT_EINVAL; }
+    for (uint32_t m = 0; m < n_meshes; ++m)
+        if ((uint64_t)w_indices + 3ull * (st->host_meshes[m].first_tri + st->host_meshes[m].n_tris) > sb.bytes[4] / 4) {
+            err = "trt_deform: a mesh's indices reach past the words";
+            return TRT_EINVAL;
+        }
+    cudaStream_t s = sb.stream;
+    if (n_meshes) {
+        if (n_matrices > st->palette_cap) {
+            if (st->palette) cudaFree(st->palette);
+            st->palette = nullptr;
+            DF_CUDA(cudaMalloc(&st->palette, 48ull * n_matrices));
+            st->palette_cap = n_matrices;
+        }
+        DF_CUDA(cudaMemcpyAsync(st->palette, palette_rows, 48ull * n_matrices, cudaMemcpyHostToDevice, s));
+    }
+    int rc = ensure_top(st, n_units, err);
+    if (rc) return rc;
+    if (stats) DF_CUDA(cudaEventRecord(st->ev[0], s));
+    float4* vertices = (float4*)sb.buf[0];
+    float4* leaves = (float4*)sb.buf[1];
+    uint4* nodes = (uint4*)sb.buf[2];
+    const uint32_t* words = (const uint32_t*)sb.buf[4];
+    if (n_meshes) k_skin<<<mesh_grid(st->max_vertices, n_meshes), 256, 0, s>>>(st->meshes, n_meshes, st->corners, st->palette, vertices);
+    if (stats) DF_CUDA(cudaEventRecord(st->ev[1], s));
+    if (n_meshes) k_gather<<<mesh_grid(st->max_tris, n_meshes), 256, 0, s>>>(st->meshes, n_meshes, vertices, words, w_indices, leaves, st->err);
+    if (stats) DF_CUDA(cudaEventRecord(st->ev[2], s));
+    if (n_meshes)
+        k_refit<<<mesh_grid(st->max_nodes, n_meshes), 256, 0, s>>>(st->meshes, n_meshes, vertices, words, w_indices, nodes,
+                                                                    st->parent, st->arrivals, st->err);
+    if (stats) DF_CUDA(cudaEventRecord(st->ev[3], s));
+    TopBuild T = st->T;
+    T.err = st->err;
+    T.nodes = nodes;
+    T.top_first = top;
+    T.n_units = n_units;
+    k_unit_boxes<<<(n_units + 255) / 256, 256, 0, s>>>((const uint4*)sb.buf[3], t_instances, n_nodes, T);
+    for (uint32_t level = 0; level < TOP_LEVELS; ++level) {
+        uint32_t most = std::min<uint32_t>(1u << level, n_units);  // a level holds at most 2^level nodes
+        uint32_t blocks = std::max(1u, std::min((most + TOP_WARPS - 1) / TOP_WARPS, 148u * 8u));
+        k_top_level<<<blocks, TOP_WARPS * 32, 0, s>>>(T, level);
+    }
+    if (stats) DF_CUDA(cudaEventRecord(st->ev[4], s));
+    DF_CUDA(cudaGetLastError());
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        DF_CUDA(cudaEventSynchronize(st->ev[4]));
+        cudaEventElapsedTime(&stats->device_ms, st->ev[0], st->ev[4]);
+        cudaEventElapsedTime(&stats->skin_ms, st->ev[0], st->ev[1]);
+        cudaEventElapsedTime(&stats->gather_ms, st->ev[1], st->ev[2]);
+        cudaEventElapsedTime(&stats->refit_ms, st->ev[2], st->ev[3]);
+        cudaEventElapsedTime(&stats->top_ms, st->ev[3], st->ev[4]);
+        rc = deform_errors(st, s, &stats->errors);
+        if (rc) return rc;
+        if (stats->errors) {
+            err = "trt_deform: the device found a bad tree (error bits " + std::to_string(stats->errors) + ")";
+            return TRT_EGUARD;
+        }
+    }
+    return TRT_OK;
+}
+
+int deform_errors(DeformState* st, cudaStream_t stream, uint32_t* errors) {
+    uint32_t e = 0;
+    if (cudaMemcpyAsync(&e, st->err, 4, cudaMemcpyDeviceToHost, stream) != cudaSuccess) return TRT_ECUDA;
+    if (cudaMemsetAsync(st->err, 0, 4, stream) != cudaSuccess) return TRT_ECUDA;
+    if (cudaStreamSynchronize(stream) != cudaSuccess) return TRT_ECUDA;
+    *errors = e;
+    return TRT_OK;
+}
+
+}  // namespace trt

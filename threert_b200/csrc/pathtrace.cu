@@ -22,6 +22,7 @@
 #include <string>
 #include <vector>
 
+#include "deform.h"
 #include "shade.cuh"
 #include "threert_cuda.h"
 #include "wide_bvh.cuh"
@@ -704,6 +705,10 @@ struct trt_scene {
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_extend, ev_shadow, ev_shade, ev_sort, ev_free;
     double extend_ms = 0, shadow_ms = 0, shade_ms = 0, sort_ms = 0;
     uint64_t extend_launches = 0, shadow_launches = 0, renders = 0, launches = 0;
+    // The per-frame deformation (trt_deform_setup), and whether the host copies still hold what the device does.
+    DeformState* deform = nullptr;
+    bool deform_stale = false;  // the nodes were written after setup: its tree checks no longer hold
+    bool deformed = false;      // a deformation ran: the host copies (and a wide BVH built from them) are old
 };
 
 namespace {
@@ -1095,6 +1100,7 @@ void trt_scene_free(trt_scene* s) {
     if (s->accum) cudaFree(s->accum);
     if (s->work) cudaFree(s->work);
     if (s->totals) cudaFree(s->totals);
+    deform_free(s->deform);
     s->wide.release();
     for (auto* v : {&s->ev_extend, &s->ev_shadow, &s->ev_shade, &s->ev_sort, &s->ev_free})
         for (auto& e : *v) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
@@ -1112,6 +1118,54 @@ int trt_scene_update(trt_scene* s, uint32_t which, uint64_t offset, const void* 
         std::memcpy(s->host[which].data() + offset, src, bytes);
         s->wide.invalidate();  // rebuilt from the edited buffers at the next render
     }
+    if (which == 2 && s->deform) s->deform_stale = true;
+    return TRT_OK;
+}
+
+int trt_scene_read(trt_scene* s, uint32_t which, uint64_t offset, void* dst, uint64_t bytes) {
+    if (!s) return TRT_EINVAL;
+    trt_ctx* c = s->ctx;
+    if (which > 4 || !dst || offset + bytes > s->bytes[which] || offset + bytes < offset)
+        return fail(c, TRT_EINVAL, "trt_scene_read: the range is not inside the buffer");
+    cudaSetDevice(c->device);
+    TRT_CUDA(c, cudaMemcpyAsync(dst, (const char*)s->buf[which] + offset, bytes, cudaMemcpyDeviceToHost, c->stream));
+    TRT_CUDA(c, cudaStreamSynchronize(c->stream));
+    return TRT_OK;
+}
+
+int trt_deform_setup(trt_scene* s, const trt_deform_desc* desc) {
+    if (!s) return TRT_EINVAL;
+    trt_ctx* c = s->ctx;
+    cudaSetDevice(c->device);
+    if (s->deformed) return fail(c, TRT_EINVAL, "trt_deform_setup: set up before the first deformation (the tree checks read the host copies)");
+    SceneBuffers sb{{s->buf[0], s->buf[1], s->buf[2], s->buf[3], s->buf[4]},
+                    {s->bytes[0], s->bytes[1], s->bytes[2], s->bytes[3], s->bytes[4]}, c->stream, s->host};
+    DeformState* st = nullptr;
+    std::string err;
+    int rc = deform_setup(&st, sb, desc, err);
+    if (rc) return fail(c, rc, err);
+    deform_free(s->deform);
+    s->deform = st;
+    s->deform_stale = false;
+    return TRT_OK;
+}
+
+int trt_deform(trt_scene* s, const uint32_t params[TRT_PARAMS_WORDS], const float* palette_rows, uint32_t n_matrices,
+               uint32_t flags, trt_deform_stats* stats) {
+    if (!s || !params) return TRT_EINVAL;
+    trt_ctx* c = s->ctx;
+    cudaSetDevice(c->device);
+    if (!s->deform) return fail(c, TRT_EINVAL, "trt_deform: no trt_deform_setup");
+    if (s->deform_stale) return fail(c, TRT_EINVAL, "trt_deform: the nodes were written after trt_deform_setup: set up again");
+    int rc = check_params(s, params);
+    if (rc) return rc;
+    SceneBuffers sb{{s->buf[0], s->buf[1], s->buf[2], s->buf[3], s->buf[4]},
+                    {s->bytes[0], s->bytes[1], s->bytes[2], s->bytes[3], s->bytes[4]}, c->stream, s->host};
+    std::string err;
+    s->deformed = true;
+    s->wide.invalidate();
+    rc = deform_run(s->deform, sb, params, palette_rows, n_matrices, flags, stats, err);
+    if (rc) return fail(c, rc, err);
     return TRT_OK;
 }
 
@@ -1141,6 +1195,7 @@ int trt_render(trt_scene* s, const uint32_t params[TRT_PARAMS_WORDS], uint32_t f
     }
     uint64_t launches0 = s->launches;
     bool count = (flags & TRT_RENDER_COUNT) != 0, binary = (flags & TRT_RENDER_WIDE) == 0;
+    if (!binary && s->deformed) return fail(c, TRT_EINVAL, "a deformed scene walks the binary trees (the wide BVH is built from host copies)");
     if (!binary && s->wide.ensure(params, s->host, c->stream) != 0) return fail(c, TRT_EINVAL, s->wide.error);
     if (spp > 0) {
         if (count) rc = binary ? render_waves<true, false>(s, P, first_sample, spp, flags) : render_waves<true, true>(s, P, first_sample, spp, flags);
@@ -1205,10 +1260,10 @@ int trt_trace(trt_scene* s, const uint32_t params[TRT_PARAMS_WORDS], const trt_r
     e = cudaMemcpyAsync(dr, rays, sizeof(trt_ray) * n, cudaMemcpyHostToDevice, c->stream);
     bool binary = (flags & TRT_RENDER_WIDE) == 0;
     bool count = (flags & TRT_RENDER_COUNT) != 0;
-    if (e == cudaSuccess && !binary && s->wide.ensure(params, s->host, c->stream) != 0) {
+    if (e == cudaSuccess && !binary && (s->deformed || s->wide.ensure(params, s->host, c->stream) != 0)) {
         cudaFree(dr);
         cudaFree(dh);
-        return fail(c, TRT_EINVAL, s->wide.error);
+        return fail(c, TRT_EINVAL, s->deformed ? "a deformed scene walks the binary trees" : s->wide.error);
     }
     DScene S = scene_view(s);
     Walk wk{S, s->wide.view(), P.w[P_MOTION + 2], P.w[P_MOTION + 3]};

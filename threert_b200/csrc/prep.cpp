@@ -32,8 +32,17 @@ inline V3 mk(float x, float y, float z) { V3 v; v.x = x; v.y = y; v.z = z; retur
 inline V3 operator+(V3 a, V3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
 inline V3 operator-(V3 a, V3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
 inline V3 operator*(V3 a, float s) { return mk(a.x * s, a.y * s, a.z * s); }
-inline V3 vmin(V3 a, V3 b) { return mk(std::min(a.x, b.x), std::min(a.y, b.y), std::min(a.z, b.z)); }
-inline V3 vmax(V3 a, V3 b) { return mk(std::max(a.x, b.x), std::max(a.y, b.y), std::max(a.z, b.z)); }
+// glam's Vec3A::min / max (SSE minps / maxps): the first operand where it is smaller (larger), else the second.
+inline float gmin(float a, float b) { return a < b ? a : b; }
+inline float gmax(float a, float b) { return a > b ? a : b; }
+inline V3 vmin(V3 a, V3 b) { return mk(gmin(a.x, b.x), gmin(a.y, b.y), gmin(a.z, b.z)); }
+inline V3 vmax(V3 a, V3 b) { return mk(gmax(a.x, b.x), gmax(a.y, b.y), gmax(a.z, b.z)); }
+// f32::total_cmp's key: orders every float, -0 before +0.
+inline int32_t total_key(float f) {
+    int32_t b;
+    std::memcpy(&b, &f, 4);
+    return b ^ (int32_t)(((uint32_t)(b >> 31)) >> 1);
+}
 inline V3 splat(float s) { return mk(s, s, s); }
 inline float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 inline V3 cross(V3 a, V3 b) { return mk(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
@@ -414,8 +423,8 @@ void build_sah(const std::vector<Box>& boxes, size_t max_depth, std::vector<GpuN
             int axis = (ext.x >= ext.y && ext.x >= ext.z) ? 0 : (ext.y >= ext.z ? 1 : 2);
             std::nth_element(order.begin() + t.start, order.begin() + t.start + count / 2, order.begin() + t.end,
                              [&](uint32_t a, uint32_t b) {
-                                 float ca = centres[a][axis], cb = centres[b][axis];
-                                 return ca < cb || (ca == cb && a < b);
+                                 int32_t ka = total_key(centres[a][axis]), kb = total_key(centres[b][axis]);
+                                 return ka < kb || (ka == kb && a < b);
                              });
             mid = count / 2;
         }
@@ -805,17 +814,29 @@ int trt_prep_build(const trt_scene_spec* spec, trt_prepared** out) {
 
         // Mesh trees (lib.rs:865-943 unit_trees): each mesh's triangles put in its tree's order, ranked in sections.
         struct Mesh {
-            uint32_t first = 0, count = 0, vfirst = 0, n_sections = 1, root = 0;
+            uint32_t first = 0, count = 0, vfirst = 0, n_vertices = 0, n_sections = 1, root = 0;
+            uint32_t like = NO_INST;  // the mesh whose triangles, tree and attributes this one repeats
             std::vector<std::array<V3, 3>> tris;
             std::vector<std::array<float, 4>> attr_n0, attr_n1, attr_n2;  // per corner normal + uv
             std::vector<uint32_t> section, rank;
             MeshTree tree;
         };
         std::vector<Mesh> meshes(S.n_meshes);
+        // A mesh's triangles, tree and attributes: its own, or those of the mesh it repeats.
+        auto data = [&](const Mesh& m) -> const Mesh& { return m.like == NO_INST ? m : meshes[m.like]; };
         uint32_t tri_total = 0;
         for (uint32_t mi = 0; mi < S.n_meshes; ++mi) {
             const trt_mesh_spec& ms = S.meshes[mi];
             Mesh& m = meshes[mi];
+            if (ms.like) {
+                if (ms.like - 1 >= mi) throw std::runtime_error("a mesh repeats one that is not before it");
+                m.like = meshes[ms.like - 1].like == NO_INST ? ms.like - 1 : meshes[ms.like - 1].like;
+                m.count = meshes[m.like].count;
+                m.n_sections = meshes[m.like].n_sections;
+                m.first = tri_total;
+                tri_total += m.count;
+                continue;
+            }
             m.count = ms.n_tris;
             m.n_sections = std::max<uint32_t>(ms.n_sections, 1);
             std::vector<std::array<V3, 3>> tris(ms.n_tris);
@@ -865,6 +886,20 @@ int trt_prep_build(const trt_scene_spec* spec, trt_prepared** out) {
         P->leaves.reserve((size_t)tri_total * 3);
         for (Mesh& m : meshes) {
             m.vfirst = (uint32_t)(P->vertices.size() / 3);
+            if (m.like != NO_INST) {
+                // A repeat: the original's vertex records, indices (counted from the mesh's first vertex) and leaves.
+                const Mesh& o = meshes[m.like];
+                m.n_vertices = o.n_vertices;
+                auto repeat = [](auto& v, size_t a, size_t b) {
+                    size_t n = b - a, at = v.size();
+                    v.resize(at + n);
+                    std::copy(v.begin() + a, v.begin() + b, v.begin() + at);
+                };
+                repeat(P->vertices, 3ull * o.vfirst, 3ull * (o.vfirst + o.n_vertices));
+                repeat(indices, 3ull * o.first, 3ull * (o.first + o.count));
+                repeat(P->leaves, 3ull * o.first, 3ull * (o.first + o.count));
+                continue;
+            }
             std::unordered_map<std::string, uint32_t> seen;
             uint32_t nv = 0;
             for (uint32_t k = 0; k < m.count; ++k) {
@@ -892,12 +927,14 @@ int trt_prep_build(const trt_scene_spec* spec, trt_prepared** out) {
                 P->leaves.push_back({e1.x, e1.y, e1.z, bf(m.rank[k])});
                 P->leaves.push_back({e2.x, e2.y, e2.z, 0.0f});
             }
+            m.n_vertices = nv;
         }
 
         // Node buffer: the mesh trees side by side, then the top tree (units.rs Layout).
         for (Mesh& m : meshes) {
             m.root = (uint32_t)P->nodes.size();
-            P->nodes.insert(P->nodes.end(), m.tree.nodes.begin(), m.tree.nodes.end());
+            const auto& tn = data(m).tree.nodes;
+            P->nodes.insert(P->nodes.end(), tn.begin(), tn.end());
         }
         uint32_t top_first = (uint32_t)P->nodes.size();
 
@@ -919,13 +956,13 @@ int trt_prep_build(const trt_scene_spec* spec, trt_prepared** out) {
                 if (mat >= mats.size()) throw std::runtime_error("an instance names a material that is not there");
                 uint32_t sfirst = m.first;
                 for (uint32_t k = 0; k < m.count; ++k)
-                    if (m.section[k] == s) { sfirst = m.first + k; break; }
+                    if (data(m).section[k] == s) { sfirst = m.first + k; break; }
                 rows.push_back({mat, sfirst, NO_EMITTER, 0u});  // scene.rs:115-118 row_of (class 0: opaque)
             }
             GpuInstance g = instance_gpu(worlds[r], m.first, is.object, m.vfirst, inst_rows[r], 0u);
             unit_record(g, m.root, is.cast_shadow != 0);
             insts.push_back(g);
-            unit_boxes.push_back(unit_box(worlds[r], m.tree.lo, m.tree.hi));
+            unit_boxes.push_back(unit_box(worlds[r], data(m).tree.lo, data(m).tree.hi));
             unit_records.push_back(r);
         }
         if (unit_boxes.size() > MAX_UNITS) throw std::runtime_error("more units than a top tree holds");
@@ -950,7 +987,8 @@ int trt_prep_build(const trt_scene_spec* spec, trt_prepared** out) {
             Mesh& m = meshes[is.mesh];
             std::vector<int64_t> starts(m.n_sections, -1);
             std::vector<uint32_t> sec_count(m.n_sections, 0);
-            for (uint32_t k = 0; k < m.count; ++k) sec_count[m.section[k]]++;
+            const Mesh& md = data(m);
+            for (uint32_t k = 0; k < m.count; ++k) sec_count[md.section[k]]++;
             uint32_t at = 0;
             for (uint32_t s = 0; s < m.n_sections; ++s)
                 if (emits(rows[inst_rows[r] + s][0])) { starts[s] = at; at += sec_count[s]; }
@@ -961,12 +999,12 @@ int trt_prep_build(const trt_scene_spec* spec, trt_prepared** out) {
             std::vector<ETri> out(at);
             std::vector<GpuEmitterTri> gout(at);
             for (uint32_t k = 0; k < m.count; ++k) {
-                uint32_t s = m.section[k];
+                uint32_t s = md.section[k];
                 if (starts[s] < 0) continue;
-                uint32_t slot = (uint32_t)starts[s] + m.rank[k];
+                uint32_t slot = (uint32_t)starts[s] + md.rank[k];
                 uint32_t mat = rows[inst_rows[r] + s][0];
                 V3 w[3];
-                for (int c = 0; c < 3; ++c) w[c] = transform_point(worlds[r], m.tris[k][c]);
+                for (int c = 0; c < 3; ++c) w[c] = transform_point(worlds[r], md.tris[k][c]);
                 V3 cr = cross(w[1] - w[0], w[2] - w[0]);
                 float area = 0.5f * std::sqrt(dot(cr, cr));
                 V3 cen = w[0] + w[1] + w[2];
@@ -1227,6 +1265,40 @@ uint32_t trt_prep_bvh(const float* tris, uint32_t n_tris, uint32_t max_depth, ui
         g_error = e.what();
         return 0;
     }
+}
+
+int trt_prep_unit_records(uint32_t n, const float* worlds, const uint32_t* info, const uint32_t* roots,
+                          const uint32_t* cast_shadow, uint32_t* out) {
+    if (n && (!worlds || !info || !roots || !cast_shadow || !out)) return 1;
+    for (uint32_t i = 0; i < n; ++i) {
+        Mat34 w;
+        std::memcpy(w.m, worlds + 12ull * i, sizeof(w.m));
+        GpuInstance g = instance_gpu(w, info[4ull * i], info[4ull * i + 1], info[4ull * i + 2], info[4ull * i + 3], 0u);
+        unit_record(g, roots[i], cast_shadow[i] != 0);
+        std::memcpy(out + 40ull * i, &g, sizeof(g));
+    }
+    return 0;
+}
+
+int trt_prep_units_top(uint32_t n, const float* worlds, const float* local_boxes, uint32_t* nodes, uint32_t* depth) {
+    if (n == 0 || n > MAX_UNITS || !worlds || !local_boxes || !nodes) return 1;
+    std::vector<Box> boxes(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        Mat34 w;
+        std::memcpy(w.m, worlds + 12ull * i, sizeof(w.m));
+        const float* b = local_boxes + 6ull * i;
+        boxes[i] = unit_box(w, mk(b[0], b[1], b[2]), mk(b[3], b[4], b[5]));
+    }
+    std::vector<GpuNode> top;
+    std::vector<uint32_t> order;
+    build_sah(boxes, TOP_DEPTH - 1, top, order);
+    for (GpuNode& nd : top)
+        if (nd.count > 0) nd.left_or_first = order[nd.left_or_first];
+    long d = check_tree(top.data(), top.size(), TOP_DEPTH, 1, n);
+    if (d < 0 || top.size() != 2ull * n - 1) return 1;
+    if (depth) *depth = (uint32_t)d;
+    std::memcpy(nodes, top.data(), top.size() * sizeof(GpuNode));
+    return 0;
 }
 
 int trt_prep_check_tree(const uint32_t* nodes, uint32_t n_nodes, uint32_t max_depth, uint32_t max_leaf,

@@ -101,6 +101,34 @@ class Scene:
         self.gpu._check(rc, "trt_trace")
         return hits
 
+    def read(self, which: int, offset: int, nbytes: int, dtype=np.uint8) -> np.ndarray:
+        """Bytes [offset, offset + nbytes) of buffer `which` (0 vertices, 1 leaves, 2 nodes, 3 tables, 4 words)."""
+        out = np.empty(nbytes, np.uint8)
+        self.gpu._check(N.lib().trt_scene_read(self.handle, which, offset, out.ctypes.data, nbytes), "trt_scene_read")
+        return out.view(dtype)
+
+    def update(self, which: int, offset: int, data: np.ndarray):
+        a = np.ascontiguousarray(data)
+        self.gpu._check(N.lib().trt_scene_update(self.handle, which, offset, a.ctypes.data, a.nbytes),
+                        "trt_scene_update")
+
+    def deform_setup(self, corners: np.ndarray, meshes: np.ndarray):
+        """corners: (n, 16) float32 skin corners (trt_corner); meshes: (m, 8) uint32 trt_deform_mesh rows."""
+        c = np.ascontiguousarray(corners, np.float32).reshape(-1, 16)
+        m = np.ascontiguousarray(meshes, np.uint32).reshape(-1, 8)
+        d = N.DeformDesc(c.ctypes.data, len(c), m.ctypes.data_as(C.POINTER(N.DeformMesh)), len(m))
+        self.gpu._check(N.lib().trt_deform_setup(self.handle, C.byref(d)), "trt_deform_setup")
+
+    def deform(self, params: np.ndarray, palette: np.ndarray, stats: bool = True) -> dict | None:
+        """One frame's deformation; palette: (n, 3, 4) float32 matrices. With stats, waits and returns the times."""
+        p = np.ascontiguousarray(params, dtype=np.uint32)
+        pal = np.ascontiguousarray(palette, np.float32).reshape(-1, 12)
+        st = N.DeformStats() if stats else None
+        rc = N.lib().trt_deform(self.handle, p.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                pal.ctypes.data_as(C.POINTER(C.c_float)), len(pal), 0, C.byref(st) if stats else None)
+        self.gpu._check(rc, "trt_deform")
+        return {f[0]: getattr(st, f[0]) for f in N.DeformStats._fields_} if stats else None
+
     def totals(self) -> dict:
         t = N.Totals()
         self.gpu._check(N.lib().trt_scene_totals(self.handle, C.byref(t)), "trt_scene_totals")

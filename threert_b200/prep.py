@@ -26,6 +26,7 @@ class Mesh:
     uvs: np.ndarray | None = None         # (n, 3, 2)
     sections: np.ndarray | None = None    # (n,) section of each triangle
     n_sections: int = 1
+    like: int | None = None               # an earlier mesh this one repeats (own vertices, leaves and tree)
 
 
 @dataclass
@@ -165,13 +166,18 @@ def prepare(desc: SceneDescription) -> Prepared:
     keep = []
     meshes = (N.MeshSpec * len(desc.meshes))()
     for k, m in enumerate(desc.meshes):
+        if m.like is not None:
+            src = desc.meshes[m.like]
+            meshes[k] = N.MeshSpec(len(np.asarray(src.positions).reshape(-1, 9)), None, None, None, None,
+                                   src.n_sections, m.like + 1)
+            continue
         pos = _f32(m.positions, (-1, 9))
         nrm = _f32(m.normals, (-1, 9)) if m.normals is not None else None
         uvs = _f32(m.uvs, (-1, 6)) if m.uvs is not None else None
         sec = np.ascontiguousarray(m.sections, dtype=np.uint32) if m.sections is not None else None
         keep += [pos, nrm, uvs, sec]
         meshes[k] = N.MeshSpec(pos.shape[0], _ptr(pos, C.c_float), _ptr(nrm, C.c_float), _ptr(uvs, C.c_float),
-                               _ptr(sec, C.c_uint32), m.n_sections)
+                               _ptr(sec, C.c_uint32), m.n_sections, 0)
     mats = (N.MaterialSpec * max(1, len(desc.materials)))()
     for k, m in enumerate(desc.materials):
         mats[k] = N.MaterialSpec((C.c_float * 4)(*m.base[:3], m.opacity), (C.c_float * 3)(*m.emissive), m.metallic,
@@ -233,6 +239,33 @@ def prepare(desc: SceneDescription) -> Prepared:
             env_w=b.env_w, env_h=b.env_h, params=params, info=d)
     finally:
         L.trt_prep_free(h)
+
+
+def unit_records(worlds: np.ndarray, info: np.ndarray, roots: np.ndarray, cast_shadow: np.ndarray) -> np.ndarray:
+    """trt_prep_unit_records: (n, 40) uint32 instance records for worlds (n, 3, 4), info (n, 4), roots (n,)."""
+    w = _f32(worlds, (-1, 12))
+    n = len(w)
+    inf = np.ascontiguousarray(info, np.uint32).reshape(n, 4)
+    r = np.ascontiguousarray(roots, np.uint32).reshape(n)
+    cs = np.ascontiguousarray(cast_shadow, np.uint32).reshape(n)
+    out = np.zeros((n, 40), np.uint32)
+    if N.lib().trt_prep_unit_records(n, _ptr(w, C.c_float), _ptr(inf, C.c_uint32), _ptr(r, C.c_uint32),
+                                     _ptr(cs, C.c_uint32), _ptr(out, C.c_uint32)) != 0:
+        raise ValueError("trt_prep_unit_records failed")
+    return out
+
+
+def units_top(worlds: np.ndarray, local_boxes: np.ndarray) -> tuple[np.ndarray, int]:
+    """trt_prep_units_top: the top tree's (2n - 1, 8) uint32 nodes over units with these worlds and model boxes."""
+    w = _f32(worlds, (-1, 12))
+    n = len(w)
+    b = _f32(local_boxes, (n, 6))
+    nodes = np.zeros((2 * n - 1, 8), np.uint32)
+    depth = C.c_uint32()
+    if N.lib().trt_prep_units_top(n, _ptr(w, C.c_float), _ptr(b, C.c_float), _ptr(nodes, C.c_uint32),
+                                  C.byref(depth)) != 0:
+        raise ValueError("trt_prep_units_top failed")
+    return nodes, depth.value
 
 
 def params_with(params: np.ndarray, **kw) -> np.ndarray:
