@@ -207,6 +207,110 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+CROWD_DEPTH = 3
+CROWD_METRIC = "Mrays/s (closest + shadow rays, crowd 720p 1 spp depth 3, skin + refit + top rebuild each frame)"
+
+
+def run_crowd(args, rank, world, local, dist):
+    """Config 2: 5,000 walking humanoids (20,160 triangles each, 30 bones) in `--groups` pose groups on a 49,928-
+    triangle ground under config 1's lights; each frame writes the walkers' records (trt_scene_update), deforms the
+    scene on the device (trt_deform: skin, leaf gather, refit of every group's tree, the top tree rebuilt) and renders
+    it. The frame's records and palettes are made before the timed region; their copies to the device are in it."""
+    import torch
+    from threert_b200 import Gpu, crowd, prep
+    from threert_b200 import _native as N
+    t0 = time.perf_counter()
+    c = crowd.crowd(n=5000, groups=args.groups, width=WIDTH, height=HEIGHT, max_depth=CROWD_DEPTH)
+    P = prep.prepare(c.desc)
+    corners, jobs = crowd.deform_jobs(P, c)
+    log(f"crowd: {P.info['n_tris']} tris, {P.info['n_units']} units, {args.groups} pose groups, "
+        f"prep {time.perf_counter() - t0:.1f} s")
+    gpu = Gpu(local)
+    name, sms = gpu.device_info()
+    S = gpu.upload(P)
+    S.deform_setup(corners, jobs)
+    t_inst, _ = crowd.records(P)
+    warm_frames, frames = rank_frames(rank, world, args.warmup, args.steps)
+    inputs = {}
+    for f in set(warm_frames + frames):
+        t = f / crowd.FPS
+        cam = crowd.crowd_camera(f, WIDTH, HEIGHT, c.extent)
+        inputs[f] = (prep.set_camera(P.params, cam), np.ascontiguousarray(crowd.frame_records(P, c, t)),
+                     np.ascontiguousarray(crowd.palettes(t, c.phase, c.scale).reshape(-1, 12)))
+    L = N.lib()
+
+    def frame(f, acc_ptr=None):
+        params, rec, pal = inputs[f]
+        gpu._check(L.trt_scene_update(S.handle, 3, t_inst * 16, rec.ctypes.data, rec.nbytes), "trt_scene_update")
+        p = params.ctypes.data_as(C.POINTER(C.c_uint32))
+        gpu._check(L.trt_deform(S.handle, p, pal.ctypes.data_as(C.POINTER(C.c_float)), len(pal), 0, None), "trt_deform")
+        gpu._check(L.trt_render(S.handle, p, 0, SPP, 0, acc_ptr, None), "trt_render")
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    for f in warm_frames:
+        frame(f)
+    gpu.synchronize()
+    S.reset_totals()
+    S.set_profiling(True)
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        pass
+    clocks = ClockSampler(uuid)
+    barrier()
+    gpu.synchronize()
+    clocks.start()
+    gpu.timer_start()
+    for f in frames:
+        frame(f)
+    ms = gpu.timer_stop()
+    clk = clocks.stop()
+    barrier()
+    tot = S.totals()
+    S.set_profiling(False)
+    rays = tot["closest_rays"] + tot["shadow_rays"]
+    # The deformation's own stages, frame by frame, untimed above.
+    ds = [S.deform(inputs[f][0], inputs[f][2], stats=True) for f in frames[:8]]
+    deform = {k: float(np.mean([d[k] for d in ds])) for k in ("device_ms", "skin_ms", "refit_ms", "top_ms")}
+    # End to end: the same frames with the accum read back into pinned memory.
+    acc = torch.empty((WIDTH * HEIGHT, N.PIXEL_FLOATS), dtype=torch.float32, pin_memory=True)
+    acc_ptr = C.cast(acc.data_ptr(), C.POINTER(C.c_float))
+    barrier()
+    gpu.synchronize()
+    gpu.timer_start()
+    for f in frames:
+        frame(f, acc_ptr)
+    e2e_ms = gpu.timer_stop()
+    barrier()
+    ms, e2e_ms, rays_all = reduce_over_ranks(dist, ms, e2e_ms, float(rays), device="cuda")
+    rec_bytes = inputs[frames[0]][1].nbytes + inputs[frames[0]][2].nbytes + 624
+    line = {
+        "metric": CROWD_METRIC, "value": rays_all / (ms * 1e-3) / 1e6, "unit": "Mrays/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"crowd: 5000 walkers x 20160 tris in {args.groups} pose groups "
+                               f"({P.info['n_tris']} tris), 49928-tri ground, 1280x720, 1 spp, depth 3",
+                   "frames_per_rank": args.steps, "pose_groups": args.groups,
+                   "per_step": "records + palette H2D, trt_deform (skin, leaf gather, refit, top rebuild), render",
+                   "device": name, "sms": sms, "parallelism": f"replicas x{world}"},
+        "e2e": {"value": rays_all / (e2e_ms * 1e-3) / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": rec_bytes,
+                "d2h_bytes_per_step": WIDTH * HEIGHT * 80},
+        "gpu_launches": int(tot["launches"]),
+        "clocks": clk,
+        "deform_ms_per_step": deform,
+        "stage_ms_per_step": {"extend": tot["extend_ms"] / args.steps, "shadow": tot["shadow_ms"] / args.steps,
+                              "shade": tot["shade_ms"] / args.steps, "sort": tot["sort_ms"] / args.steps},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    S.close()
+    gpu.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -219,11 +323,18 @@ def main():
                     help="coherence sorts on the device: 'none', or a comma list of rays, hits, shadows "
                          "(hits by material is the pass's default; the other two measured slower here)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--workload", default="city", choices=["city", "crowd"],
+                    help="city (the headline workload) or the crowd with its per-frame deformation")
+    ap.add_argument("--groups", type=int, default=1, help="crowd: pose groups (skinned copies of the humanoid)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
+        if args.workload != "city":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the CPU arm times the city workload only"}))
+            return
         run_reference(args, rank, world)
         return
 
@@ -235,6 +346,12 @@ def main():
         torch.cuda.set_device(local)
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    if args.workload == "crowd":
+        run_crowd(args, rank, world, local, dist)
+        if dist:
+            dist.destroy_process_group()
+        return
 
     from threert_b200 import Gpu
     from threert_b200 import _native as N

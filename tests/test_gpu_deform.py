@@ -17,12 +17,16 @@ from util import luma, random_rays, small_crowd
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(scope="module")
-def scene():
-    c = small_crowd()
+def make_scene(n=160):
+    c = small_crowd(n=n)
     P = prep.prepare(c.desc)
     corners, jobs = crowd.deform_jobs(P, c)
     return c, P, corners, jobs
+
+
+@pytest.fixture(scope="module")
+def scene():
+    return make_scene()
 
 
 def run_frame(S, P, c, t):
@@ -58,8 +62,9 @@ def read_back(S, P):
             S.read(2, 0, P.nodes.nbytes, np.uint32).reshape(P.nodes.shape))
 
 
-def test_deform_matches_the_oracle(gpu, scene):
-    c, P, corners, jobs = scene
+@pytest.mark.parametrize("n", [160, 700])  # 700: the top build's first levels take the CTA-wide kernel
+def test_deform_matches_the_oracle(gpu, n):
+    c, P, corners, jobs = make_scene(n)
     S = gpu.upload(P)
     S.deform_setup(corners, jobs)
     for t in (0.4, 1.3):  # two frames: the refit's counters are zero again after each

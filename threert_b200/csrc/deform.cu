@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <unordered_map>
 
 #include "device_common.cuh"
 
@@ -22,6 +23,8 @@ constexpr uint32_t TOP_MAX_DEPTH = TOP_DEPTH - 1u;  // build_sah's max_depth
 constexpr uint32_t TOP_LEVELS = TOP_MAX_DEPTH + 1u; // levels 0 .. TOP_MAX_DEPTH
 constexpr uint32_t MAX_UNITS = 1u << TOP_MAX_DEPTH;
 constexpr uint32_t TOP_BINS = 32u;                  // units.rs:121
+// Top-tree nodes of more units than this are built by a CTA each (k_top_big), the rest by a warp each (k_top_level).
+constexpr uint32_t TOP_SMALL = 256u, BIG_WARPS = 16u;
 constexpr uint32_t REFIT_CLIMB = 64u;               // a mesh tree is less deep than the walk's 64-entry stack
 // Error bits the kernels record.
 constexpr uint32_t E_TREE = 1u, E_DEPTH = 2u, E_ROOT = 4u, E_INDEX = 8u;
@@ -85,96 +88,82 @@ __device__ __forceinline__ V3 corner(const float4* vertices, const uint32_t* wor
     return xyz(vertices[3ull * (M.first_vertex + i)]);
 }
 
-// leaf_gather.wgsl:31-52: each triangle of a mesh again from its vertices: (v0, keep w), (e1, keep w), (e2, 0).
-__global__ void k_gather(const DMesh* __restrict__ meshes, uint32_t n_meshes, const float4* __restrict__ vertices,
-                         const uint32_t* __restrict__ words, uint32_t w_indices, float4* leaves, uint32_t* err) {
-    for (uint32_t m = blockIdx.y; m < n_meshes; m += gridDim.y) {
-        DMesh M = meshes[m];
-        for (uint32_t local = blockIdx.x * blockDim.x + threadIdx.x; local < M.n_tris; local += gridDim.x * blockDim.x) {
-            uint32_t t = M.first_tri + local;
-            V3 p0 = corner(vertices, words, w_indices, M, t, 0, err);
-            V3 p1 = corner(vertices, words, w_indices, M, t, 1, err);
-            V3 p2 = corner(vertices, words, w_indices, M, t, 2, err);
-            uint64_t k = 3ull * t;
-            leaves[k] = f4(p0, leaves[k].w);
-            leaves[k + 1] = f4(p1 - p0, leaves[k + 1].w);
-            leaves[k + 2] = f4(p2 - p0, 0.0f);
-        }
-    }
-}
-
-// ---- refit (units.rs:251-275) -------------------------------------------------------------------------------------
+// ---- leaf gather (leaf_gather.wgsl) and refit (units.rs:251-275), one pass ------------------------------------------
 //
-// The reference refits a tree from its last node back to its root, one node after another. Here each leaf's thread
-// takes its box from its triangles' corners, then climbs: at each parent the first child's thread to arrive stops
-// (atomic counter) and the second, which sees both children's boxes, writes the parent's and goes on. The counter
-// is put back to zero by the thread that used it, so it is zero for the next frame.
+// The reference refits a tree from its last node back to its root, one node after another, after a separate pass
+// has gathered the leaves. Here one CTA takes a mesh's tree a level at a time, deepest first (every node of a level
+// at once, a barrier between levels): a leaf gathers its triangles again from the vertices (leaf_gather.wgsl:41-51:
+// (v0, keep w), (e1, keep w), (e2, 0)) and folds their corners into its box; an interior node joins its children's
+// boxes, written a level before. The level order of each distinct tree shape is made once, at setup.
 
 __device__ __forceinline__ void store_box(uint4* nodes, uint32_t i, V3 lo, V3 hi, uint32_t lf, uint32_t count) {
     nodes[2ull * i] = make_uint4(bu(lo.x), bu(lo.y), bu(lo.z), lf);
     nodes[2ull * i + 1] = make_uint4(bu(hi.x), bu(hi.y), bu(hi.z), count);
 }
 
-__global__ void k_refit(const DMesh* __restrict__ meshes, uint32_t n_meshes, const float4* __restrict__ vertices,
-                        const uint32_t* __restrict__ words, uint32_t w_indices, uint4* nodes,
-                        const uint32_t* __restrict__ parent, uint32_t* arrivals, uint32_t* err) {
+// A distinct tree shape: its leaves in triangle order, then its interior nodes a level at a time, deepest first
+// (level_start[levels_first .. levels_first + n_levels] are offsets into its interior nodes).
+struct Shape { uint32_t leaves_first, n_leaves, interior_first, levels_first, n_levels; };
+
+// The leaves of every deforming mesh at once (one thread a leaf, blockIdx.y a mesh), neighbours in triangle order on
+// neighbouring threads, whose corners they share.
+__global__ void k_refit_leaves(const DMesh* __restrict__ meshes, const uint32_t* __restrict__ shape_of,
+                               uint32_t n_meshes, const Shape* __restrict__ shapes,
+                               const uint32_t* __restrict__ level_nodes, const float4* __restrict__ vertices,
+                               const uint32_t* __restrict__ words, uint32_t w_indices, float4* leaves, uint4* nodes,
+                               uint32_t* err) {
     for (uint32_t m = blockIdx.y; m < n_meshes; m += gridDim.y) {
         DMesh M = meshes[m];
-        for (uint32_t local = blockIdx.x * blockDim.x + threadIdx.x; local < M.n_nodes; local += gridDim.x * blockDim.x) {
-            uint32_t i = M.root + local;
-            uint4 a = __ldcg(nodes + 2ull * i), b = __ldcg(nodes + 2ull * i + 1);
-            if (b.w == 0u) continue;  // interior: its box comes from its children
+        Shape sh = shapes[shape_of[m]];
+        for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < sh.n_leaves; j += gridDim.x * blockDim.x) {
+            uint32_t i = M.root + level_nodes[sh.leaves_first + j];
+            uint4 na = nodes[2ull * i], nb = nodes[2ull * i + 1];
             V3 lo = v3(__uint_as_float(0x7f800000u)), hi = v3(__uint_as_float(0xff800000u));
-            for (uint32_t k = a.w; k < a.w + b.w; ++k) {
+            for (uint32_t k = na.w; k < na.w + nb.w; ++k) {
                 uint32_t t = M.first_tri + k;
+                V3 p[3];
                 for (uint32_t c = 0; c < 3; ++c) {
-                    V3 v = corner(vertices, words, w_indices, M, t, c, err);
-                    if (finite1(v.x) && finite1(v.y) && finite1(v.z)) {
-                        lo = V3{gmin(lo.x, v.x), gmin(lo.y, v.y), gmin(lo.z, v.z)};
-                        hi = V3{gmax(hi.x, v.x), gmax(hi.y, v.y), gmax(hi.z, v.z)};
+                    p[c] = corner(vertices, words, w_indices, M, t, c, err);
+                    if (finite1(p[c].x) && finite1(p[c].y) && finite1(p[c].z)) {
+                        lo = V3{gmin(lo.x, p[c].x), gmin(lo.y, p[c].y), gmin(lo.z, p[c].z)};
+                        hi = V3{gmax(hi.x, p[c].x), gmax(hi.y, p[c].y), gmax(hi.z, p[c].z)};
                     }
                 }
+                uint64_t q = 3ull * t;
+                leaves[q] = f4(p[0], leaves[q].w);
+                leaves[q + 1] = f4(p[1] - p[0], leaves[q + 1].w);
+                leaves[q + 2] = f4(p[2] - p[0], 0.0f);
             }
             if (lo.x > hi.x) { lo = v3(0.0f); hi = v3(0.0f); }  // a leaf of nothing finite: a point
-            store_box(nodes, i, lo, hi, a.w, b.w);
-            uint32_t cur = i;
-            for (uint32_t climb = 0;; ++climb) {
-                uint32_t par = parent[cur];
-                if (par == NONE) break;
-                if (climb >= REFIT_CLIMB) { atomicOr(err, E_TREE); break; }
-                __threadfence();
-                if (atomicAdd(&arrivals[par], 1u) == 0u) break;  // the sibling's thread finishes the parent
-                arrivals[par] = 0u;
-                __threadfence();
-                uint4 pa = __ldcg(nodes + 2ull * par), pb = __ldcg(nodes + 2ull * par + 1);
-                uint32_t l = M.root + pa.w;
-                uint4 la = __ldcg(nodes + 2ull * l), lb = __ldcg(nodes + 2ull * l + 1);
-                uint4 ra = __ldcg(nodes + 2ull * l + 2), rb = __ldcg(nodes + 2ull * l + 3);
-                V3 plo = V3{gmin(__uint_as_float(la.x), __uint_as_float(ra.x)), gmin(__uint_as_float(la.y), __uint_as_float(ra.y)),
-                            gmin(__uint_as_float(la.z), __uint_as_float(ra.z))};
-                V3 phi = V3{gmax(__uint_as_float(lb.x), __uint_as_float(rb.x)), gmax(__uint_as_float(lb.y), __uint_as_float(rb.y)),
-                            gmax(__uint_as_float(lb.z), __uint_as_float(rb.z))};
-                store_box(nodes, par, plo, phi, pa.w, pb.w);
-                cur = par;
-            }
+            store_box(nodes, i, lo, hi, na.w, nb.w);
         }
     }
 }
 
-// Parent links of the deforming meshes' nodes (once, at setup): parent[root + left + {0,1}] = the interior node.
-__global__ void k_parents(const DMesh* __restrict__ meshes, uint32_t n_meshes, const uint4* __restrict__ nodes,
-                          uint32_t* parent) {
-    for (uint32_t m = blockIdx.y; m < n_meshes; m += gridDim.y) {
+// Then each mesh's interior nodes, a CTA a mesh, a level at a time from the deepest (a barrier between levels).
+__global__ void k_refit(const DMesh* __restrict__ meshes, const uint32_t* __restrict__ shape_of, uint32_t n_meshes,
+                        const Shape* __restrict__ shapes, const uint32_t* __restrict__ level_start,
+                        const uint32_t* __restrict__ level_nodes, uint4* nodes) {
+    for (uint32_t m = blockIdx.x; m < n_meshes; m += gridDim.x) {
         DMesh M = meshes[m];
-        for (uint32_t local = blockIdx.x * blockDim.x + threadIdx.x; local < M.n_nodes; local += gridDim.x * blockDim.x) {
-            uint32_t i = M.root + local;
-            uint4 a = nodes[2ull * i], b = nodes[2ull * i + 1];
-            if (local == 0) parent[i] = NONE;
-            if (b.w == 0u) {
-                parent[M.root + a.w] = i;
-                parent[M.root + a.w + 1] = i;
+        Shape sh = shapes[shape_of[m]];
+        for (uint32_t l = 0; l < sh.n_levels; ++l) {
+            uint32_t a = level_start[sh.levels_first + l], b = level_start[sh.levels_first + l + 1];
+            for (uint32_t j = a + threadIdx.x; j < b; j += blockDim.x) {
+                uint32_t i = M.root + level_nodes[sh.interior_first + j];
+                uint4 na = __ldcg(nodes + 2ull * i), nb = __ldcg(nodes + 2ull * i + 1);
+                uint64_t c = M.root + na.w;
+                uint4 la = __ldcg(nodes + 2 * c), lb = __ldcg(nodes + 2 * c + 1);
+                uint4 ra = __ldcg(nodes + 2 * c + 2), rb = __ldcg(nodes + 2 * c + 3);
+                V3 lo = V3{gmin(__uint_as_float(la.x), __uint_as_float(ra.x)), gmin(__uint_as_float(la.y), __uint_as_float(ra.y)),
+                           gmin(__uint_as_float(la.z), __uint_as_float(ra.z))};
+                V3 hi = V3{gmax(__uint_as_float(lb.x), __uint_as_float(rb.x)), gmax(__uint_as_float(lb.y), __uint_as_float(rb.y)),
+                           gmax(__uint_as_float(lb.z), __uint_as_float(rb.z))};
+                store_box(nodes, i, lo, hi, na.w, nb.w);
             }
+            __syncthreads();
         }
+        __syncthreads();
     }
 }
 
@@ -184,8 +173,11 @@ struct TopBuild {
     float4* box;      // 2 a unit: lo, hi
     float4* centre;   // a unit's box centre
     uint32_t* order[2];
-    uint4* tasks[2];  // a level's nodes: (start, end, final index, interior nodes before it in preorder)
-    uint32_t* cnt;    // nodes a level, TOP_LEVELS + 1
+    // A level's nodes, (start, end, final index, interior nodes before it in preorder), in two lists: those of at most
+    // TOP_SMALL units (a warp's each) and the larger (a CTA's each); cnt[2 * level + {0, 1}] counts them.
+    uint4* tasks[2];
+    uint4* big[2];
+    uint32_t* cnt;
     uint32_t* err;
     uint4* nodes;
     uint32_t top_first, n_units;
@@ -195,9 +187,10 @@ struct TopBuild {
 __global__ void k_unit_boxes(const uint4* __restrict__ tables, uint32_t t_instances, uint64_t n_nodes, TopBuild T) {
     uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
     if (u == 0) {
-        T.tasks[0][0] = make_uint4(0u, T.n_units, 0u, 0u);
-        T.cnt[0] = 1u;
-        for (uint32_t l = 1; l <= TOP_LEVELS; ++l) T.cnt[l] = 0u;
+        bool large = T.n_units > TOP_SMALL;
+        (large ? T.big[0] : T.tasks[0])[0] = make_uint4(0u, T.n_units, 0u, 0u);
+        for (uint32_t l = 0; l <= TOP_LEVELS; ++l) T.cnt[2 * l] = T.cnt[2 * l + 1] = 0u;
+        T.cnt[large ? 1 : 0] = 1u;
     }
     if (u >= T.n_units) return;
     T.order[0][u] = u;
@@ -261,6 +254,128 @@ __device__ __forceinline__ int32_t total_key(float f) {
     return b ^ (int32_t)(((uint32_t)(b >> 31)) >> 1);
 }
 
+// A node's two children onto the next level's lists: the left one's place and preorder count follow from its
+// parent's, the right one's from the left side's unit count.
+__device__ __forceinline__ void push_children(const TopBuild& T, uint32_t level, uint32_t start, uint32_t mid,
+                                              uint32_t end, uint32_t pre) {
+    uint4 kids[2] = {make_uint4(start, start + mid, 1u + 2u * pre, pre + 1u),
+                     make_uint4(start + mid, end, 2u + 2u * pre, pre + mid)};
+    for (int c = 0; c < 2; ++c) {
+        bool large = kids[c].y - kids[c].x > TOP_SMALL;
+        uint32_t at = atomicAdd(&T.cnt[2 * (level + 1u) + (large ? 1 : 0)], 1u);
+        (large ? T.big : T.tasks)[(level + 1u) & 1u][at] = kids[c];
+    }
+}
+
+// total_key is its own inverse (the sign bit is kept): the float of a key.
+__device__ __forceinline__ float key_float(int32_t k) { return __int_as_float(total_key(__int_as_float(k))); }
+
+// One axis's binning of a warp's units at once (every lane calls it; `valid` lanes hold a unit): the lanes of one bin
+// join their boxes by warp reductions over the boxes' total-order keys, and one of them updates the bin.
+__device__ __forceinline__ void bin_add_warp(float (*blo)[TOP_BINS], float (*bhi)[TOP_BINS], uint32_t* bn, bool valid,
+                                             uint32_t bin, float4 bl, float4 bh) {
+    unsigned grp = __match_any_sync(~0u, valid ? bin : 0xffffffffu);
+    int32_t a0 = __reduce_min_sync(grp, total_key(bl.x)), a1 = __reduce_min_sync(grp, total_key(bl.y));
+    int32_t a2 = __reduce_min_sync(grp, total_key(bl.z));
+    int32_t b0 = __reduce_max_sync(grp, total_key(bh.x)), b1 = __reduce_max_sync(grp, total_key(bh.y));
+    int32_t b2 = __reduce_max_sync(grp, total_key(bh.z));
+    if (valid && (threadIdx.x & 31u) == (uint32_t)(__ffs(grp) - 1)) {
+        atomic_min_f(&blo[0][bin], key_float(a0));
+        atomic_min_f(&blo[1][bin], key_float(a1));
+        atomic_min_f(&blo[2][bin], key_float(a2));
+        atomic_max_f(&bhi[0][bin], key_float(b0));
+        atomic_max_f(&bhi[1][bin], key_float(b1));
+        atomic_max_f(&bhi[2][bin], key_float(b2));
+        atomicAdd(&bn[bin], (uint32_t)__popc(grp));
+    }
+}
+
+// build_sah's sweep over one set of bins (blo / bhi [axis][component][bin], bn [axis][bin]), a warp at once: lane i
+// holds split i (bins 0 .. i-1 to the left). The left sides are an inclusive scan over the bins before, the right
+// sides one over the bins from i on (min, max and sums: exact, as the reference's running folds are), each lane then
+// computes the split's cost as build_sah does, and the warp takes the first cheapest in build_sah's order (axis, then
+// split) among the splits that leave both sides non-empty and within `room`. Every lane gets the result.
+__device__ void sah_sweep(const float (*blo)[3][TOP_BINS], const float (*bhi)[3][TOP_BINS], const uint32_t (*bn)[TOP_BINS],
+                          const bool use[3], uint32_t count, uint32_t room, float& best_cost, uint32_t& best_axis,
+                          uint32_t& best_split, uint32_t& best_left) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const float pinf = __uint_as_float(0x7f800000u);
+    float cost_best = pinf;
+    uint32_t key_best = 0xffffffffu, left_best = 0;
+    for (uint32_t ax = 0; ax < 3; ++ax) {
+        if (!use[ax]) continue;
+        // this lane's bin
+        float l0 = blo[ax][0][lane], l1 = blo[ax][1][lane], l2 = blo[ax][2][lane];
+        float h0 = bhi[ax][0][lane], h1 = bhi[ax][1][lane], h2 = bhi[ax][2][lane];
+        uint32_t c = bn[ax][lane];
+        // suffix over bins lane .. 31 (the right side of split `lane`)
+        float rl0 = l0, rl1 = l1, rl2 = l2, rh0 = h0, rh1 = h1, rh2 = h2;
+        // prefix over bins 0 .. lane (the left side of split lane + 1)
+        float pl0 = l0, pl1 = l1, pl2 = l2, ph0 = h0, ph1 = h1, ph2 = h2;
+        uint32_t pc = c;
+#pragma unroll
+        for (uint32_t o = 1; o < 32; o <<= 1) {
+            float t;
+            t = __shfl_down_sync(~0u, rl0, o); if (lane + o < 32) rl0 = gmin(rl0, t);
+            t = __shfl_down_sync(~0u, rl1, o); if (lane + o < 32) rl1 = gmin(rl1, t);
+            t = __shfl_down_sync(~0u, rl2, o); if (lane + o < 32) rl2 = gmin(rl2, t);
+            t = __shfl_down_sync(~0u, rh0, o); if (lane + o < 32) rh0 = gmax(rh0, t);
+            t = __shfl_down_sync(~0u, rh1, o); if (lane + o < 32) rh1 = gmax(rh1, t);
+            t = __shfl_down_sync(~0u, rh2, o); if (lane + o < 32) rh2 = gmax(rh2, t);
+            t = __shfl_up_sync(~0u, pl0, o); if (lane >= o) pl0 = gmin(pl0, t);
+            t = __shfl_up_sync(~0u, pl1, o); if (lane >= o) pl1 = gmin(pl1, t);
+            t = __shfl_up_sync(~0u, pl2, o); if (lane >= o) pl2 = gmin(pl2, t);
+            t = __shfl_up_sync(~0u, ph0, o); if (lane >= o) ph0 = gmax(ph0, t);
+            t = __shfl_up_sync(~0u, ph1, o); if (lane >= o) ph1 = gmax(ph1, t);
+            t = __shfl_up_sync(~0u, ph2, o); if (lane >= o) ph2 = gmax(ph2, t);
+            uint32_t u = __shfl_up_sync(~0u, pc, o);
+            if (lane >= o) pc += u;
+        }
+        // split i = lane: left = prefix of bins 0 .. i-1 (the lane below's), right = suffix from bin i
+        float ql0 = __shfl_up_sync(~0u, pl0, 1), ql1 = __shfl_up_sync(~0u, pl1, 1), ql2 = __shfl_up_sync(~0u, pl2, 1);
+        float qh0 = __shfl_up_sync(~0u, ph0, 1), qh1 = __shfl_up_sync(~0u, ph1, 1), qh2 = __shfl_up_sync(~0u, ph2, 1);
+        uint32_t nl = __shfl_up_sync(~0u, pc, 1);
+        uint32_t nr = count - nl;
+        float cost = pinf;
+        bool ok = lane >= 1 && nl != 0 && nr != 0 && nl <= room && nr <= room;
+        if (ok) cost = area3(V3{ql0, ql1, ql2}, V3{qh0, qh1, qh2}) * (float)nl +
+                       area3(V3{rl0, rl1, rl2}, V3{rh0, rh1, rh2}) * (float)nr;
+        // a split counts where it is cheaper than the best so far (the reference's `cost < best`)
+        bool cand = ok && cost < pinf;
+        uint32_t key = cand ? ax * 32u + lane : 0xffffffffu;
+        float cv = cand ? cost : pinf;
+        // the first cheapest of this axis: min by (cost, key)
+#pragma unroll
+        for (uint32_t o = 16; o > 0; o >>= 1) {
+            float oc = __shfl_xor_sync(~0u, cv, o);
+            uint32_t ok2 = __shfl_xor_sync(~0u, key, o);
+            uint32_t ol = __shfl_xor_sync(~0u, nl, o);
+            if (oc < cv || (oc == cv && ok2 < key)) { cv = oc; key = ok2; nl = ol; }
+        }
+        if (key != 0xffffffffu && cv < cost_best) { cost_best = cv; key_best = key; left_best = nl; }
+    }
+    best_cost = cost_best;
+    best_axis = key_best == 0xffffffffu ? 0u : key_best / 32u;
+    best_split = key_best == 0xffffffffu ? 0u : key_best % 32u;
+    best_left = left_best;
+}
+
+// The median split's side of unit k: its rank among the node's units by (centre along the axis in f32::total_cmp
+// order, then index) against half the count.
+__device__ __forceinline__ bool median_left(const TopBuild& T, const uint32_t* order, uint32_t start, uint32_t end,
+                                            uint32_t k, uint32_t axis) {
+    int32_t kk = total_key(comp(T.centre[k], axis));
+    uint32_t rank = 0;
+    for (uint32_t q = start; q < end; ++q) {
+        uint32_t o = order[q];
+        int32_t ko = total_key(comp(T.centre[o], axis));
+        rank += (ko < kk || (ko == kk && o < k)) ? 1u : 0u;
+    }
+    return rank < (end - start) / 2u;
+}
+
+// Tasks of more units than this are the CTA kernel's (k_top_big); the rest a warp's (k_top_level).
+
 constexpr uint32_t TOP_WARPS = 8u;
 
 // One level of the build: a warp a node. It takes the node's boxes (order[level & 1][start, end)), picks the split
@@ -274,7 +389,7 @@ __global__ void __launch_bounds__(TOP_WARPS * 32) k_top_level(TopBuild T, uint32
     __shared__ float s_lo[TOP_WARPS][3][3][TOP_BINS], s_hi[TOP_WARPS][3][3][TOP_BINS];
     __shared__ uint32_t s_n[TOP_WARPS][3][TOP_BINS];
     uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
-    uint32_t n_tasks = T.cnt[level];
+    uint32_t n_tasks = T.cnt[2 * level];
     const uint32_t* order = T.order[level & 1u];
     uint32_t* out = T.order[(level + 1u) & 1u];
     const uint4* tasks = T.tasks[level & 1u];
@@ -323,54 +438,20 @@ __global__ void __launch_bounds__(TOP_WARPS * 32) k_top_level(TopBuild T, uint32
             s_n[wib][ax][bn] = 0u;
         }
         __syncwarp();
-        for (uint32_t j = start + lane; j < end; j += 32u) {
-            uint32_t k = order[j];
+        for (uint32_t base = start; base < end; base += 32u) {
+            uint32_t j = base + lane;
+            bool valid = j < end;
+            uint32_t k = valid ? order[j] : order[start];
             float4 bl = T.box[2ull * k], bh = T.box[2ull * k + 1], c = T.centre[k];
-            for (uint32_t ax = 0; ax < 3; ++ax) {
-                if (!use[ax]) continue;
-                uint32_t bn = bin_of(comp(c, ax), comp3(clo, ax), scale[ax]);
-                atomic_min_f(&s_lo[wib][ax][0][bn], bl.x);
-                atomic_min_f(&s_lo[wib][ax][1][bn], bl.y);
-                atomic_min_f(&s_lo[wib][ax][2][bn], bl.z);
-                atomic_max_f(&s_hi[wib][ax][0][bn], bh.x);
-                atomic_max_f(&s_hi[wib][ax][1][bn], bh.y);
-                atomic_max_f(&s_hi[wib][ax][2][bn], bh.z);
-                atomicAdd(&s_n[wib][ax][bn], 1u);
-            }
+            for (uint32_t ax = 0; ax < 3; ++ax)
+                if (use[ax])
+                    bin_add_warp(s_lo[wib][ax], s_hi[wib][ax], s_n[wib][ax], valid,
+                                 bin_of(comp(c, ax), comp3(clo, ax), scale[ax]), bl, bh);
         }
         __syncwarp();
-        // build_sah's sweep, as written: right sides from the last bin back, left sides forward, the first cheapest.
-        float best_cost = __uint_as_float(0x7f800000u);
+        float best_cost = 0.0f;
         uint32_t best_axis = 0, best_split = 0, best_left = 0;
-        if (lane == 0) {
-            for (uint32_t ax = 0; ax < 3; ++ax) {
-                if (!use[ax]) continue;
-                float right[TOP_BINS];
-                V3 alo = v3(__uint_as_float(0x7f800000u)), ahi = v3(__uint_as_float(0xff800000u));
-                right[0] = 0.0f;
-                for (uint32_t i = TOP_BINS - 1u; i >= 1u; --i) {
-                    alo = V3{gmin(alo.x, s_lo[wib][ax][0][i]), gmin(alo.y, s_lo[wib][ax][1][i]), gmin(alo.z, s_lo[wib][ax][2][i])};
-                    ahi = V3{gmax(ahi.x, s_hi[wib][ax][0][i]), gmax(ahi.y, s_hi[wib][ax][1][i]), gmax(ahi.z, s_hi[wib][ax][2][i])};
-                    right[i] = area3(alo, ahi);
-                }
-                alo = v3(__uint_as_float(0x7f800000u));
-                ahi = v3(__uint_as_float(0xff800000u));
-                uint32_t nl = 0;
-                for (uint32_t i = 1; i < TOP_BINS; ++i) {
-                    alo = V3{gmin(alo.x, s_lo[wib][ax][0][i - 1]), gmin(alo.y, s_lo[wib][ax][1][i - 1]), gmin(alo.z, s_lo[wib][ax][2][i - 1])};
-                    ahi = V3{gmax(ahi.x, s_hi[wib][ax][0][i - 1]), gmax(ahi.y, s_hi[wib][ax][1][i - 1]), gmax(ahi.z, s_hi[wib][ax][2][i - 1])};
-                    nl += s_n[wib][ax][i - 1];
-                    uint32_t nr = count - nl;
-                    if (nl == 0 || nr == 0 || nl > room || nr > room) continue;
-                    float cost = area3(alo, ahi) * (float)nl + right[i] * (float)nr;
-                    if (cost < best_cost) { best_cost = cost; best_axis = ax; best_split = i; best_left = nl; }
-                }
-            }
-        }
-        best_cost = __shfl_sync(~0u, best_cost, 0);
-        best_axis = __shfl_sync(~0u, best_axis, 0);
-        best_split = __shfl_sync(~0u, best_split, 0);
-        best_left = __shfl_sync(~0u, best_left, 0);
+        sah_sweep(s_lo[wib], s_hi[wib], s_n[wib], use, count, room, best_cost, best_axis, best_split, best_left);
         bool binned = finite1(best_cost);
         uint32_t med_axis = (ext.x >= ext.y && ext.x >= ext.z) ? 0u : (ext.y >= ext.z ? 1u : 2u);
         uint32_t mid = binned ? best_left : count / 2u;
@@ -384,15 +465,7 @@ __global__ void __launch_bounds__(TOP_WARPS * 32) k_top_level(TopBuild T, uint32
                 if (binned) {
                     left = bin_of(comp(T.centre[k], best_axis), comp3(clo, best_axis), scale[best_axis]) < best_split;
                 } else {
-                    // the median by (centre along the axis, total order; then the unit's index): its rank among all
-                    int32_t kk = total_key(comp(T.centre[k], med_axis));
-                    uint32_t rank = 0;
-                    for (uint32_t q = start; q < end; ++q) {
-                        uint32_t o = order[q];
-                        int32_t ko = total_key(comp(T.centre[o], med_axis));
-                        rank += (ko < kk || (ko == kk && o < k)) ? 1u : 0u;
-                    }
-                    left = rank < count / 2u;
+                    left = median_left(T, order, start, end, k, med_axis);
                 }
             }
             unsigned lm = __ballot_sync(~0u, valid && left), rm = __ballot_sync(~0u, valid && !left);
@@ -407,11 +480,139 @@ __global__ void __launch_bounds__(TOP_WARPS * 32) k_top_level(TopBuild T, uint32
         if (lane == 0) {
             if (nl_run != mid) atomicOr(T.err, E_TREE);
             store_box(T.nodes, node, lo, hi, 1u + 2u * pre, 0u);
-            uint32_t at = atomicAdd(&T.cnt[level + 1u], 2u);
-            uint4* next = T.tasks[(level + 1u) & 1u];
-            next[at] = make_uint4(start, start + mid, 1u + 2u * pre, pre + 1u);
-            next[at + 1] = make_uint4(start + mid, end, 2u + 2u * pre, pre + mid);
+            push_children(T, level, start, mid, end, pre);
         }
+    }
+}
+
+
+// The same step for nodes of more than TOP_SMALL units, a CTA a node: each warp bins its share of the units into its
+// own set of bins, the sets are joined, one thread sweeps them, and the partition is a CTA-wide stable scan.
+__global__ void __launch_bounds__(BIG_WARPS * 32) k_top_big(TopBuild T, uint32_t level) {
+    __shared__ float s_lo[BIG_WARPS][3][3][TOP_BINS], s_hi[BIG_WARPS][3][3][TOP_BINS];
+    __shared__ uint32_t s_n[BIG_WARPS][3][TOP_BINS];
+    __shared__ float s_red[BIG_WARPS][12];
+    __shared__ uint32_t s_side[BIG_WARPS][2];
+    __shared__ float s_cost;
+    __shared__ uint32_t s_best[3];
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, w = tid >> 5, nt = BIG_WARPS * 32u;
+    const float pinf = __uint_as_float(0x7f800000u), ninf = __uint_as_float(0xff800000u);
+    uint32_t n_tasks = T.cnt[2 * level + 1];
+    const uint32_t* order = T.order[level & 1u];
+    uint32_t* out = T.order[(level + 1u) & 1u];
+    const uint4* tasks = T.big[level & 1u];
+    for (uint32_t ti = blockIdx.x; ti < n_tasks; ti += gridDim.x) {
+        uint4 task = tasks[ti];
+        uint32_t start = task.x, end = task.y, fin = task.z, pre = task.w, count = end - start;
+        if (fin >= 2u * T.n_units - 1u || end > T.n_units || level >= TOP_MAX_DEPTH) {
+            if (tid == 0) atomicOr(T.err, level >= TOP_MAX_DEPTH ? E_DEPTH : E_TREE);
+            continue;
+        }
+        // The node's box and its units' centres' box.
+        float r[12] = {pinf, pinf, pinf, ninf, ninf, ninf, pinf, pinf, pinf, ninf, ninf, ninf};
+        for (uint32_t j = start + tid; j < end; j += nt) {
+            uint32_t k = order[j];
+            float4 bl = T.box[2ull * k], bh = T.box[2ull * k + 1], c = T.centre[k];
+            r[0] = gmin(r[0], bl.x); r[1] = gmin(r[1], bl.y); r[2] = gmin(r[2], bl.z);
+            r[3] = gmax(r[3], bh.x); r[4] = gmax(r[4], bh.y); r[5] = gmax(r[5], bh.z);
+            r[6] = gmin(r[6], c.x); r[7] = gmin(r[7], c.y); r[8] = gmin(r[8], c.z);
+            r[9] = gmax(r[9], c.x); r[10] = gmax(r[10], c.y); r[11] = gmax(r[11], c.z);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+            for (int q = 0; q < 12; ++q) {
+                float v = __shfl_xor_sync(~0u, r[q], o);
+                r[q] = (q % 6) < 3 ? gmin(r[q], v) : gmax(r[q], v);
+            }
+        if (lane == 0)
+            for (int q = 0; q < 12; ++q) s_red[w][q] = r[q];
+        for (uint32_t i = tid; i < BIG_WARPS * 3u * TOP_BINS; i += nt) {
+            uint32_t ww = i / (3u * TOP_BINS), ax = (i / TOP_BINS) % 3u, bn = i % TOP_BINS;
+            for (int q = 0; q < 3; ++q) { s_lo[ww][ax][q][bn] = pinf; s_hi[ww][ax][q][bn] = ninf; }
+            s_n[ww][ax][bn] = 0u;
+        }
+        __syncthreads();
+        for (int q = 0; q < 12; ++q) {
+            float v = s_red[0][q];
+            for (uint32_t ww = 1; ww < BIG_WARPS; ++ww) v = (q % 6) < 3 ? gmin(v, s_red[ww][q]) : gmax(v, s_red[ww][q]);
+            r[q] = v;
+        }
+        V3 lo{r[0], r[1], r[2]}, hi{r[3], r[4], r[5]}, clo{r[6], r[7], r[8]}, chi{r[9], r[10], r[11]};
+        uint32_t room = 1u << (TOP_MAX_DEPTH - level - 1u);
+        V3 ext = chi - clo;
+        float scale[3] = {(float)TOP_BINS / ext.x, (float)TOP_BINS / ext.y, (float)TOP_BINS / ext.z};
+        bool use[3] = {ext.x > 0.0f, ext.y > 0.0f, ext.z > 0.0f};
+        for (uint32_t base = start; base < end; base += nt) {
+            uint32_t j = base + tid;
+            bool valid = j < end;
+            uint32_t k = valid ? order[j] : order[start];
+            float4 bl = T.box[2ull * k], bh = T.box[2ull * k + 1], c = T.centre[k];
+            for (uint32_t ax = 0; ax < 3; ++ax)
+                if (use[ax])
+                    bin_add_warp(s_lo[w][ax], s_hi[w][ax], s_n[w][ax], valid,
+                                 bin_of(comp(c, ax), comp3(clo, ax), scale[ax]), bl, bh);
+        }
+        __syncthreads();
+        // The warps' bins joined into warp 0's (min / max and sums do not depend on the order).
+        for (uint32_t i = tid; i < 3u * TOP_BINS; i += nt) {
+            uint32_t ax = i / TOP_BINS, bn = i % TOP_BINS;
+            for (uint32_t ww = 1; ww < BIG_WARPS; ++ww) {
+                for (int q = 0; q < 3; ++q) {
+                    s_lo[0][ax][q][bn] = gmin(s_lo[0][ax][q][bn], s_lo[ww][ax][q][bn]);
+                    s_hi[0][ax][q][bn] = gmax(s_hi[0][ax][q][bn], s_hi[ww][ax][q][bn]);
+                }
+                s_n[0][ax][bn] += s_n[ww][ax][bn];
+            }
+        }
+        __syncthreads();
+        if (w == 0) {
+            float c;
+            uint32_t a, sp, l;
+            sah_sweep(s_lo[0], s_hi[0], s_n[0], use, count, room, c, a, sp, l);
+            if (lane == 0) {
+                s_cost = c;
+                s_best[0] = a; s_best[1] = sp; s_best[2] = l;
+            }
+        }
+        __syncthreads();
+        bool binned = finite1(s_cost);
+        uint32_t best_axis = s_best[0], best_split = s_best[1];
+        uint32_t med_axis = (ext.x >= ext.y && ext.x >= ext.z) ? 0u : (ext.y >= ext.z ? 1u : 2u);
+        uint32_t mid = binned ? s_best[2] : count / 2u;
+        // Stable partition, a CTA-wide chunk at a time.
+        uint32_t nl_run = 0, nr_run = 0;
+        for (uint32_t base = start; base < end; base += nt) {
+            uint32_t j = base + tid;
+            bool valid = j < end, left = false;
+            uint32_t k = valid ? order[j] : 0u;
+            if (valid)
+                left = binned ? bin_of(comp(T.centre[k], best_axis), comp3(clo, best_axis), scale[best_axis]) < best_split
+                              : median_left(T, order, start, end, k, med_axis);
+            unsigned lm = __ballot_sync(~0u, valid && left), rm = __ballot_sync(~0u, valid && !left);
+            if (lane == 0) { s_side[w][0] = __popc(lm); s_side[w][1] = __popc(rm); }
+            __syncthreads();
+            uint32_t lb = 0, rb = 0, lt = 0, rt = 0;
+            for (uint32_t ww = 0; ww < BIG_WARPS; ++ww) {
+                if (ww < w) { lb += s_side[ww][0]; rb += s_side[ww][1]; }
+                lt += s_side[ww][0];
+                rt += s_side[ww][1];
+            }
+            unsigned below = (1u << lane) - 1u;
+            if (valid) {
+                if (left) out[start + nl_run + lb + __popc(lm & below)] = k;
+                else out[start + mid + nr_run + rb + __popc(rm & below)] = k;
+            }
+            nl_run += lt;
+            nr_run += rt;
+            __syncthreads();
+        }
+        if (tid == 0) {
+            if (nl_run != mid) atomicOr(T.err, E_TREE);
+            store_box(T.nodes, T.top_first + fin, lo, hi, 1u + 2u * pre, 0u);
+            push_children(T, level, start, mid, end, pre);
+        }
+        __syncthreads();
     }
 }
 
@@ -424,8 +625,11 @@ namespace trt {
 struct DeformState {
     DMesh* meshes = nullptr;
     float4* corners = nullptr;
-    uint32_t* parent = nullptr;    // a word a node of the whole node buffer
-    uint32_t* arrivals = nullptr;  // likewise, zero between frames
+    // The refit's level order: each mesh's shape, each distinct shape's levels (deepest first) and their nodes.
+    uint32_t* shape_of = nullptr;
+    Shape* shapes = nullptr;
+    uint32_t* level_start = nullptr;
+    uint32_t* level_nodes = nullptr;
     uint32_t* err = nullptr;
     float4* palette = nullptr;
     uint32_t palette_cap = 0;
@@ -434,7 +638,7 @@ struct DeformState {
     TopBuild T{};
     std::vector<DMesh> host_meshes;
     std::vector<uint32_t> max_bone;  // per mesh: the largest palette index its corners name
-    uint32_t max_vertices = 0, max_tris = 0, max_nodes = 0;
+    uint32_t max_vertices = 0, max_tris = 0, max_nodes = 0, max_leaves = 0;
     cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
 };
 
@@ -459,9 +663,10 @@ int ensure_top(DeformState* st, uint32_t n_units, std::string& err) {
     st->top = nullptr;
     uint64_t need = 0;
     auto add = [&](uint64_t b) { uint64_t at = need; need += (b + 255) / 256 * 256; return at; };
+    uint64_t n_big = n_units / (TOP_SMALL + 1u) + 1u;  // nodes of a level are disjoint: at most this many large
     uint64_t o_box = add(32ull * n_units), o_c = add(16ull * n_units), o_o0 = add(4ull * n_units),
              o_o1 = add(4ull * n_units), o_t0 = add(16ull * n_units), o_t1 = add(16ull * n_units),
-             o_cnt = add(4ull * (TOP_LEVELS + 1));
+             o_b0 = add(16ull * n_big), o_b1 = add(16ull * n_big), o_cnt = add(8ull * (TOP_LEVELS + 1));
     DF_CUDA(cudaMalloc(&st->top, need));
     char* b = (char*)st->top;
     st->T.box = (float4*)(b + o_box);
@@ -470,6 +675,8 @@ int ensure_top(DeformState* st, uint32_t n_units, std::string& err) {
     st->T.order[1] = (uint32_t*)(b + o_o1);
     st->T.tasks[0] = (uint4*)(b + o_t0);
     st->T.tasks[1] = (uint4*)(b + o_t1);
+    st->T.big[0] = (uint4*)(b + o_b0);
+    st->T.big[1] = (uint4*)(b + o_b1);
     st->T.cnt = (uint32_t*)(b + o_cnt);
     st->top_units = n_units;
     return TRT_OK;
@@ -485,8 +692,8 @@ dim3 mesh_grid(uint32_t per_mesh, uint32_t n_meshes) {
 
 void deform_free(DeformState* st) {
     if (!st) return;
-    for (void* p : {(void*)st->meshes, (void*)st->corners, (void*)st->parent, (void*)st->arrivals, (void*)st->err,
-                    (void*)st->palette, st->top})
+    for (void* p : {(void*)st->meshes, (void*)st->corners, (void*)st->shape_of, (void*)st->shapes,
+                    (void*)st->level_start, (void*)st->level_nodes, (void*)st->err, (void*)st->palette, st->top})
         if (p) cudaFree(p);
     for (auto& e : st->ev)
         if (e) cudaEventDestroy(e);
@@ -503,6 +710,10 @@ int deform_setup(DeformState** out, const SceneBuffers& sb, const trt_deform_des
     auto fail = [&](const std::string& m) { deform_free(st); err = "trt_deform_setup: " + m; return TRT_EINVAL; };
     st->host_meshes.assign((const DMesh*)d->meshes, (const DMesh*)d->meshes + d->n_meshes);
     st->max_bone.assign(d->n_meshes, 0);
+    // Distinct tree shapes (the links and counts of a tree's nodes), each with its nodes by level, deepest first.
+    std::unordered_map<std::string, uint32_t> shape_ids;
+    std::vector<Shape> shapes;
+    std::vector<uint32_t> shape_of(d->n_meshes), level_start, level_nodes;
     for (uint32_t m = 0; m < d->n_meshes; ++m) {
         const DMesh& M = st->host_meshes[m];
         std::string at = "mesh " + std::to_string(m) + ": ";
@@ -510,21 +721,68 @@ int deform_setup(DeformState** out, const SceneBuffers& sb, const trt_deform_des
         if ((uint64_t)M.first_corner + M.n_vertices > d->n_corners) return fail(at + "corners past the corners given");
         if ((uint64_t)M.first_tri + M.n_tris > n_tris) return fail(at + "triangles past the scene's");
         if (M.n_nodes == 0 || (uint64_t)M.root + M.n_nodes > n_nodes) return fail(at + "nodes past the scene's");
-        // The tree: children after their parent and inside the tree, each node a child once; leaves' triangles
-        // inside the mesh.
+        // The tree: children after their parent and inside the tree, each node a child once, each of the mesh's
+        // triangles in one leaf.
+        std::string key(8ull * M.n_nodes, '\0');
+        std::vector<uint8_t> covered(M.n_tris, 0);
         for (uint32_t k = 0; k < M.n_nodes; ++k) {
             uint32_t w[8];
             host_node(hn, M.root + k, w);
+            std::memcpy(&key[8ull * k], &w[3], 4);
+            std::memcpy(&key[8ull * k + 4], &w[7], 4);
             if (w[7] == 0) {
                 if (w[3] <= k || (uint64_t)w[3] + 1 >= M.n_nodes) return fail(at + "a node's children are not after it in its tree");
                 refs[M.root + w[3]]++;
                 refs[M.root + w[3] + 1]++;
-            } else if ((uint64_t)w[3] + w[7] > M.n_tris) {
-                return fail(at + "a leaf's triangles are past the mesh's");
+            } else {
+                if ((uint64_t)w[3] + w[7] > M.n_tris) return fail(at + "a leaf's triangles are past the mesh's");
+                for (uint32_t t = w[3]; t < w[3] + w[7]; ++t)
+                    if (covered[t]++) return fail(at + "a triangle is in two leaves");
             }
         }
         for (uint32_t k = 0; k < M.n_nodes; ++k)
             if (refs[M.root + k] != (k == 0 ? 0u : 1u)) return fail(at + "a node is not the child of one node");
+        for (uint32_t t = 0; t < M.n_tris; ++t)
+            if (!covered[t]) return fail(at + "a triangle is in no leaf");
+        auto found = shape_ids.find(key);
+        if (found != shape_ids.end()) {
+            shape_of[m] = found->second;
+        } else {
+            std::vector<uint32_t> depth(M.n_nodes, 0);
+            uint32_t deepest = 0;
+            for (uint32_t k = 0; k < M.n_nodes; ++k) {  // children after parents: a parent's depth is known first
+                uint32_t w[8];
+                host_node(hn, M.root + k, w);
+                if (w[7] == 0) depth[w[3]] = depth[w[3] + 1] = depth[k] + 1;
+                deepest = std::max(deepest, depth[k]);
+            }
+            if (deepest >= 64) return fail(at + "a tree deeper than 64 levels");
+            // The shape: its leaves by first triangle, then its interior nodes by level, deepest first
+            // (n_levels + 1 offsets into them from level_start[levels_first]).
+            Shape sh{(uint32_t)level_nodes.size(), 0, 0, (uint32_t)level_start.size(), deepest + 1};
+            std::vector<std::pair<uint32_t, uint32_t>> by_tri;
+            for (uint32_t k = 0; k < M.n_nodes; ++k) {
+                uint32_t w[8];
+                host_node(hn, M.root + k, w);
+                if (w[7] > 0) by_tri.push_back({w[3], k});
+            }
+            std::sort(by_tri.begin(), by_tri.end());
+            for (auto& pr : by_tri) level_nodes.push_back(pr.second);
+            sh.n_leaves = (uint32_t)by_tri.size();
+            sh.interior_first = (uint32_t)level_nodes.size();
+            level_start.push_back(0);
+            for (uint32_t l = deepest + 1; l-- > 0;) {
+                for (uint32_t k = 0; k < M.n_nodes; ++k) {
+                    uint32_t w[8];
+                    host_node(hn, M.root + k, w);
+                    if (depth[k] == l && w[7] == 0) level_nodes.push_back(k);
+                }
+                level_start.push_back((uint32_t)level_nodes.size() - sh.interior_first);
+            }
+            shape_of[m] = (uint32_t)shapes.size();
+            shape_ids.emplace(std::move(key), shape_of[m]);
+            shapes.push_back(sh);
+        }
         for (uint32_t v = 0; v < M.n_vertices; ++v) {
             const trt_corner& c = d->corners[M.first_corner + v];
             uint32_t a, b;
@@ -535,24 +793,23 @@ int deform_setup(DeformState** out, const SceneBuffers& sb, const trt_deform_des
         st->max_vertices = std::max(st->max_vertices, M.n_vertices);
         st->max_tris = std::max(st->max_tris, M.n_tris);
         st->max_nodes = std::max(st->max_nodes, M.n_nodes);
+        st->max_leaves = std::max(st->max_leaves, shapes[shape_of[m]].n_leaves);
     }
     cudaError_t e = cudaSuccess;
-    if (d->n_meshes) e = cudaMalloc(&st->meshes, sizeof(DMesh) * d->n_meshes);
-    if (e == cudaSuccess && d->n_meshes) e = cudaMemcpyAsync(st->meshes, d->meshes, sizeof(DMesh) * d->n_meshes, cudaMemcpyHostToDevice, sb.stream);
-    if (e == cudaSuccess && d->n_corners) e = cudaMalloc(&st->corners, sizeof(trt_corner) * d->n_corners);
-    if (e == cudaSuccess && d->n_corners) e = cudaMemcpyAsync(st->corners, d->corners, sizeof(trt_corner) * d->n_corners, cudaMemcpyHostToDevice, sb.stream);
-    if (e == cudaSuccess) e = cudaMalloc(&st->parent, 4 * std::max<uint64_t>(n_nodes, 1));
-    if (e == cudaSuccess) e = cudaMalloc(&st->arrivals, 4 * std::max<uint64_t>(n_nodes, 1));
-    if (e == cudaSuccess) e = cudaMemsetAsync(st->arrivals, 0, 4 * std::max<uint64_t>(n_nodes, 1), sb.stream);
+    auto upload = [&](auto** dst, const void* src, uint64_t bytes) {
+        if (e == cudaSuccess && bytes) e = cudaMalloc((void**)dst, bytes);
+        if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, sb.stream);
+    };
+    upload(&st->meshes, d->meshes, sizeof(DMesh) * d->n_meshes);
+    upload(&st->corners, d->corners, sizeof(trt_corner) * d->n_corners);
+    upload(&st->shape_of, shape_of.data(), 4ull * shape_of.size());
+    upload(&st->shapes, shapes.data(), sizeof(Shape) * shapes.size());
+    upload(&st->level_start, level_start.data(), 4ull * level_start.size());
+    upload(&st->level_nodes, level_nodes.data(), 4ull * level_nodes.size());
     if (e == cudaSuccess) e = cudaMalloc(&st->err, 4);
     if (e == cudaSuccess) e = cudaMemsetAsync(st->err, 0, 4, sb.stream);
     for (auto& ev : st->ev)
         if (e == cudaSuccess) e = cudaEventCreate(&ev);
-    if (e == cudaSuccess && d->n_meshes) {
-        k_parents<<<mesh_grid(st->max_nodes, d->n_meshes), 256, 0, sb.stream>>>(st->meshes, d->n_meshes,
-                                                                               (const uint4*)sb.buf[2], st->parent);
-        e = cudaGetLastError();
-    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(sb.stream);
     if (e != cudaSuccess) {
         deform_free(st);
@@ -602,11 +859,18 @@ int deform_run(DeformState* st, const SceneBuffers& sb, const uint32_t* P, const
     const uint32_t* words = (const uint32_t*)sb.buf[4];
     if (n_meshes) k_skin<<<mesh_grid(st->max_vertices, n_meshes), 256, 0, s>>>(st->meshes, n_meshes, st->corners, st->palette, vertices);
     if (stats) DF_CUDA(cudaEventRecord(st->ev[1], s));
-    if (n_meshes) k_gather<<<mesh_grid(st->max_tris, n_meshes), 256, 0, s>>>(st->meshes, n_meshes, vertices, words, w_indices, leaves, st->err);
+    // (The leaf gather is the refit's leaf level: gather_ms stays 0 and refit_ms holds both.)
     if (stats) DF_CUDA(cudaEventRecord(st->ev[2], s));
-    if (n_meshes)
-        k_refit<<<mesh_grid(st->max_nodes, n_meshes), 256, 0, s>>>(st->meshes, n_meshes, vertices, words, w_indices, nodes,
-                                                                    st->parent, st->arrivals, st->err);
+    if (n_meshes) {
+        // A CTA a mesh; few meshes get wide CTAs so that a single tree's levels still fill many warps.
+        uint32_t threads = n_meshes < 296u ? 1024u : 256u;
+        uint32_t blocks = std::min(n_meshes, 148u * (2048u / threads) * 4u);
+        k_refit_leaves<<<mesh_grid(st->max_leaves, n_meshes), 256, 0, s>>>(st->meshes, st->shape_of, n_meshes, st->shapes,
+                                                                            st->level_nodes, vertices, words, w_indices,
+                                                                            leaves, nodes, st->err);
+        k_refit<<<blocks, threads, 0, s>>>(st->meshes, st->shape_of, n_meshes, st->shapes, st->level_start,
+                                           st->level_nodes, nodes);
+    }
     if (stats) DF_CUDA(cudaEventRecord(st->ev[3], s));
     TopBuild T = st->T;
     T.err = st->err;
@@ -616,6 +880,8 @@ int deform_run(DeformState* st, const SceneBuffers& sb, const uint32_t* P, const
     k_unit_boxes<<<(n_units + 255) / 256, 256, 0, s>>>((const uint4*)sb.buf[3], t_instances, n_nodes, T);
     for (uint32_t level = 0; level < TOP_LEVELS; ++level) {
         uint32_t most = std::min<uint32_t>(1u << level, n_units);  // a level holds at most 2^level nodes
+        uint32_t big = std::min(most, n_units / (TOP_SMALL + 1u));  // ... and at most this many of over TOP_SMALL
+        if (big) k_top_big<<<std::min(big, 148u * 2u), BIG_WARPS * 32, 0, s>>>(T, level);
         uint32_t blocks = std::max(1u, std::min((most + TOP_WARPS - 1) / TOP_WARPS, 148u * 8u));
         k_top_level<<<blocks, TOP_WARPS * 32, 0, s>>>(T, level);
     }
