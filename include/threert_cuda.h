@@ -170,6 +170,46 @@ int trt_accum_read(trt_scene* scene, float* accum_host, uint64_t bytes);
 int trt_trace(trt_scene* scene, const uint32_t params[TRT_PARAMS_WORDS], const trt_ray* rays, uint64_t n, uint32_t flags,
               trt_hit* hits);
 
+/* ---- Serving: many requests on resident scenes, batched into shared waves ----
+ * Replaces the reference's `serve` loop (renderer/src/main.rs:345-397: JSON-line jobs rendered one at a time through
+ * Gpu::render). A server owns a worker thread, its own streams and one wave's device state. Requests (a resident
+ * scene, a Params block, a sample count, a host buffer for the result) wait until the device has room for their
+ * accum (free HBM less a reserve) and a slot among the active ones; each step then packs the next samples of the
+ * active requests, oldest first, into one wave of up to `wave_slots` paths that every kernel of the pass runs at once
+ * (a path finds its request through the wave's job table). A request that arrives while others are on the GPU joins
+ * the next step. Each request's accum is the one trt_render makes alone, bit for bit: a path's random numbers and
+ * sums are its own, and its samples are added in sample order. Scenes must stay uploaded and unchanged while they
+ * have requests in flight; requests walk the binary trees. */
+typedef struct trt_server trt_server;
+typedef struct {
+    uint32_t wave_slots;   /* path slots a step (0: 2,097,152); a request's image needs ceil(w/8)*ceil(h/4)*32 */
+    uint32_t max_active;   /* requests in flight at most, 1-64 (0: 64) */
+    uint64_t hbm_reserve;  /* device bytes admission leaves free (0: 1 GiB) */
+    uint32_t flags;        /* TRT_RENDER_UNSORTED_HITS / TRT_RENDER_SORT_* for every step */
+} trt_server_options;
+typedef struct {
+    uint64_t id;
+    int32_t status;        /* TRT_OK, or the error the request ended with */
+    uint32_t steps;        /* steps its samples were spread over */
+    double submit_ms, start_ms, done_ms;  /* host monotonic clock, ms since the server was created */
+} trt_request_done;
+typedef struct {
+    uint64_t steps, requests_done, paths, closest_rays, shadow_rays;
+    double busy_ms;        /* device time of the steps (events around each) */
+    uint32_t active, pending;
+} trt_server_stats;
+
+int trt_server_create(trt_ctx* ctx, const trt_server_options* opts, trt_server** out);
+/* Stops the worker after the requests already admitted are done; pending ones end with TRT_EINVAL. */
+void trt_server_destroy(trt_server* server);
+/* Queues a request; accum_host (w * h * 20 floats) receives the result and must stay valid until the request is
+ * reported done. The Params are checked here (TRT_EINVAL). Thread-safe. */
+int trt_server_submit(trt_server* server, trt_scene* scene, const uint32_t params[TRT_PARAMS_WORDS], uint32_t spp,
+                      float* accum_host, uint64_t* id);
+/* Up to cap finished requests since the last call, waiting up to wait_ms for one if none is ready. */
+int trt_server_poll(trt_server* server, trt_request_done* done, uint32_t cap, uint32_t* n, uint32_t wait_ms);
+int trt_server_stats_get(trt_server* server, trt_server_stats* out);
+
 /* The render without allocations, for callers that cannot call cudaMalloc: code inside a CUDA graph capture, or a
  * process whose device memory all belongs to one pool (an engine's caching allocator, a hard memory budget). It has
  * no counterpart in the reference. The caller owns every buffer: `dev` holds DEVICE pointers to the scene's buffers

@@ -1,0 +1,84 @@
+"""The serving loop on the device (trt_server_*): requests of different scenes, image sizes, sample counts and
+depths batched into shared waves must give each request the accum it gets rendered alone, bit for bit; the server's
+ray counts must be the sum of the requests'; what cannot be served is refused at submission."""
+import numpy as np
+import pytest
+
+from threert_b200 import RenderError, prep, scenes
+from threert_b200.prep import params_with
+from threert_b200.serve import Request, Server, run_stream
+
+from util import small_city, small_crowd
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def resident(gpu):
+    Ps = [prep.prepare(scenes.cornell(48, 48)), prep.prepare(small_city()), prep.prepare(small_crowd(n=60).desc)]
+    S = [gpu.upload(P) for P in Ps]
+    yield Ps, S
+    for s in S:
+        s.close()
+
+
+def the_mix(Ps, seed=3):
+    rng = np.random.default_rng(seed)
+    sizes = [(16, 16), (40, 24), (64, 36), (48, 48), (33, 17)]
+    reqs = []
+    for i in range(14):
+        k = i % len(Ps)
+        w, h = sizes[int(rng.integers(len(sizes)))]
+        reqs.append(Request(k, params_with(Ps[k].params, width=w, height=h), int(rng.choice([1, 3, 8]))))
+    return reqs
+
+
+@pytest.mark.parametrize("wave_slots", [16384, 1 << 20])  # small: requests spread over steps; large: one step
+def test_each_result_is_the_same_alone_and_in_the_mix(gpu, resident, wave_slots):
+    Ps, S = resident
+    reqs = the_mix(Ps)
+    srv = Server(gpu, wave_slots=wave_slots, max_active=8)
+    try:
+        before = srv.stats()
+        res = run_stream(srv, S, reqs, rate=0.0)  # all at once: they share waves
+        after = srv.stats()
+    finally:
+        srv.close()
+    assert res["failed"] == 0
+    rays = 0
+    for r in reqs:
+        alone, st = S[r.scene].render_raw(r.params, r.spp)
+        assert np.array_equal(r.accum, alone), (r.scene, r.params[16], r.params[17], r.spp)
+        rays += st.closest_rays + st.shadow_rays
+    assert after["closest_rays"] + after["shadow_rays"] - before["closest_rays"] - before["shadow_rays"] == rays
+    if wave_slots == 1 << 20:
+        assert res["steps"] < len(reqs)  # several requests a step
+    else:
+        assert max(r.done["steps"] for r in reqs) > 1  # a request's samples over several steps
+
+
+def test_requests_that_arrive_during_a_run_join_it(gpu, resident):
+    Ps, S = resident
+    reqs = the_mix(Ps, seed=5)
+    srv = Server(gpu, wave_slots=16384, max_active=4)
+    try:
+        res = run_stream(srv, S, reqs, rate=400.0)
+    finally:
+        srv.close()
+    assert res["failed"] == 0 and res["requests"] == len(reqs)
+    for r in reqs:
+        assert np.array_equal(r.accum, S[r.scene].render_raw(r.params, r.spp)[0])
+
+
+def test_what_cannot_be_served_is_refused(gpu, resident):
+    Ps, S = resident
+    srv = Server(gpu, wave_slots=4096)
+    try:
+        with pytest.raises(RenderError):  # the image needs more path slots than a step holds
+            srv.submit(S[0], Request(0, params_with(Ps[0].params, width=128, height=128), 1))
+        bad = Ps[0].params.copy()
+        bad[124] = 0xFFFFFFF  # a table section past the tables
+        with pytest.raises(RenderError):
+            srv.submit(S[0], Request(0, bad, 1))
+    finally:
+        srv.close()

@@ -131,6 +131,20 @@ class DeformStats(C.Structure):
 TRT_CORNER_NORMAL = 1
 TRT_CORNER_TANGENT = 2
 
+class ServerOptions(C.Structure):
+    _fields_ = [("wave_slots", u32), ("max_active", u32), ("hbm_reserve", u64), ("flags", u32)]
+
+
+class RequestDone(C.Structure):
+    _fields_ = [("id", u64), ("status", C.c_int32), ("steps", u32), ("submit_ms", C.c_double),
+                ("start_ms", C.c_double), ("done_ms", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("steps", u64), ("requests_done", u64), ("paths", u64), ("closest_rays", u64), ("shadow_rays", u64),
+                ("busy_ms", C.c_double), ("active", u32), ("pending", u32)]
+
+
 # Every function the C headers declare, with its signature: (name, restype, argtypes).
 SIGNATURES = [
     # threert_prep.h
@@ -163,6 +177,11 @@ SIGNATURES = [
     ("trt_trace", C.c_int, [C.c_void_p, P(u32), P(Ray), u64, u32, P(Hit)]),
     ("trt_render_noalloc", C.c_int, [P(SceneDesc), P(u32), u32, u32, u32, C.c_void_p, C.c_void_p, C.c_char_p,
                                      C.c_size_t]),
+    ("trt_server_create", C.c_int, [C.c_void_p, P(ServerOptions), P(C.c_void_p)]),
+    ("trt_server_destroy", None, [C.c_void_p]),
+    ("trt_server_submit", C.c_int, [C.c_void_p, C.c_void_p, P(u32), u32, P(f32), P(u64)]),
+    ("trt_server_poll", C.c_int, [C.c_void_p, P(RequestDone), u32, P(u32), u32]),
+    ("trt_server_stats_get", C.c_int, [C.c_void_p, P(ServerStats)]),
     ("trt_scene_totals", C.c_int, [C.c_void_p, P(Totals)]),
     ("trt_scene_reset_totals", None, [C.c_void_p]),
     ("trt_scene_set_profiling", None, [C.c_void_p, C.c_int]),

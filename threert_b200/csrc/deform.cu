@@ -17,7 +17,6 @@
 
 namespace trt {
 
-constexpr uint32_t NONE = 0xffffffffu;
 constexpr uint32_t TOP_DEPTH = 19u;                 // units.rs:30-37: leaves at most TOP_DEPTH - 1 deep
 constexpr uint32_t TOP_MAX_DEPTH = TOP_DEPTH - 1u;  // build_sah's max_depth
 constexpr uint32_t TOP_LEVELS = TOP_MAX_DEPTH + 1u; // levels 0 .. TOP_MAX_DEPTH
@@ -25,7 +24,6 @@ constexpr uint32_t MAX_UNITS = 1u << TOP_MAX_DEPTH;
 constexpr uint32_t TOP_BINS = 32u;                  // units.rs:121
 // Top-tree nodes of more units than this are built by a CTA each (k_top_big), the rest by a warp each (k_top_level).
 constexpr uint32_t TOP_SMALL = 256u, BIG_WARPS = 16u;
-constexpr uint32_t REFIT_CLIMB = 64u;               // a mesh tree is less deep than the walk's 64-entry stack
 // Error bits the kernels record.
 constexpr uint32_t E_TREE = 1u, E_DEPTH = 2u, E_ROOT = 4u, E_INDEX = 8u;
 

@@ -48,6 +48,7 @@ struct PathBufs {
     float4* nee;      // N_SLOTS contributions a path (slot-major: nee[slot * n + p])
     float4* nee_thr;  // throughput at the light samples, w: slot mask | clamp << 8 (bits)
     uint32_t* vis;    // visible slots (bits)
+    uint32_t* job;    // the job (index into the wave's job table) whose path a slot holds
     uint32_t n;       // slots
 };
 struct Queues {
@@ -120,6 +121,33 @@ __device__ __forceinline__ bool slot_pixel(uint32_t idx, uint32_t w, uint32_t h,
     return gx < w && gy < h;
 }
 
+struct Walk {
+    DScene S;
+    WideView W;
+    uint32_t top, n_units;
+};
+
+// A wave's unit of work: one request's samples [first_sample, first_sample + K) of every pixel of its image, on the
+// wave's slots [slot_first, slot_first + n_idx * K), with its own Params, scene and accum. trt_render's waves hold one
+// job; a wave may hold several requests' (of different scenes, sizes and sample counts) in the same launches. A path
+// finds its job through B.job, so nothing a path computes depends on what else the wave holds.
+struct Job {
+    Params P;
+    Walk wk;
+    float4* accum;
+    uint32_t slot_first, n_idx, K, first_sample;
+};
+constexpr uint32_t MAX_JOBS = 64u;
+// The hot kernels take the table and, for a wave of one job, that job as a kernel argument (MULTI = false): its reads
+// then come from the kernel's constant bank, not global memory.
+
+// Writes one entry of a wave's job table from a kernel argument (no host copy: the launch carries it).
+__global__ void k_put_job(Job j, Job* table, uint32_t at) {
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(&j);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(table + at);
+    for (uint32_t i = threadIdx.x; i < sizeof(Job) / 4; i += blockDim.x) dst[i] = src[i];
+}
+
 // pathtrace.wgsl:4002-4026 camera_ray
 __device__ void camera_ray(const Params& P, uint32_t gx, uint32_t gy, const float cam[4], V3& o, V3& d) {
     float w = (float)P.w[P_SIZE], h = (float)P.w[P_SIZE + 1];
@@ -138,15 +166,23 @@ __device__ void camera_ray(const Params& P, uint32_t gx, uint32_t gy, const floa
     }
 }
 
-__global__ void k_raygen(Params P, PathBufs B, Queues Q, uint32_t first_sample, uint32_t n_idx, uint32_t K) {
+__global__ void k_raygen(const Job* __restrict__ jobs, uint32_t n_jobs, PathBufs B, Queues Q, uint32_t n_slots) {
     uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    uint32_t w = P.w[P_SIZE], h = P.w[P_SIZE + 1];
     bool valid = false;
-    uint32_t gx = 0, gy = 0;
-    if (p < n_idx * K) valid = slot_pixel(p % n_idx, w, h, gx, gy);
+    uint32_t gx = 0, gy = 0, j = 0;
+    if (p < n_slots) {
+        while (j + 1 < n_jobs && p >= jobs[j + 1].slot_first) ++j;  // jobs lie in slot order
+        const Job& J = jobs[j];
+        uint32_t local = p - J.slot_first;
+        if (local < J.n_idx * J.K) valid = slot_pixel(local % J.n_idx, J.P.w[P_SIZE], J.P.w[P_SIZE + 1], gx, gy);
+    }
     uint32_t at = warp_append(&Q.cnt[0], valid);
     if (!valid) return;
-    uint32_t sample = first_sample + p / n_idx;
+    const Job& J = jobs[j];
+    const Params& P = J.P;
+    uint32_t w = P.w[P_SIZE];
+    B.job[p] = j;
+    uint32_t sample = J.first_sample + (p - J.slot_first) / J.n_idx;
     Rng R{sample, pixel_seed(gx, gy, P.w[P_SIZE + 3]), 0u};
     float cam[4];
     R.rng4(R.dim(D_CAMERA), cam);
@@ -164,12 +200,6 @@ __global__ void k_raygen(Params P, PathBufs B, Queues Q, uint32_t first_sample, 
     Q.q[0][at] = p;
 }
 
-struct Walk {
-    const DScene S;
-    const WideView W;
-    uint32_t top, n_units;
-};
-
 template <bool COUNT, bool WIDE>
 __device__ __forceinline__ Hit walk(const Walk& wk, const Sections& X, V3 o, V3 d, float tmax, uint32_t mode,
                                     WalkCount* wc, bool* guard) {
@@ -177,10 +207,9 @@ __device__ __forceinline__ Hit walk(const Walk& wk, const Sections& X, V3 o, V3 
     return trace_binary<COUNT>(wk.S, X, wk.top, wk.n_units, o, d, tmax, mode, wc, guard);
 }
 
-template <bool COUNT, bool WIDE>
-__global__ void __launch_bounds__(128, 6) k_extend(Params P, Walk wk, PathBufs B, Queues Q, uint32_t depth,
-                                                   const uint32_t* __restrict__ queue) {
-    Sections X(P);
+template <bool COUNT, bool WIDE, bool MULTI>
+__global__ void __launch_bounds__(128, 6) k_extend(const Job* __restrict__ jobs, const Job one, PathBufs B, Queues Q,
+                                                   uint32_t depth, const uint32_t* __restrict__ queue) {
     uint32_t* cnt = Q.cnt + depth * CNT_STRIDE;
     uint32_t n = *(volatile uint32_t*)&cnt[0];
     WalkCount wc{0, 0, 0};
@@ -190,9 +219,11 @@ __global__ void __launch_bounds__(128, 6) k_extend(Params P, Walk wk, PathBufs B
         if (__shfl_sync(0xffffffffu, i, 0) >= n) break;
         if (i < n) {
             uint32_t p = queue[i];
+            const Job& J = MULTI ? jobs[B.job[p]] : one;
+            Sections X(J.P);
             float4 o = B.o[p], d = B.d[p];
             bool guard = false;
-            Hit h = walk<COUNT, WIDE>(wk, X, xyz(o), xyz(d), INF, TRACE_CLOSEST, &wc, &guard);
+            Hit h = walk<COUNT, WIDE>(J.wk, X, xyz(o), xyz(d), INF, TRACE_CLOSEST, &wc, &guard);
             if (guard) guard_trips++;
             Q.hit_a[p] = make_float4(h.t, h.u, h.v, bf(h.tri));
             Q.hit_b[p] = make_uint2(h.inst, h.part);
@@ -211,10 +242,9 @@ __device__ __forceinline__ uint32_t shadow_slot(const Queues& Q, uint32_t j, uin
     return j < n0 ? Q.class_base[0] + j : (j < n0 + n1 ? Q.class_base[1] + (j - n0) : Q.class_base[2] + (j - n0 - n1));
 }
 
-template <bool COUNT, bool WIDE>
-__global__ void __launch_bounds__(128, 6) k_shadow(Params P, Walk wk, PathBufs B, Queues Q, uint32_t depth,
-                                                   const uint32_t* __restrict__ perm) {
-    Sections X(P);
+template <bool COUNT, bool WIDE, bool MULTI>
+__global__ void __launch_bounds__(128, 6) k_shadow(const Job* __restrict__ jobs, const Job one, PathBufs B, Queues Q,
+                                                   uint32_t depth, const uint32_t* __restrict__ perm) {
     uint32_t* cnt = Q.cnt + depth * CNT_STRIDE;
     uint32_t n0 = min(*(volatile uint32_t*)&cnt[4], Q.class_cap[0]);
     uint32_t n1 = min(*(volatile uint32_t*)&cnt[5], Q.class_cap[1]);
@@ -228,14 +258,14 @@ __global__ void __launch_bounds__(128, 6) k_shadow(Params P, Walk wk, PathBufs B
         if (j < n) {
             // The classes' regions one after another: the j-th ray of the three (or of their sorted order).
             uint32_t i = perm ? perm[j] : shadow_slot(Q, j, n0, n1);
+            uint32_t sp = Q.sp[i];
+            const Job& J = MULTI ? jobs[B.job[sp >> 3]] : one;
+            Sections X(J.P);
             float4 o = Q.so[i], d = Q.sd[i];
             bool guard = false;
-            Hit h = walk<COUNT, WIDE>(wk, X, xyz(o), xyz(d), o.w, bu(d.w), &wc, &guard);
+            Hit h = walk<COUNT, WIDE>(J.wk, X, xyz(o), xyz(d), o.w, bu(d.w), &wc, &guard);
             if (guard) guard_trips++;
-            if (h.tri == MISS) {
-                uint32_t sp = Q.sp[i];
-                atomicOr(&B.vis[sp >> 3], 1u << (sp & 7u));
-            }
+            if (h.tri == MISS) atomicOr(&B.vis[sp >> 3], 1u << (sp & 7u));
         }
     }
     if (COUNT) {
@@ -257,9 +287,10 @@ __device__ __forceinline__ void push_shadow(const Queues& Q, uint32_t* cnt, uint
 }
 
 // One path vertex: pathtrace.wgsl:4176-4477 from the hit on (the trace itself is k_extend's).
-__global__ void __launch_bounds__(128, 4) k_shade(Params P, DScene S, PathBufs B, Queues Q, uint32_t depth,
-                                                  const uint32_t* __restrict__ queue, uint32_t* __restrict__ next) {
-    Sections X(P);
+template <bool MULTI>
+__global__ void __launch_bounds__(128, 4) k_shade(const Job* __restrict__ jobs, const Job one, PathBufs B, Queues Q,
+                                                  uint32_t depth, const uint32_t* __restrict__ queue,
+                                                  uint32_t* __restrict__ next) {
     uint32_t* cnt = Q.cnt + depth * CNT_STRIDE;
     uint32_t n = cnt[0];
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -267,6 +298,10 @@ __global__ void __launch_bounds__(128, 4) k_shade(Params P, DScene S, PathBufs B
     uint32_t p = 0;
     if (i < n) {
         p = queue[i];
+        const Job& J = MULTI ? jobs[B.job[p]] : one;
+        const Params& P = J.P;
+        const DScene& S = J.wk.S;
+        Sections X(P);
         float4 o4 = B.o[p], d4 = B.d[p], thr4 = B.thr[p], rad4 = B.rad[p];
         V3 o = xyz(o4), d = xyz(d4), thr = xyz(thr4), radiance = xyz(rad4);
         float last_pdf = o4.w;
@@ -429,11 +464,14 @@ __global__ void __launch_bounds__(128, 4) k_shade(Params P, DScene S, PathBufs B
 
 // The vertex's direct light from its visible slots (pathtrace.wgsl:4398-4403), and a finished path's last fixes
 // (4494-4497).
-__global__ void k_resolve(PathBufs B, Queues Q, uint32_t depth, float clamp_v, const uint32_t* __restrict__ queue) {
+template <bool MULTI>
+__global__ void k_resolve(const Job* __restrict__ jobs, const Job one, PathBufs B, Queues Q, uint32_t depth,
+                          const uint32_t* __restrict__ queue) {
     uint32_t n = Q.cnt[depth * CNT_STRIDE];
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     uint32_t p = queue[i];
+    float clamp_v = pf(MULTI ? jobs[B.job[p]].P : one.P, P_MISC);
     float4 nt = B.nee_thr[p];
     uint32_t m = bu(nt.w);
     float4 rad4 = B.rad[p];
@@ -494,11 +532,14 @@ __device__ __forceinline__ uint32_t sort_item(const Queues& Q, const uint32_t* i
     return KIND == SORT_SHADOWS ? shadow_slot(Q, j, n0, n1) : in[j];
 }
 template <uint32_t KIND>
-__device__ __forceinline__ uint32_t sort_key(const DScene& S, const Sections& X, const PathBufs& B, const Queues& Q,
-                                             uint32_t j, uint32_t item, uint32_t shift) {
+__device__ __forceinline__ uint32_t sort_key(const Job* jobs, const PathBufs& B, const Queues& Q, uint32_t j,
+                                             uint32_t item, uint32_t shift) {
     if (KIND == SORT_RAYS) return ((j >> shift) << 3) | octant(B.d[item]);
     if (KIND == SORT_SHADOWS) return ((j >> shift) << 3) | octant(Q.sd[item]);
     if (bu(Q.hit_a[item].w) == MISS) return 0u;
+    const Job& J = jobs[B.job[item]];
+    const DScene& S = J.wk.S;
+    Sections X(J.P);
     uint2 hb = Q.hit_b[item];
     uint32_t mat = 0;
     if (hb.x != NO_INST) {
@@ -509,13 +550,12 @@ __device__ __forceinline__ uint32_t sort_key(const DScene& S, const Sections& X,
 }
 
 template <uint32_t KIND>
-__global__ void __launch_bounds__(SORT_THREADS) k_sort_count(Params P, DScene S, PathBufs B, Queues Q,
+__global__ void __launch_bounds__(SORT_THREADS) k_sort_count(const Job* __restrict__ jobs, PathBufs B, Queues Q,
                                                             const uint32_t* __restrict__ in, uint32_t depth,
                                                             uint32_t shift) {
     __shared__ uint32_t h[SORT_BINS];
     __shared__ uint32_t warp_sums[SORT_THREADS / 32u];
     __shared__ bool last;
-    Sections X(P);
     uint32_t n0 = 0, n1 = 0;
     uint32_t n = sort_count<KIND>(Q, depth, n0, n1);
     uint32_t base = blockIdx.x * SORT_ITEMS, tid = threadIdx.x;
@@ -527,7 +567,7 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_count(Params P, DScene S,
 #pragma unroll
         for (uint32_t k = 0; k < SORT_PER_THREAD; ++k) {
             uint32_t j = base + k * SORT_THREADS + tid;
-            key[k] = j < n ? sort_key<KIND>(S, X, B, Q, j, sort_item<KIND>(Q, in, j, n0, n1), shift) & (SORT_BINS - 1u) : 0u;
+            key[k] = j < n ? sort_key<KIND>(jobs, B, Q, j, sort_item<KIND>(Q, in, j, n0, n1), shift) & (SORT_BINS - 1u) : 0u;
         }
 #pragma unroll
         for (uint32_t k = 0; k < SORT_PER_THREAD; ++k) {
@@ -591,15 +631,18 @@ __global__ void k_sort_scatter(Queues Q, const uint32_t* __restrict__ in, uint32
 }
 
 // accum += each sample's path, in sample order (pathtrace.wgsl:4541-4557).
-__global__ void k_accumulate(Params P, PathBufs B, float4* accum, uint32_t n_idx, uint32_t K) {
+__global__ void k_accumulate(const Job* __restrict__ jobs, PathBufs B) {
+    const Job& J = jobs[blockIdx.y];
     uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
-    uint32_t w = P.w[P_SIZE], h = P.w[P_SIZE + 1];
+    uint32_t n_idx = J.n_idx, K = J.K;
+    float4* accum = J.accum;
+    uint32_t w = J.P.w[P_SIZE], h = J.P.w[P_SIZE + 1];
     uint32_t gx, gy;
     if (idx >= n_idx || !slot_pixel(idx, w, h, gx, gy)) return;
     uint32_t pix = gy * w + gx;
     float4 c = accum[pix * 5], a = accum[pix * 5 + 1], nn = accum[pix * 5 + 2];
     for (uint32_t k = 0; k < K; ++k) {
-        uint32_t p = k * n_idx + idx;
+        uint32_t p = J.slot_first + k * n_idx + idx;
         V3 r = xyz(B.rad[p]), al = xyz(B.alb[p]), nm = xyz(B.nrm[p]);
         c.x += r.x; c.y += r.y; c.z += r.z; c.w += 1.0f;
         float lum = luminance(r);
@@ -684,6 +727,18 @@ struct trt_ctx {
     cudaEvent_t t0 = nullptr, t1 = nullptr;
 };
 
+namespace trt {
+// The device state of a wave: path slots, queues, the job table (one allocation).
+struct Wave {
+    void* work = nullptr;
+    uint64_t work_bytes = 0;
+    uint32_t slots = 0, shadow_alloc = 0;
+    PathBufs B{};
+    Queues Q{};
+    Job* jobs = nullptr;
+};
+}  // namespace trt
+
 struct trt_scene {
     trt_ctx* ctx = nullptr;
     void* buf[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -694,12 +749,7 @@ struct trt_scene {
     WideBvh wide;
     float4* accum = nullptr;
     uint32_t accum_w = 0, accum_h = 0;
-    // work buffers
-    void* work = nullptr;
-    uint64_t work_bytes = 0;
-    uint32_t slots = 0, shadow_alloc = 0;
-    PathBufs B{};
-    Queues Q{};
+    Wave wave;  // the render's wave state
     unsigned long long* totals = nullptr;
     int profiling = 0;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_extend, ev_shadow, ev_shade, ev_sort, ev_free;
@@ -764,11 +814,12 @@ int check_params(trt_scene* s, const uint32_t* P) {
     return TRT_OK;
 }
 
-int ensure_work(trt_scene* s, uint32_t slots, uint32_t n_dir) {
+// A wave's device state sized for `slots` paths with up to n_dir suns each: one allocation, laid out here.
+int wave_ensure(Wave& w, uint32_t slots, uint32_t n_dir, unsigned long long* totals, cudaStream_t st, std::string& err) {
     // Shadow-ray regions: a ray a sun a path, one toward an emitter, one toward the sky.
     uint32_t caps[3] = {slots * std::max(1u, n_dir), slots, slots};
     uint32_t shadow_cap = caps[0] + caps[1] + caps[2];
-    if (!s->work || s->slots < slots || s->shadow_alloc < shadow_cap) {
+    if (!w.work || w.slots < slots || w.shadow_alloc < shadow_cap) {
         uint64_t need = 0;
         auto add = [&](uint64_t b) { uint64_t at = need; need += (b + 255) / 256 * 256; return at; };
         uint64_t o_o = add(16ull * slots), o_d = add(16ull * slots), o_thr = add(16ull * slots),
@@ -779,42 +830,58 @@ int ensure_work(trt_scene* s, uint32_t slots, uint32_t n_dir) {
                  o_sd = add(16ull * shadow_cap), o_sp = add(4ull * shadow_cap),
                  o_cnt = add(4ull * (MAX_DEPTH * CNT_STRIDE + CNT_STRIDE)), o_qx = add(4ull * slots),
                  o_kr = add(8ull * std::max(slots, shadow_cap)), o_hist = add(4ull * SORT_BINS),
-                 o_start = add(4ull * SORT_BINS), o_done = add(4ull), o_perm = add(4ull * shadow_cap);
-        if (s->work) cudaFree(s->work);
-        s->work = nullptr;
-        TRT_CUDA(s->ctx, cudaMalloc(&s->work, need));
-        s->work_bytes = need;
-        char* b = (char*)s->work;
-        s->slots = slots;
-        s->shadow_alloc = shadow_cap;
-        s->B = PathBufs{(float4*)(b + o_o), (float4*)(b + o_d), (float4*)(b + o_thr), (float4*)(b + o_rad),
-                        (float4*)(b + o_alb), (float4*)(b + o_nrm), (float4*)(b + o_mx), (float4*)(b + o_mn),
-                        (float4*)(b + o_nee), (float4*)(b + o_nt), (uint32_t*)(b + o_vis), slots};
-        s->Q.q[0] = (uint32_t*)(b + o_q0);
-        s->Q.q[1] = (uint32_t*)(b + o_q1);
-        s->Q.hit_a = (float4*)(b + o_ha);
-        s->Q.hit_b = (uint2*)(b + o_hb);
-        s->Q.so = (float4*)(b + o_so);
-        s->Q.sd = (float4*)(b + o_sd);
-        s->Q.sp = (uint32_t*)(b + o_sp);
-        s->Q.cnt = (uint32_t*)(b + o_cnt);
-        s->Q.qx = (uint32_t*)(b + o_qx);
-        s->Q.sort_kr = (uint2*)(b + o_kr);
-        s->Q.sort_hist = (uint32_t*)(b + o_hist);
-        s->Q.sort_start = (uint32_t*)(b + o_start);
-        s->Q.sort_done = (uint32_t*)(b + o_done);
-        s->Q.perm = (uint32_t*)(b + o_perm);
-        s->Q.totals = s->totals;
+                 o_start = add(4ull * SORT_BINS), o_done = add(4ull), o_perm = add(4ull * shadow_cap),
+                 o_job = add(4ull * slots), o_jobs = add(sizeof(Job) * MAX_JOBS);
+        if (w.work) cudaFree(w.work);
+        w.work = nullptr;
+        cudaError_t e = cudaMalloc(&w.work, need);
+        if (e != cudaSuccess) {
+            err = std::string("wave state (") + std::to_string(need >> 20) + " MiB): " + cudaGetErrorString(e);
+            w.slots = w.shadow_alloc = 0;
+            return TRT_ECUDA;
+        }
+        w.work_bytes = need;
+        char* b = (char*)w.work;
+        w.slots = slots;
+        w.shadow_alloc = shadow_cap;
+        w.B = PathBufs{(float4*)(b + o_o), (float4*)(b + o_d), (float4*)(b + o_thr), (float4*)(b + o_rad),
+                       (float4*)(b + o_alb), (float4*)(b + o_nrm), (float4*)(b + o_mx), (float4*)(b + o_mn),
+                       (float4*)(b + o_nee), (float4*)(b + o_nt), (uint32_t*)(b + o_vis), (uint32_t*)(b + o_job),
+                       slots};
+        w.jobs = (Job*)(b + o_jobs);
+        w.Q.q[0] = (uint32_t*)(b + o_q0);
+        w.Q.q[1] = (uint32_t*)(b + o_q1);
+        w.Q.hit_a = (float4*)(b + o_ha);
+        w.Q.hit_b = (uint2*)(b + o_hb);
+        w.Q.so = (float4*)(b + o_so);
+        w.Q.sd = (float4*)(b + o_sd);
+        w.Q.sp = (uint32_t*)(b + o_sp);
+        w.Q.cnt = (uint32_t*)(b + o_cnt);
+        w.Q.qx = (uint32_t*)(b + o_qx);
+        w.Q.sort_kr = (uint2*)(b + o_kr);
+        w.Q.sort_hist = (uint32_t*)(b + o_hist);
+        w.Q.sort_start = (uint32_t*)(b + o_start);
+        w.Q.sort_done = (uint32_t*)(b + o_done);
+        w.Q.perm = (uint32_t*)(b + o_perm);
         // The sort's counts and its finished-block count start at zero (each sort leaves them so).
-        TRT_CUDA(s->ctx, cudaMemsetAsync(b + o_hist, 0, o_start - o_hist, s->ctx->stream));
-        TRT_CUDA(s->ctx, cudaMemsetAsync(b + o_done, 0, 4, s->ctx->stream));
+        e = cudaMemsetAsync(b + o_hist, 0, o_start - o_hist, st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(b + o_done, 0, 4, st);
+        if (e != cudaSuccess) {
+            err = std::string("wave state: ") + cudaGetErrorString(e);
+            return TRT_ECUDA;
+        }
     }
-    s->Q.shadow_cap = shadow_cap;
-    s->Q.class_base[0] = 0;
-    s->Q.class_base[1] = caps[0];
-    s->Q.class_base[2] = caps[0] + caps[1];
-    for (int k = 0; k < 3; ++k) s->Q.class_cap[k] = caps[k];
+    w.Q.totals = totals;
+    w.Q.shadow_cap = shadow_cap;
+    w.Q.class_base[0] = 0;
+    w.Q.class_base[1] = caps[0];
+    w.Q.class_base[2] = caps[0] + caps[1];
+    for (int k = 0; k < 3; ++k) w.Q.class_cap[k] = caps[k];
     return TRT_OK;
+}
+
+int ensure_work(trt_scene* s, uint32_t slots, uint32_t n_dir) {
+    return wave_ensure(s->wave, slots, n_dir, s->totals, s->ctx->stream, s->ctx->err);
 }
 
 std::pair<cudaEvent_t, cudaEvent_t> take_events(trt_scene* s) {
@@ -843,11 +910,10 @@ uint32_t chunk_shift(uint32_t cap) {
 }
 
 template <uint32_t KIND>
-void launch_sort(trt_scene* s, const Params& P, const DScene& S, const uint32_t* in, uint32_t* out, uint32_t depth,
-                 uint32_t cap, cudaStream_t st) {
+void launch_sort(trt_scene* s, const uint32_t* in, uint32_t* out, uint32_t depth, uint32_t cap, cudaStream_t st) {
     uint32_t shift = chunk_shift(cap);
-    k_sort_count<KIND><<<(cap + SORT_ITEMS - 1u) / SORT_ITEMS, SORT_THREADS, 0, st>>>(P, S, s->B, s->Q, in, depth, shift);
-    k_sort_scatter<KIND><<<(cap + 255u) / 256u, 256, 0, st>>>(s->Q, in, out, depth);
+    k_sort_count<KIND><<<(cap + SORT_ITEMS - 1u) / SORT_ITEMS, SORT_THREADS, 0, st>>>(s->wave.jobs, s->wave.B, s->wave.Q, in, depth, shift);
+    k_sort_scatter<KIND><<<(cap + 255u) / 256u, 256, 0, st>>>(s->wave.Q, in, out, depth);
     s->launches += 2;
 }
 
@@ -862,14 +928,13 @@ int render_waves(trt_scene* s, const Params& P, uint32_t first_sample, uint32_t 
     uint32_t n_dir = P.w[P_COUNTS2];
     int rc = ensure_work(s, n_idx * K, n_dir);
     if (rc) return rc;
-    DScene S = scene_view(s);
-    Walk wk{S, s->wide.view(), P.w[P_MOTION + 2], P.w[P_MOTION + 3]};
+    Walk wk{scene_view(s), s->wide.view(), P.w[P_MOTION + 2], P.w[P_MOTION + 3]};
     uint32_t last = P.w[P_COUNTS + 2];
     bool sort_rays = (flags & TRT_RENDER_SORT_RAYS) != 0, sort_hits = (flags & TRT_RENDER_UNSORTED_HITS) == 0;
     bool sort_shadows = (flags & TRT_RENDER_SORT_SHADOWS) != 0;
     const int blk = 128;
-    int g_ext = grid_for((const void*)k_extend<COUNT, WIDE>, blk, c->sm_count);
-    int g_sha = grid_for((const void*)k_shadow<COUNT, WIDE>, blk, c->sm_count);
+    int g_ext = grid_for((const void*)k_extend<COUNT, WIDE, false>, blk, c->sm_count);
+    int g_sha = grid_for((const void*)k_shadow<COUNT, WIDE, false>, blk, c->sm_count);
     std::vector<uint32_t> host_cnt(MAX_DEPTH * CNT_STRIDE + CNT_STRIDE, 0);
     auto mark = [&](std::vector<std::pair<cudaEvent_t, cudaEvent_t>>& v, bool begin) {
         if (!s->profiling) return;
@@ -878,51 +943,53 @@ int render_waves(trt_scene* s, const Params& P, uint32_t first_sample, uint32_t 
     };
     for (uint32_t s0 = 0; s0 < spp; s0 += K) {
         uint32_t k = std::min(K, spp - s0);
-        TRT_CUDA(c, cudaMemcpyAsync(s->Q.cnt, host_cnt.data(), host_cnt.size() * 4, cudaMemcpyHostToDevice, st));
+        TRT_CUDA(c, cudaMemcpyAsync(s->wave.Q.cnt, host_cnt.data(), host_cnt.size() * 4, cudaMemcpyHostToDevice, st));
         uint32_t n = n_idx * k;
-        k_raygen<<<(n + blk - 1) / blk, blk, 0, st>>>(P, s->B, s->Q, first_sample + s0, n_idx, k);
-        s->launches++;
+        Job job{P, wk, s->accum, 0u, n_idx, k, first_sample + s0};
+        k_put_job<<<1, 128, 0, st>>>(job, s->wave.jobs, 0u);
+        k_raygen<<<(n + blk - 1) / blk, blk, 0, st>>>(s->wave.jobs, 1u, s->wave.B, s->wave.Q, n);
+        s->launches += 2;
         for (uint32_t depth = 0; depth <= last; ++depth) {
             // The depth's queue (raw), the order extend walks it in, the order shade takes the hits in.
-            uint32_t* raw = s->Q.q[depth & 1u];
-            uint32_t* next = s->Q.q[(depth + 1u) & 1u];
+            uint32_t* raw = s->wave.Q.q[depth & 1u];
+            uint32_t* next = s->wave.Q.q[(depth + 1u) & 1u];
             uint32_t* ext_q = raw;
             if (sort_rays && depth > 0u) {
                 mark(s->ev_sort, true);
-                launch_sort<SORT_RAYS>(s, P, S, raw, s->Q.qx, depth, n, st);
+                launch_sort<SORT_RAYS>(s, raw, s->wave.Q.qx, depth, n, st);
                 mark(s->ev_sort, false);
-                ext_q = s->Q.qx;
+                ext_q = s->wave.Q.qx;
             }
             mark(s->ev_extend, true);
-            k_extend<COUNT, WIDE><<<g_ext, blk, 0, st>>>(P, wk, s->B, s->Q, depth, ext_q);
+            k_extend<COUNT, WIDE, false><<<g_ext, blk, 0, st>>>(s->wave.jobs, job, s->wave.B, s->wave.Q, depth, ext_q);
             mark(s->ev_extend, false);
             uint32_t* shade_q = ext_q;
             if (sort_hits) {
-                shade_q = ext_q == raw ? s->Q.qx : raw;
+                shade_q = ext_q == raw ? s->wave.Q.qx : raw;
                 mark(s->ev_sort, true);
-                launch_sort<SORT_HITS>(s, P, S, ext_q, shade_q, depth, n, st);
+                launch_sort<SORT_HITS>(s, ext_q, shade_q, depth, n, st);
                 mark(s->ev_sort, false);
             }
             mark(s->ev_shade, true);
-            k_shade<<<(n + blk - 1) / blk, blk, 0, st>>>(P, S, s->B, s->Q, depth, shade_q, next);
+            k_shade<false><<<(n + blk - 1) / blk, blk, 0, st>>>(s->wave.jobs, job, s->wave.B, s->wave.Q, depth, shade_q, next);
             mark(s->ev_shade, false);
             const uint32_t* perm = nullptr;
             if (sort_shadows) {
                 mark(s->ev_sort, true);
-                launch_sort<SORT_SHADOWS>(s, P, S, nullptr, s->Q.perm, depth, s->Q.shadow_cap, st);
+                launch_sort<SORT_SHADOWS>(s, nullptr, s->wave.Q.perm, depth, s->wave.Q.shadow_cap, st);
                 mark(s->ev_sort, false);
-                perm = s->Q.perm;
+                perm = s->wave.Q.perm;
             }
             mark(s->ev_shadow, true);
-            k_shadow<COUNT, WIDE><<<g_sha, blk, 0, st>>>(P, wk, s->B, s->Q, depth, perm);
+            k_shadow<COUNT, WIDE, false><<<g_sha, blk, 0, st>>>(s->wave.jobs, job, s->wave.B, s->wave.Q, depth, perm);
             mark(s->ev_shadow, false);
-            k_resolve<<<(n + blk - 1) / blk, blk, 0, st>>>(s->B, s->Q, depth, bf(P.w[P_MISC]), shade_q);
+            k_resolve<false><<<(n + blk - 1) / blk, blk, 0, st>>>(s->wave.jobs, job, s->wave.B, s->wave.Q, depth, shade_q);
             s->launches += 4;
             s->extend_launches++;
             s->shadow_launches++;
         }
-        k_accumulate<<<(n_idx + blk - 1) / blk, blk, 0, st>>>(P, s->B, s->accum, n_idx, k);
-        k_tally<<<1, 32, 0, st>>>(s->Q, last + 1, w * h * k);
+        k_accumulate<<<dim3((n_idx + blk - 1) / blk, 1), blk, 0, st>>>(s->wave.jobs, s->wave.B);
+        k_tally<<<1, 32, 0, st>>>(s->wave.Q, last + 1, w * h * k);
         s->launches += 2;
     }
     TRT_CUDA(c, cudaGetLastError());
@@ -946,7 +1013,8 @@ constexpr uint64_t NOALLOC_BYTES =
     8 * na_round(16ull * NOALLOC_SLOTS) + na_round(16ull * NOALLOC_SLOTS * N_SLOTS) + na_round(16ull * NOALLOC_SLOTS) +
     na_round(4ull * NOALLOC_SLOTS) + 2 * na_round(4ull * NOALLOC_SLOTS) + na_round(16ull * NOALLOC_SLOTS) +
     na_round(8ull * NOALLOC_SLOTS) + 2 * na_round(16ull * NOALLOC_SHADOW) + na_round(4ull * NOALLOC_SHADOW) +
-    na_round(4ull * (MAX_DEPTH * CNT_STRIDE + CNT_STRIDE)) + na_round(8ull * T_COUNT);
+    na_round(4ull * (MAX_DEPTH * CNT_STRIDE + CNT_STRIDE)) + na_round(8ull * T_COUNT) + na_round(4ull * NOALLOC_SLOTS) +
+    na_round(sizeof(Job));
 static_assert(NOALLOC_BYTES < (32ull << 20), "the no-allocation scratch stays under 32 MiB");
 
 static __device__ __align__(256) uint8_t g_noalloc_scratch[NOALLOC_BYTES];
@@ -1080,7 +1148,7 @@ int trt_scene_upload(trt_ctx* c, const trt_scene_desc* d, trt_scene** out) {
     if (e == cudaSuccess) e = cudaMalloc(&s->totals, sizeof(unsigned long long) * T_COUNT);
     if (e == cudaSuccess) e = cudaMemsetAsync(s->totals, 0, sizeof(unsigned long long) * T_COUNT, c->stream);
     if (e != cudaSuccess) return cleanup(cuda_fail(c, e, "scene upload"));
-    s->Q.totals = s->totals;
+    s->wave.Q.totals = s->totals;
     e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return cleanup(cuda_fail(c, e, "scene upload"));
     c->scenes.push_back(s);
@@ -1098,7 +1166,7 @@ void trt_scene_free(trt_scene* s) {
         if (b) cudaFree(b);
     if (s->env) cudaFree(s->env);
     if (s->accum) cudaFree(s->accum);
-    if (s->work) cudaFree(s->work);
+    if (s->wave.work) cudaFree(s->wave.work);
     if (s->totals) cudaFree(s->totals);
     deform_free(s->deform);
     s->wide.release();
@@ -1434,6 +1502,8 @@ int trt_render_noalloc(const trt_scene_desc* dev, const uint32_t params[TRT_PARA
     uint64_t cnt_bytes = 4ull * (MAX_DEPTH * CNT_STRIDE + CNT_STRIDE);
     Q.cnt = (uint32_t*)take(cnt_bytes);
     Q.totals = (unsigned long long*)take(8ull * T_COUNT);
+    B.job = (uint32_t*)take(4ull * NOALLOC_SLOTS);
+    Job* jobs = (Job*)take(sizeof(Job));
     uint32_t n_dir = P.w[P_COUNTS2];
     uint32_t caps[3] = {slots * std::max(1u, n_dir), slots, slots};
     Q.shadow_cap = caps[0] + caps[1] + caps[2];
@@ -1459,8 +1529,8 @@ int trt_render_noalloc(const trt_scene_desc* dev, const uint32_t params[TRT_PARA
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) return na_fail(err, err_len, TRT_ECUDA, cudaGetErrorString(e));
     const int blk = 128;
-    int g_ext = grid_for((const void*)k_extend<false, false>, blk, sms);
-    int g_sha = grid_for((const void*)k_shadow<false, false>, blk, sms);
+    int g_ext = grid_for((const void*)k_extend<false, false, false>, blk, sms);
+    int g_sha = grid_for((const void*)k_shadow<false, false, false>, blk, sms);
     uint32_t last = P.w[P_COUNTS + 2];
     // What must start at zero: the accum (unless accumulating), the totals, each wave's counters.
     if (!(flags & TRT_RENDER_ACCUMULATE)) e = cudaMemsetAsync(accum_device, 0, 80ull * w * h, st);
@@ -1470,15 +1540,17 @@ int trt_render_noalloc(const trt_scene_desc* dev, const uint32_t params[TRT_PARA
         e = cudaMemsetAsync(Q.cnt, 0, cnt_bytes, st);
         if (e != cudaSuccess) break;
         uint32_t n = n_idx * k;
-        k_raygen<<<(n + blk - 1) / blk, blk, 0, st>>>(P, B, Q, first_sample + s0, n_idx, k);
+        Job job{P, wk, (float4*)accum_device, 0u, n_idx, k, first_sample + s0};
+        k_put_job<<<1, 128, 0, st>>>(job, jobs, 0u);
+        k_raygen<<<(n + blk - 1) / blk, blk, 0, st>>>(jobs, 1u, B, Q, n);
         for (uint32_t depth = 0; depth <= last; ++depth) {
             uint32_t* queue = Q.q[depth & 1u];
-            k_extend<false, false><<<g_ext, blk, 0, st>>>(P, wk, B, Q, depth, queue);
-            k_shade<<<(n + blk - 1) / blk, blk, 0, st>>>(P, S, B, Q, depth, queue, Q.q[(depth + 1u) & 1u]);
-            k_shadow<false, false><<<g_sha, blk, 0, st>>>(P, wk, B, Q, depth, nullptr);
-            k_resolve<<<(n + blk - 1) / blk, blk, 0, st>>>(B, Q, depth, bf(P.w[P_MISC]), queue);
+            k_extend<false, false, false><<<g_ext, blk, 0, st>>>(jobs, job, B, Q, depth, queue);
+            k_shade<false><<<(n + blk - 1) / blk, blk, 0, st>>>(jobs, job, B, Q, depth, queue, Q.q[(depth + 1u) & 1u]);
+            k_shadow<false, false, false><<<g_sha, blk, 0, st>>>(jobs, job, B, Q, depth, nullptr);
+            k_resolve<false><<<(n + blk - 1) / blk, blk, 0, st>>>(jobs, job, B, Q, depth, queue);
         }
-        k_accumulate<<<(n_idx + blk - 1) / blk, blk, 0, st>>>(P, B, (float4*)accum_device, n_idx, k);
+        k_accumulate<<<dim3((n_idx + blk - 1) / blk, 1), blk, 0, st>>>(jobs, B);
         k_tally<<<1, 32, 0, st>>>(Q, last + 1, w * h * k);
         e = cudaGetLastError();
     }
@@ -1487,3 +1559,5 @@ int trt_render_noalloc(const trt_scene_desc* dev, const uint32_t params[TRT_PARA
 }
 
 }  // extern "C"
+
+#include "serve.cuh"

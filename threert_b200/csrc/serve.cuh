@@ -1,0 +1,368 @@
+// The serving loop (include/threert_cuda.h trt_server_*): requests on resident scenes, admitted by free device memory,
+// their samples packed into shared waves that the pass's kernels run at once. Included by pathtrace.cu, whose kernels,
+// wave state and scene type it uses.
+//
+// The reference serves one job at a time (renderer/src/main.rs:345-397: read a JSON line, Gpu::render, write the
+// image). Here a worker thread keeps the GPU busy across requests: each step is one wave through every bounce, holding
+// the next samples of every active request that fit; a request that arrives while a step runs joins the next one.
+// Step N+1 is queued before step N's finished requests are read back (on a copy stream), so the read-back and the
+// host's bookkeeping overlap the next step's kernels.
+#pragma once
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <thread>
+
+namespace trt {
+
+struct ServeRequest {
+    uint64_t id = 0;
+    trt_scene* scene = nullptr;
+    Params P{};
+    uint32_t spp = 0, issued = 0, n_idx = 0, w = 0, h = 0, steps = 0;
+    float* host = nullptr;
+    float4* accum = nullptr;
+    uint64_t accum_bytes = 0;
+    double t_submit = 0, t_start = -1;
+    int status = TRT_OK;
+};
+
+// One step on the GPU: its events, the requests it finishes, its counts.
+struct ServeStep {
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    std::vector<ServeRequest*> finishing;
+    uint64_t paths = 0;
+};
+
+}  // namespace trt
+
+struct trt_server {
+    trt_ctx* ctx = nullptr;
+    trt_server_options opt{};
+    cudaStream_t stream = nullptr, copy = nullptr;
+    Wave wave;
+    unsigned long long* totals = nullptr;
+    Job* staging[2] = {nullptr, nullptr};  // pinned job tables, alternating between steps
+    cudaEvent_t staged[2] = {nullptr, nullptr};
+    uint32_t parity = 0;
+    std::thread worker;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    bool stop = false;
+    std::deque<trt::ServeRequest*> pending;
+    std::vector<trt::ServeRequest*> active;
+    std::vector<trt_request_done> done;
+    std::multimap<uint64_t, float4*> pool;  // accum buffers by size, free for reuse
+    uint64_t next_id = 1;
+    std::chrono::steady_clock::time_point t0;
+    trt_server_stats stats{};
+    std::string err;
+    int g_ext = 0, g_sha = 0;
+};
+
+namespace {
+
+double serve_now(const trt_server* s) {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - s->t0).count();
+}
+
+float4* serve_take_accum(trt_server* s, uint64_t bytes) {
+    auto it = s->pool.find(bytes);
+    if (it != s->pool.end()) {
+        float4* p = it->second;
+        s->pool.erase(it);
+        return p;
+    }
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess || free_b < bytes + s->opt.hbm_reserve) return nullptr;
+    float4* p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+    return p;
+}
+
+// Moves waiting requests into the active set while there is room (with the lock held).
+void serve_admit(trt_server* s) {
+    while (!s->pending.empty() && s->active.size() < s->opt.max_active) {
+        ServeRequest* r = s->pending.front();
+        float4* a = serve_take_accum(s, r->accum_bytes);
+        if (!a) break;  // no room on the device yet: it waits, and those behind it too (first come, first served)
+        r->accum = a;
+        cudaMemsetAsync(a, 0, r->accum_bytes, s->stream);
+        s->pending.pop_front();
+        s->active.push_back(r);
+    }
+}
+
+void serve_finish(trt_server* s, ServeRequest* r, int status) {
+    trt_request_done d{};
+    d.id = r->id;
+    d.status = status;
+    d.steps = r->steps;
+    d.submit_ms = r->t_submit;
+    d.start_ms = r->t_start;
+    d.done_ms = serve_now(s);
+    if (r->accum) s->pool.emplace(r->accum_bytes, r->accum);
+    s->done.push_back(d);
+    s->stats.requests_done++;
+    delete r;
+}
+
+// Plans and queues one step from the active requests; false when none has samples left to issue.
+bool serve_step(trt_server* s, ServeStep& step) {
+    std::vector<Job> jobs;
+    std::vector<ServeRequest*> owners;
+    uint32_t slot = 0, last = 0, n_idx_max = 0;
+    const uint32_t cap = s->wave.slots;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        serve_admit(s);
+        for (ServeRequest* r : s->active) {
+            if (r->issued >= r->spp) continue;
+            if (jobs.size() == MAX_JOBS) break;
+            uint32_t k = std::min(r->spp - r->issued, (cap - slot) / r->n_idx);
+            if (k == 0) continue;  // not enough slots left in this step: a smaller request may still fit
+            Job j{r->P, Walk{scene_view(r->scene), WideView{}, r->P.w[P_MOTION + 2], r->P.w[P_MOTION + 3]}, r->accum,
+                  slot, r->n_idx, k, r->issued};
+            jobs.push_back(j);
+            owners.push_back(r);
+            if (r->t_start < 0) r->t_start = serve_now(s);
+            r->issued += k;
+            r->steps++;
+            slot += r->n_idx * k;
+            last = std::max(last, r->P.w[P_COUNTS + 2]);
+            n_idx_max = std::max(n_idx_max, r->n_idx);
+            step.paths += (uint64_t)r->w * r->h * k;
+            if (r->issued == r->spp) step.finishing.push_back(r);
+        }
+    }
+    if (jobs.empty()) return false;
+    cudaStream_t st = s->stream;
+    // The job table through a pinned staging buffer (the one two steps back is free once its copy has run).
+    Job* stage = s->staging[s->parity];
+    cudaEventSynchronize(s->staged[s->parity]);
+    std::memcpy(stage, jobs.data(), sizeof(Job) * jobs.size());
+    cudaEventRecord(step.t0, st);
+    cudaMemcpyAsync(s->wave.jobs, stage, sizeof(Job) * jobs.size(), cudaMemcpyHostToDevice, st);
+    cudaEventRecord(s->staged[s->parity], st);
+    s->parity ^= 1u;
+    Wave& W = s->wave;
+    const int blk = 128;
+    uint32_t n = slot, nj = (uint32_t)jobs.size();
+    const Job none{};
+    cudaMemsetAsync(W.Q.cnt, 0, 4ull * (MAX_DEPTH * CNT_STRIDE + CNT_STRIDE), st);
+    k_raygen<<<(n + blk - 1) / blk, blk, 0, st>>>(W.jobs, nj, W.B, W.Q, n);
+    bool sort_hits = (s->opt.flags & TRT_RENDER_UNSORTED_HITS) == 0;
+    for (uint32_t depth = 0; depth <= last; ++depth) {
+        uint32_t* raw = W.Q.q[depth & 1u];
+        uint32_t* next = W.Q.q[(depth + 1u) & 1u];
+        k_extend<false, false, true><<<s->g_ext, blk, 0, st>>>(W.jobs, none, W.B, W.Q, depth, raw);
+        uint32_t* shade_q = raw;
+        if (sort_hits) {
+            shade_q = W.Q.qx;
+            uint32_t shift = chunk_shift(n);
+            k_sort_count<SORT_HITS><<<(n + SORT_ITEMS - 1u) / SORT_ITEMS, SORT_THREADS, 0, st>>>(W.jobs, W.B, W.Q, raw,
+                                                                                               depth, shift);
+            k_sort_scatter<SORT_HITS><<<(n + 255u) / 256u, 256, 0, st>>>(W.Q, raw, shade_q, depth);
+        }
+        k_shade<true><<<(n + blk - 1) / blk, blk, 0, st>>>(W.jobs, none, W.B, W.Q, depth, shade_q, next);
+        k_shadow<false, false, true><<<s->g_sha, blk, 0, st>>>(W.jobs, none, W.B, W.Q, depth, nullptr);
+        k_resolve<true><<<(n + blk - 1) / blk, blk, 0, st>>>(W.jobs, none, W.B, W.Q, depth, shade_q);
+    }
+    k_accumulate<<<dim3((n_idx_max + blk - 1) / blk, nj), blk, 0, st>>>(W.jobs, W.B);
+    k_tally<<<1, 32, 0, st>>>(W.Q, last + 1, (uint32_t)std::min<uint64_t>(step.paths, 0xffffffffu));
+    cudaEventRecord(step.t1, st);
+    return true;
+}
+
+// Waits for a queued step, reads back the requests it finished (copy stream) and reports them.
+void serve_retire(trt_server* s, ServeStep& step) {
+    cudaEventSynchronize(step.t1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, step.t0, step.t1);
+    for (ServeRequest* r : step.finishing) {
+        cudaStreamWaitEvent(s->copy, step.t1, 0);
+        cudaError_t e = cudaMemcpyAsync(r->host, r->accum, r->accum_bytes, cudaMemcpyDeviceToHost, s->copy);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s->copy);
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->active.erase(std::remove(s->active.begin(), s->active.end(), r), s->active.end());
+        serve_finish(s, r, e == cudaSuccess ? TRT_OK : TRT_ECUDA);
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stats.steps++;
+    s->stats.paths += step.paths;
+    s->stats.busy_ms += ms;
+    step.finishing.clear();
+    step.paths = 0;
+    s->cv_done.notify_all();
+}
+
+void serve_loop(trt_server* s) {
+    cudaSetDevice(s->ctx->device);
+    ServeStep steps[2];
+    for (auto& st : steps) {
+        cudaEventCreate(&st.t0);
+        cudaEventCreate(&st.t1);
+    }
+    int cur = 0;
+    bool in_flight = false;  // steps[cur ^ 1] is queued and not yet retired
+    for (;;) {
+        bool queued = serve_step(s, steps[cur]);
+        if (in_flight) serve_retire(s, steps[cur ^ 1]);
+        in_flight = queued;
+        if (queued) {
+            cur ^= 1;
+            continue;
+        }
+        // Nothing to queue: wait for work (or the stop).
+        std::unique_lock<std::mutex> lk(s->mu);
+        bool have = false;
+        for (ServeRequest* r : s->active) have |= r->issued < r->spp;
+        if (have) continue;
+        if (s->stop && s->active.empty() && s->pending.empty()) break;
+        // (A request that waits for device memory is retried when a request finishes or 5 ms pass.)
+        s->cv_work.wait_for(lk, std::chrono::milliseconds(5));
+    }
+    for (auto& st : steps) {
+        cudaEventDestroy(st.t0);
+        cudaEventDestroy(st.t1);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int trt_server_create(trt_ctx* c, const trt_server_options* opts, trt_server** out) {
+    if (!c || !out) return TRT_EINVAL;
+    *out = nullptr;
+    cudaSetDevice(c->device);
+    auto* s = new trt_server();
+    s->ctx = c;
+    s->opt = opts ? *opts : trt_server_options{};
+    if (s->opt.wave_slots == 0) s->opt.wave_slots = 2u << 20;
+    if (s->opt.max_active == 0 || s->opt.max_active > MAX_JOBS) s->opt.max_active = MAX_JOBS;
+    if (s->opt.hbm_reserve == 0) s->opt.hbm_reserve = 1ull << 30;
+    s->opt.wave_slots = (s->opt.wave_slots + 31u) / 32u * 32u;
+    auto fail_s = [&](cudaError_t e, const char* what) {
+        c->err = std::string("trt_server_create: ") + what + ": " + cudaGetErrorString(e);
+        if (s->stream) cudaStreamDestroy(s->stream);
+        if (s->copy) cudaStreamDestroy(s->copy);
+        delete s;
+        return TRT_ECUDA;
+    };
+    cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&s->totals, sizeof(unsigned long long) * T_COUNT);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->totals, 0, sizeof(unsigned long long) * T_COUNT, s->stream);
+    for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
+        e = cudaMallocHost(&s->staging[k], sizeof(Job) * MAX_JOBS);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->staged[k], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventRecord(s->staged[k], s->stream);
+    }
+    if (e != cudaSuccess) return fail_s(e, "streams and buffers");
+    std::string werr;
+    if (wave_ensure(s->wave, s->opt.wave_slots, MAX_DIR_LIGHTS, s->totals, s->stream, werr) != TRT_OK) {
+        c->err = "trt_server_create: " + werr;
+        if (s->stream) cudaStreamDestroy(s->stream);
+        if (s->copy) cudaStreamDestroy(s->copy);
+        delete s;
+        return TRT_ECUDA;
+    }
+    s->g_ext = grid_for((const void*)k_extend<false, false, true>, 128, c->sm_count);
+    s->g_sha = grid_for((const void*)k_shadow<false, false, true>, 128, c->sm_count);
+    e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return fail_s(e, "set-up");
+    s->t0 = std::chrono::steady_clock::now();
+    s->worker = std::thread(serve_loop, s);
+    *out = s;
+    return TRT_OK;
+}
+
+void trt_server_destroy(trt_server* s) {
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+        while (!s->pending.empty()) {
+            ServeRequest* r = s->pending.front();
+            s->pending.pop_front();
+            serve_finish(s, r, TRT_EINVAL);
+        }
+    }
+    s->cv_work.notify_all();
+    if (s->worker.joinable()) s->worker.join();
+    cudaSetDevice(s->ctx->device);
+    cudaStreamSynchronize(s->stream);
+    for (auto& pr : s->pool) cudaFree(pr.second);
+    if (s->wave.work) cudaFree(s->wave.work);
+    if (s->totals) cudaFree(s->totals);
+    for (int k = 0; k < 2; ++k) {
+        if (s->staging[k]) cudaFreeHost(s->staging[k]);
+        if (s->staged[k]) cudaEventDestroy(s->staged[k]);
+    }
+    cudaStreamDestroy(s->stream);
+    cudaStreamDestroy(s->copy);
+    delete s;
+}
+
+int trt_server_submit(trt_server* s, trt_scene* scene, const uint32_t params[TRT_PARAMS_WORDS], uint32_t spp,
+                      float* accum_host, uint64_t* id) {
+    if (!s || !scene || !params || !accum_host || spp == 0) return TRT_EINVAL;
+    if (scene->ctx->device != s->ctx->device) return fail(s->ctx, TRT_EINVAL, "trt_server_submit: the scene is on another device");
+    int rc = check_params(scene, params);
+    if (rc) return rc;
+    auto* r = new ServeRequest();
+    std::memcpy(r->P.w, params, sizeof(r->P.w));
+    r->scene = scene;
+    r->spp = spp;
+    r->w = r->P.w[P_SIZE];
+    r->h = r->P.w[P_SIZE + 1];
+    r->n_idx = ((r->w + 7u) / 8u) * ((r->h + 3u) / 4u) * 32u;
+    if (r->n_idx > s->wave.slots) {
+        delete r;
+        return fail(s->ctx, TRT_EINVAL, "trt_server_submit: the image needs " + std::to_string(r->n_idx) +
+                                            " path slots, more than a step holds (" + std::to_string(s->wave.slots) + ")");
+    }
+    r->host = accum_host;
+    r->accum_bytes = 80ull * r->w * r->h;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        r->id = s->next_id++;
+        r->t_submit = serve_now(s);
+        s->pending.push_back(r);
+        if (id) *id = r->id;
+    }
+    s->cv_work.notify_all();
+    return TRT_OK;
+}
+
+int trt_server_poll(trt_server* s, trt_request_done* out, uint32_t cap, uint32_t* n, uint32_t wait_ms) {
+    if (!s || !n || (cap && !out)) return TRT_EINVAL;
+    std::unique_lock<std::mutex> lk(s->mu);
+    if (s->done.empty() && wait_ms)
+        s->cv_done.wait_for(lk, std::chrono::milliseconds(wait_ms), [&] { return !s->done.empty(); });
+    uint32_t k = (uint32_t)std::min<size_t>(cap, s->done.size());
+    for (uint32_t i = 0; i < k; ++i) out[i] = s->done[i];
+    s->done.erase(s->done.begin(), s->done.begin() + k);
+    *n = k;
+    return TRT_OK;
+}
+
+int trt_server_stats_get(trt_server* s, trt_server_stats* out) {
+    if (!s || !out) return TRT_EINVAL;
+    unsigned long long t[T_COUNT];
+    // (The totals are read on the copy stream: it does not wait for queued steps.)
+    cudaError_t e = cudaMemcpyAsync(t, s->totals, sizeof(t), cudaMemcpyDeviceToHost, s->copy);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->copy);
+    if (e != cudaSuccess) return cuda_fail(s->ctx, e, "trt_server_stats_get");
+    std::lock_guard<std::mutex> lk(s->mu);
+    *out = s->stats;
+    out->closest_rays = t[T_CLOSEST];
+    out->shadow_rays = t[T_SHADOW];
+    out->active = (uint32_t)s->active.size();
+    out->pending = (uint32_t)s->pending.size();
+    return TRT_OK;
+}
+
+}  // extern "C"

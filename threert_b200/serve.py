@@ -1,0 +1,181 @@
+"""Serving from Python: the library's request loop (trt_server_*), the request mix it is measured on, an open-loop
+Poisson driver, the one-request-at-a-time baseline, and the autotuner that picks the server's wave size.
+
+The reference serves JSON-line jobs one at a time (renderer/src/main.rs:345-397). `Server` keeps scenes resident and
+lets the library's worker batch the samples of every request in flight into shared waves; a request submitted while
+others run joins the next wave. Each result is the accum `Scene.render_raw` makes alone, bit for bit.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _native as N
+from .gpu import Gpu, Scene
+from .prep import params_with
+
+
+@dataclass
+class Request:
+    scene: int            # index into the server's scene list
+    params: np.ndarray    # 156-word Params (its size is the image's)
+    spp: int
+    id: int = 0
+    accum: np.ndarray | None = None
+    done: dict = field(default_factory=dict)
+
+    @property
+    def paths(self) -> int:
+        return int(self.params[16]) * int(self.params[17]) * self.spp
+
+
+class Server:
+    """trt_server: a worker thread, its streams and wave state on the Gpu's device."""
+
+    def __init__(self, gpu: Gpu, wave_slots: int = 0, max_active: int = 0, hbm_reserve: int = 0, flags: int = 0):
+        self.gpu = gpu
+        self.handle = C.c_void_p()
+        o = N.ServerOptions(wave_slots, max_active, hbm_reserve, flags)
+        gpu._check(N.lib().trt_server_create(gpu.ctx, C.byref(o), C.byref(self.handle)), "trt_server_create")
+        self.live: dict[int, Request] = {}
+
+    def submit(self, scene: Scene, req: Request) -> int:
+        p = np.ascontiguousarray(req.params, dtype=np.uint32)
+        req.accum = np.empty((int(p[16]) * int(p[17]), N.PIXEL_FLOATS), np.float32)
+        rid = C.c_uint64()
+        self.gpu._check(N.lib().trt_server_submit(self.handle, scene.handle, p.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                                  req.spp, req.accum.ctypes.data_as(C.POINTER(C.c_float)),
+                                                  C.byref(rid)), "trt_server_submit")
+        req.id = rid.value
+        self.live[req.id] = req
+        return req.id
+
+    def poll(self, wait_ms: int = 0) -> list[Request]:
+        buf = (N.RequestDone * 64)()
+        n = C.c_uint32()
+        self.gpu._check(N.lib().trt_server_poll(self.handle, buf, 64, C.byref(n), wait_ms), "trt_server_poll")
+        out = []
+        for i in range(n.value):
+            d = {f[0]: getattr(buf[i], f[0]) for f in N.RequestDone._fields_}
+            r = self.live.pop(d["id"])
+            r.done = d
+            out.append(r)
+        return out
+
+    def stats(self) -> dict:
+        st = N.ServerStats()
+        self.gpu._check(N.lib().trt_server_stats_get(self.handle, C.byref(st)), "trt_server_stats_get")
+        return {f[0]: getattr(st, f[0]) for f in N.ServerStats._fields_}
+
+    def close(self):
+        if self.handle:
+            N.lib().trt_server_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# The serving mix: resolutions and sample counts a request draws from (uniformly).
+RESOLUTIONS = [(256, 256), (512, 512), (1280, 720), (1920, 1080)]
+SPPS = [1, 16, 64]
+
+
+def mix_requests(bases: list[np.ndarray], n: int, seed: int = 0, resolutions=RESOLUTIONS, spps=SPPS,
+                 max_bounces: int = 4) -> list[Request]:
+    """n requests over the scenes whose base Params are `bases`: scene, resolution and spp drawn uniformly."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        k = int(rng.integers(len(bases)))
+        w, h = resolutions[int(rng.integers(len(resolutions)))]
+        p = params_with(bases[k], width=w, height=h, max_bounces=max_bounces)
+        out.append(Request(k, p, int(spps[int(rng.integers(len(spps)))])))
+    return out
+
+
+def run_stream(server: Server, scenes: list[Scene], requests: list[Request], rate: float, seed: int = 1,
+               timeout_s: float = 600.0) -> dict:
+    """Submits the requests at Poisson arrival times of `rate` a second (open loop, from a thread of its own) and
+    waits for every one: latencies (done - submit, ms), the span from the first submit to the last completion, rays."""
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / rate, len(requests)) if rate > 0 else np.zeros(len(requests))
+    before = server.stats()
+    done: list[Request] = []
+    errors: list[BaseException] = []
+
+    def feed():
+        try:
+            t = time.perf_counter()
+            for r, g in zip(requests, gaps):
+                t += g
+                dt = t - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)
+                server.submit(scenes[r.scene], r)
+        except BaseException as e:  # surfaced below
+            errors.append(e)
+
+    th = threading.Thread(target=feed, daemon=True)
+    t0 = time.perf_counter()
+    th.start()
+    while len(done) < len(requests) and time.perf_counter() - t0 < timeout_s and not errors:
+        done += server.poll(wait_ms=20)
+    th.join()
+    if errors:
+        raise errors[0]
+    if len(done) < len(requests):
+        raise TimeoutError(f"{len(done)} of {len(requests)} requests done in {timeout_s} s")
+    after = server.stats()
+    lat = np.array([r.done["done_ms"] - r.done["submit_ms"] for r in done])
+    span = (max(r.done["done_ms"] for r in done) - min(r.done["submit_ms"] for r in done)) * 1e-3
+    rays = (after["closest_rays"] + after["shadow_rays"]) - (before["closest_rays"] + before["shadow_rays"])
+    return {"requests": len(done), "failed": sum(r.done["status"] != 0 for r in done),
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "mean_ms": float(lat.mean()), "span_s": span, "rays": int(rays), "mrays_per_s": rays / span / 1e6,
+            "paths": int(after["paths"] - before["paths"]), "steps": int(after["steps"] - before["steps"]),
+            "busy_s": (after["busy_ms"] - before["busy_ms"]) * 1e-3}
+
+
+def run_serial(gpu: Gpu, scenes: list[Scene], requests: list[Request]) -> dict:
+    """The reference's way: each request rendered alone through trt_render and read back before the next starts."""
+    rays = 0
+    lat = []
+    t0 = time.perf_counter()
+    for r in requests:
+        t = time.perf_counter()
+        acc, st = scenes[r.scene].render_raw(r.params, r.spp)
+        lat.append((time.perf_counter() - t) * 1e3)
+        rays += st.closest_rays + st.shadow_rays
+    span = time.perf_counter() - t0
+    return {"requests": len(requests), "span_s": span, "rays": int(rays), "mrays_per_s": rays / span / 1e6,
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))}
+
+
+def autotune(gpu: Gpu, scenes: list[Scene], requests: list[Request], candidates=(1 << 20, 2 << 20, 4 << 20),
+             flags_options=(0, N.TRT_RENDER_UNSORTED_HITS)) -> tuple[dict, list]:
+    """Times the requests back to back (all submitted at once) under each wave size and sort setting; returns the
+    fastest options and every trial (Mrays/s). The wave must hold the largest request's image."""
+    need = max(((int(r.params[16]) + 7) // 8) * ((int(r.params[17]) + 3) // 4) * 32 for r in requests)
+    trials = []
+    for slots in candidates:
+        if slots < need:
+            continue
+        for flags in flags_options:
+            srv = Server(gpu, wave_slots=slots, flags=flags)
+            try:
+                copies = [Request(r.scene, r.params, r.spp) for r in requests]
+                res = run_stream(srv, scenes, copies, rate=0.0)
+            finally:
+                srv.close()
+            trials.append({"wave_slots": slots, "flags": flags, "mrays_per_s": res["mrays_per_s"],
+                           "span_s": res["span_s"]})
+    best = max(trials, key=lambda t: t["mrays_per_s"])
+    return best, trials
