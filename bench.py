@@ -311,6 +311,90 @@ def run_crowd(args, rank, world, local, dist):
     gpu.close()
 
 
+SERVE_METRIC = "aggregate Mrays/s, serving mix (8 resident scenes; Poisson requests of 256^2..1080p, 1/16/64 spp)"
+
+
+def serve_scenes():
+    """Config 4's resident scenes: two Cornell boxes, three cities and three crowds of different seeds."""
+    from threert_b200 import crowd, prep, scenes
+    t = time.perf_counter()
+    descs = [scenes.cornell(256, 256, seed=0x5EED), scenes.cornell(256, 256, seed=0x1234)]
+    descs += [scenes.city(width=WIDTH, height=HEIGHT, max_depth=DEPTH, seed=s) for s in (1, 2, 3)]
+    descs += [crowd.crowd(n=5000, groups=1, width=WIDTH, height=HEIGHT, max_depth=DEPTH, seed=s).desc
+              for s in (11, 12, 13)]
+    Ps = [prep.prepare(d) for d in descs]
+    log(f"serve: 8 scenes prepared in {time.perf_counter() - t:.1f} s")
+    return Ps
+
+
+def run_serve(args, rank, world, local):
+    """The serving loop on one GPU (replicas beyond: each rank serves its own stream). The mix: each request a
+    scene, a resolution of {256^2, 512^2, 1280x720, 1920x1080} and 1, 16 or 64 spp, depth 4, arriving as a seeded
+    Poisson stream; then a stream of 720p 1-spp requests. Each stream is also rendered one request at a time
+    (trt_render and its read-back) as the reference's serve loop does: the baseline of the ratio."""
+    from threert_b200 import Gpu
+    from threert_b200 import serve as SV
+    from threert_b200.prep import params_with
+    Ps = serve_scenes()
+    gpu = Gpu(local)
+    name, sms = gpu.device_info()
+    S = [gpu.upload(P) for P in Ps]
+    bases = [P.params for P in Ps]
+    # The autotuner: wave size and the material sort, on a short burst of the mix (spp 1 and 16).
+    tune_reqs = SV.mix_requests(bases, 24, seed=100 + rank, spps=[1, 16])
+    best, trials = SV.autotune(gpu, S, tune_reqs)
+    log(f"autotune: {trials} -> {best}")
+    srv = SV.Server(gpu, wave_slots=best["wave_slots"], flags=best["flags"])
+    warm = SV.mix_requests(bases, 8, seed=200 + rank, spps=[1])
+    SV.run_stream(srv, S, warm, rate=0.0)
+    mix = SV.mix_requests(bases, args.requests, seed=300 + rank)
+    res = SV.run_stream(srv, S, mix, rate=args.rate, seed=400 + rank, keep=False)
+    serial = SV.run_serial(gpu, S, [SV.Request(r.scene, r.params, r.spp) for r in mix])
+    log(f"mix: served {res}, serial {serial}")
+    # 720p, 1 spp, over the three cities: the latency stream.
+    rng = np.random.default_rng(500 + rank)
+    hd = [SV.Request(int(k), params_with(bases[int(k)], max_bounces=DEPTH), 1) for k in rng.integers(2, 5, args.requests)]
+    res_hd = SV.run_stream(srv, S, hd, rate=args.rate_720p, seed=600 + rank, keep=False)
+    # ... and the same requests all at once (throughput at saturation) against one at a time.
+    sat_hd = SV.run_stream(srv, S, [SV.Request(r.scene, r.params, r.spp) for r in hd], rate=0.0, keep=False)
+    serial_hd = SV.run_serial(gpu, S, [SV.Request(r.scene, r.params, r.spp) for r in hd])
+    # 256 x 256, 1 spp over all eight scenes, as fast as they come: where one-at-a-time rendering idles the GPU.
+    small = [SV.Request(int(k), params_with(bases[int(k)], width=256, height=256, max_bounces=DEPTH), 1)
+             for k in rng.integers(0, 8, 4 * args.requests)]
+    res_small = SV.run_stream(srv, S, small, rate=args.rate_small, seed=700 + rank, keep=False)
+    serial_small = SV.run_serial(gpu, S, [SV.Request(r.scene, r.params, r.spp) for r in small])
+    srv.close()
+    line = {
+        "metric": SERVE_METRIC, "value": res["mrays_per_s"] * world, "unit": "Mrays/s", "n_gpus": world,
+        "steps": res["steps"], "warmup": len(warm), "ms_per_step": res["busy_s"] * 1e3 / max(1, res["steps"]),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"serving mix: {args.requests} requests at {args.rate} req/s Poisson over 8 resident "
+                               "scenes (2 Cornell, 3 city, 3 crowd)", "device": name, "sms": sms,
+                   "autotuned": best, "autotune_trials": trials, "parallelism": f"replicas x{world}"},
+        "p50_ms": res["p50_ms"], "p99_ms": res["p99_ms"], "span_s": res["span_s"],
+        "serial": {"mrays_per_s": serial["mrays_per_s"], "span_s": serial["span_s"]},
+        "speedup_over_serial": res["mrays_per_s"] / serial["mrays_per_s"],
+        "stream_720p_1spp": {"rate": args.rate_720p, "requests": len(hd), "p50_ms": res_hd["p50_ms"],
+                             "p99_ms": res_hd["p99_ms"], "mrays_per_s_at_rate": res_hd["mrays_per_s"],
+                             "mrays_per_s_saturated": sat_hd["mrays_per_s"],
+                             "serial_mrays_per_s": serial_hd["mrays_per_s"],
+                             "serial_p50_ms": serial_hd["p50_ms"],
+                             "speedup_over_serial": sat_hd["mrays_per_s"] / serial_hd["mrays_per_s"]},
+        "stream_256_1spp": {"rate": args.rate_small, "requests": len(small), "p50_ms": res_small["p50_ms"],
+                            "p99_ms": res_small["p99_ms"], "mrays_per_s": res_small["mrays_per_s"],
+                            "serial_mrays_per_s": serial_small["mrays_per_s"],
+                            "serial_p50_ms": serial_small["p50_ms"],
+                            "speedup_over_serial": res_small["mrays_per_s"] / serial_small["mrays_per_s"]},
+        "e2e": {"value": res["mrays_per_s"] * world, "unit": "Mrays/s",
+                "h2d_bytes_per_step": 624, "d2h_bytes_per_step": int(np.mean([80 * int(r.params[16]) * int(r.params[17]) for r in mix]))},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    for s_ in S:
+        s_.close()
+    gpu.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -323,8 +407,12 @@ def main():
                     help="coherence sorts on the device: 'none', or a comma list of rays, hits, shadows "
                          "(hits by material is the pass's default; the other two measured slower here)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
-    ap.add_argument("--workload", default="city", choices=["city", "crowd"],
-                    help="city (the headline workload) or the crowd with its per-frame deformation")
+    ap.add_argument("--workload", default="city", choices=["city", "crowd", "serve"],
+                    help="city (the headline workload), the crowd with its per-frame deformation, or the serving mix")
+    ap.add_argument("--requests", type=int, default=64, help="serve: requests a stream")
+    ap.add_argument("--rate", type=float, default=200.0, help="serve: the mix's arrival rate (requests a second)")
+    ap.add_argument("--rate-720p", type=float, default=60.0, help="serve: the 720p stream's arrival rate")
+    ap.add_argument("--rate-small", type=float, default=2000.0, help="serve: the 256^2 stream's arrival rate")
     ap.add_argument("--groups", type=int, default=1, help="crowd: pose groups (skinned copies of the humanoid)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -347,6 +435,11 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
 
+    if args.workload == "serve":
+        run_serve(args, rank, world, local)
+        if dist:
+            dist.destroy_process_group()
+        return
     if args.workload == "crowd":
         run_crowd(args, rank, world, local, dist)
         if dist:

@@ -26,6 +26,7 @@ struct ServeRequest {
     uint64_t accum_bytes = 0;
     double t_submit = 0, t_start = -1;
     int status = TRT_OK;
+    cudaEvent_t copied = nullptr;  // its read-back's completion
 };
 
 // One step on the GPU: its events, the requests it finishes, its counts.
@@ -53,6 +54,8 @@ struct trt_server {
     std::deque<trt::ServeRequest*> pending;
     std::vector<trt::ServeRequest*> active;
     std::vector<trt_request_done> done;
+    std::vector<trt::ServeRequest*> copying;  // read-backs queued on the copy stream, not yet seen complete
+    std::vector<cudaEvent_t> ev_free;
     std::multimap<uint64_t, float4*> pool;  // accum buffers by size, free for reuse
     uint64_t next_id = 1;
     std::chrono::steady_clock::time_point t0;
@@ -175,18 +178,26 @@ bool serve_step(trt_server* s, ServeStep& step) {
     return true;
 }
 
-// Waits for a queued step, reads back the requests it finished (copy stream) and reports them.
+// Waits for a queued step and queues the read-back of the requests it finished on the copy stream (into pinned host
+// memory it runs at full speed and does not hold the worker; into pageable memory the copy call itself waits).
 void serve_retire(trt_server* s, ServeStep& step) {
     cudaEventSynchronize(step.t1);
     float ms = 0;
     cudaEventElapsedTime(&ms, step.t0, step.t1);
     for (ServeRequest* r : step.finishing) {
-        cudaStreamWaitEvent(s->copy, step.t1, 0);
-        cudaError_t e = cudaMemcpyAsync(r->host, r->accum, r->accum_bytes, cudaMemcpyDeviceToHost, s->copy);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s->copy);
+        cudaEvent_t ev = nullptr;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            if (!s->ev_free.empty()) { ev = s->ev_free.back(); s->ev_free.pop_back(); }
+        }
+        if (!ev) cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        cudaError_t e = cudaStreamWaitEvent(s->copy, step.t1, 0);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(r->host, r->accum, r->accum_bytes, cudaMemcpyDeviceToHost, s->copy);
+        if (e == cudaSuccess) e = cudaEventRecord(ev, s->copy);
+        r->copied = ev;
+        if (e != cudaSuccess) r->status = TRT_ECUDA;
         std::lock_guard<std::mutex> lk(s->mu);
-        s->active.erase(std::remove(s->active.begin(), s->active.end(), r), s->active.end());
-        serve_finish(s, r, e == cudaSuccess ? TRT_OK : TRT_ECUDA);
+        s->copying.push_back(r);
     }
     std::lock_guard<std::mutex> lk(s->mu);
     s->stats.steps++;
@@ -194,6 +205,27 @@ void serve_retire(trt_server* s, ServeStep& step) {
     s->stats.busy_ms += ms;
     step.finishing.clear();
     step.paths = 0;
+}
+
+// Reports the requests whose read-back has completed (waiting for them all when `all`).
+void serve_reap(trt_server* s, bool all) {
+    std::vector<ServeRequest*> ready;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        for (ServeRequest* r : s->copying) {
+            cudaError_t q = all ? cudaEventSynchronize(r->copied) : cudaEventQuery(r->copied);
+            if (q == cudaErrorNotReady) continue;
+            if (q != cudaSuccess) r->status = TRT_ECUDA;
+            ready.push_back(r);
+        }
+        if (ready.empty()) return;
+        for (ServeRequest* r : ready) {
+            s->copying.erase(std::remove(s->copying.begin(), s->copying.end(), r), s->copying.end());
+            s->active.erase(std::remove(s->active.begin(), s->active.end(), r), s->active.end());
+            s->ev_free.push_back(r->copied);
+            serve_finish(s, r, r->status);
+        }
+    }
     s->cv_done.notify_all();
 }
 
@@ -209,19 +241,21 @@ void serve_loop(trt_server* s) {
     for (;;) {
         bool queued = serve_step(s, steps[cur]);
         if (in_flight) serve_retire(s, steps[cur ^ 1]);
+        serve_reap(s, false);
         in_flight = queued;
         if (queued) {
             cur ^= 1;
             continue;
         }
-        // Nothing to queue: wait for work (or the stop).
+        // Nothing to queue: finish the read-backs, then wait for work (or the stop).
+        serve_reap(s, true);
         std::unique_lock<std::mutex> lk(s->mu);
         bool have = false;
         for (ServeRequest* r : s->active) have |= r->issued < r->spp;
         if (have) continue;
         if (s->stop && s->active.empty() && s->pending.empty()) break;
-        // (A request that waits for device memory is retried when a request finishes or 5 ms pass.)
-        s->cv_work.wait_for(lk, std::chrono::milliseconds(5));
+        // (A request that waits for device memory is retried when a request finishes or 1 ms passes.)
+        s->cv_work.wait_for(lk, std::chrono::milliseconds(1));
     }
     for (auto& st : steps) {
         cudaEventDestroy(st.t0);
@@ -295,6 +329,7 @@ void trt_server_destroy(trt_server* s) {
     cudaSetDevice(s->ctx->device);
     cudaStreamSynchronize(s->stream);
     for (auto& pr : s->pool) cudaFree(pr.second);
+    for (cudaEvent_t e : s->ev_free) cudaEventDestroy(e);
     if (s->wave.work) cudaFree(s->wave.work);
     if (s->totals) cudaFree(s->totals);
     for (int k = 0; k < 2; ++k) {

@@ -78,12 +78,14 @@ class Scene:
             pass
 
     def render_raw(self, params: np.ndarray, spp: int, first_sample: int = 0, flags: int = 0, read: bool = True,
-                   stats: bool = True):
-        """Runs the pass; returns (accum as (w*h, 20) float32 or None, Stats or None)."""
+                   stats: bool = True, out: np.ndarray | None = None):
+        """Runs the pass; returns (accum as (w*h, 20) float32 or None, Stats or None). `out`: the array to read into."""
         L = N.lib()
         p = np.ascontiguousarray(params, dtype=np.uint32)
         w, h = int(p[16]), int(p[17])
-        acc = np.empty((w * h, N.PIXEL_FLOATS), np.float32) if read else None
+        if out is not None and (out.dtype != np.float32 or out.shape != (w * h, N.PIXEL_FLOATS) or not out.flags.c_contiguous):
+            raise ValueError("render_raw: `out` must be a C-contiguous (w*h, 20) float32 array")
+        acc = (out if out is not None else np.empty((w * h, N.PIXEL_FLOATS), np.float32)) if read else None
         st = N.Stats() if stats else None
         rc = L.trt_render(self.handle, p.ctypes.data_as(C.POINTER(C.c_uint32)), first_sample, spp, flags,
                           acc.ctypes.data_as(C.POINTER(C.c_float)) if read else None, C.byref(st) if stats else None)
