@@ -186,6 +186,8 @@ typedef struct {
     uint32_t max_active;   /* requests in flight at most, 1-64 (0: 64) */
     uint64_t hbm_reserve;  /* device bytes admission leaves free (0: 1 GiB) */
     uint32_t flags;        /* TRT_RENDER_UNSORTED_HITS / TRT_RENDER_SORT_* for every step */
+    uint32_t launch_mode;  /* 0: each step's launches replayed from a CUDA graph captured once per (depth, size
+                            * class); 1: launched one by one */
 } trt_server_options;
 typedef struct {
     uint64_t id;

@@ -33,11 +33,12 @@ def the_mix(Ps, seed=3):
     return reqs
 
 
+@pytest.mark.parametrize("launch_mode", [0, 1])  # steps replayed from CUDA graphs; launched one by one
 @pytest.mark.parametrize("wave_slots", [16384, 1 << 20])  # small: requests spread over steps; large: one step
-def test_each_result_is_the_same_alone_and_in_the_mix(gpu, resident, wave_slots):
+def test_each_result_is_the_same_alone_and_in_the_mix(gpu, resident, wave_slots, launch_mode):
     Ps, S = resident
     reqs = the_mix(Ps)
-    srv = Server(gpu, wave_slots=wave_slots, max_active=8)
+    srv = Server(gpu, wave_slots=wave_slots, max_active=8, launch_mode=launch_mode)
     try:
         before = srv.stats()
         res = run_stream(srv, S, reqs, rate=0.0)  # all at once: they share waves

@@ -132,7 +132,7 @@ TRT_CORNER_NORMAL = 1
 TRT_CORNER_TANGENT = 2
 
 class ServerOptions(C.Structure):
-    _fields_ = [("wave_slots", u32), ("max_active", u32), ("hbm_reserve", u64), ("flags", u32)]
+    _fields_ = [("wave_slots", u32), ("max_active", u32), ("hbm_reserve", u64), ("flags", u32), ("launch_mode", u32)]
 
 
 class RequestDone(C.Structure):

@@ -136,7 +136,11 @@ struct Job {
     Walk wk;
     float4* accum;
     uint32_t slot_first, n_idx, K, first_sample;
+    uint32_t idx_first;  // the earlier jobs' n_idx summed: its pixels' place in a pass over every job's pixels
 };
+// What a wave of a server step holds, in device memory ahead of its job table, so that the step's launches (and a
+// graph captured from them) do not change from step to step.
+struct StepHead { uint32_t n_jobs, paths, pad0, pad1; };
 constexpr uint32_t MAX_JOBS = 64u;
 // The hot kernels take the table and, for a wave of one job, that job as a kernel argument (MULTI = false): its reads
 // then come from the kernel's constant bank, not global memory.
@@ -166,7 +170,9 @@ __device__ void camera_ray(const Params& P, uint32_t gx, uint32_t gy, const floa
     }
 }
 
-__global__ void k_raygen(const Job* __restrict__ jobs, uint32_t n_jobs, PathBufs B, Queues Q, uint32_t n_slots) {
+__global__ void k_raygen(const Job* __restrict__ jobs, uint32_t n_jobs, PathBufs B, Queues Q, uint32_t n_slots,
+                         const StepHead* __restrict__ head) {
+    if (head) n_jobs = head->n_jobs;
     uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     bool valid = false;
     uint32_t gx = 0, gy = 0, j = 0;
@@ -631,9 +637,7 @@ __global__ void k_sort_scatter(Queues Q, const uint32_t* __restrict__ in, uint32
 }
 
 // accum += each sample's path, in sample order (pathtrace.wgsl:4541-4557).
-__global__ void k_accumulate(const Job* __restrict__ jobs, PathBufs B) {
-    const Job& J = jobs[blockIdx.y];
-    uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void accumulate_one(const Job& J, const PathBufs& B, uint32_t idx) {
     uint32_t n_idx = J.n_idx, K = J.K;
     float4* accum = J.accum;
     uint32_t w = J.P.w[P_SIZE], h = J.P.w[P_SIZE + 1];
@@ -653,10 +657,25 @@ __global__ void k_accumulate(const Job* __restrict__ jobs, PathBufs B) {
     accum[pix * 5 + 1] = a;
     accum[pix * 5 + 2] = nn;
 }
+__global__ void k_accumulate(const Job* __restrict__ jobs, PathBufs B) {
+    accumulate_one(jobs[blockIdx.y], B, blockIdx.x * blockDim.x + threadIdx.x);
+}
+// The same over every job's pixels in one flat pass (a thread a pixel index of some job).
+__global__ void k_accumulate_flat(const Job* __restrict__ jobs, const StepHead* __restrict__ head, PathBufs B,
+                                  uint32_t n_threads) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_threads) return;
+    uint32_t n_jobs = head->n_jobs, j = 0;
+    while (j + 1 < n_jobs && t >= jobs[j + 1].idx_first) ++j;
+    const Job& J = jobs[j];
+    if (n_jobs == 0 || t < J.idx_first || t - J.idx_first >= J.n_idx) return;
+    accumulate_one(J, B, t - J.idx_first);
+}
 
 // Per-wave counts into the cumulative totals.
-__global__ void k_tally(Queues Q, uint32_t depths, uint32_t paths) {
+__global__ void k_tally(Queues Q, uint32_t depths, uint32_t paths, const StepHead* __restrict__ head) {
     if (threadIdx.x != 0) return;
+    if (head) paths = head->paths;
     unsigned long long c = 0, s = 0;
     for (uint32_t d = 0; d < depths; ++d) {
         c += Q.cnt[d * CNT_STRIDE];
@@ -947,7 +966,7 @@ int render_waves(trt_scene* s, const Params& P, uint32_t first_sample, uint32_t 
         uint32_t n = n_idx * k;
         Job job{P, wk, s->accum, 0u, n_idx, k, first_sample + s0};
         k_put_job<<<1, 128, 0, st>>>(job, s->wave.jobs, 0u);
-        k_raygen<<<(n + blk - 1) / blk, blk, 0, st>>>(s->wave.jobs, 1u, s->wave.B, s->wave.Q, n);
+        k_raygen<<<(n + blk - 1) / blk, blk, 0, st>>>(s->wave.jobs, 1u, s->wave.B, s->wave.Q, n, nullptr);
         s->launches += 2;
         for (uint32_t depth = 0; depth <= last; ++depth) {
             // The depth's queue (raw), the order extend walks it in, the order shade takes the hits in.
@@ -989,7 +1008,7 @@ int render_waves(trt_scene* s, const Params& P, uint32_t first_sample, uint32_t 
             s->shadow_launches++;
         }
         k_accumulate<<<dim3((n_idx + blk - 1) / blk, 1), blk, 0, st>>>(s->wave.jobs, s->wave.B);
-        k_tally<<<1, 32, 0, st>>>(s->wave.Q, last + 1, w * h * k);
+        k_tally<<<1, 32, 0, st>>>(s->wave.Q, last + 1, w * h * k, nullptr);
         s->launches += 2;
     }
     TRT_CUDA(c, cudaGetLastError());
@@ -1542,7 +1561,7 @@ int trt_render_noalloc(const trt_scene_desc* dev, const uint32_t params[TRT_PARA
         uint32_t n = n_idx * k;
         Job job{P, wk, (float4*)accum_device, 0u, n_idx, k, first_sample + s0};
         k_put_job<<<1, 128, 0, st>>>(job, jobs, 0u);
-        k_raygen<<<(n + blk - 1) / blk, blk, 0, st>>>(jobs, 1u, B, Q, n);
+        k_raygen<<<(n + blk - 1) / blk, blk, 0, st>>>(jobs, 1u, B, Q, n, nullptr);
         for (uint32_t depth = 0; depth <= last; ++depth) {
             uint32_t* queue = Q.q[depth & 1u];
             k_extend<false, false, false><<<g_ext, blk, 0, st>>>(jobs, job, B, Q, depth, queue);
@@ -1551,7 +1570,7 @@ int trt_render_noalloc(const trt_scene_desc* dev, const uint32_t params[TRT_PARA
             k_resolve<false><<<(n + blk - 1) / blk, blk, 0, st>>>(jobs, job, B, Q, depth, queue);
         }
         k_accumulate<<<dim3((n_idx + blk - 1) / blk, 1), blk, 0, st>>>(jobs, B);
-        k_tally<<<1, 32, 0, st>>>(Q, last + 1, w * h * k);
+        k_tally<<<1, 32, 0, st>>>(Q, last + 1, w * h * k, nullptr);
         e = cudaGetLastError();
     }
     if (e != cudaSuccess) return na_fail(err, err_len, TRT_ECUDA, cudaGetErrorString(e));

@@ -44,7 +44,10 @@ struct trt_server {
     cudaStream_t stream = nullptr, copy = nullptr;
     Wave wave;
     unsigned long long* totals = nullptr;
-    Job* staging[2] = {nullptr, nullptr};  // pinned job tables, alternating between steps
+    // The step's table on the device: a StepHead, then at TABLE_JOBS the jobs; pinned staging copies alternate.
+    uint8_t* table = nullptr;
+    uint8_t* staging[2] = {nullptr, nullptr};
+    std::map<std::pair<uint32_t, uint32_t>, cudaGraphExec_t> graphs;  // by (deepest depth, launch size)
     cudaEvent_t staged[2] = {nullptr, nullptr};
     uint32_t parity = 0;
     std::thread worker;
@@ -65,6 +68,9 @@ struct trt_server {
 };
 
 namespace {
+
+constexpr uint64_t TABLE_JOBS = 256;  // the jobs' offset in the step table
+constexpr uint64_t TABLE_BYTES = TABLE_JOBS + sizeof(Job) * MAX_JOBS;
 
 double serve_now(const trt_server* s) {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - s->t0).count();
@@ -111,6 +117,36 @@ void serve_finish(trt_server* s, ServeRequest* r, int status) {
     delete r;
 }
 
+// A step's launches, all sized by `size` (the kernels stop at the counts on the device), reading the step table.
+void serve_enqueue(trt_server* s, uint32_t last, uint32_t size, cudaStream_t st) {
+    Wave& W = s->wave;
+    const StepHead* head = reinterpret_cast<const StepHead*>(s->table);
+    const Job* tj = reinterpret_cast<const Job*>(s->table + TABLE_JOBS);
+    const int blk = 128;
+    const Job none{};
+    uint32_t grid = (size + blk - 1) / blk;
+    cudaMemsetAsync(W.Q.cnt, 0, 4ull * (MAX_DEPTH * CNT_STRIDE + CNT_STRIDE), st);
+    k_raygen<<<grid, blk, 0, st>>>(tj, 0u, W.B, W.Q, size, head);
+    bool sort_hits = (s->opt.flags & TRT_RENDER_UNSORTED_HITS) == 0;
+    for (uint32_t depth = 0; depth <= last; ++depth) {
+        uint32_t* raw = W.Q.q[depth & 1u];
+        uint32_t* next = W.Q.q[(depth + 1u) & 1u];
+        k_extend<false, false, true><<<s->g_ext, blk, 0, st>>>(tj, none, W.B, W.Q, depth, raw);
+        uint32_t* shade_q = raw;
+        if (sort_hits) {
+            shade_q = W.Q.qx;
+            k_sort_count<SORT_HITS><<<(size + SORT_ITEMS - 1u) / SORT_ITEMS, SORT_THREADS, 0, st>>>(tj, W.B, W.Q, raw,
+                                                                                                  depth, 0u);
+            k_sort_scatter<SORT_HITS><<<(size + 255u) / 256u, 256, 0, st>>>(W.Q, raw, shade_q, depth);
+        }
+        k_shade<true><<<grid, blk, 0, st>>>(tj, none, W.B, W.Q, depth, shade_q, next);
+        k_shadow<false, false, true><<<s->g_sha, blk, 0, st>>>(tj, none, W.B, W.Q, depth, nullptr);
+        k_resolve<true><<<grid, blk, 0, st>>>(tj, none, W.B, W.Q, depth, shade_q);
+    }
+    k_accumulate_flat<<<grid, blk, 0, st>>>(tj, head, W.B, size);
+    k_tally<<<1, 32, 0, st>>>(W.Q, last + 1, 0u, head);
+}
+
 // Plans and queues one step from the active requests; false when none has samples left to issue.
 bool serve_step(trt_server* s, ServeStep& step) {
     std::vector<Job> jobs;
@@ -141,39 +177,52 @@ bool serve_step(trt_server* s, ServeStep& step) {
     }
     if (jobs.empty()) return false;
     cudaStream_t st = s->stream;
-    // The job table through a pinned staging buffer (the one two steps back is free once its copy has run).
-    Job* stage = s->staging[s->parity];
+    // The step's table through a pinned staging buffer (the one two steps back is free once its copy has run).
+    uint8_t* stage = s->staging[s->parity];
     cudaEventSynchronize(s->staged[s->parity]);
-    std::memcpy(stage, jobs.data(), sizeof(Job) * jobs.size());
+    StepHead head{(uint32_t)jobs.size(), (uint32_t)std::min<uint64_t>(step.paths, 0xffffffffu), 0u, 0u};
+    uint32_t idx_first = 0;
+    for (Job& j : jobs) {
+        j.idx_first = idx_first;
+        idx_first += j.n_idx;
+    }
+    std::memcpy(stage, &head, sizeof(head));
+    std::memcpy(stage + TABLE_JOBS, jobs.data(), sizeof(Job) * jobs.size());
     cudaEventRecord(step.t0, st);
-    cudaMemcpyAsync(s->wave.jobs, stage, sizeof(Job) * jobs.size(), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(s->table, stage, TABLE_JOBS + sizeof(Job) * jobs.size(), cudaMemcpyHostToDevice, st);
     cudaEventRecord(s->staged[s->parity], st);
     s->parity ^= 1u;
-    Wave& W = s->wave;
-    const int blk = 128;
-    uint32_t n = slot, nj = (uint32_t)jobs.size();
-    const Job none{};
-    cudaMemsetAsync(W.Q.cnt, 0, 4ull * (MAX_DEPTH * CNT_STRIDE + CNT_STRIDE), st);
-    k_raygen<<<(n + blk - 1) / blk, blk, 0, st>>>(W.jobs, nj, W.B, W.Q, n);
-    bool sort_hits = (s->opt.flags & TRT_RENDER_UNSORTED_HITS) == 0;
-    for (uint32_t depth = 0; depth <= last; ++depth) {
-        uint32_t* raw = W.Q.q[depth & 1u];
-        uint32_t* next = W.Q.q[(depth + 1u) & 1u];
-        k_extend<false, false, true><<<s->g_ext, blk, 0, st>>>(W.jobs, none, W.B, W.Q, depth, raw);
-        uint32_t* shade_q = raw;
-        if (sort_hits) {
-            shade_q = W.Q.qx;
-            uint32_t shift = chunk_shift(n);
-            k_sort_count<SORT_HITS><<<(n + SORT_ITEMS - 1u) / SORT_ITEMS, SORT_THREADS, 0, st>>>(W.jobs, W.B, W.Q, raw,
-                                                                                               depth, shift);
-            k_sort_scatter<SORT_HITS><<<(n + 255u) / 256u, 256, 0, st>>>(W.Q, raw, shade_q, depth);
+    // Launch sizes by the power of two at or above the slots used (at least 2^16, at most the wave): the kernels
+    // read the true counts from the device, so one graph serves every step of that size class and depth.
+    uint32_t size = 1u << 16;
+    while (size < slot && size < s->wave.slots) size <<= 1;
+    size = std::min(size, s->wave.slots);
+    if (s->opt.launch_mode == 0) {
+        auto key = std::make_pair(last, size);
+        auto it = s->graphs.find(key);
+        if (it == s->graphs.end()) {
+            cudaGraph_t g = nullptr;
+            cudaGraphExec_t exec = nullptr;
+            cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+            if (e == cudaSuccess) {
+                serve_enqueue(s, last, size, st);
+                e = cudaStreamEndCapture(st, &g);
+            }
+            if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, g, 0);
+            if (g) cudaGraphDestroy(g);
+            if (e != cudaSuccess) {
+                // (Then the server launches directly from here on.)
+                std::lock_guard<std::mutex> lk(s->mu);
+                s->err = std::string("graph capture: ") + cudaGetErrorString(e);
+                s->opt.launch_mode = 1;
+                cudaGetLastError();
+            } else {
+                it = s->graphs.emplace(key, exec).first;
+            }
         }
-        k_shade<true><<<(n + blk - 1) / blk, blk, 0, st>>>(W.jobs, none, W.B, W.Q, depth, shade_q, next);
-        k_shadow<false, false, true><<<s->g_sha, blk, 0, st>>>(W.jobs, none, W.B, W.Q, depth, nullptr);
-        k_resolve<true><<<(n + blk - 1) / blk, blk, 0, st>>>(W.jobs, none, W.B, W.Q, depth, shade_q);
+        if (s->opt.launch_mode == 0) cudaGraphLaunch(it->second, st);
     }
-    k_accumulate<<<dim3((n_idx_max + blk - 1) / blk, nj), blk, 0, st>>>(W.jobs, W.B);
-    k_tally<<<1, 32, 0, st>>>(W.Q, last + 1, (uint32_t)std::min<uint64_t>(step.paths, 0xffffffffu));
+    if (s->opt.launch_mode != 0) serve_enqueue(s, last, size, st);
     cudaEventRecord(step.t1, st);
     return true;
 }
@@ -289,8 +338,9 @@ int trt_server_create(trt_ctx* c, const trt_server_options* opts, trt_server** o
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&s->totals, sizeof(unsigned long long) * T_COUNT);
     if (e == cudaSuccess) e = cudaMemsetAsync(s->totals, 0, sizeof(unsigned long long) * T_COUNT, s->stream);
+    if (e == cudaSuccess) e = cudaMalloc(&s->table, TABLE_BYTES);
     for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
-        e = cudaMallocHost(&s->staging[k], sizeof(Job) * MAX_JOBS);
+        e = cudaMallocHost(&s->staging[k], TABLE_BYTES);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->staged[k], cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventRecord(s->staged[k], s->stream);
     }
@@ -332,6 +382,8 @@ void trt_server_destroy(trt_server* s) {
     for (cudaEvent_t e : s->ev_free) cudaEventDestroy(e);
     if (s->wave.work) cudaFree(s->wave.work);
     if (s->totals) cudaFree(s->totals);
+    if (s->table) cudaFree(s->table);
+    for (auto& g : s->graphs) cudaGraphExecDestroy(g.second);
     for (int k = 0; k < 2; ++k) {
         if (s->staging[k]) cudaFreeHost(s->staging[k]);
         if (s->staged[k]) cudaEventDestroy(s->staged[k]);

@@ -36,10 +36,11 @@ class Request:
 class Server:
     """trt_server: a worker thread, its streams and wave state on the Gpu's device."""
 
-    def __init__(self, gpu: Gpu, wave_slots: int = 0, max_active: int = 0, hbm_reserve: int = 0, flags: int = 0):
+    def __init__(self, gpu: Gpu, wave_slots: int = 0, max_active: int = 0, hbm_reserve: int = 0, flags: int = 0,
+                 launch_mode: int = 0):
         self.gpu = gpu
         self.handle = C.c_void_p()
-        o = N.ServerOptions(wave_slots, max_active, hbm_reserve, flags)
+        o = N.ServerOptions(wave_slots, max_active, hbm_reserve, flags, launch_mode)
         gpu._check(N.lib().trt_server_create(gpu.ctx, C.byref(o), C.byref(self.handle)), "trt_server_create")
         self.live: dict[int, Request] = {}
         self.pool: dict[int, list] = {}  # pinned result buffers by pixel count, free for reuse
