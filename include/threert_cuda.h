@@ -87,6 +87,9 @@ typedef struct { float t; uint32_t tri; float u; float v; uint32_t inst; uint32_
 /* Optional, measured slower on the city scene: secondary rays by (queue chunk, direction octant) before the
  * closest-hit walk, shadow rays by (position chunk, direction octant) in each light class before the shadow walk. */
 #define TRT_RENDER_SORT_RAYS      8u
+/* Also sum each sample's first-hit distance (0 where the camera ray escapes) into x of the Pixel's fourth vec4, which
+ * the offline reference leaves zero: the denoisers' depth guide (mean = x / count). */
+#define TRT_RENDER_DEPTH         64u
 #define TRT_RENDER_SORT_SHADOWS  32u
 
 int trt_create(const trt_options* opts, trt_ctx** out);
@@ -107,6 +110,12 @@ int trt_scene_update(trt_scene* scene, uint32_t which, uint64_t offset, const vo
 /* Copies bytes [offset, offset + bytes) of one of the scene's buffers (numbered as for trt_scene_update) to host
  * memory: what a deformation wrote, for checks. */
 int trt_scene_read(trt_scene* scene, uint32_t which, uint64_t offset, void* dst, uint64_t bytes);
+
+/* The denoiser fallback on the scene's last accum (renderer/src/denoise.rs `denoise`, what main.rs:548-557 runs
+ * when OIDN is absent): the Frame of each Pixel (gpu.rs:4219-4232), demodulated by the albedo, `iterations` a-trous
+ * passes (4 in the reference) guided by albedo, normal and the 3 x 3-filtered variance, modulated again. Writes
+ * w * h RGB floats to rgb_host; ms (may be NULL): the device time of the filter. */
+int trt_denoise_atrous(trt_scene* scene, uint32_t iterations, float* rgb_host, float* ms);
 
 /* ---- Scenes that move: the per-frame deformation, on the device ----
  * The reference poses skinned meshes with two shaders (renderer/shaders/skin.wgsl, leaf_gather.wgsl), refits their

@@ -31,7 +31,7 @@ class Stats(C.Structure):
 def build(force: bool = False) -> Path:
     """Builds liboracle.so with make (g++)."""
     if force or not LIB_PATH.exists() or any(
-            p.stat().st_mtime > LIB_PATH.stat().st_mtime for p in (HERE / "oracle.cpp", HERE / "deform.cpp", HERE / "oracle.h")):
+            p.stat().st_mtime > LIB_PATH.stat().st_mtime for p in (HERE / "oracle.cpp", HERE / "deform.cpp", HERE / "denoise.cpp", HERE / "oracle.h")):
         subprocess.run(["make", "-s", "-C", str(HERE), "-B" if force else "liboracle.so"], check=True)
     return LIB_PATH
 
@@ -62,6 +62,7 @@ def lib():
         L.orc_skin.argtypes = [P(C.c_uint32), C.c_uint32, P(C.c_float), P(C.c_float), P(C.c_float)]
         L.orc_leaf_gather.argtypes = [P(C.c_uint32), C.c_uint32, P(C.c_float), P(C.c_uint32), C.c_uint32, P(C.c_float)]
         L.orc_refit.argtypes = [P(C.c_uint32), C.c_uint32, P(C.c_float), P(C.c_uint32), C.c_uint32, P(C.c_uint32)]
+        L.orc_denoise.argtypes = [P(C.c_float), C.c_uint32, C.c_uint32, C.c_uint32, P(C.c_float)]
         _lib = L
     return _lib
 
@@ -161,3 +162,11 @@ def deform(jobs, corners, palette, vertices, leaves, nodes, words, w_indices: in
     L.orc_leaf_gather(_p(j, C.c_uint32), len(j), _p(v, C.c_float), _p(w, C.c_uint32), w_indices, _p(lv, C.c_float))
     L.orc_refit(_p(j, C.c_uint32), len(j), _p(v, C.c_float), _p(w, C.c_uint32), w_indices, _p(nd, C.c_uint32))
     return v, lv, nd
+
+
+def denoise(accum, width: int, height: int, iterations: int = 4) -> np.ndarray:
+    """denoise.rs over the Frame of the accum: (height, width, 3) float32."""
+    a = np.ascontiguousarray(accum, np.float32).reshape(-1, 20)
+    out = np.zeros((height, width, 3), np.float32)
+    lib().orc_denoise(_p(a, C.c_float), width, height, iterations, _p(out, C.c_float))
+    return out

@@ -70,6 +70,9 @@ int orc_leaf_gather(const uint32_t* jobs, uint32_t n_jobs, const float* vertices
 /* units.rs:251-275 refit of each job's tree from the vertices, in place: */
 int orc_refit(const uint32_t* jobs, uint32_t n_jobs, const float* vertices, const uint32_t* words, uint32_t w_indices,
               uint32_t* nodes);
+/* The denoiser fallback (denoise.cpp): denoise.rs over the Frame of w * h Pixel records (20 floats each), `iterations`
+ * a-trous passes; w * h RGB floats out. */
+int orc_denoise(const float* accum, uint32_t w, uint32_t h, uint32_t iterations, float* rgb);
 /* sample.wgsl rng4 for a pixel seed, an index and a dimension id (tests pin the sampler with it). */
 void orc_rng4(uint32_t pixel_seed, uint32_t index, uint32_t dim, float out[4]);
 /* The Sobol direction numbers (3 dimensions x 32, bit-reversed) the sampler's tables hold. */

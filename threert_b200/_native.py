@@ -22,6 +22,7 @@ TRT_RENDER_WIDE = 4
 TRT_RENDER_SORT_RAYS = 8
 TRT_RENDER_UNSORTED_HITS = 16
 TRT_RENDER_SORT_SHADOWS = 32
+TRT_RENDER_DEPTH = 64
 
 ERRORS = {1: "TRT_EINVAL", 2: "TRT_ECUDA", 3: "TRT_EGUARD"}
 
@@ -169,6 +170,7 @@ SIGNATURES = [
     ("trt_scene_free", None, [C.c_void_p]),
     ("trt_scene_update", C.c_int, [C.c_void_p, u32, u64, C.c_void_p, u64]),
     ("trt_scene_read", C.c_int, [C.c_void_p, u32, u64, C.c_void_p, u64]),
+    ("trt_denoise_atrous", C.c_int, [C.c_void_p, u32, P(f32), P(f32)]),
     ("trt_deform_setup", C.c_int, [C.c_void_p, P(DeformDesc)]),
     ("trt_deform", C.c_int, [C.c_void_p, P(u32), P(f32), u32, u32, P(DeformStats)]),
     ("trt_render", C.c_int, [C.c_void_p, P(u32), u32, u32, u32, P(f32), P(Stats)]),

@@ -24,6 +24,7 @@
 
 #include "deform.h"
 #include "shade.cuh"
+#include "denoise.cuh"
 #include "threert_cuda.h"
 #include "wide_bvh.cuh"
 
@@ -137,6 +138,7 @@ struct Job {
     float4* accum;
     uint32_t slot_first, n_idx, K, first_sample;
     uint32_t idx_first;  // the earlier jobs' n_idx summed: its pixels' place in a pass over every job's pixels
+    uint32_t depth;      // 1: accumulate the first hit's distance into the Pixel's fourth vec4 (TRT_RENDER_DEPTH)
 };
 // What a wave of a server step holds, in device memory ahead of its job table, so that the step's launches (and a
 // graph captured from them) do not change from step to step.
@@ -334,7 +336,7 @@ __global__ void __launch_bounds__(128, 4) k_shade(const Job* __restrict__ jobs, 
             Surface s = surface(S, X, o, d, hit);
             if (depth == 0u) {
                 V3 albedo = s.card ? s.emissive / fmaxf(fmaxf(s.emissive.x, fmaxf(s.emissive.y, s.emissive.z)), 1e-6f) : s.base;
-                B.alb[p] = f4(albedo, 0.0f);
+                B.alb[p] = f4(albedo, hit.t);  // (w: the first hit's distance, for TRT_RENDER_DEPTH)
                 B.nrm[p] = f4(s.n, 0.0f);
             }
             if (any_gt0(s.emissive) && (s.front || !s.card)) {
@@ -645,9 +647,12 @@ __device__ __forceinline__ void accumulate_one(const Job& J, const PathBufs& B, 
     if (idx >= n_idx || !slot_pixel(idx, w, h, gx, gy)) return;
     uint32_t pix = gy * w + gx;
     float4 c = accum[pix * 5], a = accum[pix * 5 + 1], nn = accum[pix * 5 + 2];
+    float dsum = 0.0f;
     for (uint32_t k = 0; k < K; ++k) {
         uint32_t p = J.slot_first + k * n_idx + idx;
-        V3 r = xyz(B.rad[p]), al = xyz(B.alb[p]), nm = xyz(B.nrm[p]);
+        float4 al4 = B.alb[p];
+        V3 r = xyz(B.rad[p]), al = xyz(al4), nm = xyz(B.nrm[p]);
+        dsum += al4.w;
         c.x += r.x; c.y += r.y; c.z += r.z; c.w += 1.0f;
         float lum = luminance(r);
         a.x += al.x; a.y += al.y; a.z += al.z; a.w += lum;
@@ -656,6 +661,7 @@ __device__ __forceinline__ void accumulate_one(const Job& J, const PathBufs& B, 
     accum[pix * 5] = c;
     accum[pix * 5 + 1] = a;
     accum[pix * 5 + 2] = nn;
+    if (J.depth) accum[pix * 5 + 3].x += dsum;  // the sum of first-hit distances (0 where the camera ray escaped)
 }
 __global__ void k_accumulate(const Job* __restrict__ jobs, PathBufs B) {
     accumulate_one(jobs[blockIdx.y], B, blockIdx.x * blockDim.x + threadIdx.x);
@@ -769,6 +775,10 @@ struct trt_scene {
     float4* accum = nullptr;
     uint32_t accum_w = 0, accum_h = 0;
     Wave wave;  // the render's wave state
+    void* dn = nullptr;  // the denoiser's buffers, for dn_w x dn_h pixels
+    uint32_t dn_w = 0, dn_h = 0;
+    DenoiseBufs D{};
+    float* dn_rgb = nullptr;
     unsigned long long* totals = nullptr;
     int profiling = 0;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_extend, ev_shadow, ev_shade, ev_sort, ev_free;
@@ -964,7 +974,7 @@ int render_waves(trt_scene* s, const Params& P, uint32_t first_sample, uint32_t 
         uint32_t k = std::min(K, spp - s0);
         TRT_CUDA(c, cudaMemcpyAsync(s->wave.Q.cnt, host_cnt.data(), host_cnt.size() * 4, cudaMemcpyHostToDevice, st));
         uint32_t n = n_idx * k;
-        Job job{P, wk, s->accum, 0u, n_idx, k, first_sample + s0};
+        Job job{P, wk, s->accum, 0u, n_idx, k, first_sample + s0, 0u, (flags & TRT_RENDER_DEPTH) ? 1u : 0u};
         k_put_job<<<1, 128, 0, st>>>(job, s->wave.jobs, 0u);
         k_raygen<<<(n + blk - 1) / blk, blk, 0, st>>>(s->wave.jobs, 1u, s->wave.B, s->wave.Q, n, nullptr);
         s->launches += 2;
@@ -1186,6 +1196,7 @@ void trt_scene_free(trt_scene* s) {
     if (s->env) cudaFree(s->env);
     if (s->accum) cudaFree(s->accum);
     if (s->wave.work) cudaFree(s->wave.work);
+    if (s->dn) cudaFree(s->dn);
     if (s->totals) cudaFree(s->totals);
     deform_free(s->deform);
     s->wide.release();
@@ -1206,6 +1217,48 @@ int trt_scene_update(trt_scene* s, uint32_t which, uint64_t offset, const void* 
         s->wide.invalidate();  // rebuilt from the edited buffers at the next render
     }
     if (which == 2 && s->deform) s->deform_stale = true;
+    return TRT_OK;
+}
+
+int trt_denoise_atrous(trt_scene* s, uint32_t iterations, float* rgb_host, float* ms) {
+    if (!s || !rgb_host || iterations > 16) return TRT_EINVAL;
+    trt_ctx* c = s->ctx;
+    if (!s->accum) return fail(c, TRT_EINVAL, "trt_denoise_atrous: nothing rendered yet");
+    cudaSetDevice(c->device);
+    cudaStream_t st = c->stream;
+    uint32_t w = s->accum_w, h = s->accum_h, n = w * h;
+    if (!s->dn || s->dn_w != w || s->dn_h != h) {
+        if (s->dn) cudaFree(s->dn);
+        s->dn = nullptr;
+        uint64_t need = 0;
+        auto add = [&](uint64_t b) { uint64_t at = need; need += (b + 255) / 256 * 256; return at; };
+        uint64_t o_c0 = add(16ull * n), o_c1 = add(16ull * n), o_v0 = add(4ull * n), o_v1 = add(4ull * n),
+                 o_vf = add(4ull * n), o_a = add(16ull * n), o_n = add(16ull * n), o_rgb = add(12ull * n);
+        (void)o_rgb;
+        TRT_CUDA(c, cudaMalloc(&s->dn, need));
+        char* b = (char*)s->dn;
+        s->D = DenoiseBufs{{(float4*)(b + o_c0), (float4*)(b + o_c1)}, {(float*)(b + o_v0), (float*)(b + o_v1)},
+                           (float*)(b + o_vf), (float4*)(b + o_a), (float4*)(b + o_n)};
+        s->dn_rgb = (float*)(b + o_rgb);
+        s->dn_w = w;
+        s->dn_h = h;
+    }
+    const int blk = 256;
+    uint32_t grid = (n + blk - 1) / blk;
+    if (ms) TRT_CUDA(c, cudaEventRecord(c->t0, st));
+    k_dn_prep<<<grid, blk, 0, st>>>(s->accum, n, s->D);
+    uint32_t src = 0;
+    for (uint32_t it = 0; it < iterations; ++it) {
+        k_dn_var3<<<grid, blk, 0, st>>>(s->D.var[src], s->D.var_f, w, h);
+        k_dn_atrous<<<grid, blk, 0, st>>>(s->D, src, w, h, 1 << it);
+        src ^= 1u;
+    }
+    k_dn_remod<<<grid, blk, 0, st>>>(s->D, src, n, s->dn_rgb);
+    if (ms) TRT_CUDA(c, cudaEventRecord(c->t1, st));
+    TRT_CUDA(c, cudaGetLastError());
+    TRT_CUDA(c, cudaMemcpyAsync(rgb_host, s->dn_rgb, 12ull * n, cudaMemcpyDeviceToHost, st));
+    TRT_CUDA(c, cudaStreamSynchronize(st));
+    if (ms) cudaEventElapsedTime(ms, c->t0, c->t1);
     return TRT_OK;
 }
 

@@ -87,6 +87,7 @@ class Scene:
             raise ValueError("render_raw: `out` must be a C-contiguous (w*h, 20) float32 array")
         acc = (out if out is not None else np.empty((w * h, N.PIXEL_FLOATS), np.float32)) if read else None
         st = N.Stats() if stats else None
+        self.last_size = (w, h)
         rc = L.trt_render(self.handle, p.ctypes.data_as(C.POINTER(C.c_uint32)), first_sample, spp, flags,
                           acc.ctypes.data_as(C.POINTER(C.c_float)) if read else None, C.byref(st) if stats else None)
         self.gpu._check(rc, "trt_render")
@@ -130,6 +131,15 @@ class Scene:
                                 pal.ctypes.data_as(C.POINTER(C.c_float)), len(pal), 0, C.byref(st) if stats else None)
         self.gpu._check(rc, "trt_deform")
         return {f[0]: getattr(st, f[0]) for f in N.DeformStats._fields_} if stats else None
+
+    def denoise_atrous(self, iterations: int = 4) -> tuple[np.ndarray, float]:
+        """The fallback denoiser (denoise.rs) on the last render's accum: (h, w, 3) RGB and its device ms."""
+        w, h = self.last_size
+        out = np.empty((h, w, 3), np.float32)
+        ms = C.c_float()
+        self.gpu._check(N.lib().trt_denoise_atrous(self.handle, iterations, out.ctypes.data_as(C.POINTER(C.c_float)),
+                                                   C.byref(ms)), "trt_denoise_atrous")
+        return out, ms.value
 
     def totals(self) -> dict:
         t = N.Totals()
