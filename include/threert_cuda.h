@@ -117,6 +117,32 @@ int trt_scene_read(trt_scene* scene, uint32_t which, uint64_t offset, void* dst,
  * w * h RGB floats to rgb_host; ms (may be NULL): the device time of the filter. */
 int trt_denoise_atrous(trt_scene* scene, uint32_t iterations, float* rgb_host, float* ms);
 
+/* ---- The learned denoiser (no counterpart in the reference, whose learned denoiser is the external OIDN library,
+ * renderer/src/denoise.rs:80-103): a 4-level U-Net (32 / 64 / 96 / 128 channels, 3 x 3 convolutions, 2 x 2 average
+ * pooling, nearest upsampling, skip concatenations) on bf16 tensor cores with f32 accumulation; its training (forward,
+ * backward, Adam) runs on the device too. Input a pixel: log1p(radiance * s), albedo, normal, log1p(depth * sd) (10
+ * floats; s = 1 / the image's mean luminance, sd = 1 / its mean first-hit distance); output: log1p(radiance * s). */
+typedef struct trt_unet trt_unet;
+/* A network for batches of up to max_batch images of up to max_h x max_w (multiples of 8) on `device`. */
+int trt_unet_create(int device, uint32_t max_batch, uint32_t max_h, uint32_t max_w, trt_unet** out);
+void trt_unet_destroy(trt_unet* net);
+const char* trt_unet_last_error(const trt_unet* net);
+/* Parameters (f32) in the network's layout: per layer, weights [9][cin padded to 32][cout padded to 64] then the bias
+ * (cout padded to 64); the layers in order e0a e0b e1a e1b e2a e2b e3a e3b d2a d2b d1a d1b d0a d0b out. Setting them
+ * resets the optimiser. */
+uint64_t trt_unet_param_count(void);
+int trt_unet_set_params(trt_unet* net, const float* params);
+int trt_unet_get_params(trt_unet* net, float* params);
+/* features: b * h * w * 10 floats (NHWC); pred: b * h * w * 3. ms (may be NULL): device time of the network. */
+int trt_unet_forward(trt_unet* net, const float* features, uint32_t b, uint32_t h, uint32_t w, float* pred, float* ms);
+/* One step of training on (features, targets = log1p(reference radiance * s)): the L1 loss's gradient by the
+ * backward pass, then (update != 0) an Adam step at rate lr. loss, grads (param_count floats), ms: may be NULL. */
+int trt_unet_train_step(trt_unet* net, const float* features, const float* targets, uint32_t b, uint32_t h, uint32_t w,
+                        float lr, int update, float* loss, float* grads, float* ms);
+/* Denoises a rendered accum in device memory (w * h Pixel records with TRT_RENDER_DEPTH's depth; trt_accum_device_ptr)
+ * into w * h RGB floats: features, network and output transform all on the device. */
+int trt_unet_denoise_accum(trt_unet* net, const void* accum_device, uint32_t w, uint32_t h, float* rgb_host, float* ms);
+
 /* ---- Scenes that move: the per-frame deformation, on the device ----
  * The reference poses skinned meshes with two shaders (renderer/shaders/skin.wgsl, leaf_gather.wgsl), refits their
  * mesh trees on the CPU (units.rs:251-275 refit, live/edits.rs:2395-2450) and builds the top tree on the CPU

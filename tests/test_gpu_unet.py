@@ -1,0 +1,94 @@
+"""The learned denoiser's network on the device against its CPU oracle (oracle/unet_ref.py, itself pinned by finite
+differences): outputs and every layer's gradients within bf16's rounding; training fits a batch; inference on a
+scene's accum on the device equals the host-side feature path."""
+import numpy as np
+import pytest
+
+from oracle import unet_ref as R
+from threert_b200 import prep, unet
+from threert_b200 import _native as N
+
+from util import small_city
+
+pytestmark = pytest.mark.gpu
+
+
+def bf16(a):
+    """Round to bfloat16 (nearest even), as the device stores weights and inputs."""
+    u = np.asarray(a, np.float32).view(np.uint32).astype(np.uint64)
+    u = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return u.astype(np.uint32).view(np.float32)
+
+
+def case(seed=3, b=2, h=16, w=16):
+    rng = np.random.default_rng(seed)
+    p = unet.init_params(seed)
+    o = 0
+    for cin, cout in unet.LAYERS:
+        o += 9 * cin * unet.r64(cout)
+        p[o:o + cout] = rng.normal(0, 0.05, cout)
+        o += unet.r64(cout)
+    feats = rng.normal(0, 1, (b, h, w, 10)).astype(np.float32)
+    tgt = rng.normal(0, 1, (b, h, w, 3)).astype(np.float32)
+    return p, feats, tgt
+
+
+@pytest.fixture(scope="module")
+def net():
+    n = unet.UNet(0, max_batch=4, max_h=64, max_w=64)
+    yield n
+    n.close()
+
+
+def test_forward_matches_the_oracle(net):
+    p, feats, _ = case()
+    net.set_params(p)
+    got, ms = net.forward(feats)
+    want, _ = R.forward(R.unpack(bf16(p).astype(np.float64)), bf16(feats).astype(np.float64))
+    err = np.linalg.norm(got - want) / np.linalg.norm(want)
+    assert err < 0.03, err
+    assert ms > 0
+
+
+def test_every_layers_gradient_matches_the_oracle(net):
+    p, feats, tgt = case(seed=5)
+    net.set_params(p)
+    loss, g, _ = net.step(feats, tgt, update=False, grads=True)
+    ref_loss, G, _ = R.loss_and_grads(R.unpack(bf16(p).astype(np.float64)), bf16(feats).astype(np.float64), tgt)
+    assert abs(loss / ref_loss - 1) < 0.02
+    gp = R.unpack(g.astype(np.float64))
+    for name in R.NAMES:
+        for k in range(2):  # weights, bias
+            a, b = gp[name][k].ravel(), G[name][k].ravel()
+            cos = a @ b / (np.linalg.norm(a) * np.linalg.norm(b) + 1e-30)
+            ratio = np.linalg.norm(a) / (np.linalg.norm(b) + 1e-30)
+            assert cos > 0.98 and abs(ratio - 1) < 0.1, (name, k, cos, ratio)
+    # the padding's gradients are zero
+    flat = R.pack(gp, g)
+    assert np.allclose(g[flat == 0], 0.0)
+
+
+def test_training_fits_a_batch(net):
+    p, feats, _ = case(seed=7, b=4, h=32, w=32)
+    rng = np.random.default_rng(8)
+    tgt = (0.5 * feats[..., 0:3] + 0.3 * rng.normal(0, 1, feats[..., 0:3].shape)).astype(np.float32)
+    net.set_params(p)
+    first, _, _ = net.step(feats, tgt, lr=1e-3)
+    for _ in range(150):
+        last, _, _ = net.step(feats, tgt, lr=1e-3)
+    assert last < 0.6 * first, (first, last)
+
+
+def test_inference_on_the_device_is_the_host_path(gpu, net):
+    P = prep.prepare(small_city(width=64, height=32))
+    S = gpu.upload(P)
+    acc, _ = S.render_raw(P.params, 2, flags=N.TRT_RENDER_DEPTH)
+    p, _, _ = case(seed=9)
+    net.set_params(p)
+    got, ms = net.denoise(S)
+    f, s = unet.features(acc, 64, 32)
+    pred, _ = net.forward(f[None])
+    want = unet.radiance(pred[0], s)
+    assert ms > 0
+    assert np.linalg.norm(got - want) / np.linalg.norm(want) < 0.02
+    S.close()

@@ -184,6 +184,15 @@ SIGNATURES = [
     ("trt_server_submit", C.c_int, [C.c_void_p, C.c_void_p, P(u32), u32, P(f32), P(u64)]),
     ("trt_server_poll", C.c_int, [C.c_void_p, P(RequestDone), u32, P(u32), u32]),
     ("trt_server_stats_get", C.c_int, [C.c_void_p, P(ServerStats)]),
+    ("trt_unet_create", C.c_int, [C.c_int, u32, u32, u32, P(C.c_void_p)]),
+    ("trt_unet_destroy", None, [C.c_void_p]),
+    ("trt_unet_last_error", C.c_char_p, [C.c_void_p]),
+    ("trt_unet_param_count", u64, []),
+    ("trt_unet_set_params", C.c_int, [C.c_void_p, P(f32)]),
+    ("trt_unet_get_params", C.c_int, [C.c_void_p, P(f32)]),
+    ("trt_unet_forward", C.c_int, [C.c_void_p, P(f32), u32, u32, u32, P(f32), P(f32)]),
+    ("trt_unet_train_step", C.c_int, [C.c_void_p, P(f32), P(f32), u32, u32, u32, f32, C.c_int, P(f32), P(f32), P(f32)]),
+    ("trt_unet_denoise_accum", C.c_int, [C.c_void_p, C.c_void_p, u32, u32, P(f32), P(f32)]),
     ("trt_scene_totals", C.c_int, [C.c_void_p, P(Totals)]),
     ("trt_scene_reset_totals", None, [C.c_void_p]),
     ("trt_scene_set_profiling", None, [C.c_void_p, C.c_int]),

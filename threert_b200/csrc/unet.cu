@@ -1,0 +1,766 @@
+// The learned denoiser's kernels: a 4-level U-Net (32 / 64 / 96 / 128 channels, 3 x 3 convolutions) over the pass's
+// radiance, albedo, normal and depth, its forward pass, its backward pass and its optimiser, all hand-written. It has
+// no counterpart in the reference (whose learned denoiser is the external OIDN library, renderer/src/denoise.rs:80-103).
+//
+// Tensors are NHWC bf16 with channel counts padded to multiples of 32; a convolution is an implicit GEMM (M = pixels,
+// N = output channels, K = 9 taps x input channels) on bf16 tensor-core MMAs with f32 accumulation. The input gradient
+// is the same kernel run on the output gradient with the weights flipped and transposed; the weight gradient is a GEMM
+// over pixels (split across CTAs, summed with f32 atomics). Master weights, gradients and Adam's moments are f32.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "threert_cuda.h"
+
+namespace unet {
+
+typedef __nv_bfloat16 bf16;
+
+// ---- tensor-core fragments (mma.sync m16n8k16, bf16 in, f32 accumulate) ---------------------------------------------
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void ldsm_x4(uint32_t& r0, uint32_t& r1, uint32_t& r2, uint32_t& r3, const void* p) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];\n"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3) : "r"(smem_addr(p)));
+}
+__device__ __forceinline__ void ldsm_x4_t(uint32_t& r0, uint32_t& r1, uint32_t& r2, uint32_t& r3, const void* p) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0, %1, %2, %3}, [%4];\n"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3) : "r"(smem_addr(p)));
+}
+__device__ __forceinline__ void mma16816(float* c, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
+                                         uint32_t b1) {
+    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+                 "{%0, %1, %2, %3};\n"
+                 : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+                 : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// ---- convolution (forward; and the input gradient with flipped, transposed weights) -------------------------------
+
+struct Conv {
+    const bf16* x;            // input, NHWC
+    uint32_t x_stride, x_off; // channel stride and first channel read
+    uint32_t cin;             // channels read (a multiple of 32)
+    const bf16* w;            // [9][cin][co_pad]: tap-major rows of output channels
+    uint32_t co_pad;          // a multiple of 64
+    const float* bias;        // co_pad, or null
+    bf16* y;                  // output, NHWC
+    uint32_t y_stride, y_off, cout;
+    float* yf;                // or f32 output (stride cout), for the last layer
+    uint32_t B, H, W;
+    int relu;
+};
+
+constexpr int CM = 128, CN = 64, CK = 32, APAD = 8, BPAD = 8;
+
+// y[p][n] = bias[n] + sum over taps t and channels c of x[p + off(t)][c] * w[t][c][n], zero outside the image.
+// A CTA: 128 pixels x 64 output channels; 8 warps of 32 x 32.
+__global__ void __launch_bounds__(256) k_conv(Conv a) {
+    __shared__ __align__(16) bf16 As[CM][CK + APAD];
+    __shared__ __align__(16) bf16 Bs[CK][CN + BPAD];
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    const uint32_t wm = warp & 3u, wn = warp >> 2;
+    const uint32_t M = a.B * a.H * a.W, m0 = blockIdx.x * CM, n0 = blockIdx.y * CN;
+    float acc[2][4][4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) acc[i][j][k] = 0.0f;
+    // this thread's two A rows (pixels) and their coordinates
+    uint32_t apx[2], apart[2];
+    int ab[2], ay[2], ax[2];
+    bool aval[2];
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        uint32_t idx = tid + r * 256u;
+        apx[r] = idx >> 2;
+        apart[r] = idx & 3u;
+        uint32_t m = m0 + apx[r];
+        aval[r] = m < M;
+        uint32_t hw = a.H * a.W, mm = aval[r] ? m : 0u;
+        ab[r] = (int)(mm / hw);
+        ay[r] = (int)((mm % hw) / a.W);
+        ax[r] = (int)(mm % a.W);
+    }
+    const uint32_t bk = tid >> 3, bpart = tid & 7u;
+    for (int tap = 0; tap < 9; ++tap) {
+        const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+        for (uint32_t c0 = 0; c0 < a.cin; c0 += CK) {
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                int sy = ay[r] + dy, sx = ax[r] + dx;
+                uint4 v = make_uint4(0u, 0u, 0u, 0u);
+                if (aval[r] && sy >= 0 && sx >= 0 && sy < (int)a.H && sx < (int)a.W) {
+                    uint64_t pix = ((uint64_t)ab[r] * a.H + (uint32_t)sy) * a.W + (uint32_t)sx;
+                    v = *reinterpret_cast<const uint4*>(a.x + pix * a.x_stride + a.x_off + c0 + apart[r] * 8u);
+                }
+                *reinterpret_cast<uint4*>(&As[apx[r]][apart[r] * 8u]) = v;
+            }
+            *reinterpret_cast<uint4*>(&Bs[bk][bpart * 8u]) =
+                *reinterpret_cast<const uint4*>(a.w + ((uint64_t)tap * a.cin + c0 + bk) * a.co_pad + n0 + bpart * 8u);
+            __syncthreads();
+#pragma unroll
+            for (uint32_t kk = 0; kk < CK; kk += 16) {
+                uint32_t af[2][4], bfr[4][2];
+#pragma unroll
+                for (int mt = 0; mt < 2; ++mt)
+                    ldsm_x4(af[mt][0], af[mt][1], af[mt][2], af[mt][3],
+                            &As[wm * 32u + mt * 16u + (lane & 15u)][kk + (lane >> 4) * 8u]);
+#pragma unroll
+                for (int np = 0; np < 2; ++np)
+                    ldsm_x4_t(bfr[np * 2][0], bfr[np * 2][1], bfr[np * 2 + 1][0], bfr[np * 2 + 1][1],
+                              &Bs[kk + (lane & 7u) + ((lane >> 3) & 1u) * 8u][wn * 32u + np * 16u + (lane >> 4) * 8u]);
+#pragma unroll
+                for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+                    for (int nt = 0; nt < 4; ++nt)
+                        mma16816(acc[mt][nt], af[mt][0], af[mt][1], af[mt][2], af[mt][3], bfr[nt][0], bfr[nt][1]);
+            }
+            __syncthreads();
+        }
+    }
+    const uint32_t g = lane >> 2, t4 = lane & 3u;
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            uint32_t m = m0 + wm * 32u + mt * 16u + g + h * 8u;
+            if (m >= M) continue;
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt) {
+                uint32_t n = n0 + wn * 32u + nt * 8u + t4 * 2u;
+                float v0 = acc[mt][nt][h * 2], v1 = acc[mt][nt][h * 2 + 1];
+                if (a.bias) { v0 += a.bias[n]; v1 += a.bias[n + 1]; }
+                if (a.relu) { v0 = fmaxf(v0, 0.0f); v1 = fmaxf(v1, 0.0f); }
+                if (a.yf) {
+                    if (n < a.cout) a.yf[(uint64_t)m * a.cout + n] = v0;
+                    if (n + 1 < a.cout) a.yf[(uint64_t)m * a.cout + n + 1] = v1;
+                } else if (n < a.cout) {
+                    bf16* dst = a.y + (uint64_t)m * a.y_stride + a.y_off + n;
+                    if (n + 1 < a.cout) *reinterpret_cast<__nv_bfloat162*>(dst) = __floats2bfloat162_rn(v0, v1);
+                    else *dst = __float2bfloat16_rn(v0);
+                }
+            }
+        }
+}
+
+// ---- weight gradient: dw[t][c][n] += sum over pixels p of x[p + off(t)][c] * dy[p][n] ------------------------------
+
+struct WGrad {
+    const bf16* x; uint32_t x_stride, x_off, cin;
+    const bf16* dy; uint32_t dy_stride, cout;  // cout a multiple of 32
+    float* dw;                                 // [9][cin][co_pad] f32, summed into
+    uint32_t co_pad;
+    uint32_t B, H, W, chunk;                   // pixels a CTA
+};
+
+// A CTA: one tap, 32 input x 32 output channels, `chunk` pixels; 4 warps of 16 x 16.
+__global__ void __launch_bounds__(128) k_wgrad(WGrad a) {
+    __shared__ __align__(16) bf16 Xs[32][32 + 8];
+    __shared__ __align__(16) bf16 Ys[32][32 + 8];
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    const uint32_t wm = warp & 1u, wn = warp >> 1;
+    const int tap = (int)blockIdx.y, dy = tap / 3 - 1, dx = tap % 3 - 1;
+    const uint32_t ct = a.cout / 32u, c0 = (blockIdx.z / ct) * 32u, n0 = (blockIdx.z % ct) * 32u;
+    const uint32_t M = a.B * a.H * a.W, hw = a.H * a.W;
+    const uint32_t p_begin = blockIdx.x * a.chunk, p_end = min(M, p_begin + a.chunk);
+    float acc[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+    const uint32_t lrow = tid >> 2, lpart = tid & 3u;  // 32 rows x 4 parts of 16 bytes
+    for (uint32_t p0 = p_begin; p0 < p_end; p0 += 32) {
+        uint32_t p = p0 + lrow;
+        uint4 xv = make_uint4(0u, 0u, 0u, 0u), yv = make_uint4(0u, 0u, 0u, 0u);
+        if (p < p_end) {
+            uint32_t b = p / hw, y = (p % hw) / a.W, x = p % a.W;
+            int sy = (int)y + dy, sx = (int)x + dx;
+            if (sy >= 0 && sx >= 0 && sy < (int)a.H && sx < (int)a.W) {
+                uint64_t pix = ((uint64_t)b * a.H + (uint32_t)sy) * a.W + (uint32_t)sx;
+                xv = *reinterpret_cast<const uint4*>(a.x + pix * a.x_stride + a.x_off + c0 + lpart * 8u);
+            }
+            yv = *reinterpret_cast<const uint4*>(a.dy + (uint64_t)p * a.dy_stride + n0 + lpart * 8u);
+        }
+        *reinterpret_cast<uint4*>(&Xs[lrow][lpart * 8u]) = xv;
+        *reinterpret_cast<uint4*>(&Ys[lrow][lpart * 8u]) = yv;
+        __syncthreads();
+#pragma unroll
+        for (uint32_t kk = 0; kk < 32; kk += 16) {
+            // A[m = c][k = p] = Xs[p][c]: transposed 8 x 8 blocks
+            uint32_t a0, a1, a2, a3, b0, b1, b2, b3;
+            ldsm_x4_t(a0, a1, a2, a3,
+                      &Xs[kk + (lane & 7u) + (lane >> 4) * 8u][wm * 16u + ((lane >> 3) & 1u) * 8u]);
+            ldsm_x4_t(b0, b1, b2, b3, &Ys[kk + (lane & 7u) + ((lane >> 3) & 1u) * 8u][wn * 16u + (lane >> 4) * 8u]);
+            mma16816(acc[0], a0, a1, a2, a3, b0, b1);
+            mma16816(acc[1], a0, a1, a2, a3, b2, b3);
+        }
+        __syncthreads();
+    }
+    const uint32_t g = lane >> 2, t4 = lane & 3u;
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            uint32_t c = c0 + wm * 16u + g + h * 8u, n = n0 + wn * 16u + nt * 8u + t4 * 2u;
+            float* dst = a.dw + ((uint64_t)tap * a.cin + c) * a.co_pad + n;
+            atomicAdd(dst, acc[nt][h * 2]);
+            atomicAdd(dst + 1, acc[nt][h * 2 + 1]);
+        }
+}
+
+// ---- the other layers ----------------------------------------------------------------------------------------------
+
+// 2 x 2 average pooling: y[b][y][x][c] = mean of x over the 2 x 2 block (H, W even).
+__global__ void k_pool(const bf16* x, uint32_t xs, uint32_t xo, bf16* y, uint32_t ys, uint32_t C, uint32_t B,
+                       uint32_t H, uint32_t W) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t h2 = H / 2, w2 = W / 2;
+    uint64_t n = (uint64_t)B * h2 * w2 * C;
+    if (i >= n) return;
+    uint32_t c = (uint32_t)(i % C);
+    uint64_t q = i / C;
+    uint32_t xx = (uint32_t)(q % w2), yy = (uint32_t)((q / w2) % h2), b = (uint32_t)(q / ((uint64_t)w2 * h2));
+    float s = 0.0f;
+    for (int j = 0; j < 2; ++j)
+        for (int k = 0; k < 2; ++k)
+            s += __bfloat162float(x[(((uint64_t)b * H + 2 * yy + j) * W + 2 * xx + k) * xs + xo + c]);
+    y[q * ys + c] = __float2bfloat16_rn(0.25f * s);
+}
+// ... its gradient, added: dx[2y + j][2x + k] += dy[y][x] / 4.
+__global__ void k_pool_back(const bf16* dy, uint32_t dys, bf16* dx, uint32_t dxs, uint32_t dxo, uint32_t C, uint32_t B,
+                            uint32_t H, uint32_t W) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t n = (uint64_t)B * H * W * C;
+    if (i >= n) return;
+    uint32_t c = (uint32_t)(i % C);
+    uint64_t q = i / C;
+    uint32_t x = (uint32_t)(q % W), y = (uint32_t)((q / W) % H), b = (uint32_t)(q / ((uint64_t)W * H));
+    float g = 0.25f * __bfloat162float(dy[(((uint64_t)b * (H / 2) + y / 2) * (W / 2) + x / 2) * dys + c]);
+    bf16* d = dx + q * dxs + dxo + c;
+    *d = __float2bfloat16_rn(__bfloat162float(*d) + g);
+}
+// Nearest 2x upsampling into channels [0, C) of y: y[2y + j][2x + k] = x[y][x].
+__global__ void k_up(const bf16* x, uint32_t xs, bf16* y, uint32_t ys, uint32_t C, uint32_t B, uint32_t H, uint32_t W) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;  // over the output (H, W: the output's)
+    uint64_t n = (uint64_t)B * H * W * C;
+    if (i >= n) return;
+    uint32_t c = (uint32_t)(i % C);
+    uint64_t q = i / C;
+    uint32_t px = (uint32_t)(q % W), py = (uint32_t)((q / W) % H), b = (uint32_t)(q / ((uint64_t)W * H));
+    y[q * ys + c] = x[(((uint64_t)b * (H / 2) + py / 2) * (W / 2) + px / 2) * xs + c];
+}
+// ... its gradient: dx[y][x] = sum of dy over the 2 x 2 block (channels [0, C) of dy).
+__global__ void k_up_back(const bf16* dy, uint32_t dys, bf16* dx, uint32_t dxs, uint32_t C, uint32_t B, uint32_t H,
+                          uint32_t W) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;  // over dx (H, W: dx's)
+    uint64_t n = (uint64_t)B * H * W * C;
+    if (i >= n) return;
+    uint32_t c = (uint32_t)(i % C);
+    uint64_t q = i / C;
+    uint32_t x = (uint32_t)(q % W), y = (uint32_t)((q / W) % H), b = (uint32_t)(q / ((uint64_t)W * H));
+    float s = 0.0f;
+    for (int j = 0; j < 2; ++j)
+        for (int k = 0; k < 2; ++k)
+            s += __bfloat162float(dy[(((uint64_t)b * 2 * H + 2 * y + j) * 2 * W + 2 * x + k) * dys + c]);
+    dx[q * dxs + c] = __float2bfloat16_rn(s);
+}
+// ReLU's gradient in place: dy = 0 where the layer's output y was 0.
+__global__ void k_relu_back(bf16* dy, uint32_t dys, uint32_t dyo, const bf16* y, uint32_t ys, uint32_t yo, uint32_t C,
+                            uint64_t P) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P * C) return;
+    uint64_t p = i / C;
+    uint32_t c = (uint32_t)(i % C);
+    if (!(__bfloat162float(y[p * ys + yo + c]) > 0.0f)) dy[p * dys + dyo + c] = __float2bfloat16_rn(0.0f);
+}
+// Copies channels [so, so + C) of a to channels [0, C) of b (the skip part of a concatenation's gradient).
+__global__ void k_copy_ch(const bf16* a, uint32_t as, uint32_t so, bf16* b, uint32_t bs, uint32_t bo, uint32_t C,
+                          uint64_t P) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P * C) return;
+    uint64_t p = i / C;
+    uint32_t c = (uint32_t)(i % C);
+    b[p * bs + bo + c] = a[p * as + so + c];
+}
+// The L1 loss on log radiance and its gradient (as bf16 into a 32-channel buffer): dpred = sign(pred - t) / count.
+__global__ void k_loss(const float* pred, const float* target, uint64_t P, bf16* dpred, float* loss) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    float l = 0.0f;
+    if (i < P * 3) {
+        float d = pred[i] - target[i];
+        l = fabsf(d);
+        float g = (d > 0.0f ? 1.0f : (d < 0.0f ? -1.0f : 0.0f)) / (float)(P * 3);
+        dpred[(i / 3) * 32 + i % 3] = __float2bfloat16_rn(g);
+    }
+    for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(~0u, l, o);
+    if ((threadIdx.x & 31u) == 0 && l != 0.0f) atomicAdd(loss, l / (float)(P * 3));
+}
+// Bias gradient: db[n] += sum over pixels of dy[p][n].
+__global__ void k_bgrad(const bf16* dy, uint32_t dys, uint32_t C, uint64_t P, float* db) {
+    uint32_t c = threadIdx.x;
+    if (c >= C) return;
+    float s = 0.0f;
+    for (uint64_t p = blockIdx.x; p < P; p += gridDim.x) s += __bfloat162float(dy[p * dys + c]);
+    atomicAdd(&db[c], s);
+}
+// Adam (Kingma & Ba 2015) on the f32 master values, then the bf16 forward copy.
+__global__ void k_adam(float* w, const float* g, float* m, float* v, uint64_t n, float lr, float b1, float b2,
+                       float c1, float c2, float eps) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float gi = g[i];
+    float mi = b1 * m[i] + (1.0f - b1) * gi, vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+// The bf16 weights of a layer from its f32 masters: forward [t][c][n] (c < cin, n < co_pad), and the input
+// gradient's [8 - t][n][c] (n < cout32: the output gradient's channels, c < cin, rows ci_pad64 wide).
+__global__ void k_weights(const float* wf, uint32_t cin, uint32_t co_pad, uint32_t cout32, bf16* wfw, bf16* wbw,
+                          uint32_t ci_pad64) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t n = 9ull * cin * co_pad;
+    if (i >= n) return;
+    uint32_t nn = (uint32_t)(i % co_pad), c = (uint32_t)((i / co_pad) % cin), t = (uint32_t)(i / ((uint64_t)co_pad * cin));
+    bf16 v = __float2bfloat16_rn(wf[i]);
+    wfw[i] = v;
+    if (wbw && nn < cout32) wbw[((uint64_t)(8 - t) * cout32 + nn) * ci_pad64 + c] = v;
+}
+
+// ---- features from a rendered accum (inference on a scene's result) ----------------------------------------------
+
+// The image's mean luminance and mean first-hit distance (over pixels that hit): sums into acc[0..2].
+__global__ void k_feat_sums(const float4* __restrict__ accum, uint64_t n, float* acc) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    float l = 0.0f, d = 0.0f, dn = 0.0f;
+    if (i < n) {
+        float4 c = accum[5 * i], e = accum[5 * i + 3];
+        float cnt = fmaxf(c.w, 1.0f);
+        l = (0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z) / cnt;
+        if (!isfinite(l)) l = 0.0f;
+        float dd = e.x / cnt;
+        if (dd > 0.0f && isfinite(dd)) { d = dd; dn = 1.0f; }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        l += __shfl_xor_sync(~0u, l, o);
+        d += __shfl_xor_sync(~0u, d, o);
+        dn += __shfl_xor_sync(~0u, dn, o);
+    }
+    if ((threadIdx.x & 31u) == 0) {
+        atomicAdd(&acc[0], l);
+        atomicAdd(&acc[1], d);
+        atomicAdd(&acc[2], dn);
+    }
+}
+__device__ __forceinline__ float fin0(float v) { return isfinite(v) ? v : 0.0f; }
+// The network's input from the accum: log1p(radiance * s), albedo, normal, log1p(depth * sd), 32 channels (bf16).
+__global__ void k_feat(const float4* __restrict__ accum, uint64_t n, const float* sums, bf16* x) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float s = 1.0f / fmaxf(sums[0] / (float)n, 1e-6f), sd = 1.0f / fmaxf(sums[1] / fmaxf(sums[2], 1.0f), 1e-6f);
+    float4 c = accum[5 * i], a = accum[5 * i + 1], nn = accum[5 * i + 2], e = accum[5 * i + 3];
+    float cnt = fmaxf(c.w, 1.0f);
+    float f[10] = {log1pf(fmaxf(fin0(c.x / cnt) * s, 0.0f)), log1pf(fmaxf(fin0(c.y / cnt) * s, 0.0f)),
+                   log1pf(fmaxf(fin0(c.z / cnt) * s, 0.0f)), fin0(a.x / cnt), fin0(a.y / cnt), fin0(a.z / cnt),
+                   fin0(nn.x / cnt), fin0(nn.y / cnt), fin0(nn.z / cnt), log1pf(fmaxf(fin0(e.x / cnt) * sd, 0.0f))};
+    bf16* row = x + i * 32;
+    for (int k = 0; k < 32; ++k) row[k] = __float2bfloat16_rn(k < 10 ? f[k] : 0.0f);
+}
+// The prediction back to radiance: expm1(pred) / s.
+__global__ void k_unfeat(const float* pred, uint64_t n, const float* sums, float* rgb) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n * 3) return;
+    float s = 1.0f / fmaxf(sums[0] / (float)n, 1e-6f);
+    rgb[i] = fmaxf(expm1f(pred[i]), 0.0f) / s;
+}
+// Host features (f32, 10 a pixel) to the network's 32-channel bf16 input.
+__global__ void k_feat_host(const float* f, uint64_t n, bf16* x) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n * 32) return;
+    uint64_t p = i / 32;
+    uint32_t c = (uint32_t)(i % 32);
+    x[i] = __float2bfloat16_rn(c < 10 ? f[p * 10 + c] : 0.0f);
+}
+
+// ---- the network ----------------------------------------------------------------------------------------------------
+
+struct Layer { uint32_t cin, cout; int relu; };  // cin: padded to 32 (the input's 10 channels: 32)
+constexpr int N_LAYERS = 15;
+constexpr Layer LAYERS[N_LAYERS] = {
+    {32, 32, 1},  {32, 32, 1},  {32, 64, 1},  {64, 64, 1},  {64, 96, 1},  {96, 96, 1},  {96, 128, 1}, {128, 128, 1},
+    {224, 96, 1}, {96, 96, 1},  {160, 64, 1}, {64, 64, 1},  {96, 32, 1},  {32, 32, 1},  {32, 3, 0}};
+enum { E0A, E0B, E1A, E1B, E2A, E2B, E3A, E3B, D2A, D2B, D1A, D1B, D0A, D0B, OUT };
+
+inline uint32_t r32(uint32_t v) { return (v + 31u) / 32u * 32u; }
+inline uint32_t r64(uint32_t v) { return (v + 63u) / 64u * 64u; }
+inline uint64_t w_count(const Layer& l) { return 9ull * l.cin * r64(l.cout); }
+inline uint64_t layer_params(const Layer& l) { return w_count(l) + r64(l.cout); }
+
+uint64_t param_count() {
+    uint64_t n = 0;
+    for (const Layer& l : LAYERS) n += layer_params(l);
+    return n;
+}
+
+// An activation tensor: pixels x stride channels of bf16.
+struct Act { bf16* p = nullptr; uint32_t stride = 0; };
+
+struct Net {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    uint32_t maxB = 0, maxH = 0, maxW = 0;
+    std::string err;
+    // f32 masters, gradients, Adam moments (one flat array each, layer after layer: weights then bias)
+    float *w = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;
+    uint64_t n_params = 0, off[N_LAYERS] = {};
+    bf16* wf[N_LAYERS] = {};  // forward weights
+    bf16* wb[N_LAYERS] = {};  // input-gradient weights
+    uint64_t t = 0;           // Adam steps
+    // activations and their gradients
+    Act in0, a0, cat0, pool0, a1, cat1, pool1, a2, cat2, pool2, a3, b3, t2, u2, t1, u1, t0, u0;
+    Act dpred, du0, dt0, dcat0, du1, dt1, dcat1, du2, dt2, dcat2, db3, da3, dpool2, de2b, da2, dpool1, de1b, da1,
+        dpool0, de0b, da0;
+    float *pred = nullptr, *target = nullptr, *feat = nullptr, *loss = nullptr, *sums = nullptr, *rgb = nullptr;
+    std::vector<void*> allocs;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+};
+
+}  // namespace unet
+
+struct trt_unet : unet::Net {};
+
+namespace unet {
+namespace {
+
+template <class T>
+cudaError_t alloc(Net* n, T** p, uint64_t count) {
+    cudaError_t e = cudaMalloc((void**)p, sizeof(T) * std::max<uint64_t>(count, 1));
+    if (e == cudaSuccess) {
+        n->allocs.push_back(*p);
+        e = cudaMemset(*p, 0, sizeof(T) * std::max<uint64_t>(count, 1));
+    }
+    return e;
+}
+cudaError_t act(Net* n, Act& a, uint64_t pixels, uint32_t stride) {
+    a.stride = stride;
+    return alloc(n, &a.p, pixels * stride);
+}
+
+uint32_t blocks(uint64_t n, uint32_t b = 256) { return (uint32_t)((n + b - 1) / b); }
+
+void conv(Net* n, int li, const Act& x, uint32_t x_off, const Act& y, uint32_t y_off, uint32_t B, uint32_t H, uint32_t W,
+          float* yf = nullptr) {
+    const Layer& L = LAYERS[li];
+    Conv a{x.p, x.stride, x_off, L.cin, n->wf[li], r64(L.cout), n->w + n->off[li] + w_count(L),
+           y.p, y.stride, y_off, L.cout, yf, B, H, W, L.relu};
+    uint32_t M = B * H * W;
+    k_conv<<<dim3((M + CM - 1) / CM, r64(L.cout) / CN), 256, 0, n->stream>>>(a);
+}
+// The input gradient of layer li: dx (channels [0, cin_logical)) from dy (cout rounded to 32 channels).
+void conv_dx(Net* n, int li, const Act& dy, const Act& dx, uint32_t B, uint32_t H, uint32_t W) {
+    const Layer& L = LAYERS[li];
+    Conv a{dy.p, dy.stride, 0u, r32(L.cout), n->wb[li], r64(L.cin), nullptr, dx.p, dx.stride, 0u, L.cin, nullptr,
+           B, H, W, 0};
+    uint32_t M = B * H * W;
+    k_conv<<<dim3((M + CM - 1) / CM, r64(L.cin) / CN), 256, 0, n->stream>>>(a);
+}
+void wgrad(Net* n, int li, const Act& x, uint32_t x_off, const Act& dy, uint32_t B, uint32_t H, uint32_t W) {
+    const Layer& L = LAYERS[li];
+    uint32_t M = B * H * W, chunk = 2048;
+    WGrad a{x.p, x.stride, x_off, L.cin, dy.p, dy.stride, r32(L.cout), n->g + n->off[li], r64(L.cout), B, H, W, chunk};
+    k_wgrad<<<dim3((M + chunk - 1) / chunk, 9, (L.cin / 32) * (r32(L.cout) / 32)), 128, 0, n->stream>>>(a);
+    k_bgrad<<<std::min<uint32_t>(1024, M), 128, 0, n->stream>>>(dy.p, dy.stride, r32(L.cout), M,
+                                                                 n->g + n->off[li] + w_count(L));
+}
+void relu_back(Net* n, const Act& dy, uint32_t dyo, const Act& y, uint32_t yo, uint32_t C, uint64_t P) {
+    k_relu_back<<<blocks(P * C), 256, 0, n->stream>>>(dy.p, dy.stride, dyo, y.p, y.stride, yo, C, P);
+}
+
+void forward(Net* n, uint32_t B, uint32_t H, uint32_t W) {
+    cudaStream_t s = n->stream;
+    uint32_t H1 = H / 2, W1 = W / 2, H2 = H / 4, W2 = W / 4, H3 = H / 8, W3 = W / 8;
+    uint64_t P0 = (uint64_t)B * H * W, P1 = (uint64_t)B * H1 * W1, P2 = (uint64_t)B * H2 * W2, P3 = (uint64_t)B * H3 * W3;
+    conv(n, E0A, n->in0, 0, n->a0, 0, B, H, W);
+    conv(n, E0B, n->a0, 0, n->cat0, 64, B, H, W);
+    k_pool<<<blocks(P1 * 32), 256, 0, s>>>(n->cat0.p, 96, 64, n->pool0.p, 32, 32, B, H, W);
+    conv(n, E1A, n->pool0, 0, n->a1, 0, B, H1, W1);
+    conv(n, E1B, n->a1, 0, n->cat1, 96, B, H1, W1);
+    k_pool<<<blocks(P2 * 64), 256, 0, s>>>(n->cat1.p, 160, 96, n->pool1.p, 64, 64, B, H1, W1);
+    conv(n, E2A, n->pool1, 0, n->a2, 0, B, H2, W2);
+    conv(n, E2B, n->a2, 0, n->cat2, 128, B, H2, W2);
+    k_pool<<<blocks(P3 * 96), 256, 0, s>>>(n->cat2.p, 224, 128, n->pool2.p, 96, 96, B, H2, W2);
+    conv(n, E3A, n->pool2, 0, n->a3, 0, B, H3, W3);
+    conv(n, E3B, n->a3, 0, n->b3, 0, B, H3, W3);
+    k_up<<<blocks(P2 * 128), 256, 0, s>>>(n->b3.p, 128, n->cat2.p, 224, 128, B, H2, W2);
+    conv(n, D2A, n->cat2, 0, n->t2, 0, B, H2, W2);
+    conv(n, D2B, n->t2, 0, n->u2, 0, B, H2, W2);
+    k_up<<<blocks(P1 * 96), 256, 0, s>>>(n->u2.p, 96, n->cat1.p, 160, 96, B, H1, W1);
+    conv(n, D1A, n->cat1, 0, n->t1, 0, B, H1, W1);
+    conv(n, D1B, n->t1, 0, n->u1, 0, B, H1, W1);
+    k_up<<<blocks(P0 * 64), 256, 0, s>>>(n->u1.p, 64, n->cat0.p, 96, 64, B, H, W);
+    conv(n, D0A, n->cat0, 0, n->t0, 0, B, H, W);
+    conv(n, D0B, n->t0, 0, n->u0, 0, B, H, W);
+    conv(n, OUT, n->u0, 0, Act{}, 0, B, H, W, n->pred);
+    (void)P0;
+}
+
+void backward(Net* n, uint32_t B, uint32_t H, uint32_t W) {
+    cudaStream_t s = n->stream;
+    uint32_t H1 = H / 2, W1 = W / 2, H2 = H / 4, W2 = W / 4, H3 = H / 8, W3 = W / 8;
+    uint64_t P0 = (uint64_t)B * H * W, P1 = (uint64_t)B * H1 * W1, P2 = (uint64_t)B * H2 * W2, P3 = (uint64_t)B * H3 * W3;
+    // output layer (linear)
+    wgrad(n, OUT, n->u0, 0, n->dpred, B, H, W);
+    conv_dx(n, OUT, n->dpred, n->du0, B, H, W);
+    // level 0 decoder
+    relu_back(n, n->du0, 0, n->u0, 0, 32, P0);
+    wgrad(n, D0B, n->t0, 0, n->du0, B, H, W);
+    conv_dx(n, D0B, n->du0, n->dt0, B, H, W);
+    relu_back(n, n->dt0, 0, n->t0, 0, 32, P0);
+    wgrad(n, D0A, n->cat0, 0, n->dt0, B, H, W);
+    conv_dx(n, D0A, n->dt0, n->dcat0, B, H, W);
+    k_up_back<<<blocks(P1 * 64), 256, 0, s>>>(n->dcat0.p, 96, n->du1.p, 64, 64, B, H1, W1);
+    k_copy_ch<<<blocks(P0 * 32), 256, 0, s>>>(n->dcat0.p, 96, 64, n->de0b.p, 32, 0, 32, P0);
+    // level 1 decoder
+    relu_back(n, n->du1, 0, n->u1, 0, 64, P1);
+    wgrad(n, D1B, n->t1, 0, n->du1, B, H1, W1);
+    conv_dx(n, D1B, n->du1, n->dt1, B, H1, W1);
+    relu_back(n, n->dt1, 0, n->t1, 0, 64, P1);
+    wgrad(n, D1A, n->cat1, 0, n->dt1, B, H1, W1);
+    conv_dx(n, D1A, n->dt1, n->dcat1, B, H1, W1);
+    k_up_back<<<blocks(P2 * 96), 256, 0, s>>>(n->dcat1.p, 160, n->du2.p, 96, 96, B, H2, W2);
+    k_copy_ch<<<blocks(P1 * 64), 256, 0, s>>>(n->dcat1.p, 160, 96, n->de1b.p, 64, 0, 64, P1);
+    // level 2 decoder
+    relu_back(n, n->du2, 0, n->u2, 0, 96, P2);
+    wgrad(n, D2B, n->t2, 0, n->du2, B, H2, W2);
+    conv_dx(n, D2B, n->du2, n->dt2, B, H2, W2);
+    relu_back(n, n->dt2, 0, n->t2, 0, 96, P2);
+    wgrad(n, D2A, n->cat2, 0, n->dt2, B, H2, W2);
+    conv_dx(n, D2A, n->dt2, n->dcat2, B, H2, W2);
+    k_up_back<<<blocks(P3 * 128), 256, 0, s>>>(n->dcat2.p, 224, n->db3.p, 128, 128, B, H3, W3);
+    k_copy_ch<<<blocks(P2 * 96), 256, 0, s>>>(n->dcat2.p, 224, 128, n->de2b.p, 96, 0, 96, P2);
+    // bottleneck
+    relu_back(n, n->db3, 0, n->b3, 0, 128, P3);
+    wgrad(n, E3B, n->a3, 0, n->db3, B, H3, W3);
+    conv_dx(n, E3B, n->db3, n->da3, B, H3, W3);
+    relu_back(n, n->da3, 0, n->a3, 0, 128, P3);
+    wgrad(n, E3A, n->pool2, 0, n->da3, B, H3, W3);
+    conv_dx(n, E3A, n->da3, n->dpool2, B, H3, W3);
+    // level 2 encoder (its output's gradient: the skip's and the pooling's)
+    k_pool_back<<<blocks(P2 * 96), 256, 0, s>>>(n->dpool2.p, 96, n->de2b.p, 96, 0, 96, B, H2, W2);
+    relu_back(n, n->de2b, 0, n->cat2, 128, 96, P2);
+    wgrad(n, E2B, n->a2, 0, n->de2b, B, H2, W2);
+    conv_dx(n, E2B, n->de2b, n->da2, B, H2, W2);
+    relu_back(n, n->da2, 0, n->a2, 0, 96, P2);
+    wgrad(n, E2A, n->pool1, 0, n->da2, B, H2, W2);
+    conv_dx(n, E2A, n->da2, n->dpool1, B, H2, W2);
+    // level 1 encoder
+    k_pool_back<<<blocks(P1 * 64), 256, 0, s>>>(n->dpool1.p, 64, n->de1b.p, 64, 0, 64, B, H1, W1);
+    relu_back(n, n->de1b, 0, n->cat1, 96, 64, P1);
+    wgrad(n, E1B, n->a1, 0, n->de1b, B, H1, W1);
+    conv_dx(n, E1B, n->de1b, n->da1, B, H1, W1);
+    relu_back(n, n->da1, 0, n->a1, 0, 64, P1);
+    wgrad(n, E1A, n->pool0, 0, n->da1, B, H1, W1);
+    conv_dx(n, E1A, n->da1, n->dpool0, B, H1, W1);
+    // level 0 encoder
+    k_pool_back<<<blocks(P0 * 32), 256, 0, s>>>(n->dpool0.p, 32, n->de0b.p, 32, 0, 32, B, H, W);
+    relu_back(n, n->de0b, 0, n->cat0, 64, 32, P0);
+    wgrad(n, E0B, n->a0, 0, n->de0b, B, H, W);
+    conv_dx(n, E0B, n->de0b, n->da0, B, H, W);
+    relu_back(n, n->da0, 0, n->a0, 0, 32, P0);
+    wgrad(n, E0A, n->in0, 0, n->da0, B, H, W);
+}
+
+void refresh_weights(Net* n) {
+    for (int li = 0; li < N_LAYERS; ++li) {
+        const Layer& L = LAYERS[li];
+        uint64_t cnt = w_count(L);
+        k_weights<<<blocks(cnt), 256, 0, n->stream>>>(n->w + n->off[li], L.cin, r64(L.cout), r32(L.cout), n->wf[li],
+                                                       li == E0A ? nullptr : n->wb[li], r64(L.cin));
+    }
+}
+
+int check_size(Net* n, uint32_t B, uint32_t H, uint32_t W) {
+    if (B == 0 || H == 0 || W == 0 || B > n->maxB || H > n->maxH || W > n->maxW || H % 8 || W % 8) {
+        n->err = "unet: batch and image must be within the sizes given at creation, the image a multiple of 8";
+        return TRT_EINVAL;
+    }
+    return TRT_OK;
+}
+
+int cuda_check(Net* n, cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return TRT_OK;
+    n->err = std::string(what) + ": " + cudaGetErrorString(e);
+    return TRT_ECUDA;
+}
+
+}  // namespace
+}  // namespace unet
+
+using namespace unet;
+
+extern "C" {
+
+uint64_t trt_unet_param_count(void) { return param_count(); }
+
+int trt_unet_create(int device, uint32_t max_batch, uint32_t max_h, uint32_t max_w, trt_unet** out) {
+    if (!out || max_batch == 0 || max_h < 8 || max_w < 8 || max_h % 8 || max_w % 8) return TRT_EINVAL;
+    *out = nullptr;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return TRT_ECUDA;
+    auto* n = new trt_unet();
+    n->device = device;
+    n->maxB = max_batch;
+    n->maxH = max_h;
+    n->maxW = max_w;
+    n->n_params = param_count();
+    uint64_t o = 0;
+    for (int li = 0; li < N_LAYERS; ++li) {
+        n->off[li] = o;
+        o += layer_params(LAYERS[li]);
+    }
+    uint64_t P0 = (uint64_t)max_batch * max_h * max_w, P1 = P0 / 4, P2 = P0 / 16, P3 = P0 / 64;
+    e = cudaStreamCreateWithFlags(&n->stream, cudaStreamNonBlocking);
+    auto A = [&](Act& a, uint64_t px, uint32_t st) { if (e == cudaSuccess) e = act(n, a, px, st); };
+    if (e == cudaSuccess) e = alloc(n, &n->w, n->n_params);
+    if (e == cudaSuccess) e = alloc(n, &n->g, n->n_params);
+    if (e == cudaSuccess) e = alloc(n, &n->m, n->n_params);
+    if (e == cudaSuccess) e = alloc(n, &n->v, n->n_params);
+    for (int li = 0; li < N_LAYERS && e == cudaSuccess; ++li) {
+        const Layer& L = LAYERS[li];
+        e = alloc(n, &n->wf[li], w_count(L));
+        if (e == cudaSuccess) e = alloc(n, &n->wb[li], 9ull * r32(L.cout) * r64(L.cin));
+    }
+    A(n->in0, P0, 32); A(n->a0, P0, 32); A(n->cat0, P0, 96); A(n->pool0, P1, 32); A(n->a1, P1, 64);
+    A(n->cat1, P1, 160); A(n->pool1, P2, 64); A(n->a2, P2, 96); A(n->cat2, P2, 224); A(n->pool2, P3, 96);
+    A(n->a3, P3, 128); A(n->b3, P3, 128); A(n->t2, P2, 96); A(n->u2, P2, 96); A(n->t1, P1, 64); A(n->u1, P1, 64);
+    A(n->t0, P0, 32); A(n->u0, P0, 32);
+    A(n->dpred, P0, 32); A(n->du0, P0, 32); A(n->dt0, P0, 32); A(n->dcat0, P0, 96); A(n->du1, P1, 64);
+    A(n->dt1, P1, 64); A(n->dcat1, P1, 160); A(n->du2, P2, 96); A(n->dt2, P2, 96); A(n->dcat2, P2, 224);
+    A(n->db3, P3, 128); A(n->da3, P3, 128); A(n->dpool2, P3, 96); A(n->de2b, P2, 96); A(n->da2, P2, 96);
+    A(n->dpool1, P2, 64); A(n->de1b, P1, 64); A(n->da1, P1, 64); A(n->dpool0, P1, 32); A(n->de0b, P0, 32);
+    A(n->da0, P0, 32);
+    if (e == cudaSuccess) e = alloc(n, &n->pred, P0 * 3);
+    if (e == cudaSuccess) e = alloc(n, &n->target, P0 * 3);
+    if (e == cudaSuccess) e = alloc(n, &n->feat, P0 * 10);
+    if (e == cudaSuccess) e = alloc(n, &n->rgb, P0 * 3);
+    if (e == cudaSuccess) e = alloc(n, &n->loss, 4);
+    if (e == cudaSuccess) e = alloc(n, &n->sums, 4);
+    if (e == cudaSuccess) e = cudaEventCreate(&n->e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&n->e1);
+    if (e != cudaSuccess) {
+        std::fprintf(stderr, "trt_unet_create: %s\n", cudaGetErrorString(e));
+        trt_unet_destroy(n);
+        return TRT_ECUDA;
+    }
+    *out = n;
+    return TRT_OK;
+}
+
+void trt_unet_destroy(trt_unet* n) {
+    if (!n) return;
+    cudaSetDevice(n->device);
+    if (n->stream) cudaStreamSynchronize(n->stream);
+    for (void* p : n->allocs) cudaFree(p);
+    if (n->e0) cudaEventDestroy(n->e0);
+    if (n->e1) cudaEventDestroy(n->e1);
+    if (n->stream) cudaStreamDestroy(n->stream);
+    delete n;
+}
+
+const char* trt_unet_last_error(const trt_unet* n) { return n ? n->err.c_str() : "no network"; }
+
+int trt_unet_set_params(trt_unet* n, const float* params) {
+    if (!n || !params) return TRT_EINVAL;
+    cudaSetDevice(n->device);
+    int rc = cuda_check(n, cudaMemcpyAsync(n->w, params, 4 * n->n_params, cudaMemcpyHostToDevice, n->stream), "params");
+    if (rc) return rc;
+    cudaMemsetAsync(n->m, 0, 4 * n->n_params, n->stream);
+    cudaMemsetAsync(n->v, 0, 4 * n->n_params, n->stream);
+    n->t = 0;
+    refresh_weights(n);
+    return cuda_check(n, cudaStreamSynchronize(n->stream), "params");
+}
+
+int trt_unet_get_params(trt_unet* n, float* params) {
+    if (!n || !params) return TRT_EINVAL;
+    cudaSetDevice(n->device);
+    cudaMemcpyAsync(params, n->w, 4 * n->n_params, cudaMemcpyDeviceToHost, n->stream);
+    return cuda_check(n, cudaStreamSynchronize(n->stream), "params");
+}
+
+int trt_unet_forward(trt_unet* n, const float* features, uint32_t B, uint32_t H, uint32_t W, float* pred, float* ms) {
+    if (!n || !features || !pred) return TRT_EINVAL;
+    cudaSetDevice(n->device);
+    int rc = check_size(n, B, H, W);
+    if (rc) return rc;
+    uint64_t P = (uint64_t)B * H * W;
+    cudaMemcpyAsync(n->feat, features, 40 * P, cudaMemcpyHostToDevice, n->stream);
+    cudaEventRecord(n->e0, n->stream);
+    k_feat_host<<<blocks(P * 32), 256, 0, n->stream>>>(n->feat, P, n->in0.p);
+    forward(n, B, H, W);
+    cudaEventRecord(n->e1, n->stream);
+    cudaMemcpyAsync(pred, n->pred, 12 * P, cudaMemcpyDeviceToHost, n->stream);
+    rc = cuda_check(n, cudaStreamSynchronize(n->stream), "trt_unet_forward");
+    if (!rc && ms) cudaEventElapsedTime(ms, n->e0, n->e1);
+    return rc;
+}
+
+int trt_unet_train_step(trt_unet* n, const float* features, const float* targets, uint32_t B, uint32_t H, uint32_t W,
+                        float lr, int update, float* loss, float* grads, float* ms) {
+    if (!n || !features || !targets) return TRT_EINVAL;
+    cudaSetDevice(n->device);
+    int rc = check_size(n, B, H, W);
+    if (rc) return rc;
+    uint64_t P = (uint64_t)B * H * W;
+    cudaStream_t s = n->stream;
+    cudaMemcpyAsync(n->feat, features, 40 * P, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(n->target, targets, 12 * P, cudaMemcpyHostToDevice, s);
+    cudaEventRecord(n->e0, s);
+    k_feat_host<<<blocks(P * 32), 256, 0, s>>>(n->feat, P, n->in0.p);
+    forward(n, B, H, W);
+    cudaMemsetAsync(n->loss, 0, 4, s);
+    cudaMemsetAsync(n->dpred.p, 0, 2 * 32 * P, s);
+    cudaMemsetAsync(n->g, 0, 4 * n->n_params, s);
+    k_loss<<<blocks(P * 3), 256, 0, s>>>(n->pred, n->target, P, n->dpred.p, n->loss);
+    backward(n, B, H, W);
+    if (update) {
+        n->t++;
+        const float b1 = 0.9f, b2 = 0.999f;
+        float c1 = 1.0f - std::pow(b1, (float)n->t), c2 = 1.0f - std::pow(b2, (float)n->t);
+        k_adam<<<blocks(n->n_params), 256, 0, s>>>(n->w, n->g, n->m, n->v, n->n_params, lr, b1, b2, c1, c2, 1e-8f);
+        refresh_weights(n);
+    }
+    cudaEventRecord(n->e1, s);
+    if (loss) cudaMemcpyAsync(loss, n->loss, 4, cudaMemcpyDeviceToHost, s);
+    if (grads) cudaMemcpyAsync(grads, n->g, 4 * n->n_params, cudaMemcpyDeviceToHost, s);
+    rc = cuda_check(n, cudaStreamSynchronize(s), "trt_unet_train_step");
+    if (!rc && ms) cudaEventElapsedTime(ms, n->e0, n->e1);
+    return rc;
+}
+
+int trt_unet_denoise_accum(trt_unet* n, const void* accum_device, uint32_t W, uint32_t H, float* rgb_host, float* ms) {
+    if (!n || !accum_device || !rgb_host) return TRT_EINVAL;
+    cudaSetDevice(n->device);
+    int rc = check_size(n, 1, H, W);
+    if (rc) return rc;
+    uint64_t P = (uint64_t)H * W;
+    cudaStream_t s = n->stream;
+    cudaEventRecord(n->e0, s);
+    cudaMemsetAsync(n->sums, 0, 16, s);
+    k_feat_sums<<<blocks(P), 256, 0, s>>>((const float4*)accum_device, P, n->sums);
+    k_feat<<<blocks(P), 256, 0, s>>>((const float4*)accum_device, P, n->sums, n->in0.p);
+    forward(n, 1, H, W);
+    k_unfeat<<<blocks(P * 3), 256, 0, s>>>(n->pred, P, n->sums, n->rgb);
+    cudaEventRecord(n->e1, s);
+    cudaMemcpyAsync(rgb_host, n->rgb, 12 * P, cudaMemcpyDeviceToHost, s);
+    rc = cuda_check(n, cudaStreamSynchronize(s), "trt_unet_denoise_accum");
+    if (!rc && ms) cudaEventElapsedTime(ms, n->e0, n->e1);
+    return rc;
+}
+
+}  // extern "C"
