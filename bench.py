@@ -395,6 +395,49 @@ def run_serve(args, rank, world, local):
     gpu.close()
 
 
+DENOISE_METRIC = "mean ΔE against 4096 spp at 1280x720: the learned denoiser at 4 spp"
+
+
+def run_denoise(args, rank, world, local):
+    """The learned denoiser, trained here: pairs rendered by the pass (procedural cities of many seeds, 128 x 128,
+    1-4 spp with depth against 256 spp), Adam on the device, then judged at 1280 x 720 on held-out seeds against 4096
+    spp, beside the a-trous fallback and the plain path at 64 spp (ΔE as renderer/src/compare.rs reports it)."""
+    from threert_b200 import Gpu, unet
+    from threert_b200 import denoise_train as DT
+    gpu = Gpu(local)
+    name, sms = gpu.device_info()
+    t0 = time.perf_counter()
+    F, T = DT.make_dataset(gpu, range(100, 100 + args.scenes), args.views, 128, 128, 256, log=log)
+    t_data = time.perf_counter() - t0
+    net = unet.UNet(local, max_batch=16, max_h=720, max_w=1280)
+    net.set_params(unet.init_params(rank))
+    t0 = time.perf_counter()
+    losses = DT.train(net, F, T, args.train_steps, batch=16, lr=1e-3, seed=rank, log=log, log_every=2000)
+    t_train = time.perf_counter() - t0
+    if args.save:
+        np.save(args.save, net.params())
+    r = DT.judge(gpu, net, [900 + 10 * rank, 901 + 10 * rank], WIDTH, HEIGHT, 4, 64, 4096)
+    log(f"judged: {r}")
+    line = {
+        "metric": DENOISE_METRIC, "value": r["net"]["delta_e"], "unit": "ΔE (CIE76, mean)", "n_gpus": world,
+        "steps": args.train_steps, "warmup": 0, "ms_per_step": r["net"]["ms"], "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "bf16", "data": "synthetic",
+        "config": {"workload": "learned denoiser: 4-level U-Net 32/64/96/128, trained on pairs rendered by the pass, "
+                               "judged at 1280x720 on two held-out procedural cities against 4096 spp",
+                   "pairs": int(len(F)), "pair_size": "128x128, 1-4 spp vs 256 spp", "batch": 16, "crop": 64,
+                   "device": name, "sms": sms},
+        "judged": r,
+        "target_met": bool(r["net"]["delta_e"] <= r["plain_high"]["delta_e"]
+                           and r["net"]["ms"] <= 0.25 * r["plain_high"]["ms"]),
+        "training": {"dataset_s": t_data, "train_s": t_train, "first_loss": float(np.mean(losses[:100])),
+                     "last_loss": float(np.mean(losses[-100:]))},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    net.close()
+    gpu.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -407,8 +450,13 @@ def main():
                     help="coherence sorts on the device: 'none', or a comma list of rays, hits, shadows "
                          "(hits by material is the pass's default; the other two measured slower here)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
-    ap.add_argument("--workload", default="city", choices=["city", "crowd", "serve"],
-                    help="city (the headline workload), the crowd with its per-frame deformation, or the serving mix")
+    ap.add_argument("--workload", default="city", choices=["city", "crowd", "serve", "denoise"],
+                    help="city (the headline workload), the crowd with its per-frame deformation, the serving mix, or "
+                         "the learned denoiser (trained, then judged)")
+    ap.add_argument("--scenes", type=int, default=64, help="denoise: procedural cities rendered for training")
+    ap.add_argument("--views", type=int, default=16, help="denoise: views of each")
+    ap.add_argument("--train-steps", type=int, default=20000, help="denoise: Adam steps")
+    ap.add_argument("--save", default="", help="denoise: where to save the trained parameters (.npy)")
     ap.add_argument("--requests", type=int, default=64, help="serve: requests a stream")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: the mix's arrival rate (requests a second)")
     ap.add_argument("--rate-720p", type=float, default=60.0, help="serve: the 720p stream's arrival rate")
@@ -435,6 +483,11 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
 
+    if args.workload == "denoise":
+        run_denoise(args, rank, world, local)
+        if dist:
+            dist.destroy_process_group()
+        return
     if args.workload == "serve":
         run_serve(args, rank, world, local)
         if dist:

@@ -120,8 +120,9 @@ int trt_denoise_atrous(trt_scene* scene, uint32_t iterations, float* rgb_host, f
 /* ---- The learned denoiser (no counterpart in the reference, whose learned denoiser is the external OIDN library,
  * renderer/src/denoise.rs:80-103): a 4-level U-Net (32 / 64 / 96 / 128 channels, 3 x 3 convolutions, 2 x 2 average
  * pooling, nearest upsampling, skip concatenations) on bf16 tensor cores with f32 accumulation; its training (forward,
- * backward, Adam) runs on the device too. Input a pixel: log1p(radiance * s), albedo, normal, log1p(depth * sd) (10
- * floats; s = 1 / the image's mean luminance, sd = 1 / its mean first-hit distance); output: log1p(radiance * s). */
+ * backward, Adam) runs on the device too. Input a pixel: log1p(radiance * s), albedo, normal, log1p(depth * sd),
+ * log1p(variance of the mean luminance * s^2) (11 floats; s = 1 / the image's mean luminance, sd = 1 / its mean
+ * first-hit distance); output: log1p(radiance * s). */
 typedef struct trt_unet trt_unet;
 /* A network for batches of up to max_batch images of up to max_h x max_w (multiples of 8) on `device`. */
 int trt_unet_create(int device, uint32_t max_batch, uint32_t max_h, uint32_t max_w, trt_unet** out);
@@ -133,7 +134,7 @@ const char* trt_unet_last_error(const trt_unet* net);
 uint64_t trt_unet_param_count(void);
 int trt_unet_set_params(trt_unet* net, const float* params);
 int trt_unet_get_params(trt_unet* net, float* params);
-/* features: b * h * w * 10 floats (NHWC); pred: b * h * w * 3. ms (may be NULL): device time of the network. */
+/* features: b * h * w * 11 floats (NHWC); pred: b * h * w * 3. ms (may be NULL): device time of the network. */
 int trt_unet_forward(trt_unet* net, const float* features, uint32_t b, uint32_t h, uint32_t w, float* pred, float* ms);
 /* One step of training on (features, targets = log1p(reference radiance * s)): the L1 loss's gradient by the
  * backward pass, then (update != 0) an Adam step at rate lr. loss, grads (param_count floats), ms: may be NULL. */

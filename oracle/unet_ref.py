@@ -93,10 +93,10 @@ def up_back(dy):
 
 
 def forward(p, feats):
-    """feats (B, H, W, 10): the prediction (B, H, W, 3) and the activations the backward pass needs."""
-    B, H, W, _ = feats.shape
+    """feats (B, H, W, k <= 32): the prediction (B, H, W, 3) and the activations the backward pass needs."""
+    B, H, W, k = feats.shape
     x = np.zeros((B, H, W, 32))
-    x[..., :10] = feats
+    x[..., :k] = feats
     A = {"in": x}
     relu = lambda v: np.maximum(v, 0.0)
 

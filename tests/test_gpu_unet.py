@@ -28,7 +28,7 @@ def case(seed=3, b=2, h=16, w=16):
         o += 9 * cin * unet.r64(cout)
         p[o:o + cout] = rng.normal(0, 0.05, cout)
         o += unet.r64(cout)
-    feats = rng.normal(0, 1, (b, h, w, 10)).astype(np.float32)
+    feats = rng.normal(0, 1, (b, h, w, unet.N_FEAT)).astype(np.float32)
     tgt = rng.normal(0, 1, (b, h, w, 3)).astype(np.float32)
     return p, feats, tgt
 

@@ -22,7 +22,7 @@ def test_oracle_gradients_are_the_loss_slopes():
         o += 9 * cin * R.r64(cout)
         p[o:o + cout] = rng.normal(0, 0.05, cout)
         o += R.r64(cout)
-    feats = rng.normal(0, 1, (1, 8, 8, 10))
+    feats = rng.normal(0, 1, (1, 8, 8, unet.N_FEAT))
     tgt = rng.normal(0, 1, (1, 8, 8, 3))
     loss, G, _ = R.loss_and_grads(R.unpack(p), feats, tgt)
     flat = R.pack(G, p)
@@ -45,7 +45,7 @@ def test_features_and_their_inverse():
     acc[:, 4:7] = 2.0
     acc[:, 12] = 4 * 3.0
     f, s = unet.features(acc, w, h)
-    assert f.shape == (h, w, 10)
+    assert f.shape == (h, w, unet.N_FEAT)
     rad = acc[:, 0:3] / 4
     back = unet.radiance(f[..., 0:3], s).reshape(-1, 3)
     assert np.allclose(back, rad, rtol=1e-5)

@@ -334,6 +334,8 @@ __global__ void k_weights(const float* wf, uint32_t cin, uint32_t co_pad, uint32
 
 // ---- features from a rendered accum (inference on a scene's result) ----------------------------------------------
 
+constexpr int N_FEAT = 11;  // input channels a pixel
+
 // The image's mean luminance and mean first-hit distance (over pixels that hit): sums into acc[0..2].
 __global__ void k_feat_sums(const float4* __restrict__ accum, uint64_t n, float* acc) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -358,18 +360,21 @@ __global__ void k_feat_sums(const float4* __restrict__ accum, uint64_t n, float*
     }
 }
 __device__ __forceinline__ float fin0(float v) { return isfinite(v) ? v : 0.0f; }
-// The network's input from the accum: log1p(radiance * s), albedo, normal, log1p(depth * sd), 32 channels (bf16).
+// The network's input from the accum: log1p(radiance * s), albedo, normal, log1p(depth * sd) and log1p(the variance of
+// the mean luminance * s^2), 32 channels (bf16).
 __global__ void k_feat(const float4* __restrict__ accum, uint64_t n, const float* sums, bf16* x) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float s = 1.0f / fmaxf(sums[0] / (float)n, 1e-6f), sd = 1.0f / fmaxf(sums[1] / fmaxf(sums[2], 1.0f), 1e-6f);
     float4 c = accum[5 * i], a = accum[5 * i + 1], nn = accum[5 * i + 2], e = accum[5 * i + 3];
     float cnt = fmaxf(c.w, 1.0f);
-    float f[10] = {log1pf(fmaxf(fin0(c.x / cnt) * s, 0.0f)), log1pf(fmaxf(fin0(c.y / cnt) * s, 0.0f)),
-                   log1pf(fmaxf(fin0(c.z / cnt) * s, 0.0f)), fin0(a.x / cnt), fin0(a.y / cnt), fin0(a.z / cnt),
-                   fin0(nn.x / cnt), fin0(nn.y / cnt), fin0(nn.z / cnt), log1pf(fmaxf(fin0(e.x / cnt) * sd, 0.0f))};
+    float mean = fin0(a.w) / cnt, var = fmaxf(fin0(nn.w) / cnt - mean * mean, 0.0f) / cnt;
+    float f[N_FEAT] = {log1pf(fmaxf(fin0(c.x / cnt) * s, 0.0f)), log1pf(fmaxf(fin0(c.y / cnt) * s, 0.0f)),
+                       log1pf(fmaxf(fin0(c.z / cnt) * s, 0.0f)), fin0(a.x / cnt), fin0(a.y / cnt), fin0(a.z / cnt),
+                       fin0(nn.x / cnt), fin0(nn.y / cnt), fin0(nn.z / cnt), log1pf(fmaxf(fin0(e.x / cnt) * sd, 0.0f)),
+                       log1pf(fmaxf(var * s * s, 0.0f))};
     bf16* row = x + i * 32;
-    for (int k = 0; k < 32; ++k) row[k] = __float2bfloat16_rn(k < 10 ? f[k] : 0.0f);
+    for (int k = 0; k < 32; ++k) row[k] = __float2bfloat16_rn(k < N_FEAT ? f[k] : 0.0f);
 }
 // The prediction back to radiance: expm1(pred) / s.
 __global__ void k_unfeat(const float* pred, uint64_t n, const float* sums, float* rgb) {
@@ -378,13 +383,13 @@ __global__ void k_unfeat(const float* pred, uint64_t n, const float* sums, float
     float s = 1.0f / fmaxf(sums[0] / (float)n, 1e-6f);
     rgb[i] = fmaxf(expm1f(pred[i]), 0.0f) / s;
 }
-// Host features (f32, 10 a pixel) to the network's 32-channel bf16 input.
+// Host features (f32, N_FEAT a pixel) to the network's 32-channel bf16 input.
 __global__ void k_feat_host(const float* f, uint64_t n, bf16* x) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n * 32) return;
     uint64_t p = i / 32;
     uint32_t c = (uint32_t)(i % 32);
-    x[i] = __float2bfloat16_rn(c < 10 ? f[p * 10 + c] : 0.0f);
+    x[i] = __float2bfloat16_rn(c < N_FEAT ? f[p * N_FEAT + c] : 0.0f);
 }
 
 // ---- the network ----------------------------------------------------------------------------------------------------
@@ -646,7 +651,7 @@ int trt_unet_create(int device, uint32_t max_batch, uint32_t max_h, uint32_t max
     A(n->da0, P0, 32);
     if (e == cudaSuccess) e = alloc(n, &n->pred, P0 * 3);
     if (e == cudaSuccess) e = alloc(n, &n->target, P0 * 3);
-    if (e == cudaSuccess) e = alloc(n, &n->feat, P0 * 10);
+    if (e == cudaSuccess) e = alloc(n, &n->feat, P0 * N_FEAT);
     if (e == cudaSuccess) e = alloc(n, &n->rgb, P0 * 3);
     if (e == cudaSuccess) e = alloc(n, &n->loss, 4);
     if (e == cudaSuccess) e = alloc(n, &n->sums, 4);
@@ -699,7 +704,7 @@ int trt_unet_forward(trt_unet* n, const float* features, uint32_t B, uint32_t H,
     int rc = check_size(n, B, H, W);
     if (rc) return rc;
     uint64_t P = (uint64_t)B * H * W;
-    cudaMemcpyAsync(n->feat, features, 40 * P, cudaMemcpyHostToDevice, n->stream);
+    cudaMemcpyAsync(n->feat, features, 4ull * N_FEAT * P, cudaMemcpyHostToDevice, n->stream);
     cudaEventRecord(n->e0, n->stream);
     k_feat_host<<<blocks(P * 32), 256, 0, n->stream>>>(n->feat, P, n->in0.p);
     forward(n, B, H, W);
@@ -718,7 +723,7 @@ int trt_unet_train_step(trt_unet* n, const float* features, const float* targets
     if (rc) return rc;
     uint64_t P = (uint64_t)B * H * W;
     cudaStream_t s = n->stream;
-    cudaMemcpyAsync(n->feat, features, 40 * P, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(n->feat, features, 4ull * N_FEAT * P, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(n->target, targets, 12 * P, cudaMemcpyHostToDevice, s);
     cudaEventRecord(n->e0, s);
     k_feat_host<<<blocks(P * 32), 256, 0, s>>>(n->feat, P, n->in0.p);

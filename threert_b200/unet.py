@@ -1,8 +1,9 @@
 """The learned denoiser from Python: the network (trt_unet_*), its inputs made from a render's accum, the training
 pairs rendered by the pass itself, training and inference.
 
-The network is the library's U-Net (include/threert_cuda.h): input a pixel's log1p(radiance * s), albedo, normal and
-log1p(depth * sd), where s and sd normalise by the image's mean luminance and mean first-hit distance; it predicts
+The network is the library's U-Net (include/threert_cuda.h): input a pixel's log1p(radiance * s), albedo, normal,
+log1p(depth * sd) and log1p(variance * s^2), where s and sd normalise by the image's mean luminance and mean first-hit
+distance; it predicts
 log1p(radiance * s) of the converged image. Pairs for training are noisy renders (1-4 spp, TRT_RENDER_DEPTH) against
 renders of many more samples of the same view; both come from this repository's path tracer.
 """
@@ -20,7 +21,8 @@ LUM = np.array([0.2126, 0.7152, 0.0722], np.float32)
 # (cin padded to 32, cout): the layers in the library's order
 LAYERS = [(32, 32), (32, 32), (32, 64), (64, 64), (64, 96), (96, 96), (96, 128), (128, 128), (224, 96), (96, 96),
           (160, 64), (64, 64), (96, 32), (32, 32), (32, 3)]
-FAN_IN = [10, 32, 32, 64, 64, 96, 96, 128, 224, 96, 160, 64, 96, 32, 32]  # the real input channels
+N_FEAT = 11  # input channels a pixel: log radiance (3), albedo (3), normal (3), log depth, log variance
+FAN_IN = [N_FEAT, 32, 32, 64, 64, 96, 96, 128, 224, 96, 160, 64, 96, 32, 32]  # the real input channels
 
 
 def r64(v):
@@ -47,7 +49,7 @@ def init_params(seed: int = 0) -> np.ndarray:
 
 
 def features(accum: np.ndarray, width: int, height: int) -> tuple[np.ndarray, float]:
-    """The network's input (height, width, 10) from an accum with depth (TRT_RENDER_DEPTH), and the radiance scale s;
+    """The network's input (height, width, N_FEAT) from an accum with depth (TRT_RENDER_DEPTH), and the radiance scale s;
     the same transform the device applies (trt_unet_denoise_accum)."""
     px = np.asarray(accum, np.float32).reshape(-1, N.PIXEL_FLOATS)
     px = np.where(np.isfinite(px), px, 0.0)
@@ -58,8 +60,11 @@ def features(accum: np.ndarray, width: int, height: int) -> tuple[np.ndarray, fl
     s = 1.0 / max(float(lum.mean()), 1e-6)
     hit = depth > 0
     sd = 1.0 / max(float(depth[hit].sum()) / max(int(hit.sum()), 1), 1e-6)
-    f = np.concatenate([np.log1p(np.maximum(rad * s, 0.0)), alb, nrm, np.log1p(np.maximum(depth * sd, 0.0))[:, None]], 1)
-    return f.reshape(height, width, 10).astype(np.float32), s
+    mean = px[:, 7] / cnt[:, 0]
+    var = np.maximum(px[:, 11] / cnt[:, 0] - mean * mean, 0.0) / cnt[:, 0]
+    f = np.concatenate([np.log1p(np.maximum(rad * s, 0.0)), alb, nrm, np.log1p(np.maximum(depth * sd, 0.0))[:, None],
+                        np.log1p(np.maximum(var * s * s, 0.0))[:, None]], 1)
+    return f.reshape(height, width, N_FEAT).astype(np.float32), s
 
 
 def target(rgb: np.ndarray, s: float) -> np.ndarray:
