@@ -34,7 +34,8 @@ sys.path.insert(0, str(ROOT))
 
 FRAMES = 240
 WIDTH, HEIGHT, DEPTH, SPP = 1280, 720, 4, 1
-WORKLOAD = "procedural city 1984402 tris / 4002 units, 1280x720, 1 spp, depth 4, sun + sky + 400 emitter tris"
+WORKLOAD = ("procedural city 1984402 tris / 4002 units, 1280x720, 1 spp, depth 4, sun + atmosphere sky (baked on the "
+            "device, 1024x512) + 400 emitter tris")
 METRIC = "Mrays/s (closest + shadow rays, city 720p 1 spp depth 4)"
 # Algorithmic bytes a walk reads: a node record, a triangle's leaf record, the part of a unit record the walk reads.
 NODE_BYTES, LEAF_BYTES, UNIT_BYTES = 32, 48, 64
@@ -184,11 +185,33 @@ def cpu_model():
     return "unknown"
 
 
+def bake_sky_on_host(P):
+    """The city's atmosphere baked by the oracle's restatement of sky.rs on the host (the CPU arm uses no GPU), written
+    into P as the device bake would be (prep.apply_sky)."""
+    if P.sky_pending is None:
+        return
+    import oracle
+    from threert_b200 import prep
+    atm, sun_light = P.sky_pending
+    sky = oracle.Sky(atm.rayleigh_scale, atm.mie_scale, atm.mie_g, tuple(atm.ground_albedo))
+    glow = tuple(atm.glow_uniform) + tuple(atm.glow_horizon) + (atm.glow_height,)
+    tex, sun, hv = sky.bake(tuple(atm.sun_dir), tuple(atm.sun_lux), atm.altitude_m, atm.width, atm.height, glow,
+                            atm.cloud_cover, bool(atm.planet))
+    sky.close()
+
+    class _Baked:
+        sun_illuminance = tuple(float(v) for v in sun)
+        horizon_v = hv
+
+    prep.apply_sky(P, tex, _Baked, sun_light)
+
+
 def run_reference(args, rank, world):
     """The reference algorithm on the host's cores (its CPU restatement): rank 0 alone."""
     if rank != 0:
         return
     P = city_scene()
+    bake_sky_on_host(P)
     steps = max(1, args.steps)
     warm = max(0, args.warmup)
     # Whole run about 100 s: warm-up frames get a small sample, timed frames share the rest.

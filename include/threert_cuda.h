@@ -107,8 +107,8 @@ void trt_scene_free(trt_scene* scene);
  * 4 words) from host memory: in-place record edits and refits (gpu.rs:4028 write_nodes). */
 int trt_scene_update(trt_scene* scene, uint32_t which, uint64_t offset, const void* src, uint64_t bytes);
 
-/* Copies bytes [offset, offset + bytes) of one of the scene's buffers (numbered as for trt_scene_update) to host
- * memory: what a deformation wrote, for checks. */
+/* Copies bytes [offset, offset + bytes) of one of the scene's buffers (numbered as for trt_scene_update; 5: the
+ * environment's RGBA16F texels, 8 bytes each) to host memory: what a deformation or a sky bake wrote, for checks. */
 int trt_scene_read(trt_scene* scene, uint32_t which, uint64_t offset, void* dst, uint64_t bytes);
 
 /* The denoiser fallback on the scene's last accum (renderer/src/denoise.rs `denoise`, what main.rs:548-557 runs
@@ -116,6 +116,44 @@ int trt_scene_read(trt_scene* scene, uint32_t which, uint64_t offset, void* dst,
  * passes (4 in the reference) guided by albedo, normal and the 3 x 3-filtered variance, modulated again. Writes
  * w * h RGB floats to rgb_host; ms (may be NULL): the device time of the filter. */
 int trt_denoise_atrous(trt_scene* scene, uint32_t iterations, float* rgb_host, float* ms);
+
+/* ---- The atmosphere's sky baked on the device (renderer/src/sky.rs:643-819 bake_atmosphere /
+ * bake_atmosphere_tables, with the tables of Luts::build, sky.rs:386-433): the environment map the pass samples, for
+ * prep without a CPU bake and for re-baking a scene's sky in place when its sun moves. */
+typedef struct {
+    float sun_dir[3];        /* toward the sun (world, Y up; any length) */
+    float sun_lux[3];        /* the sun's illuminance above the atmosphere: colour x intensity (lux) */
+    float rayleigh_scale, mie_scale, mie_g;
+    float ground_albedo[3];
+    float altitude_m;        /* the viewer's altitude: the camera's height, or the planet's (planet = 1) */
+    uint32_t planet;         /* 0: a flat world's horizon (sky.rs Horizon::Level); 1: a planet's, dipped */
+    float glow_uniform[3];   /* the night sky's glow (sky.rs Glow), nits */
+    float glow_horizon[3];
+    float glow_height;       /* radians to 1/e */
+    float cloud_cover;       /* 0..1: the overcast blend (sky.rs:775-811) */
+    uint32_t width, height;  /* the bake: 1024 x 512 (lib.rs:966), 256 x 128 for a moving sun (sky.rs:633) */
+} trt_atmosphere;
+
+typedef struct {
+    float sun_illuminance[3];  /* lux at the ground: the atmosphere's sun light's colour (lib.rs:682-684) */
+    float horizon_v;           /* a planet's limb row (Params.sky_color.w), 0 otherwise */
+    float brightest;           /* the bake's brightest luminance (lib.rs:1013 sky_brightest); trt_scene_set_sky only */
+    float tables_ms;           /* device time of the tables (0 when those of the same atmosphere were reused) */
+    float bake_ms;             /* device time of the bake (and, for trt_scene_set_sky, of the texels and CDF) */
+} trt_sky_result;
+
+/* Bakes on the ctx's device. texels_host: NULL or width * height * 4 floats (RGBA f32, equirect, row 0 the zenith);
+ * tables_host: NULL or TRT_SKY_TABLE_FLOATS floats (the sun's optical depth 128 x 257 x 3, the scattered light
+ * 32 x 64 x 3, the ground's 64 x 3). The tables are kept and reused while the atmosphere (scales, anisotropy, ground
+ * albedo) stays the same. */
+#define TRT_SKY_TABLE_FLOATS (3 * (257 * 128 + 64 * 32 + 64))
+int trt_sky_bake(trt_ctx* ctx, const trt_atmosphere* atm, float* texels_host, float* tables_host, trt_sky_result* out);
+/* Bakes into a scene's environment in place: its RGBA16F texels, its CDF (the words' first section, lib.rs:916-941),
+ * the colour of light `sun_light` (-1: none) in the tables, and in params: env (1, w, h), sky_color.w and
+ * counts2.y (the sky light-sampled when its brightest luminance reaches env_nee_floor, lib.rs:1005-1021). The
+ * scene's environment must already be width x height (its prep reserved it). */
+int trt_scene_set_sky(trt_scene* scene, const trt_atmosphere* atm, int32_t sun_light, float env_nee_floor,
+                      uint32_t params[TRT_PARAMS_WORDS], trt_sky_result* out);
 
 /* ---- The learned denoiser (no counterpart in the reference, whose learned denoiser is the external OIDN library,
  * renderer/src/denoise.rs:80-103): a 4-level U-Net (32 / 64 / 96 / 128 channels, 3 x 3 convolutions, 2 x 2 average

@@ -58,7 +58,8 @@ typedef struct {
     float specular_scale;
 } trt_dirlight_spec;
 
-/* The sky: 0 none (black), 1 a uniform colour (nits), 2 a gradient bake (sky.rs:941-975: zenith, horizon, ground). */
+/* The sky: 0 none (black), 1 a uniform colour (nits), 2 a gradient bake (sky.rs:941-975: zenith, horizon, ground),
+ * 3 the atmosphere (sky.rs:643), baked on the device: the prep reserves a black width x height map for it. */
 typedef struct {
     uint32_t kind;
     float color[3];
@@ -113,6 +114,10 @@ typedef struct trt_prepared trt_prepared;
 /* 0 on success; on failure a message in `trt_prep_last_error`. */
 int trt_prep_build(const trt_scene_spec* spec, trt_prepared** out);
 void trt_prep_free(trt_prepared* p);
+/* A baked sky as the prep packs it (lib.rs:916-944 build_env_cdf, lib.rs:1013 sky_brightest): RGBA16F texels (w * h
+ * * 4 halves, or NULL), the CDF (h + w * h floats, or NULL) and the brightest luminance (or NULL) of w * h RGBA f32
+ * texels. 0 on success. */
+int trt_prep_env(const float* texels, uint32_t w, uint32_t h, uint16_t* env_half, float* cdf, float* brightest);
 void trt_prep_buffers(const trt_prepared* p, trt_prepared_buffers* out);
 /* The 156-word Params block with `size.z` (the sample index) 0. */
 void trt_prep_params(const trt_prepared* p, uint32_t out[156]);

@@ -31,7 +31,7 @@ class Stats(C.Structure):
 def build(force: bool = False) -> Path:
     """Builds liboracle.so with make (g++)."""
     if force or not LIB_PATH.exists() or any(
-            p.stat().st_mtime > LIB_PATH.stat().st_mtime for p in (HERE / "oracle.cpp", HERE / "deform.cpp", HERE / "denoise.cpp", HERE / "oracle.h")):
+            p.stat().st_mtime > LIB_PATH.stat().st_mtime for p in (HERE / "oracle.cpp", HERE / "deform.cpp", HERE / "denoise.cpp", HERE / "sky.cpp", HERE / "oracle.h")):
         subprocess.run(["make", "-s", "-C", str(HERE), "-B" if force else "liboracle.so"], check=True)
     return LIB_PATH
 
@@ -63,6 +63,28 @@ def lib():
         L.orc_leaf_gather.argtypes = [P(C.c_uint32), C.c_uint32, P(C.c_float), P(C.c_uint32), C.c_uint32, P(C.c_float)]
         L.orc_refit.argtypes = [P(C.c_uint32), C.c_uint32, P(C.c_float), P(C.c_uint32), C.c_uint32, P(C.c_uint32)]
         L.orc_denoise.argtypes = [P(C.c_float), C.c_uint32, C.c_uint32, C.c_uint32, P(C.c_float)]
+        L.orc_sky_exp4.argtypes = [P(C.c_double), P(C.c_double)]
+        L.orc_sky_exp4.restype = None
+        L.orc_sky_columns.argtypes = [C.c_double, C.c_double, P(C.c_double)]
+        L.orc_sky_columns.restype = None
+        L.orc_sky_sun_transmittance.argtypes = [C.c_float, C.c_float, C.c_float, P(C.c_float), P(C.c_float),
+                                                P(C.c_float)]
+        L.orc_sky_sun_transmittance.restype = None
+        L.orc_sky_horizon_elevation.argtypes = [C.c_float]
+        L.orc_sky_horizon_elevation.restype = C.c_float
+        L.orc_sky_tables.argtypes = [C.c_float, C.c_float, C.c_float, P(C.c_float)]
+        L.orc_sky_tables.restype = C.c_void_p
+        L.orc_sky_tables_free.argtypes = [C.c_void_p]
+        L.orc_sky_tables_free.restype = None
+        L.orc_sky_tables_get.argtypes = [C.c_void_p, P(C.c_float), P(C.c_float), P(C.c_float)]
+        L.orc_sky_tables_get.restype = None
+        L.orc_sky_transmittances.argtypes = [C.c_void_p, C.c_double, C.c_double, P(C.c_double), P(C.c_double)]
+        L.orc_sky_transmittances.restype = None
+        L.orc_sky_radiance.argtypes = [C.c_void_p, C.c_float, P(C.c_float), P(C.c_float), P(C.c_float)]
+        L.orc_sky_radiance.restype = None
+        L.orc_sky_bake.argtypes = [C.c_void_p, P(C.c_float), P(C.c_float), C.c_float, C.c_uint32, C.c_uint32,
+                                   P(C.c_float), C.c_float, C.c_int, P(C.c_float), P(C.c_float), P(C.c_float)]
+        L.orc_sky_bake.restype = None
         _lib = L
     return _lib
 
@@ -170,3 +192,89 @@ def denoise(accum, width: int, height: int, iterations: int = 4) -> np.ndarray:
     out = np.zeros((height, width, 3), np.float32)
     lib().orc_denoise(_p(a, C.c_float), width, height, iterations, _p(out, C.c_float))
     return out
+
+
+def _f32(v, n=None):
+    a = np.ascontiguousarray(v, np.float32).ravel()
+    assert n is None or a.size == n
+    return a
+
+
+class Sky:
+    """renderer/src/sky.rs's atmosphere on the CPU: Atmosphere::earth(rayleigh, mie, g, ground) and its Luts::build
+    tables (built once, in the constructor), the sky's radiance and the equirectangular bake."""
+
+    SUN_TABLE = (257, 128)
+    SCATTER_TABLE = (64, 32)
+
+    def __init__(self, rayleigh: float = 1.0, mie: float = 1.0, g: float = 0.8, ground=(0.401978,) * 3):
+        self.args = (float(rayleigh), float(mie), float(g), _f32(ground, 3))
+        self.h = lib().orc_sky_tables(*self.args[:3], _p(self.args[3], C.c_float))
+
+    def close(self):
+        if self.h:
+            lib().orc_sky_tables_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def tables(self):
+        """(sun (128, 257, 3), scattered (32, 64, 3), ground (64, 3)) float32."""
+        (sc, sr), (gc, gr) = self.SUN_TABLE, self.SCATTER_TABLE
+        sun = np.zeros((sr, sc, 3), np.float32)
+        scat = np.zeros((gr, gc, 3), np.float32)
+        ground = np.zeros((gc, 3), np.float32)
+        lib().orc_sky_tables_get(self.h, _p(sun, C.c_float), _p(scat, C.c_float), _p(ground, C.c_float))
+        return sun, scat, ground
+
+    def transmittances(self, r: float, mu: float):
+        """(exp(-optical_depth(r, mu)), the sun table's transmittance at (mu, r)), each 3 float64."""
+        a, b = np.zeros(3), np.zeros(3)
+        lib().orc_sky_transmittances(self.h, r, mu, _p(a, C.c_double), _p(b, C.c_double))
+        return a, b
+
+    def radiance(self, altitude_km: float, direction, sun) -> np.ndarray:
+        """Luts::sky: radiance per unit of the sun's illuminance, planet frame (Z up)."""
+        d, s, out = _f32(direction, 3), _f32(sun, 3), np.zeros(3, np.float32)
+        lib().orc_sky_radiance(self.h, altitude_km, _p(d, C.c_float), _p(s, C.c_float), _p(out, C.c_float))
+        return out
+
+    def bake(self, sun_dir, sun_lux, altitude_m: float, width: int, height: int, glow=(0.0,) * 7,
+             cover: float = 0.0, planet: bool = False):
+        """bake_atmosphere_with: (texels (height, width, 4) float32, sun illuminance (3,), horizon_v)."""
+        tex = np.zeros((height, width, 4), np.float32)
+        sd, sl, gl = _f32(sun_dir, 3), _f32(sun_lux, 3), _f32(glow, 7)
+        sun = np.zeros(3, np.float32)
+        hv = C.c_float()
+        lib().orc_sky_bake(self.h, _p(sd, C.c_float), _p(sl, C.c_float), altitude_m, width, height,
+                           _p(gl, C.c_float), cover, 1 if planet else 0, _p(tex, C.c_float), _p(sun, C.c_float),
+                           C.byref(hv))
+        return tex, sun, hv.value
+
+
+def sky_exp4(x) -> np.ndarray:
+    a = np.ascontiguousarray(x, np.float64)
+    out = np.zeros(4)
+    lib().orc_sky_exp4(_p(a, C.c_double), _p(out, C.c_double))
+    return out
+
+
+def sky_columns(r: float, mu: float) -> np.ndarray:
+    out = np.zeros(3)
+    lib().orc_sky_columns(r, mu, _p(out, C.c_double))
+    return out
+
+
+def sky_sun_transmittance(direction, rayleigh=1.0, mie=1.0, g=0.8, ground=(0.0,) * 3) -> np.ndarray:
+    out = np.zeros(3, np.float32)
+    gr, d = _f32(ground, 3), _f32(direction, 3)
+    lib().orc_sky_sun_transmittance(rayleigh, mie, g, _p(gr, C.c_float), _p(d, C.c_float), _p(out, C.c_float))
+    return out
+
+
+def sky_horizon_elevation(altitude_km: float) -> float:
+    return float(lib().orc_sky_horizon_elevation(altitude_km))

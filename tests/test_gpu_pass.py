@@ -53,7 +53,7 @@ def image_parity(acc_g, acc_o, w, h, spp):
 
 @pytest.mark.parametrize("flags", [0, N.TRT_RENDER_WIDE])
 @pytest.mark.parametrize("make,spp", [(lambda: scenes.cornell(64, 64), 16), (small_city, 4),
-                                      (scaled_units_scene, 4)])
+                                      (lambda: small_city(sky="atmosphere"), 4), (scaled_units_scene, 4)])
 def test_render_matches_the_oracle(gpu, make, spp, flags):
     P = prep.prepare(make())
     w, h = P.width, P.height

@@ -36,7 +36,7 @@ def _rank(rank, world, port, out):
         from threert_b200 import prep, scenes
         from threert_b200.gpu import frame_of
         d = scenes.city(n_objects=30, width=24, height=16, seed=5, extent=40.0, n_emitters=20, box_segments=1,
-                        sphere_slices=6, sphere_stacks=5, sky_size=(32, 16))
+                        sphere_slices=6, sphere_stacks=5, sky_size=(32, 16), sky="gradient")
         P = prep.prepare(d)
         _, frames = bench.rank_frames(rank, world, 1, 2, frames=8)
         O = oracle.Oracle(P)
@@ -77,7 +77,7 @@ def test_two_ranks_render_the_frames_one_rank_renders():
     from threert_b200 import prep, scenes
     from threert_b200.gpu import frame_of
     d = scenes.city(n_objects=30, width=24, height=16, seed=5, extent=40.0, n_emitters=20, box_segments=1,
-                    sphere_slices=6, sphere_stacks=5, sky_size=(32, 16))
+                    sphere_slices=6, sphere_stacks=5, sky_size=(32, 16), sky="gradient")
     P = prep.prepare(d)
     O = oracle.Oracle(P)
     for imgs, _ in gathered:

@@ -12,11 +12,12 @@ def luma(c):
     return 0.2126 * c[..., 0] + 0.7152 * c[..., 1] + 0.0722 * c[..., 2]
 
 
-def small_city(seed=3, n_objects=80, width=64, height=36, n_emitters=140, max_depth=4):
+def small_city(seed=3, n_objects=80, width=64, height=36, n_emitters=140, max_depth=4, sky="gradient"):
     """A city small enough for the oracle: boxes turned about y (units with normal rows), spheres placed by a
     translation alone (UNIT_SHIFTED), a ground, emissive quads past the light tree's 256 triangles."""
     return scenes.city(n_objects=n_objects, width=width, height=height, seed=seed, extent=60.0, n_emitters=n_emitters,
-                       box_segments=2, sphere_slices=10, sphere_stacks=8, max_depth=max_depth, sky_size=(64, 32))
+                       box_segments=2, sphere_slices=10, sphere_stacks=8, max_depth=max_depth, sky_size=(64, 32),
+                       sky=sky)
 
 
 def scaled_units_scene():
@@ -67,10 +68,10 @@ def region_mean(acc, w, h, spp, region):
     return f.color.reshape(-1, 3)[px].mean(0)
 
 
-def small_crowd(n=160, groups=3, width=64, height=36, max_depth=3):
+def small_crowd(n=160, groups=3, width=64, height=36, max_depth=3, sky="gradient"):
     """Config 2 small enough for the oracle: a lighter humanoid (30 capsules of 8 x 9 quads), n walkers in `groups`
     pose groups, a small ground, 12 lamps."""
     from threert_b200 import crowd
     body = crowd.humanoid(segments=8, hemi_rings=3, body_rings=4)
     return crowd.crowd(n=n, groups=groups, width=width, height=height, max_depth=max_depth, extent=12.0,
-                       ground_segments=12, n_emitters=12, body=body, sky_size=(64, 32))
+                       ground_segments=12, n_emitters=12, body=body, sky_size=(64, 32), sky=sky)

@@ -146,11 +146,26 @@ class ServerStats(C.Structure):
                 ("busy_ms", C.c_double), ("active", u32), ("pending", u32)]
 
 
+class Atmosphere(C.Structure):
+    _fields_ = [("sun_dir", f32 * 3), ("sun_lux", f32 * 3), ("rayleigh_scale", f32), ("mie_scale", f32),
+                ("mie_g", f32), ("ground_albedo", f32 * 3), ("altitude_m", f32), ("planet", u32),
+                ("glow_uniform", f32 * 3), ("glow_horizon", f32 * 3), ("glow_height", f32), ("cloud_cover", f32),
+                ("width", u32), ("height", u32)]
+
+
+class SkyResult(C.Structure):
+    _fields_ = [("sun_illuminance", f32 * 3), ("horizon_v", f32), ("brightest", f32), ("tables_ms", f32),
+                ("bake_ms", f32)]
+
+
+SKY_TABLE_FLOATS = 3 * (257 * 128 + 64 * 32 + 64)
+
 # Every function the C headers declare, with its signature: (name, restype, argtypes).
 SIGNATURES = [
     # threert_prep.h
     ("trt_prep_build", C.c_int, [P(SceneSpec), P(C.c_void_p)]),
     ("trt_prep_free", None, [C.c_void_p]),
+    ("trt_prep_env", C.c_int, [P(f32), u32, u32, P(C.c_uint16), P(f32), P(f32)]),
     ("trt_prep_buffers", None, [C.c_void_p, P(PreparedBuffers)]),
     ("trt_prep_params", None, [C.c_void_p, P(u32)]),
     ("trt_prep_get_info", None, [C.c_void_p, P(PrepInfo)]),
@@ -171,6 +186,8 @@ SIGNATURES = [
     ("trt_scene_update", C.c_int, [C.c_void_p, u32, u64, C.c_void_p, u64]),
     ("trt_scene_read", C.c_int, [C.c_void_p, u32, u64, C.c_void_p, u64]),
     ("trt_denoise_atrous", C.c_int, [C.c_void_p, u32, P(f32), P(f32)]),
+    ("trt_sky_bake", C.c_int, [C.c_void_p, P(Atmosphere), P(f32), P(f32), P(SkyResult)]),
+    ("trt_scene_set_sky", C.c_int, [C.c_void_p, P(Atmosphere), C.c_int32, f32, P(u32), P(SkyResult)]),
     ("trt_deform_setup", C.c_int, [C.c_void_p, P(DeformDesc)]),
     ("trt_deform", C.c_int, [C.c_void_p, P(u32), P(f32), u32, u32, P(DeformStats)]),
     ("trt_render", C.c_int, [C.c_void_p, P(u32), u32, u32, u32, P(f32), P(Stats)]),

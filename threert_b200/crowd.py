@@ -237,10 +237,11 @@ class Crowd:
 
 def crowd(n: int = 5000, groups: int = 1, width: int = 1280, height: int = 720, max_depth: int = 3,
           extent: float = 75.0, ground_segments: int = 158, n_emitters: int = 200, seed: int = 11,
-          body: Humanoid | None = None, sky_size=(1024, 512)) -> Crowd:
+          body: Humanoid | None = None, sky_size=(1024, 512), sky: str = "atmosphere") -> Crowd:
     """Config 2 at frame 0: n walkers (meshes 0 .. groups - 1: the humanoid and its repeats, instance i on mesh
     i % groups), the ground (158 x 158 quads: 49,928 triangles) and config 1's light set: 200 emissive quads of
-    log-uniform 10-1000 nits (here lamps 4-6 m up, facing down), the 90,000-lux sun at 28 degrees, the gradient sky."""
+    log-uniform 10-1000 nits (here lamps 4-6 m up, facing down), the 90,000-lux sun at 28 degrees and config 1's sky
+    (the atmosphere baked on the device, or with sky="gradient" the gradient sky)."""
     rng = np.random.default_rng(seed)
     body = body or humanoid()
     meshes = [body.mesh] + [Mesh(body.mesh.positions, like=0) for _ in range(groups - 1)]
@@ -275,11 +276,15 @@ def crowd(n: int = 5000, groups: int = 1, width: int = 1280, height: int = 720, 
         instances.append(Instance(len(meshes) - 1, list(range(first_mat, first_mat + n_emitters)), object=n + 1))
     el, az = math.radians(28.0), math.radians(35.0)
     to_sun = (math.cos(el) * math.cos(az), math.sin(el), math.cos(el) * math.sin(az))
-    sun = DirLight(direction=tuple(-np.asarray(to_sun)), color=(1.0, 0.96, 0.9), intensity=90000.0)
-    sky = Sky("gradient", zenith=(1200.0, 2000.0, 4000.0), horizon=(5250.0, 5950.0, 7000.0), ground=(600.0, 600.0, 600.0),
-              width=sky_size[0], height=sky_size[1])
+    if sky == "atmosphere":
+        sun = DirLight(direction=tuple(-np.asarray(to_sun)), color=(1.0, 1.0, 1.0), intensity=90000.0)
+        sky_desc = Sky("atmosphere", sun_light=0, width=sky_size[0], height=sky_size[1])
+    else:
+        sun = DirLight(direction=tuple(-np.asarray(to_sun)), color=(1.0, 0.96, 0.9), intensity=90000.0)
+        sky_desc = Sky("gradient", zenith=(1200.0, 2000.0, 4000.0), horizon=(5250.0, 5950.0, 7000.0),
+                       ground=(600.0, 600.0, 600.0), width=sky_size[0], height=sky_size[1])
     cam = crowd_camera(0, width, height, extent)
-    desc = SceneDescription(meshes, materials, instances, cam, lights=[sun], sky=sky,
+    desc = SceneDescription(meshes, materials, instances, cam, lights=[sun], sky=sky_desc,
                             preset=Preset(max_bounces=max_depth, rr_depth=3, clamp_indirect=1.0e9), seed=0x5EED)
     phase, scale = group_params(groups, seed + 2)
     return Crowd(desc, body, groups, n, walk, phase, scale, extent)

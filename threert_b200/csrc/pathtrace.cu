@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "deform.h"
+#include "sky.h"
 #include "shade.cuh"
 #include "denoise.cuh"
 #include "threert_cuda.h"
@@ -750,6 +751,7 @@ struct trt_ctx {
     char name[256] = {0};
     std::string err;
     cudaEvent_t t0 = nullptr, t1 = nullptr;
+    SkyState* sky = nullptr;  // the sky bake's tables and texels (trt_sky_bake, trt_scene_set_sky)
 };
 
 namespace trt {
@@ -1133,6 +1135,7 @@ void trt_destroy(trt_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     while (!c->scenes.empty()) trt_scene_free(c->scenes.back());
+    sky_free(c->sky);
     if (c->t0) cudaEventDestroy(c->t0);
     if (c->t1) cudaEventDestroy(c->t1);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -1265,11 +1268,65 @@ int trt_denoise_atrous(trt_scene* s, uint32_t iterations, float* rgb_host, float
 int trt_scene_read(trt_scene* s, uint32_t which, uint64_t offset, void* dst, uint64_t bytes) {
     if (!s) return TRT_EINVAL;
     trt_ctx* c = s->ctx;
-    if (which > 4 || !dst || offset + bytes > s->bytes[which] || offset + bytes < offset)
+    const void* base = which < 5 ? s->buf[which] : (const void*)s->env;
+    uint64_t size = which < 5 ? s->bytes[which] : (uint64_t)s->env_w * s->env_h * 8;
+    if (which > 5 || !dst || offset + bytes > size || offset + bytes < offset)
         return fail(c, TRT_EINVAL, "trt_scene_read: the range is not inside the buffer");
     cudaSetDevice(c->device);
-    TRT_CUDA(c, cudaMemcpyAsync(dst, (const char*)s->buf[which] + offset, bytes, cudaMemcpyDeviceToHost, c->stream));
+    TRT_CUDA(c, cudaMemcpyAsync(dst, (const char*)base + offset, bytes, cudaMemcpyDeviceToHost, c->stream));
     TRT_CUDA(c, cudaStreamSynchronize(c->stream));
+    return TRT_OK;
+}
+
+int trt_sky_bake(trt_ctx* c, const trt_atmosphere* a, float* texels_host, float* tables_host, trt_sky_result* out) {
+    if (!c || !a) return TRT_EINVAL;
+    cudaSetDevice(c->device);
+    std::string err;
+    int rc = sky_bake(&c->sky, c->device, c->stream, *a, texels_host, tables_host, out, &err);
+    return rc ? fail(c, rc, err) : TRT_OK;
+}
+
+// lib.rs:947-1010 bake_sky + SkyBaked::write on the device, in place: the texels, the CDF, the sun's colour, Params.
+int trt_scene_set_sky(trt_scene* s, const trt_atmosphere* a, int32_t sun_light, float env_nee_floor, uint32_t* P,
+                      trt_sky_result* out) {
+    if (!s || !a || !P) return TRT_EINVAL;
+    trt_ctx* c = s->ctx;
+    if (a->width != s->env_w || a->height != s->env_h)
+        return fail(c, TRT_EINVAL, "trt_scene_set_sky: the scene's environment is not width x height");
+    uint64_t cdf_words = (uint64_t)a->height + (uint64_t)a->width * a->height;
+    uint64_t cdf_at = (uint64_t)P[P_WORD_FIRST] * 4;
+    if (cdf_at + cdf_words * 4 > s->bytes[4] || cdf_at + cdf_words * 4 < cdf_at)
+        return fail(c, TRT_EINVAL, "trt_scene_set_sky: the CDF's section does not fit in the words");
+    uint64_t light_at = 0;
+    if (sun_light >= 0) {
+        if ((uint32_t)sun_light >= P[P_COUNTS]) return fail(c, TRT_EINVAL, "trt_scene_set_sky: no such light");
+        light_at = ((uint64_t)P[P_TABLE_FIRST + 2] + (uint64_t)sun_light * 5 + 2) * 16;
+        if (light_at + 16 > s->bytes[3]) return fail(c, TRT_EINVAL, "trt_scene_set_sky: the light is not in the tables");
+    }
+    cudaSetDevice(c->device);
+    trt_sky_result r{};
+    std::string err;
+    int rc = sky_bake(&c->sky, c->device, c->stream, *a, nullptr, nullptr, &r, &err);
+    if (rc) return fail(c, rc, err);
+    // lib.rs:920: each row's sin(theta) as the host prep computes it, so that the CDF rounds the same.
+    std::vector<float> sin_rows(a->height);
+    for (uint32_t y = 0; y < a->height; ++y)
+        sin_rows[y] = std::sin((((float)y) + 0.5f) / (float)a->height * 3.14159265358979323846f);
+    rc = sky_env(c->sky, c->stream, sin_rows.data(), s->env, (float*)((char*)s->buf[4] + cdf_at), &r, &err);
+    if (rc) return fail(c, rc, err);
+    if (sun_light >= 0) {
+        float col[4] = {r.sun_illuminance[0], r.sun_illuminance[1], r.sun_illuminance[2], 0.0f};
+        TRT_CUDA(c, cudaMemcpyAsync((char*)s->buf[3] + light_at, col, 16, cudaMemcpyHostToDevice, c->stream));
+        if (s->host[3].size() >= light_at + 16) std::memcpy(s->host[3].data() + light_at, col, 16);
+        TRT_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
+    auto put = [&](int w, float v) { std::memcpy(&P[w], &v, 4); };
+    put(P_ENV, 1.0f);
+    put(P_ENV + 1, (float)a->width);
+    put(P_ENV + 2, (float)a->height);
+    put(P_SKY + 3, r.horizon_v);
+    P[P_COUNTS2 + 1] = r.brightest >= env_nee_floor ? 1u : 0u;
+    if (out) *out = r;
     return TRT_OK;
 }
 

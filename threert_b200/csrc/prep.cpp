@@ -1113,6 +1113,13 @@ int trt_prep_build(const trt_scene_spec* spec, trt_prepared** out) {
         if (S.sky.kind == 2) {
             env = bake_gradient(S.sky);
             has_env = true;
+        } else if (S.sky.kind == 3) {
+            // The atmosphere (lib.rs:960-982): baked on the device (trt_sky_bake) and written over this black map of
+            // the bake's size, its CDF, the sun's colour and Params (trt_prep_env, or trt_scene_set_sky in place).
+            env.w = S.sky.width ? S.sky.width : 1024;
+            env.h = S.sky.height ? S.sky.height : 512;
+            env.texels.assign((size_t)env.w * env.h, {0.0f, 0.0f, 0.0f, 1.0f});
+            has_env = true;
         } else {
             if (S.sky.kind == 1) sky_color = mk(S.sky.color[0], S.sky.color[1], S.sky.color[2]);
             env.texels.push_back({sky_color.x, sky_color.y, sky_color.z, S.sky.kind == 1 ? 1.0f : 0.0f});
@@ -1219,6 +1226,31 @@ int trt_prep_build(const trt_scene_spec* spec, trt_prepared** out) {
 }
 
 void trt_prep_free(trt_prepared* p) { delete p; }
+
+int trt_prep_env(const float* texels, uint32_t w, uint32_t h, uint16_t* env_half, float* cdf, float* brightest) {
+    if (!texels || !w || !h) {
+        g_error = "trt_prep_env: no texels";
+        return 1;
+    }
+    EnvMap env;
+    env.w = w;
+    env.h = h;
+    env.texels.resize((size_t)w * h);
+    std::memcpy(env.texels.data(), texels, (size_t)w * h * 16);
+    if (env_half)
+        for (size_t i = 0; i < env.texels.size(); ++i)
+            for (int c = 0; c < 4; ++c) env_half[i * 4 + c] = float_to_half(env.texels[i][c]);
+    if (cdf) {
+        std::vector<float> v = build_env_cdf(env);
+        std::memcpy(cdf, v.data(), v.size() * 4);
+    }
+    if (brightest) {
+        float b = 0.0f;
+        for (const auto& t : env.texels) b = std::max(b, 0.2126f * t[0] + 0.7152f * t[1] + 0.0722f * t[2]);
+        *brightest = b;
+    }
+    return 0;
+}
 
 void trt_prep_buffers(const trt_prepared* p, trt_prepared_buffers* o) {
     o->vertices = reinterpret_cast<const float*>(p->vertices.data());

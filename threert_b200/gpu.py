@@ -14,7 +14,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _native as N
-from .prep import Prepared
+from .prep import Prepared, apply_sky
 
 
 class RenderError(RuntimeError):
@@ -104,8 +104,20 @@ class Scene:
         self.gpu._check(rc, "trt_trace")
         return hits
 
+    def set_sky(self, atmosphere: N.Atmosphere, sun_light: int, env_nee_floor: float, params: np.ndarray) -> N.SkyResult:
+        """Re-bakes the scene's atmosphere in place on the device (trt_scene_set_sky): texels, CDF, the sun light's
+        colour, and `params` (uint32 (156,), updated in place). Returns the bake's results."""
+        if params.dtype != np.uint32 or not params.flags.c_contiguous:
+            raise ValueError("set_sky: params must be a C-contiguous uint32 array")
+        r = N.SkyResult()
+        self.gpu._check(N.lib().trt_scene_set_sky(self.handle, C.byref(atmosphere), sun_light, env_nee_floor,
+                                                  params.ctypes.data_as(C.POINTER(C.c_uint32)), C.byref(r)),
+                        "trt_scene_set_sky")
+        return r
+
     def read(self, which: int, offset: int, nbytes: int, dtype=np.uint8) -> np.ndarray:
-        """Bytes [offset, offset + nbytes) of buffer `which` (0 vertices, 1 leaves, 2 nodes, 3 tables, 4 words)."""
+        """Bytes [offset, offset + nbytes) of buffer `which` (0 vertices, 1 leaves, 2 nodes, 3 tables, 4 words, 5 the
+        environment's RGBA16F texels)."""
         out = np.empty(nbytes, np.uint8)
         self.gpu._check(N.lib().trt_scene_read(self.handle, which, offset, out.ctypes.data, nbytes), "trt_scene_read")
         return out.view(dtype)
@@ -175,7 +187,23 @@ class Gpu:
         return name.value.decode(), sms.value
 
     def upload(self, prepared: Prepared) -> Scene:
+        """Uploads a prepared scene; an atmosphere sky still to bake is baked on this device first and written into
+        `prepared` (prep.apply_sky), so that its buffers are then the scene's."""
+        if prepared.sky_pending is not None:
+            atm, sun_light = prepared.sky_pending
+            tex, res = self.bake_sky(atm)
+            apply_sky(prepared, tex, res, sun_light)
         return Scene(self, prepared)
+
+    def bake_sky(self, atmosphere: N.Atmosphere, tables: bool = False):
+        """trt_sky_bake: (texels (height, width, 4) float32, SkyResult[, the tables as TRT_SKY_TABLE_FLOATS floats])."""
+        tex = np.zeros((atmosphere.height, atmosphere.width, 4), np.float32)
+        tab = np.zeros(N.SKY_TABLE_FLOATS, np.float32) if tables else None
+        r = N.SkyResult()
+        self._check(N.lib().trt_sky_bake(self.ctx, C.byref(atmosphere), tex.ctypes.data_as(C.POINTER(C.c_float)),
+                                         tab.ctypes.data_as(C.POINTER(C.c_float)) if tables else None, C.byref(r)),
+                    "trt_sky_bake")
+        return (tex, r, tab) if tables else (tex, r)
 
     def render(self, prepared: Prepared | Scene, base: np.ndarray, spp: int, timings: list | None = None,
                first_sample: int = 0, flags: int = 0) -> Frame:

@@ -67,13 +67,25 @@ class DirLight:
 
 @dataclass
 class Sky:
-    kind: str = "none"                    # none | color | gradient
+    kind: str = "none"                    # none | color | gradient | atmosphere
     color: tuple = (0.0, 0.0, 0.0)
     zenith: tuple = (0.0, 0.0, 0.0)
     horizon: tuple = (0.0, 0.0, 0.0)
     ground: tuple = (0.0, 0.0, 0.0)
     width: int = 1024
     height: int = 512
+    # The atmosphere (packages/scene/src/core.ts:2319-2359 SkyAtmosphere; scene.rs:1397-1414): its sun is directional
+    # light `sun_light` (its direction and colour x intensity); baked on the device (sky.rs:643) at width x height.
+    sun_light: int = 0
+    rayleigh_scale: float = 1.0
+    mie_scale: float = 1.0
+    mie_anisotropy: float = 0.8
+    ground_albedo: tuple = (0.401978, 0.401978, 0.401978)
+    altitude: float | None = None         # a planet's viewer altitude (m); None: the camera's height, a flat world
+    glow: tuple = (0.0, 0.0, 0.0)         # nits
+    horizon_glow: tuple = (0.0, 0.0, 0.0)
+    horizon_glow_height: float = 0.06
+    cloud_cover: float = 0.0
 
 
 @dataclass
@@ -133,6 +145,8 @@ class Prepared:
     env_h: int
     params: np.ndarray     # uint32 (156,)
     info: dict
+    # An atmosphere sky still to bake on a device (Gpu.upload bakes it): (its trt_atmosphere, the sun light's index).
+    sky_pending: tuple | None = None
 
     def with_size(self, width: int, height: int) -> np.ndarray:
         p = self.params.copy()
@@ -193,7 +207,7 @@ def prepare(desc: SceneDescription) -> Prepared:
     for k, l in enumerate(desc.lights):
         lights[k] = N.DirLightSpec((C.c_float * 3)(*l.direction), (C.c_float * 3)(*l.color), l.intensity,
                                    l.angular_diameter, 1 if l.cast_shadow else 0, l.specular_scale)
-    kinds = {"none": 0, "color": 1, "gradient": 2}
+    kinds = {"none": 0, "color": 1, "gradient": 2, "atmosphere": 3}
     s = desc.sky
     sky = N.SkySpec(kinds[s.kind], (C.c_float * 3)(*s.color), (C.c_float * 3)(*s.zenith), (C.c_float * 3)(*s.horizon),
                     (C.c_float * 3)(*s.ground), s.width, s.height)
@@ -236,9 +250,59 @@ def prepare(desc: SceneDescription) -> Prepared:
             tables=take(b.tables, b.tables_bytes, np.uint32),
             words=take(b.words, b.words_bytes, np.uint32),
             env_half=take(b.env_half, b.env_w * b.env_h * 8, np.uint16),
-            env_w=b.env_w, env_h=b.env_h, params=params, info=d)
+            env_w=b.env_w, env_h=b.env_h, params=params, info=d,
+            sky_pending=(atmosphere_of(desc), desc.sky.sun_light if desc.lights else -1)
+            if s.kind == "atmosphere" else None)
     finally:
         L.trt_prep_free(h)
+
+
+def atmosphere_of(desc: SceneDescription) -> N.Atmosphere:
+    """The trt_atmosphere of a scene's atmosphere sky (lib.rs:958-982 bake_sky; scene.rs:1397-1414): toward its sun
+    light, that light's colour x intensity above the atmosphere, the camera's height unless a planet's altitude."""
+    s = desc.sky
+    if desc.lights and 0 <= s.sun_light < len(desc.lights):
+        l = desc.lights[s.sun_light]
+        sun_dir = tuple(-float(v) for v in l.direction)
+        sun_lux = tuple(float(c) * float(l.intensity) for c in l.color)
+    else:
+        sun_dir, sun_lux = (0.0, 1.0, 0.0), (0.0, 0.0, 0.0)
+    planet = s.altitude is not None
+    altitude = max(float(s.altitude), 0.0) if planet else max(float(desc.camera.position[1]), 0.0)
+    return N.Atmosphere((C.c_float * 3)(*sun_dir), (C.c_float * 3)(*sun_lux), s.rayleigh_scale, s.mie_scale,
+                        s.mie_anisotropy, (C.c_float * 3)(*s.ground_albedo), altitude, 1 if planet else 0,
+                        (C.c_float * 3)(*s.glow), (C.c_float * 3)(*s.horizon_glow), s.horizon_glow_height,
+                        s.cloud_cover, s.width, s.height)
+
+
+def apply_sky(P: Prepared, texels: np.ndarray, result, sun_light: int) -> None:
+    """Writes a sky bake into a prepared scene as lib.rs:680-684 and 1005-1010 do: the RGBA16F texels, the CDF (the
+    words' first section), the sun light's colour (the illuminance the atmosphere leaves it), Params' env, sky_color.w
+    and counts2.y (the sky light-sampled when its brightest luminance reaches the emitters' floor)."""
+    L = N.lib()
+    h, w = texels.shape[:2]
+    if (w, h) != (P.env_w, P.env_h):
+        raise ValueError(f"apply_sky: the bake is {w} x {h}, the scene's map {P.env_w} x {P.env_h}")
+    tex = np.ascontiguousarray(texels, np.float32)
+    env = np.zeros(w * h * 4, np.uint16)
+    cdf = np.zeros(h + w * h, np.float32)
+    bright = C.c_float()
+    if L.trt_prep_env(tex.ctypes.data_as(C.POINTER(C.c_float)), w, h, env.ctypes.data_as(C.POINTER(C.c_uint16)),
+                      cdf.ctypes.data_as(C.POINTER(C.c_float)), C.byref(bright)) != 0:
+        raise ValueError("trt_prep_env: " + L.trt_prep_last_error().decode())
+    P.env_half = env
+    at = int(P.params[136])
+    P.words[at:at + cdf.size] = cdf.view(np.uint32)
+    if sun_light >= 0:
+        lt = (int(P.params[126]) + sun_light * 5 + 2) * 4
+        P.tables[lt:lt + 4] = np.array([*result.sun_illuminance, 0.0], np.float32).view(np.uint32)
+    pf = P.params.view(np.float32)
+    pf[24], pf[25], pf[26] = 1.0, float(w), float(h)
+    pf[35] = result.horizon_v
+    sampled = float(bright.value) >= float(P.info["env_nee_floor"])
+    P.params[37] = 1 if sampled else 0
+    P.info["env_sampled"] = 1 if sampled else 0
+    P.sky_pending = None
 
 
 def unit_records(worlds: np.ndarray, info: np.ndarray, roots: np.ndarray, cast_shadow: np.ndarray) -> np.ndarray:

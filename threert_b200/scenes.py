@@ -165,12 +165,14 @@ def city_camera(frame: int, frames: int, seed: int, width: int, height: int, ext
 
 def city(n_objects: int = 4000, width: int = 1280, height: int = 720, max_depth: int = 4, seed: int = 1,
          extent: float = 500.0, n_emitters: int = 200, box_segments: int = 4, sphere_slices: int = 20,
-         sphere_stacks: int = 21, frame: int = 0, frames: int = 240, sky_size=(1024, 512)) -> SceneDescription:
+         sphere_stacks: int = 21, frame: int = 0, frames: int = 240, sky_size=(1024, 512),
+         sky: str = "atmosphere") -> SceneDescription:
     """Config 1: `n_objects` seeded boxes (faces split 4 x 4: 192 triangles) and UV spheres (20 x 21: 800 triangles),
     half each, on a 1 km grid: 1,984,000 triangles at 4,000, one mesh and one unit each. GGX materials with roughness
     U(0.05, 1), metallic Bernoulli(0.3) and base colour uniform in sRGB. 200 emissive quads (400 triangles, a light
-    tree) of log-uniform 10-1000 nits, a 90,000-lux sun at 28 degrees elevation, and a gradient sky baked as the
-    reference bakes its skies (1024 x 512)."""
+    tree) of log-uniform 10-1000 nits, a 90,000-lux sun at 28 degrees elevation, and the sky: the physical atmosphere
+    lit by that sun (sky.rs:643 bake_atmosphere, baked on the device at 1024 x 512; its sun light tinted by the
+    atmosphere's transmittance), or with sky="gradient" a gradient sky (sky.rs:941) that the host prep bakes."""
     rng = np.random.default_rng(seed)
     meshes, materials, instances = [], [], []
     side = int(math.ceil(math.sqrt(n_objects)))
@@ -224,11 +226,15 @@ def city(n_objects: int = 4000, width: int = 1280, height: int = 720, max_depth:
         instances.append(Instance(len(meshes) - 1, list(range(first_mat, first_mat + n_emitters)), object=n_objects + 1))
     el, az = math.radians(28.0), math.radians(35.0)
     to_sun = (math.cos(el) * math.cos(az), math.sin(el), math.cos(el) * math.sin(az))
-    sun = DirLight(direction=tuple(-np.asarray(to_sun)), color=(1.0, 0.96, 0.9), intensity=90000.0)
-    sky = Sky("gradient", zenith=(1200.0, 2000.0, 4000.0), horizon=(5250.0, 5950.0, 7000.0), ground=(600.0, 600.0, 600.0),
-              width=sky_size[0], height=sky_size[1])
+    if sky == "atmosphere":
+        sun = DirLight(direction=tuple(-np.asarray(to_sun)), color=(1.0, 1.0, 1.0), intensity=90000.0)
+        sky_desc = Sky("atmosphere", sun_light=0, width=sky_size[0], height=sky_size[1])
+    else:
+        sun = DirLight(direction=tuple(-np.asarray(to_sun)), color=(1.0, 0.96, 0.9), intensity=90000.0)
+        sky_desc = Sky("gradient", zenith=(1200.0, 2000.0, 4000.0), horizon=(5250.0, 5950.0, 7000.0),
+                       ground=(600.0, 600.0, 600.0), width=sky_size[0], height=sky_size[1])
     cam = city_camera(frame, frames, seed, width, height, extent)
-    return SceneDescription(meshes, materials, instances, cam, lights=[sun], sky=sky,
+    return SceneDescription(meshes, materials, instances, cam, lights=[sun], sky=sky_desc,
                             preset=Preset(max_bounces=max_depth, rr_depth=3, clamp_indirect=1.0e9), seed=0x5EED)
 
 
