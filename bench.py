@@ -461,6 +461,77 @@ def run_denoise(args, rank, world, local):
     gpu.close()
 
 
+SKY_METRIC = "ms per sky re-bake on the device (atmosphere 1024x512, a moving sun: sky.rs bake_atmosphere_tables)"
+
+
+def run_sky(args, rank, world, local):
+    """The atmosphere's sky on the device: the tables once (Luts::build), then a re-bake each step with the sun moved
+    a quarter degree (a dynamic sun: the tables kept), 1024 x 512 as the offline bake's size; and the same re-bake
+    into a resident scene in place (trt_scene_set_sky: texels, CDF, the sun's colour). CPU baseline: the oracle's
+    restatement of sky.rs on all host threads (the reference bakes with rayon on all cores)."""
+    import math
+    import ctypes as C
+    from threert_b200 import Gpu, prep, scenes
+    from threert_b200 import _native as N
+    gpu = Gpu(local)
+    name, sms = gpu.device_info()
+    d = scenes.city(n_objects=60, width=64, height=36, n_emitters=20, sky_size=(1024, 512))
+    P = prep.prepare(d)
+    atm, sun_light = P.sky_pending
+
+    def at(elev_deg):
+        e, a = math.radians(elev_deg), math.radians(35.0)
+        atm.sun_dir = (N.f32 * 3)(math.cos(e) * math.cos(a), math.sin(e), math.cos(e) * math.sin(a))
+        return atm
+
+    _, cold = gpu.bake_sky(at(28.0))
+    S = gpu.upload(P)
+    elevs = [28.0 + 0.25 * k for k in range(args.warmup + args.steps)]
+    for e in elevs[:args.warmup]:
+        gpu.bake_sky(at(e))
+        S.set_sky(at(e), sun_light, P.info["env_nee_floor"], P.params.copy())
+    bake_ms, scene_ms, wall = [], [], []
+    for e in elevs[args.warmup:]:
+        _, r = gpu.bake_sky(at(e))
+        bake_ms.append(r.bake_ms)
+        t = time.perf_counter()
+        r2 = S.set_sky(at(e), sun_light, P.info["env_nee_floor"], P.params.copy())
+        wall.append((time.perf_counter() - t) * 1e3)
+        scene_ms.append(r2.bake_ms)
+    ms = float(np.mean(bake_ms))
+    line = {
+        "metric": SKY_METRIC, "value": ms, "unit": "ms", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "atmosphere sky bake 1024x512 (orders 2-4, 12 / 16 Simpson steps), sun moving "
+                               "0.25 degrees a step from 28 degrees", "device": name, "sms": sms},
+        "tables_ms": cold.tables_ms, "first_bake_ms": cold.bake_ms,
+        "scene_rebake_ms": float(np.mean(scene_ms)),
+        "e2e": {"value": float(np.mean(wall)), "unit": "ms", "h2d_bytes_per_step": 2048,
+                "d2h_bytes_per_step": 24},
+    }
+    if not args.no_cpu and rank == 0:
+        import oracle
+        t = time.perf_counter()
+        sky = oracle.Sky(atm.rayleigh_scale, atm.mie_scale, atm.mie_g, tuple(atm.ground_albedo))
+        t_tables = (time.perf_counter() - t) * 1e3
+        t = time.perf_counter()
+        n_cpu = 3
+        for k in range(n_cpu):
+            a = at(28.0 + 0.25 * k)
+            sky.bake(tuple(a.sun_dir), tuple(a.sun_lux), a.altitude_m, 1024, 512)
+        t_bake = (time.perf_counter() - t) * 1e3 / n_cpu
+        sky.close()
+        line["cpu_baseline"] = {"value": t_bake, "unit": "ms", "cores": min(oracle.hardware_threads(), 32),
+                                "kind": "port", "sample": f"{n_cpu} bakes of 1024x512 after the tables "
+                                                          f"({t_tables:.0f} ms)",
+                                "tables_ms": t_tables}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    S.close()
+    gpu.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -473,9 +544,9 @@ def main():
                     help="coherence sorts on the device: 'none', or a comma list of rays, hits, shadows "
                          "(hits by material is the pass's default; the other two measured slower here)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
-    ap.add_argument("--workload", default="city", choices=["city", "crowd", "serve", "denoise"],
-                    help="city (the headline workload), the crowd with its per-frame deformation, the serving mix, or "
-                         "the learned denoiser (trained, then judged)")
+    ap.add_argument("--workload", default="city", choices=["city", "crowd", "serve", "denoise", "sky"],
+                    help="city (the headline workload), the crowd with its per-frame deformation, the serving mix, "
+                         "the learned denoiser (trained, then judged), or the atmosphere's sky bake")
     ap.add_argument("--scenes", type=int, default=64, help="denoise: procedural cities rendered for training")
     ap.add_argument("--views", type=int, default=16, help="denoise: views of each")
     ap.add_argument("--train-steps", type=int, default=20000, help="denoise: Adam steps")
@@ -506,6 +577,11 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
 
+    if args.workload == "sky":
+        run_sky(args, rank, world, local)
+        if dist:
+            dist.destroy_process_group()
+        return
     if args.workload == "denoise":
         run_denoise(args, rank, world, local)
         if dist:

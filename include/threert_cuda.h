@@ -155,6 +155,15 @@ int trt_sky_bake(trt_ctx* ctx, const trt_atmosphere* atm, float* texels_host, fl
 int trt_scene_set_sky(trt_scene* scene, const trt_atmosphere* atm, int32_t sun_light, float env_nee_floor,
                       uint32_t params[TRT_PARAMS_WORDS], trt_sky_result* out);
 
+/* The light list's weights made again on the device (renderer/shaders/emitter_weights.wgsl, run by gpu.rs:3219
+ * weigh_emitters): each emitter's weight from its record, instance, material and object power as the tables hold
+ * them now, the cumulative table and its guide, the light tree's node powers (tree_nodes of them, 0: no tree) and the
+ * header. After edits of object powers, materials or emitter records (trt_scene_update). lod: NULL, or the light
+ * LOD's reference point and d0 (on when d0 > 0); cull: NULL, or radius, far distance, cone cosine, cone direction
+ * (6 floats). ms (may be NULL): device time. */
+int trt_scene_weigh_emitters(trt_scene* scene, const uint32_t params[TRT_PARAMS_WORDS], uint32_t tree_nodes,
+                             const float* lod, const float* cull, float* ms);
+
 /* ---- The learned denoiser (no counterpart in the reference, whose learned denoiser is the external OIDN library,
  * renderer/src/denoise.rs:80-103): a 4-level U-Net (32 / 64 / 96 / 128 channels, 3 x 3 convolutions, 2 x 2 average
  * pooling, nearest upsampling, skip concatenations) on bf16 tensor cores with f32 accumulation; its training (forward,

@@ -31,7 +31,7 @@ class Stats(C.Structure):
 def build(force: bool = False) -> Path:
     """Builds liboracle.so with make (g++)."""
     if force or not LIB_PATH.exists() or any(
-            p.stat().st_mtime > LIB_PATH.stat().st_mtime for p in (HERE / "oracle.cpp", HERE / "deform.cpp", HERE / "denoise.cpp", HERE / "sky.cpp", HERE / "oracle.h")):
+            p.stat().st_mtime > LIB_PATH.stat().st_mtime for p in (HERE / "oracle.cpp", HERE / "deform.cpp", HERE / "denoise.cpp", HERE / "sky.cpp", HERE / "emitters.cpp", HERE / "oracle.h")):
         subprocess.run(["make", "-s", "-C", str(HERE), "-B" if force else "liboracle.so"], check=True)
     return LIB_PATH
 
@@ -85,6 +85,9 @@ def lib():
         L.orc_sky_bake.argtypes = [C.c_void_p, P(C.c_float), P(C.c_float), C.c_float, C.c_uint32, C.c_uint32,
                                    P(C.c_float), C.c_float, C.c_int, P(C.c_float), P(C.c_float), P(C.c_float)]
         L.orc_sky_bake.restype = None
+        L.orc_weigh_emitters.argtypes = [P(C.c_uint32), C.c_uint64, P(C.c_uint32), C.c_uint64, P(C.c_uint32),
+                                         C.c_uint32, P(C.c_float), P(C.c_float)]
+        L.orc_weigh_emitters.restype = None
         _lib = L
     return _lib
 
@@ -278,3 +281,17 @@ def sky_sun_transmittance(direction, rayleigh=1.0, mie=1.0, g=0.8, ground=(0.0,)
 
 def sky_horizon_elevation(altitude_km: float) -> float:
     return float(lib().orc_sky_horizon_elevation(altitude_km))
+
+
+def weigh_emitters(tables, words, params, tree_nodes: int, lod=None, cull=None) -> np.ndarray:
+    """emitter_weights.wgsl over a copy of the scene's tables: the tables with the emitters' entries, guide, header
+    and the light tree's powers made again."""
+    t = np.array(tables, np.uint32, copy=True, order="C")
+    w = np.ascontiguousarray(words, np.uint32)
+    p = np.ascontiguousarray(params, np.uint32)
+    lo = _f32(lod, 4) if lod is not None else None
+    cu = _f32(cull, 6) if cull is not None else None
+    lib().orc_weigh_emitters(_p(t, C.c_uint32), t.size // 4, _p(w, C.c_uint32), w.size, _p(p, C.c_uint32), tree_nodes,
+                             _p(lo, C.c_float) if lo is not None else None,
+                             _p(cu, C.c_float) if cu is not None else None)
+    return t

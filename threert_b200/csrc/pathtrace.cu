@@ -788,6 +788,8 @@ struct trt_scene {
     uint64_t extend_launches = 0, shadow_launches = 0, renders = 0, launches = 0;
     // The per-frame deformation (trt_deform_setup), and whether the host copies still hold what the device does.
     DeformState* deform = nullptr;
+    void* em = nullptr;  // the emitter re-weigh's scratch (trt_scene_weigh_emitters)
+    uint64_t em_bytes = 0;
     bool deform_stale = false;  // the nodes were written after setup: its tree checks no longer hold
     bool deformed = false;      // a deformation ran: the host copies (and a wide BVH built from them) are old
 };
@@ -1202,6 +1204,7 @@ void trt_scene_free(trt_scene* s) {
     if (s->dn) cudaFree(s->dn);
     if (s->totals) cudaFree(s->totals);
     deform_free(s->deform);
+    if (s->em) cudaFree(s->em);
     s->wide.release();
     for (auto* v : {&s->ev_extend, &s->ev_shadow, &s->ev_shade, &s->ev_sort, &s->ev_free})
         for (auto& e : *v) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
@@ -1690,3 +1693,4 @@ int trt_render_noalloc(const trt_scene_desc* dev, const uint32_t params[TRT_PARA
 }  // extern "C"
 
 #include "serve.cuh"
+#include "emitters.cuh"

@@ -115,6 +115,19 @@ class Scene:
                         "trt_scene_set_sky")
         return r
 
+    def weigh_emitters(self, params: np.ndarray, tree_nodes: int, lod=None, cull=None) -> float:
+        """Re-weighs the emitters on the device from the tables as they are now (trt_scene_weigh_emitters); lod: None
+        or (x, y, z, d0); cull: None or (radius, far, cos, dx, dy, dz). Returns the device ms."""
+        p = np.ascontiguousarray(params, np.uint32)
+        lo = np.ascontiguousarray(lod, np.float32) if lod is not None else None
+        cu = np.ascontiguousarray(cull, np.float32) if cull is not None else None
+        ms = C.c_float()
+        fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float)) if a is not None else None
+        self.gpu._check(N.lib().trt_scene_weigh_emitters(self.handle, p.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                                         tree_nodes, fp(lo), fp(cu), C.byref(ms)),
+                        "trt_scene_weigh_emitters")
+        return float(ms.value)
+
     def read(self, which: int, offset: int, nbytes: int, dtype=np.uint8) -> np.ndarray:
         """Bytes [offset, offset + nbytes) of buffer `which` (0 vertices, 1 leaves, 2 nodes, 3 tables, 4 words, 5 the
         environment's RGBA16F texels)."""
