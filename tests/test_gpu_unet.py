@@ -35,7 +35,7 @@ def case(seed=3, b=2, h=16, w=16):
 
 @pytest.fixture(scope="module")
 def net():
-    n = unet.UNet(0, max_batch=4, max_h=64, max_w=64)
+    n = unet.UNet(0, max_batch=4, max_h=64, max_w=80)
     yield n
     n.close()
 
@@ -48,6 +48,17 @@ def test_forward_matches_the_oracle(net):
     err = np.linalg.norm(got - want) / np.linalg.norm(want)
     assert err < 0.03, err
     assert ms > 0
+
+
+def test_forward_on_ragged_tiles_matches_the_oracle(net):
+    # 72 x 40: tiles of 8 x 16 pixels at the top level (the last row of tiles half outside the image), 4 x 32,
+    # 2 x 64, then 1 x 128 over a 9 x 5 level
+    p, feats, _ = case(seed=4, b=1, h=40, w=72)
+    net.set_params(p)
+    got, _ = net.forward(feats)
+    want, _ = R.forward(R.unpack(bf16(p).astype(np.float64)), bf16(feats).astype(np.float64))
+    err = np.linalg.norm(got - want) / np.linalg.norm(want)
+    assert err < 0.03, err
 
 
 def test_every_layers_gradient_matches_the_oracle(net):

@@ -6,12 +6,14 @@
 // N = output channels, K = 9 taps x input channels) on bf16 tensor-core MMAs with f32 accumulation. The input gradient
 // is the same kernel run on the output gradient with the weights flipped and transposed; the weight gradient is a GEMM
 // over pixels (split across CTAs, summed with f32 atomics). Master weights, gradients and Adam's moments are f32.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -42,114 +44,237 @@ __device__ __forceinline__ void mma16816(float* c, uint32_t a0, uint32_t a1, uin
 }
 
 // ---- convolution (forward; and the input gradient with flipped, transposed weights) -------------------------------
+//
+// y[p][n] = bias[n] + sum over taps t and channels c of x[p + off(t)][c] * w[t][c][n], zero outside the image.
+// A CTA computes a tile of 128 pixels (a bw x bh rectangle of one image, bw the largest power of two <= 128 that
+// divides the width) x N output channels (N 128 where 128 divides co_pad, else 64; blockIdx.y their tile) on the
+// 5th-generation tensor cores:
+//  - one thread issues the loads: per K stage (one tap, 32 input channels) four TMA boxes of 8 channels x bw x bh
+//    pixels, shifted by the tap (the halo and the image's border read as zeros), and four bulk copies of the stage's
+//    weights (N rows of each 8-channel chunk); each lands in the canonical K-major layout without swizzle (8-row x
+//    16-byte core matrices);
+//  - one thread issues two tcgen05.mma (M 128, N, K 16, bf16 in, f32 accumulate in tensor memory) a stage and
+//    commits each stage's buffers back to the loader through an mbarrier; TS stages in flight;
+//  - the four warps read the accumulator out of tensor memory (each its 32 lanes = pixels), add the bias, apply the
+//    ReLU and store bf16 (or f32) NHWC.
+// Every mbarrier wait is bounded (about a second); a wait that gives up sets the error word and the CTA finishes.
 
 struct Conv {
-    const bf16* x;            // input, NHWC
-    uint32_t x_stride, x_off; // channel stride and first channel read
+    const bf16* w;            // [9][cin / 8][co_pad][8]: per tap and 8-channel chunk, co_pad rows of 8 channels
     uint32_t cin;             // channels read (a multiple of 32)
-    const bf16* w;            // [9][cin][co_pad]: tap-major rows of output channels
-    uint32_t co_pad;          // a multiple of 64
+    uint32_t co_pad;          // a multiple of 64 (up to 256)
+    uint32_t nt;              // output channels a CTA: 128 where they divide co_pad, else 64 (blockIdx.y the tile)
     const float* bias;        // co_pad, or null
     bf16* y;                  // output, NHWC
     uint32_t y_stride, y_off, cout;
     float* yf;                // or f32 output (stride cout), for the last layer
-    uint32_t B, H, W;
+    uint32_t B, H, W, x_off;
+    uint32_t bw, bh, tiles_x, tiles_y;
     int relu;
+    uint32_t* err;
 };
 
-constexpr int CM = 128, CN = 64, CK = 32, APAD = 8, BPAD = 8;
+constexpr uint32_t TS = 4;                  // pipeline stages
+constexpr uint32_t A_STAGE = 128u * 32u * 2u, B_STAGE = 128u * 32u * 2u;
+constexpr uint32_t CONV_SMEM = TS * (A_STAGE + B_STAGE) + 256u + 1024u;  // + room to align the stages to 1 KB
 
-// y[p][n] = bias[n] + sum over taps t and channels c of x[p + off(t)][c] * w[t][c][n], zero outside the image.
-// A CTA: 128 pixels x 64 output channels; 8 warps of 32 x 32.
-__global__ void __launch_bounds__(256) k_conv(Conv a) {
-    __shared__ __align__(16) bf16 As[CM][CK + APAD];
-    __shared__ __align__(16) bf16 Bs[CK][CN + BPAD];
+__device__ __forceinline__ void mbar_init(uint32_t a, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t a, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t a, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    return ok != 0u;
+}
+// A bounded wait: about 2^31 cycles (a second at the B200's clock), then the error word.
+__device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity, uint32_t* err) {
+    long long t0 = clock64();
+    while (!mbar_try_wait(a, parity)) {
+        if (clock64() - t0 > (1ll << 31)) {
+            atomicOr(err, 1u);
+            return false;
+        }
+    }
+    return true;
+}
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const void* map, int c0, int c1, int c2, int c3,
+                                            uint32_t mbar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];" ::"r"(dst),
+        "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(mbar)
+        : "memory");
+}
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"((uint64_t)src), "r"(bytes), "r"(mbar)
+                 : "memory");
+}
+// The canonical K-major shared-memory matrix without swizzle: core matrices of 8 rows x 16 bytes, `lbo` bytes apart
+// along K, `sbo` bytes apart along M / N; descriptor version 1 (sm_100).
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+// kind::f16 instruction descriptor: f32 accumulator, bf16 A and B, both K-major, M x N.
+__host__ __device__ constexpr uint32_t umma_idesc(uint32_t M, uint32_t N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((N >> 3) << 17) | ((M >> 4) << 24);
+}
+__device__ __forceinline__ void umma_f16(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d),
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+__device__ __forceinline__ void umma_commit(uint32_t mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+                 : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, "
+        "[%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__global__ void __launch_bounds__(128) k_conv(const __grid_constant__ CUtensorMap xmap, Conv a) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
-    const uint32_t wm = warp & 3u, wn = warp >> 2;
-    const uint32_t M = a.B * a.H * a.W, m0 = blockIdx.x * CM, n0 = blockIdx.y * CN;
-    float acc[2][4][4];
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-#pragma unroll
-            for (int k = 0; k < 4; ++k) acc[i][j][k] = 0.0f;
-    // this thread's two A rows (pixels) and their coordinates
-    uint32_t apx[2], apart[2];
-    int ab[2], ay[2], ax[2];
-    bool aval[2];
-#pragma unroll
-    for (int r = 0; r < 2; ++r) {
-        uint32_t idx = tid + r * 256u;
-        apx[r] = idx >> 2;
-        apart[r] = idx & 3u;
-        uint32_t m = m0 + apx[r];
-        aval[r] = m < M;
-        uint32_t hw = a.H * a.W, mm = aval[r] ? m : 0u;
-        ab[r] = (int)(mm / hw);
-        ay[r] = (int)((mm % hw) / a.W);
-        ax[r] = (int)(mm % a.W);
-    }
-    const uint32_t bk = tid >> 3, bpart = tid & 7u;
-    for (int tap = 0; tap < 9; ++tap) {
-        const int dy = tap / 3 - 1, dx = tap % 3 - 1;
-        for (uint32_t c0 = 0; c0 < a.cin; c0 += CK) {
-#pragma unroll
-            for (int r = 0; r < 2; ++r) {
-                int sy = ay[r] + dy, sx = ax[r] + dx;
-                uint4 v = make_uint4(0u, 0u, 0u, 0u);
-                if (aval[r] && sy >= 0 && sx >= 0 && sy < (int)a.H && sx < (int)a.W) {
-                    uint64_t pix = ((uint64_t)ab[r] * a.H + (uint32_t)sy) * a.W + (uint32_t)sx;
-                    v = *reinterpret_cast<const uint4*>(a.x + pix * a.x_stride + a.x_off + c0 + apart[r] * 8u);
-                }
-                *reinterpret_cast<uint4*>(&As[apx[r]][apart[r] * 8u]) = v;
-            }
-            *reinterpret_cast<uint4*>(&Bs[bk][bpart * 8u]) =
-                *reinterpret_cast<const uint4*>(a.w + ((uint64_t)tap * a.cin + c0 + bk) * a.co_pad + n0 + bpart * 8u);
-            __syncthreads();
-#pragma unroll
-            for (uint32_t kk = 0; kk < CK; kk += 16) {
-                uint32_t af[2][4], bfr[4][2];
-#pragma unroll
-                for (int mt = 0; mt < 2; ++mt)
-                    ldsm_x4(af[mt][0], af[mt][1], af[mt][2], af[mt][3],
-                            &As[wm * 32u + mt * 16u + (lane & 15u)][kk + (lane >> 4) * 8u]);
-#pragma unroll
-                for (int np = 0; np < 2; ++np)
-                    ldsm_x4_t(bfr[np * 2][0], bfr[np * 2][1], bfr[np * 2 + 1][0], bfr[np * 2 + 1][1],
-                              &Bs[kk + (lane & 7u) + ((lane >> 3) & 1u) * 8u][wn * 32u + np * 16u + (lane >> 4) * 8u]);
-#pragma unroll
-                for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-                    for (int nt = 0; nt < 4; ++nt)
-                        mma16816(acc[mt][nt], af[mt][0], af[mt][1], af[mt][2], af[mt][3], bfr[nt][0], bfr[nt][1]);
-            }
-            __syncthreads();
+    const uint32_t sraw = smem_addr(smem_raw), sbase = (sraw + 1023u) & ~1023u;
+    uint8_t* smem = smem_raw + (sbase - sraw);
+    const uint32_t sA = sbase, sB = sbase + TS * A_STAGE, sBar = sbase + TS * (A_STAGE + B_STAGE);
+    // barriers: full[TS], empty[TS], done; then the tensor-memory address
+    auto full = [&](uint32_t s) { return sBar + 8u * s; };
+    auto empty = [&](uint32_t s) { return sBar + 8u * (TS + s); };
+    const uint32_t done = sBar + 8u * (2u * TS);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + TS * (A_STAGE + B_STAGE) + 8u * (2u * TS + 1u));
+    const uint32_t per_img = a.tiles_x * a.tiles_y;
+    const uint32_t b = blockIdx.x / per_img, t = blockIdx.x % per_img;
+    const int x0 = (int)((t % a.tiles_x) * a.bw), y0 = (int)((t / a.tiles_x) * a.bh);
+    const uint32_t ncols = a.nt;  // 64 or 128 tensor-memory columns
+    const uint32_t n0 = blockIdx.y * a.nt;
+
+    if (tid == 0) {
+        for (uint32_t s = 0; s < TS; ++s) {
+            mbar_init(full(s), 1);
+            mbar_init(empty(s), 1);
         }
+        mbar_init(done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    const uint32_t g = lane >> 2, t4 = lane & 3u;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tslot)),
+                     "r"(ncols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+
+    const uint32_t kc = a.cin / 32u, nk = 9u * kc;
+    const uint32_t bbytes = 4u * a.nt * 16u;
+    bool ok = true;
+    if (warp == 0) {
+        if (lane == 0) {
+            // the loader
+            for (uint32_t k = 0; k < nk && ok; ++k) {
+                const uint32_t s = k % TS, round = k / TS;
+                if (k >= TS) ok = mbar_wait(empty(s), (round - 1u) & 1u, a.err);
+                if (!ok) break;
+                mbar_expect_tx(full(s), A_STAGE + bbytes);
+                const uint32_t tap = k / kc, c0 = (k % kc) * 32u;
+                const int dy = (int)(tap / 3u) - 1, dx = (int)(tap % 3u) - 1;
 #pragma unroll
-    for (int mt = 0; mt < 2; ++mt)
+                for (uint32_t j = 0; j < 4u; ++j)
+                    tma_load_4d(sA + s * A_STAGE + j * 2048u, &xmap, (int)(a.x_off + c0 + 8u * j), x0 + dx, y0 + dy,
+                                (int)b, full(s));
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            uint32_t m = m0 + wm * 32u + mt * 16u + g + h * 8u;
-            if (m >= M) continue;
-#pragma unroll
-            for (int nt = 0; nt < 4; ++nt) {
-                uint32_t n = n0 + wn * 32u + nt * 8u + t4 * 2u;
-                float v0 = acc[mt][nt][h * 2], v1 = acc[mt][nt][h * 2 + 1];
-                if (a.bias) { v0 += a.bias[n]; v1 += a.bias[n + 1]; }
-                if (a.relu) { v0 = fmaxf(v0, 0.0f); v1 = fmaxf(v1, 0.0f); }
-                if (a.yf) {
-                    if (n < a.cout) a.yf[(uint64_t)m * a.cout + n] = v0;
-                    if (n + 1 < a.cout) a.yf[(uint64_t)m * a.cout + n + 1] = v1;
-                } else if (n < a.cout) {
-                    bf16* dst = a.y + (uint64_t)m * a.y_stride + a.y_off + n;
-                    if (n + 1 < a.cout) *reinterpret_cast<__nv_bfloat162*>(dst) = __floats2bfloat162_rn(v0, v1);
-                    else *dst = __float2bfloat16_rn(v0);
+                for (uint32_t j = 0; j < 4u; ++j) {
+                    const bf16* src = a.w + (((uint64_t)tap * (a.cin / 8u) + c0 / 8u + j) * a.co_pad + n0) * 8u;
+                    bulk_load(sB + s * B_STAGE + j * a.nt * 16u, src, a.nt * 16u, full(s));
                 }
             }
         }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // the MMA issuer
+            const uint32_t idesc = umma_idesc(128u, a.nt);
+            const uint32_t lbo_b = a.nt * 16u;
+            for (uint32_t k = 0; k < nk && ok; ++k) {
+                const uint32_t s = k % TS;
+                ok = mbar_wait(full(s), (k / TS) & 1u, a.err);
+                if (!ok) break;
+                tc_fence_after();
+#pragma unroll
+                for (uint32_t j = 0; j < 2u; ++j) {
+                    uint64_t ad = umma_desc(sA + s * A_STAGE + j * 2u * 2048u, 2048u, 128u);
+                    uint64_t bd = umma_desc(sB + s * B_STAGE + j * 2u * lbo_b, lbo_b, 128u);
+                    umma_f16(tmem, ad, bd, idesc, (k | j) != 0u ? 1u : 0u);
+                }
+                umma_commit(empty(s));
+            }
+            umma_commit(done);
+        }
+    }
+    __syncwarp();
+    // the epilogue: every warp its 32 lanes (pixels) of the accumulator
+    bool fin = mbar_wait(done, 0u, a.err);
+    __syncwarp();
+    tc_fence_after();
+    const uint32_t m = warp * 32u + lane;
+    const int px = x0 + (int)(m % a.bw), py = y0 + (int)(m / a.bw);
+    const bool valid = fin && px < (int)a.W && py < (int)a.H;
+    const uint64_t p = ((uint64_t)b * a.H + (uint32_t)py) * a.W + (uint32_t)px;
+    for (uint32_t cc = 0; cc < a.nt; cc += 16u) {
+        float v[16];
+        tmem_ld16(tmem + ((warp * 32u) << 16) + cc, v);
+        const uint32_t c = n0 + cc;
+        if (!valid) continue;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            if (a.bias) v[i] += a.bias[c + i];
+            if (a.relu) v[i] = fmaxf(v[i], 0.0f);
+        }
+        if (a.yf) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+                if (c + i < a.cout) a.yf[p * a.cout + c + i] = v[i];
+        } else if (c + 16u <= a.cout) {
+            uint32_t pk[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                __nv_bfloat162 h2 = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+                pk[i] = *reinterpret_cast<uint32_t*>(&h2);
+            }
+            uint4* dst = reinterpret_cast<uint4*>(a.y + p * a.y_stride + a.y_off + c);
+            dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+            dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+        } else {
+            for (int i = 0; i < 16; ++i)
+                if (c + i < a.cout) a.y[p * a.y_stride + a.y_off + c + i] = __float2bfloat16_rn(v[i]);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
 }
 
 // ---- weight gradient: dw[t][c][n] += sum over pixels p of x[p + off(t)][c] * dy[p][n] ------------------------------
@@ -319,8 +444,10 @@ __global__ void k_adam(float* w, const float* g, float* m, float* v, uint64_t n,
     v[i] = vi;
     w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
 }
-// The bf16 weights of a layer from its f32 masters: forward [t][c][n] (c < cin, n < co_pad), and the input
-// gradient's [8 - t][n][c] (n < cout32: the output gradient's channels, c < cin, rows ci_pad64 wide).
+// The bf16 weights of a layer from its f32 masters w[t][c][n], laid out as the convolution's B operand (per tap and
+// 8-channel chunk of its input, the output channels' rows of 8 input channels): forward [t][c / 8][n][c % 8] (c <
+// cin, n < co_pad), and the input gradient's [8 - t][n / 8][c][n % 8] (n < cout32: the output gradient's channels, its
+// input; c < cin of ci_pad64 rows, its output).
 __global__ void k_weights(const float* wf, uint32_t cin, uint32_t co_pad, uint32_t cout32, bf16* wfw, bf16* wbw,
                           uint32_t ci_pad64) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -328,8 +455,9 @@ __global__ void k_weights(const float* wf, uint32_t cin, uint32_t co_pad, uint32
     if (i >= n) return;
     uint32_t nn = (uint32_t)(i % co_pad), c = (uint32_t)((i / co_pad) % cin), t = (uint32_t)(i / ((uint64_t)co_pad * cin));
     bf16 v = __float2bfloat16_rn(wf[i]);
-    wfw[i] = v;
-    if (wbw && nn < cout32) wbw[((uint64_t)(8 - t) * cout32 + nn) * ci_pad64 + c] = v;
+    wfw[(((uint64_t)t * (cin / 8u) + c / 8u) * co_pad + nn) * 8u + c % 8u] = v;
+    if (wbw && nn < cout32)
+        wbw[(((uint64_t)(8 - t) * (cout32 / 8u) + nn / 8u) * ci_pad64 + c) * 8u + nn % 8u] = v;
 }
 
 // ---- features from a rendered accum (inference on a scene's result) ----------------------------------------------
@@ -433,6 +561,8 @@ struct Net {
     float *pred = nullptr, *target = nullptr, *feat = nullptr, *loss = nullptr, *sums = nullptr, *rgb = nullptr;
     std::vector<void*> allocs;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
+    uint32_t* dev_err = nullptr;  // set by a convolution whose pipeline wait gave up
+    std::string conv_err;         // a tensor map that could not be made
 };
 
 }  // namespace unet
@@ -458,21 +588,63 @@ cudaError_t act(Net* n, Act& a, uint64_t pixels, uint32_t stride) {
 
 uint32_t blocks(uint64_t n, uint32_t b = 256) { return (uint32_t)((n + b - 1) / b); }
 
+// cuTensorMapEncodeTiled from the driver, found through the runtime (no libcuda link).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(f);
+    });
+    return fn;
+}
+
+// One convolution: x (NHWC bf16, x_stride channels a pixel, channels [x_off, x_off + cin) read) into y or yf.
+void conv_run(Net* n, const bf16* x, uint32_t x_stride, uint32_t x_off, uint32_t cin, const bf16* w, uint32_t co_pad,
+              const float* bias, bf16* y, uint32_t y_stride, uint32_t y_off, uint32_t cout, float* yf, uint32_t B,
+              uint32_t H, uint32_t W, int relu) {
+    uint32_t bw = 1;
+    while (bw < 128u && W % (bw * 2u) == 0u) bw *= 2u;
+    const uint32_t bh = 128u / bw, tiles_x = W / bw, tiles_y = (H + bh - 1u) / bh;
+    EncodeTiledFn enc = encode_tiled();
+    if (!enc) {
+        n->conv_err = "unet: cuTensorMapEncodeTiled is not available";
+        return;
+    }
+    CUtensorMap map;
+    cuuint64_t dims[4] = {x_stride, W, H, B};
+    cuuint64_t strides[3] = {(cuuint64_t)x_stride * 2u, (cuuint64_t)W * x_stride * 2u, (cuuint64_t)H * W * x_stride * 2u};
+    cuuint32_t box[4] = {8u, bw, bh, 1u}, es[4] = {1u, 1u, 1u, 1u};
+    CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16*>(x), dims, strides, box, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        n->conv_err = "unet: a convolution's tensor map was refused (" + std::to_string((int)r) + ")";
+        return;
+    }
+    const uint32_t nt = co_pad % 128u == 0u ? 128u : 64u;  // co_pad: a multiple of 64
+    Conv a{w, cin, co_pad, nt, bias, y, y_stride, y_off, cout, yf, B, H, W, x_off, bw, bh, tiles_x, tiles_y, relu,
+           n->dev_err};
+    k_conv<<<dim3(B * tiles_x * tiles_y, co_pad / nt), 128, CONV_SMEM, n->stream>>>(map, a);
+}
+
 void conv(Net* n, int li, const Act& x, uint32_t x_off, const Act& y, uint32_t y_off, uint32_t B, uint32_t H, uint32_t W,
           float* yf = nullptr) {
     const Layer& L = LAYERS[li];
-    Conv a{x.p, x.stride, x_off, L.cin, n->wf[li], r64(L.cout), n->w + n->off[li] + w_count(L),
-           y.p, y.stride, y_off, L.cout, yf, B, H, W, L.relu};
-    uint32_t M = B * H * W;
-    k_conv<<<dim3((M + CM - 1) / CM, r64(L.cout) / CN), 256, 0, n->stream>>>(a);
+    conv_run(n, x.p, x.stride, x_off, L.cin, n->wf[li], r64(L.cout), n->w + n->off[li] + w_count(L), y.p, y.stride,
+             y_off, L.cout, yf, B, H, W, L.relu);
 }
 // The input gradient of layer li: dx (channels [0, cin_logical)) from dy (cout rounded to 32 channels).
 void conv_dx(Net* n, int li, const Act& dy, const Act& dx, uint32_t B, uint32_t H, uint32_t W) {
     const Layer& L = LAYERS[li];
-    Conv a{dy.p, dy.stride, 0u, r32(L.cout), n->wb[li], r64(L.cin), nullptr, dx.p, dx.stride, 0u, L.cin, nullptr,
-           B, H, W, 0};
-    uint32_t M = B * H * W;
-    k_conv<<<dim3((M + CM - 1) / CM, r64(L.cin) / CN), 256, 0, n->stream>>>(a);
+    conv_run(n, dy.p, dy.stride, 0u, r32(L.cout), n->wb[li], r64(L.cin), nullptr, dx.p, dx.stride, 0u, L.cin, nullptr,
+             B, H, W, 0);
 }
 void wgrad(Net* n, int li, const Act& x, uint32_t x_off, const Act& dy, uint32_t B, uint32_t H, uint32_t W) {
     const Layer& L = LAYERS[li];
@@ -603,6 +775,28 @@ int cuda_check(Net* n, cudaError_t e, const char* what) {
     return TRT_ECUDA;
 }
 
+// The end of a call: its stream drained, then what its convolutions reported (a refused tensor map on the host, a
+// pipeline wait that gave up on the device).
+int finish(Net* n, const char* what) {
+    int rc = cuda_check(n, cudaStreamSynchronize(n->stream), what);
+    if (!rc) rc = cuda_check(n, cudaGetLastError(), what);
+    if (rc) return rc;
+    if (!n->conv_err.empty()) {
+        n->err = n->conv_err;
+        n->conv_err.clear();
+        return TRT_ECUDA;
+    }
+    uint32_t e = 0;
+    rc = cuda_check(n, cudaMemcpy(&e, n->dev_err, 4, cudaMemcpyDeviceToHost), what);
+    if (rc) return rc;
+    if (e) {
+        cudaMemset(n->dev_err, 0, 4);
+        n->err = std::string(what) + ": a convolution's pipeline wait gave up";
+        return TRT_ECUDA;
+    }
+    return TRT_OK;
+}
+
 }  // namespace
 }  // namespace unet
 
@@ -655,6 +849,8 @@ int trt_unet_create(int device, uint32_t max_batch, uint32_t max_h, uint32_t max
     if (e == cudaSuccess) e = alloc(n, &n->rgb, P0 * 3);
     if (e == cudaSuccess) e = alloc(n, &n->loss, 4);
     if (e == cudaSuccess) e = alloc(n, &n->sums, 4);
+    if (e == cudaSuccess) e = alloc(n, &n->dev_err, 1);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CONV_SMEM);
     if (e == cudaSuccess) e = cudaEventCreate(&n->e0);
     if (e == cudaSuccess) e = cudaEventCreate(&n->e1);
     if (e != cudaSuccess) {
@@ -710,7 +906,7 @@ int trt_unet_forward(trt_unet* n, const float* features, uint32_t B, uint32_t H,
     forward(n, B, H, W);
     cudaEventRecord(n->e1, n->stream);
     cudaMemcpyAsync(pred, n->pred, 12 * P, cudaMemcpyDeviceToHost, n->stream);
-    rc = cuda_check(n, cudaStreamSynchronize(n->stream), "trt_unet_forward");
+    rc = finish(n, "trt_unet_forward");
     if (!rc && ms) cudaEventElapsedTime(ms, n->e0, n->e1);
     return rc;
 }
@@ -743,7 +939,7 @@ int trt_unet_train_step(trt_unet* n, const float* features, const float* targets
     cudaEventRecord(n->e1, s);
     if (loss) cudaMemcpyAsync(loss, n->loss, 4, cudaMemcpyDeviceToHost, s);
     if (grads) cudaMemcpyAsync(grads, n->g, 4 * n->n_params, cudaMemcpyDeviceToHost, s);
-    rc = cuda_check(n, cudaStreamSynchronize(s), "trt_unet_train_step");
+    rc = finish(n, "trt_unet_train_step");
     if (!rc && ms) cudaEventElapsedTime(ms, n->e0, n->e1);
     return rc;
 }
@@ -763,7 +959,7 @@ int trt_unet_denoise_accum(trt_unet* n, const void* accum_device, uint32_t W, ui
     k_unfeat<<<blocks(P * 3), 256, 0, s>>>(n->pred, P, n->sums, n->rgb);
     cudaEventRecord(n->e1, s);
     cudaMemcpyAsync(rgb_host, n->rgb, 12 * P, cudaMemcpyDeviceToHost, s);
-    rc = cuda_check(n, cudaStreamSynchronize(s), "trt_unet_denoise_accum");
+    rc = finish(n, "trt_unet_denoise_accum");
     if (!rc && ms) cudaEventElapsedTime(ms, n->e0, n->e1);
     return rc;
 }
