@@ -10,6 +10,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -74,9 +75,11 @@ struct Conv {
     uint32_t* err;
 };
 
-constexpr uint32_t TS = 4;                  // pipeline stages
+constexpr uint32_t TS = 5;                  // pipeline stages (82 KB of shared memory: two CTAs an SM)
 constexpr uint32_t A_STAGE = 128u * 32u * 2u, B_STAGE = 128u * 32u * 2u;
 constexpr uint32_t CONV_SMEM = TS * (A_STAGE + B_STAGE) + 256u + 1024u;  // + room to align the stages to 1 KB
+constexpr uint32_t CONV_EPI_THREADS = 128u, CONV_THREADS = 64u + CONV_EPI_THREADS;  // loader, MMA, 4 epilogue warps
+constexpr uint32_t CONV_CTAS_PER_SM = 2u;
 
 __device__ __forceinline__ void mbar_init(uint32_t a, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count) : "memory");
@@ -93,12 +96,15 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t a, uint32_t parity) {
         : "memory");
     return ok != 0u;
 }
-// A bounded wait: about 2^31 cycles (a second at the B200's clock), then the error word.
-__device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity, uint32_t* err) {
+// A bounded wait: about 2^31 cycles (a second at the B200's clock), then the error word and the CTA's abort word,
+// which ends every other wait of the CTA at once.
+__device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity, uint32_t* err, volatile uint32_t* abort_flag) {
     long long t0 = clock64();
     while (!mbar_try_wait(a, parity)) {
+        if (*abort_flag) return false;
         if (clock64() - t0 > (1ll << 31)) {
             atomicOr(err, 1u);
+            *abort_flag = 1u;
             return false;
         }
     }
@@ -152,32 +158,38 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-__global__ void __launch_bounds__(128) k_conv(const __grid_constant__ CUtensorMap xmap, Conv a) {
+__global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ CUtensorMap xmap, Conv a) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
     const uint32_t sraw = smem_addr(smem_raw), sbase = (sraw + 1023u) & ~1023u;
     uint8_t* smem = smem_raw + (sbase - sraw);
     const uint32_t sA = sbase, sB = sbase + TS * A_STAGE, sBar = sbase + TS * (A_STAGE + B_STAGE);
-    // barriers: full[TS], empty[TS], done; then the tensor-memory address
+    // barriers: full[TS], empty[TS] (the stages), acc_full[2], acc_empty[2] (the accumulators); the tensor-memory
+    // address and the abort word after them
     auto full = [&](uint32_t s) { return sBar + 8u * s; };
     auto empty = [&](uint32_t s) { return sBar + 8u * (TS + s); };
-    const uint32_t done = sBar + 8u * (2u * TS);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + TS * (A_STAGE + B_STAGE) + 8u * (2u * TS + 1u));
-    const uint32_t per_img = a.tiles_x * a.tiles_y;
-    const uint32_t b = blockIdx.x / per_img, t = blockIdx.x % per_img;
-    const int x0 = (int)((t % a.tiles_x) * a.bw), y0 = (int)((t / a.tiles_x) * a.bh);
-    const uint32_t ncols = a.nt;  // 64 or 128 tensor-memory columns
-    const uint32_t n0 = blockIdx.y * a.nt;
+    auto acc_full = [&](uint32_t i) { return sBar + 8u * (2u * TS + i); };
+    auto acc_empty = [&](uint32_t i) { return sBar + 8u * (2u * TS + 2u + i); };
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + TS * (A_STAGE + B_STAGE) + 8u * (2u * TS + 4u));
+    volatile uint32_t* abort_flag = tslot + 1;
+    const uint32_t ncols = 2u * a.nt;  // two accumulators of nt columns: 128 or 256
+    const uint32_t per_img = a.tiles_x * a.tiles_y, n_ntiles = a.co_pad / a.nt;
+    const uint32_t tiles = a.B * per_img * n_ntiles;
+    const uint32_t kc = a.cin / 32u, nk = 9u * kc;
 
     if (tid == 0) {
         for (uint32_t s = 0; s < TS; ++s) {
             mbar_init(full(s), 1);
             mbar_init(empty(s), 1);
         }
-        mbar_init(done, 1);
+        for (uint32_t i = 0; i < 2u; ++i) {
+            mbar_init(acc_full(i), 1);
+            mbar_init(acc_empty(i), CONV_EPI_THREADS);
+        }
+        *abort_flag = 0u;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 0) {
+    if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tslot)),
                      "r"(ncols)
                      : "memory");
@@ -188,92 +200,125 @@ __global__ void __launch_bounds__(128) k_conv(const __grid_constant__ CUtensorMa
     tc_fence_after();
     const uint32_t tmem = *tslot;
 
-    const uint32_t kc = a.cin / 32u, nk = 9u * kc;
-    const uint32_t bbytes = 4u * a.nt * 16u;
-    bool ok = true;
+    // A tile: its image, its pixel rectangle, its output-channel slice.
+    auto tile_of = [&](uint32_t t, uint32_t& b, int& x0, int& y0, uint32_t& n0) {
+        const uint32_t nt_i = t % n_ntiles, pt = t / n_ntiles;
+        b = pt / per_img;
+        const uint32_t r = pt % per_img;
+        x0 = (int)((r % a.tiles_x) * a.bw);
+        y0 = (int)((r / a.tiles_x) * a.bh);
+        n0 = nt_i * a.nt;
+    };
+
     if (warp == 0) {
         if (lane == 0) {
-            // the loader
-            for (uint32_t k = 0; k < nk && ok; ++k) {
-                const uint32_t s = k % TS, round = k / TS;
-                if (k >= TS) ok = mbar_wait(empty(s), (round - 1u) & 1u, a.err);
-                if (!ok) break;
-                mbar_expect_tx(full(s), A_STAGE + bbytes);
-                const uint32_t tap = k / kc, c0 = (k % kc) * 32u;
-                const int dy = (int)(tap / 3u) - 1, dx = (int)(tap % 3u) - 1;
+            // the loader: the stages of every tile of this CTA, in order
+            uint32_t it = 0;
+            bool ok = true;
+            for (uint32_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+                uint32_t b, n0;
+                int x0, y0;
+                tile_of(t, b, x0, y0, n0);
+                for (uint32_t k = 0; k < nk; ++k, ++it) {
+                    const uint32_t s = it % TS;
+                    if (it >= TS && !(ok = mbar_wait(empty(s), ((it / TS) - 1u) & 1u, a.err, abort_flag))) break;
+                    mbar_expect_tx(full(s), A_STAGE + 4u * a.nt * 16u);
+                    const uint32_t tap = k / kc, c0 = (k % kc) * 32u;
+                    const int dy = (int)(tap / 3u) - 1, dx = (int)(tap % 3u) - 1;
 #pragma unroll
-                for (uint32_t j = 0; j < 4u; ++j)
-                    tma_load_4d(sA + s * A_STAGE + j * 2048u, &xmap, (int)(a.x_off + c0 + 8u * j), x0 + dx, y0 + dy,
-                                (int)b, full(s));
+                    for (uint32_t j = 0; j < 4u; ++j)
+                        tma_load_4d(sA + s * A_STAGE + j * 2048u, &xmap, (int)(a.x_off + c0 + 8u * j), x0 + dx,
+                                    y0 + dy, (int)b, full(s));
 #pragma unroll
-                for (uint32_t j = 0; j < 4u; ++j) {
-                    const bf16* src = a.w + (((uint64_t)tap * (a.cin / 8u) + c0 / 8u + j) * a.co_pad + n0) * 8u;
-                    bulk_load(sB + s * B_STAGE + j * a.nt * 16u, src, a.nt * 16u, full(s));
+                    for (uint32_t j = 0; j < 4u; ++j) {
+                        const bf16* src = a.w + (((uint64_t)tap * (a.cin / 8u) + c0 / 8u + j) * a.co_pad + n0) * 8u;
+                        bulk_load(sB + s * B_STAGE + j * a.nt * 16u, src, a.nt * 16u, full(s));
+                    }
                 }
             }
         }
     } else if (warp == 1) {
         if (lane == 0) {
-            // the MMA issuer
+            // the MMA issuer: a tile's stages into accumulator (tile count % 2), then that accumulator to the epilogue
             const uint32_t idesc = umma_idesc(128u, a.nt);
             const uint32_t lbo_b = a.nt * 16u;
-            for (uint32_t k = 0; k < nk && ok; ++k) {
-                const uint32_t s = k % TS;
-                ok = mbar_wait(full(s), (k / TS) & 1u, a.err);
-                if (!ok) break;
+            uint32_t it = 0, ti = 0;
+            bool ok = true;
+            for (uint32_t t = blockIdx.x; t < tiles && ok; t += gridDim.x, ++ti) {
+                const uint32_t acc = ti & 1u;
+                if (ti >= 2u && !(ok = mbar_wait(acc_empty(acc), ((ti / 2u) - 1u) & 1u, a.err, abort_flag))) break;
                 tc_fence_after();
+                const uint32_t d = tmem + acc * a.nt;
+                for (uint32_t k = 0; k < nk; ++k, ++it) {
+                    const uint32_t s = it % TS;
+                    if (!(ok = mbar_wait(full(s), (it / TS) & 1u, a.err, abort_flag))) break;
+                    tc_fence_after();
 #pragma unroll
-                for (uint32_t j = 0; j < 2u; ++j) {
-                    uint64_t ad = umma_desc(sA + s * A_STAGE + j * 2u * 2048u, 2048u, 128u);
-                    uint64_t bd = umma_desc(sB + s * B_STAGE + j * 2u * lbo_b, lbo_b, 128u);
-                    umma_f16(tmem, ad, bd, idesc, (k | j) != 0u ? 1u : 0u);
+                    for (uint32_t j = 0; j < 2u; ++j) {
+                        uint64_t ad = umma_desc(sA + s * A_STAGE + j * 2u * 2048u, 2048u, 128u);
+                        uint64_t bd = umma_desc(sB + s * B_STAGE + j * 2u * lbo_b, lbo_b, 128u);
+                        umma_f16(d, ad, bd, idesc, (k | j) != 0u ? 1u : 0u);
+                    }
+                    umma_commit(empty(s));
                 }
-                umma_commit(empty(s));
+                umma_commit(acc_full(acc));
             }
-            umma_commit(done);
+        }
+    } else {
+        // the epilogue: warp w reads tensor-memory lanes 32 (w % 4) ... (its rows: pixels of the tile)
+        const uint32_t quarter = warp & 3u;
+        const uint32_t m = quarter * 32u + lane;
+        uint32_t ti = 0;
+        for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x, ++ti) {
+            const uint32_t acc = ti & 1u;
+            const bool fin = mbar_wait(acc_full(acc), (ti / 2u) & 1u, a.err, abort_flag);
+            __syncwarp();
+            tc_fence_after();
+            uint32_t b, n0;
+            int x0, y0;
+            tile_of(t, b, x0, y0, n0);
+            const int px = x0 + (int)(m % a.bw), py = y0 + (int)(m / a.bw);
+            const bool valid = fin && px < (int)a.W && py < (int)a.H;
+            const uint64_t p = ((uint64_t)b * a.H + (uint32_t)py) * a.W + (uint32_t)px;
+            for (uint32_t cc = 0; cc < a.nt; cc += 16u) {
+                float v[16];
+                tmem_ld16(tmem + ((quarter * 32u) << 16) + acc * a.nt + cc, v);
+                const uint32_t c = n0 + cc;
+                if (!valid) continue;
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    if (a.bias) v[i] += a.bias[c + i];
+                    if (a.relu) v[i] = fmaxf(v[i], 0.0f);
+                }
+                if (a.yf) {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i)
+                        if (c + i < a.cout) a.yf[p * a.cout + c + i] = v[i];
+                } else if (c + 16u <= a.cout) {
+                    uint32_t pk[8];
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) {
+                        __nv_bfloat162 h2 = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+                        pk[i] = *reinterpret_cast<uint32_t*>(&h2);
+                    }
+                    uint4* dst = reinterpret_cast<uint4*>(a.y + p * a.y_stride + a.y_off + c);
+                    dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                    dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+                } else {
+                    for (int i = 0; i < 16; ++i)
+                        if (c + i < a.cout) a.y[p * a.y_stride + a.y_off + c + i] = __float2bfloat16_rn(v[i]);
+                }
+            }
+            // this accumulator is read: the MMA issuer may fill it again
+            tc_fence_before();
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(acc_empty(acc)) : "memory");
+            if (!fin) break;
         }
     }
     __syncwarp();
-    // the epilogue: every warp its 32 lanes (pixels) of the accumulator
-    bool fin = mbar_wait(done, 0u, a.err);
-    __syncwarp();
-    tc_fence_after();
-    const uint32_t m = warp * 32u + lane;
-    const int px = x0 + (int)(m % a.bw), py = y0 + (int)(m / a.bw);
-    const bool valid = fin && px < (int)a.W && py < (int)a.H;
-    const uint64_t p = ((uint64_t)b * a.H + (uint32_t)py) * a.W + (uint32_t)px;
-    for (uint32_t cc = 0; cc < a.nt; cc += 16u) {
-        float v[16];
-        tmem_ld16(tmem + ((warp * 32u) << 16) + cc, v);
-        const uint32_t c = n0 + cc;
-        if (!valid) continue;
-#pragma unroll
-        for (int i = 0; i < 16; ++i) {
-            if (a.bias) v[i] += a.bias[c + i];
-            if (a.relu) v[i] = fmaxf(v[i], 0.0f);
-        }
-        if (a.yf) {
-#pragma unroll
-            for (int i = 0; i < 16; ++i)
-                if (c + i < a.cout) a.yf[p * a.cout + c + i] = v[i];
-        } else if (c + 16u <= a.cout) {
-            uint32_t pk[8];
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                __nv_bfloat162 h2 = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
-                pk[i] = *reinterpret_cast<uint32_t*>(&h2);
-            }
-            uint4* dst = reinterpret_cast<uint4*>(a.y + p * a.y_stride + a.y_off + c);
-            dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-            dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
-        } else {
-            for (int i = 0; i < 16; ++i)
-                if (c + i < a.cout) a.y[p * a.y_stride + a.y_off + c + i] = __float2bfloat16_rn(v[i]);
-        }
-    }
     tc_fence_before();
     __syncthreads();
-    if (warp == 0)
+    if (warp == 1)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
 }
 
@@ -343,18 +388,33 @@ __global__ void __launch_bounds__(128) k_wgrad(WGrad a) {
 // 2 x 2 average pooling: y[b][y][x][c] = mean of x over the 2 x 2 block (H, W even).
 __global__ void k_pool(const bf16* x, uint32_t xs, uint32_t xo, bf16* y, uint32_t ys, uint32_t C, uint32_t B,
                        uint32_t H, uint32_t W) {
+    // 8 channels (16 bytes) a thread: C, the strides and the offsets are multiples of 32 channels
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    uint32_t h2 = H / 2, w2 = W / 2;
-    uint64_t n = (uint64_t)B * h2 * w2 * C;
+    const uint32_t h2 = H / 2, w2 = W / 2, c8 = C / 8u;
+    uint64_t n = (uint64_t)B * h2 * w2 * c8;
     if (i >= n) return;
-    uint32_t c = (uint32_t)(i % C);
-    uint64_t q = i / C;
+    uint32_t c = (uint32_t)(i % c8) * 8u;
+    uint64_t q = i / c8;
     uint32_t xx = (uint32_t)(q % w2), yy = (uint32_t)((q / w2) % h2), b = (uint32_t)(q / ((uint64_t)w2 * h2));
-    float s = 0.0f;
+    float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
     for (int j = 0; j < 2; ++j)
-        for (int k = 0; k < 2; ++k)
-            s += __bfloat162float(x[(((uint64_t)b * H + 2 * yy + j) * W + 2 * xx + k) * xs + xo + c]);
-    y[q * ys + c] = __float2bfloat16_rn(0.25f * s);
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            uint4 v = *reinterpret_cast<const uint4*>(x + (((uint64_t)b * H + 2 * yy + j) * W + 2 * xx + k) * xs + xo + c);
+            const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&v);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                float2 f = __bfloat1622float2(h[e]);
+                s[2 * e] += f.x;
+                s[2 * e + 1] += f.y;
+            }
+        }
+    uint4 o;
+    __nv_bfloat162* oh = reinterpret_cast<__nv_bfloat162*>(&o);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) oh[e] = __floats2bfloat162_rn(0.25f * s[2 * e], 0.25f * s[2 * e + 1]);
+    *reinterpret_cast<uint4*>(y + q * ys + c) = o;
 }
 // ... its gradient, added: dx[2y + j][2x + k] += dy[y][x] / 4.
 __global__ void k_pool_back(const bf16* dy, uint32_t dys, bf16* dx, uint32_t dxs, uint32_t dxo, uint32_t C, uint32_t B,
@@ -371,13 +431,16 @@ __global__ void k_pool_back(const bf16* dy, uint32_t dys, bf16* dx, uint32_t dxs
 }
 // Nearest 2x upsampling into channels [0, C) of y: y[2y + j][2x + k] = x[y][x].
 __global__ void k_up(const bf16* x, uint32_t xs, bf16* y, uint32_t ys, uint32_t C, uint32_t B, uint32_t H, uint32_t W) {
-    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;  // over the output (H, W: the output's)
-    uint64_t n = (uint64_t)B * H * W * C;
+    // over the output (H, W: the output's), 8 channels (16 bytes) a thread
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t c8 = C / 8u;
+    uint64_t n = (uint64_t)B * H * W * c8;
     if (i >= n) return;
-    uint32_t c = (uint32_t)(i % C);
-    uint64_t q = i / C;
+    uint32_t c = (uint32_t)(i % c8) * 8u;
+    uint64_t q = i / c8;
     uint32_t px = (uint32_t)(q % W), py = (uint32_t)((q / W) % H), b = (uint32_t)(q / ((uint64_t)W * H));
-    y[q * ys + c] = x[(((uint64_t)b * (H / 2) + py / 2) * (W / 2) + px / 2) * xs + c];
+    *reinterpret_cast<uint4*>(y + q * ys + c) =
+        *reinterpret_cast<const uint4*>(x + (((uint64_t)b * (H / 2) + py / 2) * (W / 2) + px / 2) * xs + c);
 }
 // ... its gradient: dx[y][x] = sum of dy over the 2 x 2 block (channels [0, C) of dy).
 __global__ void k_up_back(const bf16* dy, uint32_t dys, bf16* dx, uint32_t dxs, uint32_t C, uint32_t B, uint32_t H,
@@ -562,6 +625,7 @@ struct Net {
     std::vector<void*> allocs;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     uint32_t* dev_err = nullptr;  // set by a convolution whose pipeline wait gave up
+    uint32_t sms = 148;           // the device's SMs (the persistent convolution's grid)
     std::string conv_err;         // a tensor map that could not be made
 };
 
@@ -631,7 +695,9 @@ void conv_run(Net* n, const bf16* x, uint32_t x_stride, uint32_t x_off, uint32_t
     const uint32_t nt = co_pad % 128u == 0u ? 128u : 64u;  // co_pad: a multiple of 64
     Conv a{w, cin, co_pad, nt, bias, y, y_stride, y_off, cout, yf, B, H, W, x_off, bw, bh, tiles_x, tiles_y, relu,
            n->dev_err};
-    k_conv<<<dim3(B * tiles_x * tiles_y, co_pad / nt), 128, CONV_SMEM, n->stream>>>(map, a);
+    const uint32_t tiles = B * tiles_x * tiles_y * (co_pad / nt);
+    const uint32_t grid = std::min<uint32_t>(tiles, n->sms * CONV_CTAS_PER_SM);
+    k_conv<<<grid, CONV_THREADS, CONV_SMEM, n->stream>>>(map, a);
 }
 
 void conv(Net* n, int li, const Act& x, uint32_t x_off, const Act& y, uint32_t y_off, uint32_t B, uint32_t H, uint32_t W,
@@ -664,22 +730,22 @@ void forward(Net* n, uint32_t B, uint32_t H, uint32_t W) {
     uint64_t P0 = (uint64_t)B * H * W, P1 = (uint64_t)B * H1 * W1, P2 = (uint64_t)B * H2 * W2, P3 = (uint64_t)B * H3 * W3;
     conv(n, E0A, n->in0, 0, n->a0, 0, B, H, W);
     conv(n, E0B, n->a0, 0, n->cat0, 64, B, H, W);
-    k_pool<<<blocks(P1 * 32), 256, 0, s>>>(n->cat0.p, 96, 64, n->pool0.p, 32, 32, B, H, W);
+    k_pool<<<blocks(P1 * 32 / 8), 256, 0, s>>>(n->cat0.p, 96, 64, n->pool0.p, 32, 32, B, H, W);
     conv(n, E1A, n->pool0, 0, n->a1, 0, B, H1, W1);
     conv(n, E1B, n->a1, 0, n->cat1, 96, B, H1, W1);
-    k_pool<<<blocks(P2 * 64), 256, 0, s>>>(n->cat1.p, 160, 96, n->pool1.p, 64, 64, B, H1, W1);
+    k_pool<<<blocks(P2 * 64 / 8), 256, 0, s>>>(n->cat1.p, 160, 96, n->pool1.p, 64, 64, B, H1, W1);
     conv(n, E2A, n->pool1, 0, n->a2, 0, B, H2, W2);
     conv(n, E2B, n->a2, 0, n->cat2, 128, B, H2, W2);
-    k_pool<<<blocks(P3 * 96), 256, 0, s>>>(n->cat2.p, 224, 128, n->pool2.p, 96, 96, B, H2, W2);
+    k_pool<<<blocks(P3 * 96 / 8), 256, 0, s>>>(n->cat2.p, 224, 128, n->pool2.p, 96, 96, B, H2, W2);
     conv(n, E3A, n->pool2, 0, n->a3, 0, B, H3, W3);
     conv(n, E3B, n->a3, 0, n->b3, 0, B, H3, W3);
-    k_up<<<blocks(P2 * 128), 256, 0, s>>>(n->b3.p, 128, n->cat2.p, 224, 128, B, H2, W2);
+    k_up<<<blocks(P2 * 128 / 8), 256, 0, s>>>(n->b3.p, 128, n->cat2.p, 224, 128, B, H2, W2);
     conv(n, D2A, n->cat2, 0, n->t2, 0, B, H2, W2);
     conv(n, D2B, n->t2, 0, n->u2, 0, B, H2, W2);
-    k_up<<<blocks(P1 * 96), 256, 0, s>>>(n->u2.p, 96, n->cat1.p, 160, 96, B, H1, W1);
+    k_up<<<blocks(P1 * 96 / 8), 256, 0, s>>>(n->u2.p, 96, n->cat1.p, 160, 96, B, H1, W1);
     conv(n, D1A, n->cat1, 0, n->t1, 0, B, H1, W1);
     conv(n, D1B, n->t1, 0, n->u1, 0, B, H1, W1);
-    k_up<<<blocks(P0 * 64), 256, 0, s>>>(n->u1.p, 64, n->cat0.p, 96, 64, B, H, W);
+    k_up<<<blocks(P0 * 64 / 8), 256, 0, s>>>(n->u1.p, 64, n->cat0.p, 96, 64, B, H, W);
     conv(n, D0A, n->cat0, 0, n->t0, 0, B, H, W);
     conv(n, D0B, n->t0, 0, n->u0, 0, B, H, W);
     conv(n, OUT, n->u0, 0, Act{}, 0, B, H, W, n->pred);
@@ -851,6 +917,11 @@ int trt_unet_create(int device, uint32_t max_batch, uint32_t max_h, uint32_t max
     if (e == cudaSuccess) e = alloc(n, &n->sums, 4);
     if (e == cudaSuccess) e = alloc(n, &n->dev_err, 1);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CONV_SMEM);
+    if (e == cudaSuccess) {
+        int sms = 0;
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        if (sms > 0) n->sms = (uint32_t)sms;
+    }
     if (e == cudaSuccess) e = cudaEventCreate(&n->e0);
     if (e == cudaSuccess) e = cudaEventCreate(&n->e1);
     if (e != cudaSuccess) {
