@@ -50,10 +50,10 @@ __device__ __forceinline__ void mma16816(float* c, uint32_t a0, uint32_t a1, uin
 // A CTA computes a tile of 128 pixels (a bw x bh rectangle of one image, bw the largest power of two <= 128 that
 // divides the width) x N output channels (N 128 where 128 divides co_pad, else 64; blockIdx.y their tile) on the
 // 5th-generation tensor cores:
-//  - one thread issues the loads: per K stage (one tap, 32 input channels) four TMA boxes of 8 channels x bw x bh
-//    pixels, shifted by the tap (the halo and the image's border read as zeros), and four bulk copies of the stage's
-//    weights (N rows of each 8-channel chunk); each lands in the canonical K-major layout without swizzle (8-row x
-//    16-byte core matrices);
+//  - one thread issues the loads: per K stage (one tap, 32 input channels) a TMA box of 32 channels x bw x bh pixels,
+//    shifted by the tap (the halo and the image's border read as zeros), and a TMA box of the tap's weights (N
+//    output channels x the 32 input channels); both land as 64-byte rows with the 64-byte swizzle, the canonical
+//    K-major layout the MMA reads (8-row atoms of 512 bytes);
 //  - one thread issues two tcgen05.mma (M 128, N, K 16, bf16 in, f32 accumulate in tensor memory) a stage and
 //    commits each stage's buffers back to the loader through an mbarrier; TS stages in flight;
 //  - the four warps read the accumulator out of tensor memory (each its 32 lanes = pixels), add the bias, apply the
@@ -61,7 +61,6 @@ __device__ __forceinline__ void mma16816(float* c, uint32_t a0, uint32_t a1, uin
 // Every mbarrier wait is bounded (about a second); a wait that gives up sets the error word and the CTA finishes.
 
 struct Conv {
-    const bf16* w;            // [9][cin / 8][co_pad][8]: per tap and 8-channel chunk, co_pad rows of 8 channels
     uint32_t cin;             // channels read (a multiple of 32)
     uint32_t co_pad;          // a multiple of 64 (up to 256)
     uint32_t nt;              // output channels a CTA: 128 where they divide co_pad, else 64 (blockIdx.y the tile)
@@ -118,16 +117,19 @@ __device__ __forceinline__ void tma_load_4d(uint32_t dst, const void* map, int c
         "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(mbar)
         : "memory");
 }
-__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-                 "l"((uint64_t)src), "r"(bytes), "r"(mbar)
-                 : "memory");
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const void* map, int c0, int c1, int c2, uint32_t mbar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+            dst),
+        "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(mbar)
+        : "memory");
 }
-// The canonical K-major shared-memory matrix without swizzle: core matrices of 8 rows x 16 bytes, `lbo` bytes apart
-// along K, `sbo` bytes apart along M / N; descriptor version 1 (sm_100).
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
-    return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
-           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+// The canonical K-major shared-memory matrix with the 64-byte swizzle: rows of 64 bytes (32 bf16 of K), atoms of 8
+// rows (512 bytes) `sbo` bytes apart along M / N; the leading offset unused (1); descriptor version 1 (sm_100),
+// layout type 4 (SWIZZLE_64B). A K step of 16 inside the row advances the start by 32 bytes.
+__device__ __forceinline__ uint64_t umma_desc_sw64(uint32_t saddr, uint32_t sbo) {
+    return (uint64_t)((saddr & 0x3FFFFu) >> 4) | (1ull << 16) | ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) |
+           (1ull << 46) | (4ull << 61);
 }
 // kind::f16 instruction descriptor: f32 accumulator, bf16 A and B, both K-major, M x N.
 __host__ __device__ constexpr uint32_t umma_idesc(uint32_t M, uint32_t N) {
@@ -158,7 +160,8 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-__global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ CUtensorMap xmap, Conv a) {
+__global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ CUtensorMap xmap,
+                                                       const __grid_constant__ CUtensorMap wmap, Conv a) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
     const uint32_t sraw = smem_addr(smem_raw), sbase = (sraw + 1023u) & ~1023u;
@@ -222,18 +225,11 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ C
                 for (uint32_t k = 0; k < nk; ++k, ++it) {
                     const uint32_t s = it % TS;
                     if (it >= TS && !(ok = mbar_wait(empty(s), ((it / TS) - 1u) & 1u, a.err, abort_flag))) break;
-                    mbar_expect_tx(full(s), A_STAGE + 4u * a.nt * 16u);
+                    mbar_expect_tx(full(s), A_STAGE + a.nt * 64u);
                     const uint32_t tap = k / kc, c0 = (k % kc) * 32u;
                     const int dy = (int)(tap / 3u) - 1, dx = (int)(tap % 3u) - 1;
-#pragma unroll
-                    for (uint32_t j = 0; j < 4u; ++j)
-                        tma_load_4d(sA + s * A_STAGE + j * 2048u, &xmap, (int)(a.x_off + c0 + 8u * j), x0 + dx,
-                                    y0 + dy, (int)b, full(s));
-#pragma unroll
-                    for (uint32_t j = 0; j < 4u; ++j) {
-                        const bf16* src = a.w + (((uint64_t)tap * (a.cin / 8u) + c0 / 8u + j) * a.co_pad + n0) * 8u;
-                        bulk_load(sB + s * B_STAGE + j * a.nt * 16u, src, a.nt * 16u, full(s));
-                    }
+                    tma_load_4d(sA + s * A_STAGE, &xmap, (int)(a.x_off + c0), x0 + dx, y0 + dy, (int)b, full(s));
+                    tma_load_3d(sB + s * B_STAGE, &wmap, (int)c0, (int)n0, (int)tap, full(s));
                 }
             }
         }
@@ -241,7 +237,6 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ C
         if (lane == 0) {
             // the MMA issuer: a tile's stages into accumulator (tile count % 2), then that accumulator to the epilogue
             const uint32_t idesc = umma_idesc(128u, a.nt);
-            const uint32_t lbo_b = a.nt * 16u;
             uint32_t it = 0, ti = 0;
             bool ok = true;
             for (uint32_t t = blockIdx.x; t < tiles && ok; t += gridDim.x, ++ti) {
@@ -255,8 +250,8 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ C
                     tc_fence_after();
 #pragma unroll
                     for (uint32_t j = 0; j < 2u; ++j) {
-                        uint64_t ad = umma_desc(sA + s * A_STAGE + j * 2u * 2048u, 2048u, 128u);
-                        uint64_t bd = umma_desc(sB + s * B_STAGE + j * 2u * lbo_b, lbo_b, 128u);
+                        uint64_t ad = umma_desc_sw64(sA + s * A_STAGE + j * 32u, 512u);
+                        uint64_t bd = umma_desc_sw64(sB + s * B_STAGE + j * 32u, 512u);
                         umma_f16(d, ad, bd, idesc, (k | j) != 0u ? 1u : 0u);
                     }
                     umma_commit(empty(s));
@@ -507,10 +502,9 @@ __global__ void k_adam(float* w, const float* g, float* m, float* v, uint64_t n,
     v[i] = vi;
     w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
 }
-// The bf16 weights of a layer from its f32 masters w[t][c][n], laid out as the convolution's B operand (per tap and
-// 8-channel chunk of its input, the output channels' rows of 8 input channels): forward [t][c / 8][n][c % 8] (c <
-// cin, n < co_pad), and the input gradient's [8 - t][n / 8][c][n % 8] (n < cout32: the output gradient's channels, its
-// input; c < cin of ci_pad64 rows, its output).
+// The bf16 weights of a layer from its f32 masters w[t][c][n], laid out as the convolution's B operand (per tap, the
+// output channels' rows of input channels): forward [t][n][c] (n < co_pad rows of cin), and the input gradient's
+// [8 - t][c][n] (c < cin of ci_pad64 rows: its output; n < cout32: the output gradient's channels, its input).
 __global__ void k_weights(const float* wf, uint32_t cin, uint32_t co_pad, uint32_t cout32, bf16* wfw, bf16* wbw,
                           uint32_t ci_pad64) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -518,9 +512,8 @@ __global__ void k_weights(const float* wf, uint32_t cin, uint32_t co_pad, uint32
     if (i >= n) return;
     uint32_t nn = (uint32_t)(i % co_pad), c = (uint32_t)((i / co_pad) % cin), t = (uint32_t)(i / ((uint64_t)co_pad * cin));
     bf16 v = __float2bfloat16_rn(wf[i]);
-    wfw[(((uint64_t)t * (cin / 8u) + c / 8u) * co_pad + nn) * 8u + c % 8u] = v;
-    if (wbw && nn < cout32)
-        wbw[(((uint64_t)(8 - t) * (cout32 / 8u) + nn / 8u) * ci_pad64 + c) * 8u + nn % 8u] = v;
+    wfw[((uint64_t)t * co_pad + nn) * cin + c] = v;
+    if (wbw && nn < cout32) wbw[((uint64_t)(8 - t) * ci_pad64 + c) * cout32 + nn] = v;
 }
 
 // ---- features from a rendered accum (inference on a scene's result) ----------------------------------------------
@@ -669,35 +662,45 @@ EncodeTiledFn encode_tiled() {
     return fn;
 }
 
-// One convolution: x (NHWC bf16, x_stride channels a pixel, channels [x_off, x_off + cin) read) into y or yf.
+// One convolution: x (NHWC bf16, x_stride channels a pixel, channels [x_off, x_off + cin) read) into y or yf, with
+// w [9][co_pad][cin] (each tap's output channels, their input channels contiguous).
 void conv_run(Net* n, const bf16* x, uint32_t x_stride, uint32_t x_off, uint32_t cin, const bf16* w, uint32_t co_pad,
               const float* bias, bf16* y, uint32_t y_stride, uint32_t y_off, uint32_t cout, float* yf, uint32_t B,
               uint32_t H, uint32_t W, int relu) {
     uint32_t bw = 1;
     while (bw < 128u && W % (bw * 2u) == 0u) bw *= 2u;
     const uint32_t bh = 128u / bw, tiles_x = W / bw, tiles_y = (H + bh - 1u) / bh;
+    const uint32_t nt = co_pad % 128u == 0u ? 128u : 64u;  // co_pad: a multiple of 64
     EncodeTiledFn enc = encode_tiled();
     if (!enc) {
         n->conv_err = "unet: cuTensorMapEncodeTiled is not available";
         return;
     }
-    CUtensorMap map;
-    cuuint64_t dims[4] = {x_stride, W, H, B};
-    cuuint64_t strides[3] = {(cuuint64_t)x_stride * 2u, (cuuint64_t)W * x_stride * 2u, (cuuint64_t)H * W * x_stride * 2u};
-    cuuint32_t box[4] = {8u, bw, bh, 1u}, es[4] = {1u, 1u, 1u, 1u};
-    CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16*>(x), dims, strides, box, es,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+    // the activations: (channels, x, y, image), boxes of 32 channels x bw x bh; the weights: (input channel, output
+    // channel, tap), boxes of 32 x nt x 1; both 64-byte rows with the 64-byte swizzle
+    CUtensorMap xmap, wmap;
+    cuuint64_t xd[4] = {x_stride, W, H, B};
+    cuuint64_t xs[3] = {(cuuint64_t)x_stride * 2u, (cuuint64_t)W * x_stride * 2u, (cuuint64_t)H * W * x_stride * 2u};
+    cuuint32_t xb[4] = {32u, bw, bh, 1u}, es[4] = {1u, 1u, 1u, 1u};
+    cuuint64_t wd[3] = {cin, co_pad, 9u};
+    cuuint64_t ws[2] = {(cuuint64_t)cin * 2u, (cuuint64_t)co_pad * cin * 2u};
+    cuuint32_t wb[3] = {32u, nt, 1u};
+    CUresult r = enc(&xmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16*>(x), xd, xs, xb, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r == CUDA_SUCCESS)
+        r = enc(&wmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<bf16*>(w), wd, ws, wb, es,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
         n->conv_err = "unet: a convolution's tensor map was refused (" + std::to_string((int)r) + ")";
         return;
     }
-    const uint32_t nt = co_pad % 128u == 0u ? 128u : 64u;  // co_pad: a multiple of 64
-    Conv a{w, cin, co_pad, nt, bias, y, y_stride, y_off, cout, yf, B, H, W, x_off, bw, bh, tiles_x, tiles_y, relu,
+    Conv a{cin, co_pad, nt, bias, y, y_stride, y_off, cout, yf, B, H, W, x_off, bw, bh, tiles_x, tiles_y, relu,
            n->dev_err};
     const uint32_t tiles = B * tiles_x * tiles_y * (co_pad / nt);
     const uint32_t grid = std::min<uint32_t>(tiles, n->sms * CONV_CTAS_PER_SM);
-    k_conv<<<grid, CONV_THREADS, CONV_SMEM, n->stream>>>(map, a);
+    k_conv<<<grid, CONV_THREADS, CONV_SMEM, n->stream>>>(xmap, wmap, a);
 }
 
 void conv(Net* n, int li, const Act& x, uint32_t x_off, const Act& y, uint32_t y_off, uint32_t B, uint32_t H, uint32_t W,
