@@ -3,9 +3,10 @@
 // no counterpart in the reference (whose learned denoiser is the external OIDN library, renderer/src/denoise.rs:80-103).
 //
 // Tensors are NHWC bf16 with channel counts padded to multiples of 32; a convolution is an implicit GEMM (M = pixels,
-// N = output channels, K = 9 taps x input channels) on bf16 tensor-core MMAs with f32 accumulation. The input gradient
-// is the same kernel run on the output gradient with the weights flipped and transposed; the weight gradient is a GEMM
-// over pixels (split across CTAs, summed with f32 atomics). Master weights, gradients and Adam's moments are f32.
+// N = output channels, K = 9 taps x input channels) on the 5th-generation tensor cores (TMA loads, tcgen05.mma into
+// tensor memory, f32 accumulation). The input gradient is the same kernel run on the output gradient with the
+// weights flipped and transposed; the weight gradient is a GEMM over pixels on mma.sync (split across CTAs, summed
+// with f32 atomics). Master weights, gradients and Adam's moments are f32.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -24,7 +25,7 @@ namespace unet {
 
 typedef __nv_bfloat16 bf16;
 
-// ---- tensor-core fragments (mma.sync m16n8k16, bf16 in, f32 accumulate) ---------------------------------------------
+// ---- tensor-core fragments of the weight gradient (mma.sync m16n8k16, bf16 in, f32 accumulate) ---------------------
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
