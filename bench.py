@@ -353,9 +353,11 @@ def serve_scenes():
 def run_serve(args, rank, world, local):
     """The serving loop on one GPU (replicas beyond: each rank serves its own stream). The mix: each request a
     scene, a resolution of {256^2, 512^2, 1280x720, 1920x1080} and 1, 16 or 64 spp, depth 4, arriving as a seeded
-    Poisson stream; then a stream of 720p 1-spp requests. Each stream is also rendered one request at a time
-    (trt_render and its read-back) as the reference's serve loop does: the baseline of the ratio."""
-    from threert_b200 import Gpu
+    Poisson stream; then a stream of 720p 1-spp requests. Requests of at most 4 samples get the learned denoiser
+    (configs' serving mix): the server denoises them on the device and returns the image. Each stream is also
+    rendered one request at a time (trt_render, the denoiser where asked, the read-back) as the reference's serve loop
+    does: the baseline of the ratio."""
+    from threert_b200 import Gpu, unet
     from threert_b200 import serve as SV
     from threert_b200.prep import params_with
     Ps = serve_scenes()
@@ -367,33 +369,42 @@ def run_serve(args, rank, world, local):
     tune_reqs = SV.mix_requests(bases, 24, seed=100 + rank, spps=[1, 16])
     best, trials = SV.autotune(gpu, S, tune_reqs)
     log(f"autotune: {trials} -> {best}")
-    srv = SV.Server(gpu, wave_slots=best["wave_slots"], flags=best["flags"])
+    net = unet.UNet(local, max_batch=1, max_h=1080, max_w=1920)
+    net.set_params(np.load(args.denoiser_params) if args.denoiser_params else unet.init_params(0))
+    srv = SV.Server(gpu, wave_slots=best["wave_slots"], flags=best["flags"], denoiser=net)
+    same = lambda rs: [SV.Request(r.scene, r.params, r.spp, denoise=r.denoise) for r in rs]
     warm = SV.mix_requests(bases, 8, seed=200 + rank, spps=[1])
     SV.run_stream(srv, S, warm, rate=0.0)
-    mix = SV.mix_requests(bases, args.requests, seed=300 + rank)
+    mix = SV.mix_requests(bases, args.requests, seed=300 + rank, denoise_max_spp=4)
     res = SV.run_stream(srv, S, mix, rate=args.rate, seed=400 + rank, keep=False)
-    serial = SV.run_serial(gpu, S, [SV.Request(r.scene, r.params, r.spp) for r in mix])
+    serial = SV.run_serial(gpu, S, same(mix), denoiser=net)
     log(f"mix: served {res}, serial {serial}")
     # 720p, 1 spp, over the three cities: the latency stream.
     rng = np.random.default_rng(500 + rank)
-    hd = [SV.Request(int(k), params_with(bases[int(k)], max_bounces=DEPTH), 1) for k in rng.integers(2, 5, args.requests)]
+    hd = [SV.Request(int(k), params_with(bases[int(k)], max_bounces=DEPTH), 1, denoise=True)
+          for k in rng.integers(2, 5, args.requests)]
     res_hd = SV.run_stream(srv, S, hd, rate=args.rate_720p, seed=600 + rank, keep=False)
     # ... and the same requests all at once (throughput at saturation) against one at a time.
-    sat_hd = SV.run_stream(srv, S, [SV.Request(r.scene, r.params, r.spp) for r in hd], rate=0.0, keep=False)
-    serial_hd = SV.run_serial(gpu, S, [SV.Request(r.scene, r.params, r.spp) for r in hd])
+    sat_hd = SV.run_stream(srv, S, same(hd), rate=0.0, keep=False)
+    serial_hd = SV.run_serial(gpu, S, same(hd), denoiser=net)
     # 256 x 256, 1 spp over all eight scenes, as fast as they come: where one-at-a-time rendering idles the GPU.
-    small = [SV.Request(int(k), params_with(bases[int(k)], width=256, height=256, max_bounces=DEPTH), 1)
+    small = [SV.Request(int(k), params_with(bases[int(k)], width=256, height=256, max_bounces=DEPTH), 1, denoise=True)
              for k in rng.integers(0, 8, 4 * args.requests)]
     res_small = SV.run_stream(srv, S, small, rate=args.rate_small, seed=700 + rank, keep=False)
-    serial_small = SV.run_serial(gpu, S, [SV.Request(r.scene, r.params, r.spp) for r in small])
+    serial_small = SV.run_serial(gpu, S, same(small), denoiser=net)
     srv.close()
+    net.close()
     line = {
         "metric": SERVE_METRIC, "value": res["mrays_per_s"] * world, "unit": "Mrays/s", "n_gpus": world,
         "steps": res["steps"], "warmup": len(warm), "ms_per_step": res["busy_s"] * 1e3 / max(1, res["steps"]),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"serving mix: {args.requests} requests at {args.rate} req/s Poisson over 8 resident "
                                "scenes (2 Cornell, 3 city, 3 crowd)", "device": name, "sms": sms,
-                   "autotuned": best, "autotune_trials": trials, "parallelism": f"replicas x{world}"},
+                   "autotuned": best, "autotune_trials": trials, "parallelism": f"replicas x{world}",
+                   "denoiser": "the learned U-Net on requests of <= 4 spp (" +
+                               (f"parameters {args.denoiser_params}" if args.denoiser_params else
+                                "initial parameters: timing only") + ")",
+                   "denoised": int(sum(r.denoise for r in mix))},
         "p50_ms": res["p50_ms"], "p99_ms": res["p99_ms"], "span_s": res["span_s"],
         "serial": {"mrays_per_s": serial["mrays_per_s"], "span_s": serial["span_s"]},
         "speedup_over_serial": res["mrays_per_s"] / serial["mrays_per_s"],
@@ -408,8 +419,9 @@ def run_serve(args, rank, world, local):
                             "serial_mrays_per_s": serial_small["mrays_per_s"],
                             "serial_p50_ms": serial_small["p50_ms"],
                             "speedup_over_serial": res_small["mrays_per_s"] / serial_small["mrays_per_s"]},
-        "e2e": {"value": res["mrays_per_s"] * world, "unit": "Mrays/s",
-                "h2d_bytes_per_step": 624, "d2h_bytes_per_step": int(np.mean([80 * int(r.params[16]) * int(r.params[17]) for r in mix]))},
+        "e2e": {"value": res["mrays_per_s"] * world, "unit": "Mrays/s", "h2d_bytes_per_step": 624,
+                "d2h_bytes_per_step": int(np.mean([(12 if r.denoise else 80) * int(r.params[16]) * int(r.params[17])
+                                                   for r in mix]))},
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -551,6 +563,7 @@ def main():
     ap.add_argument("--views", type=int, default=16, help="denoise: views of each")
     ap.add_argument("--train-steps", type=int, default=20000, help="denoise: Adam steps")
     ap.add_argument("--save", default="", help="denoise: where to save the trained parameters (.npy)")
+    ap.add_argument("--denoiser-params", default="", help="serve: the learned denoiser's parameters (.npy)")
     ap.add_argument("--requests", type=int, default=64, help="serve: requests a stream")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: the mix's arrival rate (requests a second)")
     ap.add_argument("--rate-720p", type=float, default=60.0, help="serve: the 720p stream's arrival rate")

@@ -271,6 +271,9 @@ typedef struct {
     uint32_t flags;        /* TRT_RENDER_UNSORTED_HITS / TRT_RENDER_SORT_* for every step */
     uint32_t launch_mode;  /* 0: each step's launches replayed from a CUDA graph captured once per (depth, size
                             * class); 1: launched one by one */
+    trt_unet* denoiser;    /* NULL, or the learned denoiser for requests of few samples (trt_server_submit_rgb); the
+                            * server owns it until destroyed: no other call may use it meanwhile */
+    uint32_t denoise_max_spp; /* the most samples a request may have to be denoised (0: 4) */
 } trt_server_options;
 typedef struct {
     uint64_t id;
@@ -291,6 +294,12 @@ void trt_server_destroy(trt_server* server);
  * reported done. The Params are checked here (TRT_EINVAL). Thread-safe. */
 int trt_server_submit(trt_server* server, trt_scene* scene, const uint32_t params[TRT_PARAMS_WORDS], uint32_t spp,
                       float* accum_host, uint64_t* id);
+/* A request whose result is also (or only) the denoised image (configs' serving mix: the denoiser on for spp <= 4):
+ * rendered with the first-hit depth (TRT_RENDER_DEPTH), its accum denoised on the device by the server's network when
+ * its samples are done, rgb_host (w * h * 3 floats) receiving the image. accum_host may be NULL. TRT_EINVAL without a
+ * denoiser, above denoise_max_spp samples, or at a size the network does not take. */
+int trt_server_submit_rgb(trt_server* server, trt_scene* scene, const uint32_t params[TRT_PARAMS_WORDS], uint32_t spp,
+                          float* accum_host, float* rgb_host, uint64_t* id);
 /* Up to cap finished requests since the last call, waiting up to wait_ms for one if none is ready. */
 int trt_server_poll(trt_server* server, trt_request_done* done, uint32_t cap, uint32_t* n, uint32_t wait_ms);
 int trt_server_stats_get(trt_server* server, trt_server_stats* out);

@@ -83,3 +83,40 @@ def test_what_cannot_be_served_is_refused(gpu, resident):
             srv.submit(S[0], Request(0, bad, 1))
     finally:
         srv.close()
+
+
+def test_denoised_requests_are_the_denoise_of_their_render_alone(gpu, resident):
+    """The serving mix's denoiser (configs: on for spp <= 4): a request submitted for its denoised image gets what the
+    learned denoiser makes of the same request rendered alone with its depth guide, bit for bit, beside requests that
+    are not denoised; what the network cannot take is refused."""
+    from threert_b200 import unet
+    from threert_b200 import _native as N
+    Ps, S = resident
+    net = unet.UNet(0, max_batch=1, max_h=64, max_w=64)
+    net.set_params(unet.init_params(11))
+    sizes = [(16, 16), (40, 24), (64, 32), (48, 48)]
+    reqs = []
+    for i in range(10):
+        k = i % len(Ps)
+        w, h = sizes[i % len(sizes)]
+        spp = [1, 2, 4, 8][i % 4]
+        reqs.append(Request(k, params_with(Ps[k].params, width=w, height=h), spp, denoise=spp <= 4))
+    srv = Server(gpu, wave_slots=16384, max_active=8, denoiser=net)
+    try:
+        res = run_stream(srv, S, reqs, rate=0.0)
+        with pytest.raises(RenderError):  # more samples than the server denoises
+            srv.submit(S[0], Request(0, params_with(Ps[0].params, width=16, height=16), 8, denoise=True))
+        with pytest.raises(RenderError):  # not a multiple of 8
+            srv.submit(S[0], Request(0, params_with(Ps[0].params, width=20, height=16), 1, denoise=True))
+    finally:
+        srv.close()
+    assert res["failed"] == 0
+    for r in reqs:
+        w, h = int(r.params[16]), int(r.params[17])
+        if r.denoise:
+            S[r.scene].render_raw(r.params, r.spp, flags=N.TRT_RENDER_DEPTH, read=False)
+            alone, _ = net.denoise(S[r.scene])
+            assert r.accum is None and np.array_equal(r.rgb.reshape(h, w, 3), alone), (r.scene, w, h, r.spp)
+        else:
+            assert np.array_equal(r.accum, S[r.scene].render_raw(r.params, r.spp)[0])
+    net.close()

@@ -133,7 +133,8 @@ TRT_CORNER_NORMAL = 1
 TRT_CORNER_TANGENT = 2
 
 class ServerOptions(C.Structure):
-    _fields_ = [("wave_slots", u32), ("max_active", u32), ("hbm_reserve", u64), ("flags", u32), ("launch_mode", u32)]
+    _fields_ = [("wave_slots", u32), ("max_active", u32), ("hbm_reserve", u64), ("flags", u32), ("launch_mode", u32),
+                ("denoiser", C.c_void_p), ("denoise_max_spp", u32)]
 
 
 class RequestDone(C.Structure):
@@ -200,6 +201,7 @@ SIGNATURES = [
     ("trt_server_create", C.c_int, [C.c_void_p, P(ServerOptions), P(C.c_void_p)]),
     ("trt_server_destroy", None, [C.c_void_p]),
     ("trt_server_submit", C.c_int, [C.c_void_p, C.c_void_p, P(u32), u32, P(f32), P(u64)]),
+    ("trt_server_submit_rgb", C.c_int, [C.c_void_p, C.c_void_p, P(u32), u32, P(f32), P(f32), P(u64)]),
     ("trt_server_poll", C.c_int, [C.c_void_p, P(RequestDone), u32, P(u32), u32]),
     ("trt_server_stats_get", C.c_int, [C.c_void_p, P(ServerStats)]),
     ("trt_unet_create", C.c_int, [C.c_int, u32, u32, u32, P(C.c_void_p)]),

@@ -37,6 +37,7 @@
 #define TRT_BLOCKS_SHADE 6
 #endif
 #include "sky.h"
+#include "unet.h"
 #include "shade.cuh"
 #include "denoise.cuh"
 #include "threert_cuda.h"

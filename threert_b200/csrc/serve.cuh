@@ -21,7 +21,8 @@ struct ServeRequest {
     trt_scene* scene = nullptr;
     Params P{};
     uint32_t spp = 0, issued = 0, n_idx = 0, w = 0, h = 0, steps = 0;
-    float* host = nullptr;
+    float* host = nullptr;     // the accum's host buffer, or null
+    float* rgb = nullptr;      // the denoised image's host buffer, or null
     float4* accum = nullptr;
     uint64_t accum_bytes = 0;
     double t_submit = 0, t_start = -1;
@@ -163,6 +164,7 @@ bool serve_step(trt_server* s, ServeStep& step) {
             if (k == 0) continue;  // not enough slots left in this step: a smaller request may still fit
             Job j{r->P, Walk{scene_view(r->scene), WideView{}, r->P.w[P_MOTION + 2], r->P.w[P_MOTION + 3]}, r->accum,
                   slot, r->n_idx, k, r->issued};
+            j.depth = r->rgb ? 1u : 0u;  // the denoiser's depth guide
             jobs.push_back(j);
             owners.push_back(r);
             if (r->t_start < 0) r->t_start = serve_now(s);
@@ -241,7 +243,14 @@ void serve_retire(trt_server* s, ServeStep& step) {
         }
         if (!ev) cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
         cudaError_t e = cudaStreamWaitEvent(s->copy, step.t1, 0);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(r->host, r->accum, r->accum_bytes, cudaMemcpyDeviceToHost, s->copy);
+        if (e == cudaSuccess && r->rgb) {
+            // the learned denoiser on the copy stream, beside the next step's kernels
+            const float* rgb = unet_denoise_on_stream(s->opt.denoiser, r->accum, r->w, r->h, s->copy);
+            if (!rgb) r->status = TRT_ECUDA;
+            else e = cudaMemcpyAsync(r->rgb, rgb, 12ull * r->w * r->h, cudaMemcpyDeviceToHost, s->copy);
+        }
+        if (e == cudaSuccess && r->host)
+            e = cudaMemcpyAsync(r->host, r->accum, r->accum_bytes, cudaMemcpyDeviceToHost, s->copy);
         if (e == cudaSuccess) e = cudaEventRecord(ev, s->copy);
         r->copied = ev;
         if (e != cudaSuccess) r->status = TRT_ECUDA;
@@ -395,7 +404,23 @@ void trt_server_destroy(trt_server* s) {
 
 int trt_server_submit(trt_server* s, trt_scene* scene, const uint32_t params[TRT_PARAMS_WORDS], uint32_t spp,
                       float* accum_host, uint64_t* id) {
-    if (!s || !scene || !params || !accum_host || spp == 0) return TRT_EINVAL;
+    if (!accum_host) return TRT_EINVAL;
+    return trt_server_submit_rgb(s, scene, params, spp, accum_host, nullptr, id);
+}
+
+int trt_server_submit_rgb(trt_server* s, trt_scene* scene, const uint32_t params[TRT_PARAMS_WORDS], uint32_t spp,
+                          float* accum_host, float* rgb_host, uint64_t* id) {
+    if (!s || !scene || !params || (!accum_host && !rgb_host) || spp == 0) return TRT_EINVAL;
+    if (rgb_host) {
+        uint32_t w = params[P_SIZE], h = params[P_SIZE + 1];
+        uint32_t most = s->opt.denoise_max_spp ? s->opt.denoise_max_spp : 4u;
+        if (!s->opt.denoiser) return fail(s->ctx, TRT_EINVAL, "trt_server_submit_rgb: the server has no denoiser");
+        if (spp > most)
+            return fail(s->ctx, TRT_EINVAL, "trt_server_submit_rgb: more samples than the server denoises");
+        if (!unet_fits(s->opt.denoiser, w, h))
+            return fail(s->ctx, TRT_EINVAL, "trt_server_submit_rgb: the denoiser does not take a " + std::to_string(w) +
+                                                " x " + std::to_string(h) + " image");
+    }
     if (scene->ctx->device != s->ctx->device) return fail(s->ctx, TRT_EINVAL, "trt_server_submit: the scene is on another device");
     int rc = check_params(scene, params);
     if (rc) return rc;
@@ -412,6 +437,7 @@ int trt_server_submit(trt_server* s, trt_scene* scene, const uint32_t params[TRT
                                             " path slots, more than a step holds (" + std::to_string(s->wave.slots) + ")");
     }
     r->host = accum_host;
+    r->rgb = rgb_host;
     r->accum_bytes = 80ull * r->w * r->h;
     {
         std::lock_guard<std::mutex> lk(s->mu);

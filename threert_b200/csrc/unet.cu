@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "threert_cuda.h"
+#include "unet.h"
 
 namespace unet {
 
@@ -522,27 +523,40 @@ __global__ void k_weights(const float* wf, uint32_t cin, uint32_t co_pad, uint32
 constexpr int N_FEAT = 11;  // input channels a pixel
 
 // The image's mean luminance and mean first-hit distance (over pixels that hit): sums into acc[0..2].
-__global__ void k_feat_sums(const float4* __restrict__ accum, uint64_t n, float* acc) {
-    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+// The image's mean luminance and mean first-hit distance (over pixels that hit), in a fixed order so that a denoise
+// is the same bit for bit however it is scheduled: each of FEAT_BLOCKS blocks sums its stride of pixels, then one
+// block sums the blocks' partials into acc[0..2].
+constexpr uint32_t FEAT_BLOCKS = 256, FEAT_THREADS = 256;
+__global__ void k_feat_sums(const float4* __restrict__ accum, uint64_t n, float* partial) {
+    __shared__ float sh[3][FEAT_THREADS];
     float l = 0.0f, d = 0.0f, dn = 0.0f;
-    if (i < n) {
+    for (uint64_t i = (uint64_t)blockIdx.x * FEAT_THREADS + threadIdx.x; i < n; i += (uint64_t)FEAT_BLOCKS * FEAT_THREADS) {
         float4 c = accum[5 * i], e = accum[5 * i + 3];
         float cnt = fmaxf(c.w, 1.0f);
-        l = (0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z) / cnt;
-        if (!isfinite(l)) l = 0.0f;
+        float li = (0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z) / cnt;
+        if (isfinite(li)) l += li;
         float dd = e.x / cnt;
-        if (dd > 0.0f && isfinite(dd)) { d = dd; dn = 1.0f; }
+        if (dd > 0.0f && isfinite(dd)) {
+            d += dd;
+            dn += 1.0f;
+        }
     }
-    for (int o = 16; o > 0; o >>= 1) {
-        l += __shfl_xor_sync(~0u, l, o);
-        d += __shfl_xor_sync(~0u, d, o);
-        dn += __shfl_xor_sync(~0u, dn, o);
+    sh[0][threadIdx.x] = l;
+    sh[1][threadIdx.x] = d;
+    sh[2][threadIdx.x] = dn;
+    __syncthreads();
+    for (uint32_t w = FEAT_THREADS / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w)
+            for (int k = 0; k < 3; ++k) sh[k][threadIdx.x] += sh[k][threadIdx.x + w];
+        __syncthreads();
     }
-    if ((threadIdx.x & 31u) == 0) {
-        atomicAdd(&acc[0], l);
-        atomicAdd(&acc[1], d);
-        atomicAdd(&acc[2], dn);
-    }
+    if (threadIdx.x < 3) partial[3 * blockIdx.x + threadIdx.x] = sh[threadIdx.x][0];
+}
+__global__ void k_feat_total(const float* __restrict__ partial, float* acc) {
+    if (threadIdx.x >= 3) return;
+    float t = 0.0f;
+    for (uint32_t b = 0; b < FEAT_BLOCKS; ++b) t += partial[3 * b + threadIdx.x];
+    acc[threadIdx.x] = t;
 }
 __device__ __forceinline__ float fin0(float v) { return isfinite(v) ? v : 0.0f; }
 // The network's input from the accum: log1p(radiance * s), albedo, normal, log1p(depth * sd) and log1p(the variance of
@@ -620,6 +634,7 @@ struct Net {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     uint32_t* dev_err = nullptr;  // set by a convolution whose pipeline wait gave up
     uint32_t sms = 148;           // the device's SMs (the persistent convolution's grid)
+    float* partial = nullptr;     // the feature sums' block partials
     std::string conv_err;         // a tensor map that could not be made
 };
 
@@ -845,6 +860,18 @@ int cuda_check(Net* n, cudaError_t e, const char* what) {
     return TRT_ECUDA;
 }
 
+// The denoise of a device accum (rendered with TRT_RENDER_DEPTH) into the network's RGB buffer, on the network's
+// current stream: the features, the forward pass, the radiance back.
+void denoise_device(Net* n, const void* accum_device, uint32_t W, uint32_t H) {
+    uint64_t P = (uint64_t)H * W;
+    cudaStream_t s = n->stream;
+    k_feat_sums<<<FEAT_BLOCKS, FEAT_THREADS, 0, s>>>((const float4*)accum_device, P, n->partial);
+    k_feat_total<<<1, 32, 0, s>>>(n->partial, n->sums);
+    k_feat<<<blocks(P), 256, 0, s>>>((const float4*)accum_device, P, n->sums, n->in0.p);
+    forward(n, 1, H, W);
+    k_unfeat<<<blocks(P * 3), 256, 0, s>>>(n->pred, P, n->sums, n->rgb);
+}
+
 // The end of a call: its stream drained, then what its convolutions reported (a refused tensor map on the host, a
 // pipeline wait that gave up on the device).
 int finish(Net* n, const char* what) {
@@ -920,6 +947,7 @@ int trt_unet_create(int device, uint32_t max_batch, uint32_t max_h, uint32_t max
     if (e == cudaSuccess) e = alloc(n, &n->loss, 4);
     if (e == cudaSuccess) e = alloc(n, &n->sums, 4);
     if (e == cudaSuccess) e = alloc(n, &n->dev_err, 1);
+    if (e == cudaSuccess) e = alloc(n, &n->partial, 3 * FEAT_BLOCKS);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CONV_SMEM);
     if (e == cudaSuccess) {
         int sms = 0;
@@ -1027,11 +1055,7 @@ int trt_unet_denoise_accum(trt_unet* n, const void* accum_device, uint32_t W, ui
     uint64_t P = (uint64_t)H * W;
     cudaStream_t s = n->stream;
     cudaEventRecord(n->e0, s);
-    cudaMemsetAsync(n->sums, 0, 16, s);
-    k_feat_sums<<<blocks(P), 256, 0, s>>>((const float4*)accum_device, P, n->sums);
-    k_feat<<<blocks(P), 256, 0, s>>>((const float4*)accum_device, P, n->sums, n->in0.p);
-    forward(n, 1, H, W);
-    k_unfeat<<<blocks(P * 3), 256, 0, s>>>(n->pred, P, n->sums, n->rgb);
+    denoise_device(n, accum_device, W, H);
     cudaEventRecord(n->e1, s);
     cudaMemcpyAsync(rgb_host, n->rgb, 12 * P, cudaMemcpyDeviceToHost, s);
     rc = finish(n, "trt_unet_denoise_accum");
@@ -1040,3 +1064,19 @@ int trt_unet_denoise_accum(trt_unet* n, const void* accum_device, uint32_t W, ui
 }
 
 }  // extern "C"
+
+// The serving loop's denoise: on its stream, into the network's RGB buffer (returned; null when the image is not a
+// size the network takes, or a convolution's tensor map was refused). The network belongs to the server meanwhile.
+const float* unet_denoise_on_stream(trt_unet* n, const void* accum_device, uint32_t w, uint32_t h, cudaStream_t st) {
+    if (!n || !accum_device || w == 0 || h == 0 || h > n->maxH || w > n->maxW || h % 8 || w % 8) return nullptr;
+    cudaStream_t own = n->stream;
+    n->stream = st;
+    denoise_device(n, accum_device, w, h);
+    n->stream = own;
+    if (!n->conv_err.empty()) return nullptr;
+    return n->rgb;
+}
+
+bool unet_fits(const trt_unet* n, uint32_t w, uint32_t h) {
+    return n && w > 0 && h > 0 && h <= n->maxH && w <= n->maxW && h % 8 == 0 && w % 8 == 0;
+}

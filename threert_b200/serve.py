@@ -27,6 +27,8 @@ class Request:
     id: int = 0
     accum: np.ndarray | None = None
     done: dict = field(default_factory=dict)
+    denoise: bool = False             # the server's learned denoiser on its result (rgb) instead of the accum
+    rgb: np.ndarray | None = None     # (h * w, 3) float32, the denoised image
 
     @property
     def paths(self) -> int:
@@ -37,47 +39,60 @@ class Server:
     """trt_server: a worker thread, its streams and wave state on the Gpu's device."""
 
     def __init__(self, gpu: Gpu, wave_slots: int = 0, max_active: int = 0, hbm_reserve: int = 0, flags: int = 0,
-                 launch_mode: int = 0):
+                 launch_mode: int = 0, denoiser=None, denoise_max_spp: int = 4):
+        """denoiser: None, or a threert_b200.unet.UNet the server owns until closed (requests with denoise=True)."""
         self.gpu = gpu
         self.handle = C.c_void_p()
-        o = N.ServerOptions(wave_slots, max_active, hbm_reserve, flags, launch_mode)
+        self.denoiser = denoiser
+        o = N.ServerOptions(wave_slots, max_active, hbm_reserve, flags, launch_mode,
+                            denoiser.handle if denoiser is not None else None, denoise_max_spp)
         gpu._check(N.lib().trt_server_create(gpu.ctx, C.byref(o), C.byref(self.handle)), "trt_server_create")
         self.live: dict[int, Request] = {}
         self.pool: dict[int, list] = {}  # pinned result buffers by pixel count, free for reuse
         self.pinned: dict[int, object] = {}  # the pinned allocation behind each buffer, by address
 
-    def _buffer(self, pixels: int) -> np.ndarray:
+    def _buffer(self, pixels: int, cols: int = N.PIXEL_FLOATS) -> np.ndarray:
         """A result buffer in pinned host memory (the read-back then runs at full speed, off the worker's path)."""
-        free = self.pool.get(pixels)
+        free = self.pool.get((pixels, cols))
         if free:
             return free.pop()
-        return pinned_buffer(pixels, self.pinned)
+        return pinned_buffer(pixels, self.pinned, cols)
 
     def reserve(self, requests: list[Request]):
         """Allocates, ahead of time, a pinned result buffer for each of these requests (pinned allocations take
         milliseconds: made while submitting, they would hold the submitter back)."""
-        need: dict[int, int] = {}
+        need: dict[tuple, int] = {}
         for r in requests:
-            px = int(r.params[16]) * int(r.params[17])
-            need[px] = need.get(px, 0) + 1
-        for px, n in need.items():
-            have = self.pool.setdefault(px, [])
+            key = (int(r.params[16]) * int(r.params[17]), 3 if r.denoise else N.PIXEL_FLOATS)
+            need[key] = need.get(key, 0) + 1
+        for key, n in need.items():
+            have = self.pool.setdefault(key, [])
             while len(have) < n:
-                have.append(pinned_buffer(px, self.pinned))
+                have.append(pinned_buffer(key[0], self.pinned, key[1]))
 
     def release(self, req: Request):
         """Returns a finished request's result buffer to the pool (its accum is not to be read after this)."""
-        if req.accum is not None:
-            self.pool.setdefault(len(req.accum), []).append(req.accum)
-            req.accum = None
+        for name in ("accum", "rgb"):
+            a = getattr(req, name)
+            if a is not None:
+                self.pool.setdefault(a.shape, []).append(a)
+                setattr(req, name, None)
 
     def submit(self, scene: Scene, req: Request) -> int:
         p = np.ascontiguousarray(req.params, dtype=np.uint32)
-        req.accum = self._buffer(int(p[16]) * int(p[17]))
+        px = int(p[16]) * int(p[17])
         rid = C.c_uint64()
-        self.gpu._check(N.lib().trt_server_submit(self.handle, scene.handle, p.ctypes.data_as(C.POINTER(C.c_uint32)),
-                                                  req.spp, req.accum.ctypes.data_as(C.POINTER(C.c_float)),
-                                                  C.byref(rid)), "trt_server_submit")
+        fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float)) if a is not None else None
+        if req.denoise:
+            req.accum, req.rgb = None, self._buffer(px, 3)
+            self.gpu._check(N.lib().trt_server_submit_rgb(self.handle, scene.handle,
+                                                          p.ctypes.data_as(C.POINTER(C.c_uint32)), req.spp, None,
+                                                          fp(req.rgb), C.byref(rid)), "trt_server_submit_rgb")
+        else:
+            req.accum = self._buffer(px)
+            self.gpu._check(N.lib().trt_server_submit(self.handle, scene.handle,
+                                                      p.ctypes.data_as(C.POINTER(C.c_uint32)), req.spp, fp(req.accum),
+                                                      C.byref(rid)), "trt_server_submit")
         req.id = rid.value
         self.live[req.id] = req
         return req.id
@@ -116,25 +131,27 @@ RESOLUTIONS = [(256, 256), (512, 512), (1280, 720), (1920, 1080)]
 SPPS = [1, 16, 64]
 
 
-def pinned_buffer(pixels: int, keep: dict) -> np.ndarray:
-    """A (pixels, 20) float32 array in pinned host memory; `keep` holds the allocation for as long as it is used."""
+def pinned_buffer(pixels: int, keep: dict, cols: int = N.PIXEL_FLOATS) -> np.ndarray:
+    """A (pixels, cols) float32 array in pinned host memory; `keep` holds the allocation for as long as it is used."""
     import torch
-    t = torch.empty((pixels, N.PIXEL_FLOATS), dtype=torch.float32, pin_memory=True)
+    t = torch.empty((pixels, cols), dtype=torch.float32, pin_memory=True)
     a = t.numpy()
     keep[a.ctypes.data] = t
     return a
 
 
 def mix_requests(bases: list[np.ndarray], n: int, seed: int = 0, resolutions=RESOLUTIONS, spps=SPPS,
-                 max_bounces: int = 4) -> list[Request]:
-    """n requests over the scenes whose base Params are `bases`: scene, resolution and spp drawn uniformly."""
+                 max_bounces: int = 4, denoise_max_spp: int = 0) -> list[Request]:
+    """n requests over the scenes whose base Params are `bases`: scene, resolution and spp drawn uniformly; those of
+    at most `denoise_max_spp` samples denoised (0: none)."""
     rng = np.random.default_rng(seed)
     out = []
     for _ in range(n):
         k = int(rng.integers(len(bases)))
         w, h = resolutions[int(rng.integers(len(resolutions)))]
         p = params_with(bases[k], width=w, height=h, max_bounces=max_bounces)
-        out.append(Request(k, p, int(spps[int(rng.integers(len(spps)))])))
+        spp = int(spps[int(rng.integers(len(spps)))])
+        out.append(Request(k, p, spp, denoise=spp <= denoise_max_spp))
     return out
 
 
@@ -186,8 +203,9 @@ def run_stream(server: Server, scenes: list[Scene], requests: list[Request], rat
             "busy_s": (after["busy_ms"] - before["busy_ms"]) * 1e-3}
 
 
-def run_serial(gpu: Gpu, scenes: list[Scene], requests: list[Request]) -> dict:
-    """The reference's way: each request rendered alone through trt_render and read back before the next starts."""
+def run_serial(gpu: Gpu, scenes: list[Scene], requests: list[Request], denoiser=None) -> dict:
+    """The reference's way: each request rendered alone through trt_render and read back before the next starts (a
+    denoised request: rendered with its depth guide, denoised by `denoiser`, its image read back)."""
     rays = 0
     lat = []
     keep, bufs = {}, {}
@@ -198,7 +216,12 @@ def run_serial(gpu: Gpu, scenes: list[Scene], requests: list[Request]) -> dict:
     t0 = time.perf_counter()
     for r in requests:
         t = time.perf_counter()
-        acc, st = scenes[r.scene].render_raw(r.params, r.spp, out=bufs[int(r.params[16]) * int(r.params[17])])
+        S = scenes[r.scene]
+        if r.denoise:
+            _, st = S.render_raw(r.params, r.spp, flags=N.TRT_RENDER_DEPTH, read=False)
+            denoiser.denoise(S)
+        else:
+            acc, st = S.render_raw(r.params, r.spp, out=bufs[int(r.params[16]) * int(r.params[17])])
         lat.append((time.perf_counter() - t) * 1e3)
         rays += st.closest_rays + st.shadow_rays
     span = time.perf_counter() - t0
