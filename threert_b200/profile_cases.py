@@ -2,6 +2,7 @@
 CASE`): each case prepares its input, runs the kernels of interest a few times and exits.
 
   city     one warm-up and two frames of the city at 1280 x 720, 1 spp, depth 4 (k_extend, k_shade, k_shadow, ...)
+  city_wide  the same frames walking the 8-wide BVH
   unet     the learned denoiser's network on a 1280 x 720 image, three times (k_conv), and one training step on a
            batch of 16 crops of 64 x 64 (k_conv, k_wgrad)
   crowd    the crowd's deformation, three frames, at K pose groups (k_skin, k_refit_leaves, k_refit, k_top_*)
@@ -13,14 +14,14 @@ import sys
 import numpy as np
 
 
-def city():
+def city(flags: int = 0):
     from threert_b200 import Gpu, prep, scenes
     P = prep.prepare(scenes.city())
     g = Gpu(0)
     S = g.upload(P)
     for f in range(3):
         cam = scenes.city_camera(f, 240, 1, P.width, P.height)
-        S.render_raw(prep.set_camera(P.params, cam), 1, read=False, stats=False)
+        S.render_raw(prep.set_camera(P.params, cam), 1, flags=flags, read=False, stats=False)
     g.synchronize()
     S.close()
     g.close()
@@ -61,6 +62,9 @@ if __name__ == "__main__":
     case = sys.argv[1] if len(sys.argv) > 1 else "city"
     if case == "city":
         city()
+    elif case == "city_wide":
+        from threert_b200 import _native as N
+        city(N.TRT_RENDER_WIDE)
     elif case == "unet":
         unet_case()
     elif case == "crowd":
