@@ -473,6 +473,54 @@ def run_denoise(args, rank, world, local):
     gpu.close()
 
 
+CORNELL_METRIC = "Mrays/s (closest + shadow rays, Cornell box 256x256, 16 spp, depth 5)"
+
+
+def run_cornell(args, rank, world, local):
+    """Config 0: the Cornell box (36 triangles) at 256 x 256, 16 spp a frame, depth 5, clamp off; a step is one frame
+    of 16 samples (trt_render), device-timed. Its working set sits in L1 / L2: the walks' issue rate, not HBM, bounds
+    it. CPU baseline: the oracle on the host's threads, the same frames."""
+    from threert_b200 import Gpu, prep, scenes
+    gpu = Gpu(local)
+    name, sms = gpu.device_info()
+    P = prep.prepare(scenes.cornell(256, 256))
+    S = gpu.upload(P)
+    spp = 16
+    for k in range(args.warmup):
+        S.render_raw(prep.params_with(P.params, seed=1000 + k), spp, read=False)
+    ms, rays, paths = 0.0, 0, 0
+    for k in range(args.steps):
+        _, st = S.render_raw(prep.params_with(P.params, seed=k + 1), spp, read=False)
+        ms += st.device_ms
+        rays += st.closest_rays + st.shadow_rays
+        paths += st.paths
+    t = time.perf_counter()
+    acc, st = S.render_raw(P.params, spp)
+    e2e_ms = (time.perf_counter() - t) * 1e3
+    line = {
+        "metric": CORNELL_METRIC, "value": rays * world / (ms * 1e-3) / 1e6, "unit": "Mrays/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "Cornell box 36 tris, 256x256, 16 spp a step, depth 5", "device": name, "sms": sms},
+        "paths_per_s": paths / (ms * 1e-3), "rays_per_path": rays / max(1, paths),
+        "e2e": {"value": (st.closest_rays + st.shadow_rays) / (e2e_ms * 1e-3) / 1e6, "unit": "Mrays/s",
+                "h2d_bytes_per_step": 624, "d2h_bytes_per_step": 256 * 256 * 80},
+    }
+    if not args.no_cpu and rank == 0:
+        import oracle
+        O = oracle.Oracle(P)
+        t = time.perf_counter()
+        _, cs = O.render(P.params, spp)
+        dt = time.perf_counter() - t
+        line["cpu_baseline"] = {"value": (cs["closest_rays"] + cs["shadow_rays"]) / dt / 1e6, "unit": "Mrays/s",
+                                "cores": oracle.hardware_threads(), "kind": "port",
+                                "sample": "one frame of 16 spp on every host thread"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    S.close()
+    gpu.close()
+
+
 SKY_METRIC = "ms per sky re-bake on the device (atmosphere 1024x512, a moving sun: sky.rs bake_atmosphere_tables)"
 
 
@@ -556,9 +604,9 @@ def main():
                     help="coherence sorts on the device: 'none', or a comma list of rays, hits, shadows "
                          "(hits by material is the pass's default; the other two measured slower here)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
-    ap.add_argument("--workload", default="city", choices=["city", "crowd", "serve", "denoise", "sky"],
+    ap.add_argument("--workload", default="city", choices=["city", "crowd", "serve", "denoise", "sky", "cornell"],
                     help="city (the headline workload), the crowd with its per-frame deformation, the serving mix, "
-                         "the learned denoiser (trained, then judged), or the atmosphere's sky bake")
+                         "the learned denoiser (trained, then judged), the atmosphere's sky bake, or the Cornell box")
     ap.add_argument("--scenes", type=int, default=64, help="denoise: procedural cities rendered for training")
     ap.add_argument("--views", type=int, default=16, help="denoise: views of each")
     ap.add_argument("--train-steps", type=int, default=20000, help="denoise: Adam steps")
@@ -590,6 +638,11 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
 
+    if args.workload == "cornell":
+        run_cornell(args, rank, world, local)
+        if dist:
+            dist.destroy_process_group()
+        return
     if args.workload == "sky":
         run_sky(args, rank, world, local)
         if dist:
