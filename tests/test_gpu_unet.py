@@ -61,6 +61,19 @@ def test_forward_on_ragged_tiles_matches_the_oracle(net):
     assert err < 0.03, err
 
 
+def test_forward_on_wide_rows_matches_the_oracle():
+    # 256 x 24: rows of 128-pixel tiles at the two widest levels, where the convolution loads each tile's halo once
+    # and keeps the layer's weights resident (all but d1a, whose 160 input channels take the general kernel)
+    wide = unet.UNet(0, max_batch=1, max_h=24, max_w=256)
+    p, feats, _ = case(seed=6, b=1, h=24, w=256)
+    wide.set_params(p)
+    got, _ = wide.forward(feats)
+    want, _ = R.forward(R.unpack(bf16(p).astype(np.float64)), bf16(feats).astype(np.float64))
+    err = np.linalg.norm(got - want) / np.linalg.norm(want)
+    assert err < 0.03, err
+    wide.close()
+
+
 def test_every_layers_gradient_matches_the_oracle(net):
     p, feats, tgt = case(seed=5)
     net.set_params(p)
