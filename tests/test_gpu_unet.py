@@ -62,8 +62,8 @@ def test_forward_on_ragged_tiles_matches_the_oracle(net):
 
 
 def test_forward_on_wide_rows_matches_the_oracle():
-    # 256 x 24: rows of 128-pixel tiles at the two widest levels, where the convolution loads each tile's halo once
-    # and keeps the layer's weights resident (all but d1a, whose 160 input channels take the general kernel)
+    # 256 x 24: tiles of 128 x 1 pixels at the two widest levels (a tile a row, its halo rows above and below read by
+    # the shifted TMA boxes), 64 x 2 and 32 x 4 below
     wide = unet.UNet(0, max_batch=1, max_h=24, max_w=256)
     p, feats, _ = case(seed=6, b=1, h=24, w=256)
     wide.set_params(p)

@@ -149,17 +149,51 @@ __device__ __forceinline__ void umma_commit(uint32_t mbar) {
 }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, "
-        "[%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
-          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
+// 64 accumulator columns of this warp's lanes in one load and one wait.
+__device__ __forceinline__ void tmem_ld64(uint32_t taddr, float* v) {
+    uint32_t r[64];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, %48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63}, [%64];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+                 : "r"(taddr));
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+    for (int i = 0; i < 64; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// The epilogue of one accumulator row (a pixel) and 16 columns from `c`: bias, ReLU, bf16 NHWC (or the f32 output).
+__device__ __forceinline__ void conv_store16(const Conv& a, uint64_t p, uint32_t c, float* v) {
+    if (a.bias) {
+        const float4* b4 = reinterpret_cast<const float4*>(a.bias + c);  // (16 floats, 64-byte aligned)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            float4 bq = __ldg(b4 + q);
+            v[4 * q] += bq.x;
+            v[4 * q + 1] += bq.y;
+            v[4 * q + 2] += bq.z;
+            v[4 * q + 3] += bq.w;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+        if (a.relu) v[i] = fmaxf(v[i], 0.0f);
+    if (a.yf) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i)
+            if (c + i < a.cout) a.yf[p * a.cout + c + i] = v[i];
+    } else if (c + 16u <= a.cout) {
+        uint32_t pk[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            __nv_bfloat162 h2 = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+            pk[i] = *reinterpret_cast<uint32_t*>(&h2);
+        }
+        uint4* dst = reinterpret_cast<uint4*>(a.y + p * a.y_stride + a.y_off + c);
+        dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+        dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+    } else {
+        for (int i = 0; i < 16; ++i)
+            if (c + i < a.cout) a.y[p * a.y_stride + a.y_off + c + i] = __float2bfloat16_rn(v[i]);
+    }
 }
 
 __global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ CUtensorMap xmap,
@@ -277,34 +311,12 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ C
             const int px = x0 + (int)(m % a.bw), py = y0 + (int)(m / a.bw);
             const bool valid = fin && px < (int)a.W && py < (int)a.H;
             const uint64_t p = ((uint64_t)b * a.H + (uint32_t)py) * a.W + (uint32_t)px;
-            for (uint32_t cc = 0; cc < a.nt; cc += 16u) {
-                float v[16];
-                tmem_ld16(tmem + ((quarter * 32u) << 16) + acc * a.nt + cc, v);
-                const uint32_t c = n0 + cc;
-                if (!valid) continue;
+            for (uint32_t cc = 0; cc < a.nt; cc += 64u) {
+                float v[64];
+                tmem_ld64(tmem + ((quarter * 32u) << 16) + acc * a.nt + cc, v);
+                if (valid)
 #pragma unroll
-                for (int i = 0; i < 16; ++i) {
-                    if (a.bias) v[i] += a.bias[c + i];
-                    if (a.relu) v[i] = fmaxf(v[i], 0.0f);
-                }
-                if (a.yf) {
-#pragma unroll
-                    for (int i = 0; i < 16; ++i)
-                        if (c + i < a.cout) a.yf[p * a.cout + c + i] = v[i];
-                } else if (c + 16u <= a.cout) {
-                    uint32_t pk[8];
-#pragma unroll
-                    for (int i = 0; i < 8; ++i) {
-                        __nv_bfloat162 h2 = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
-                        pk[i] = *reinterpret_cast<uint32_t*>(&h2);
-                    }
-                    uint4* dst = reinterpret_cast<uint4*>(a.y + p * a.y_stride + a.y_off + c);
-                    dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-                    dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
-                } else {
-                    for (int i = 0; i < 16; ++i)
-                        if (c + i < a.cout) a.y[p * a.y_stride + a.y_off + c + i] = __float2bfloat16_rn(v[i]);
-                }
+                    for (uint32_t q = 0; q < 4u; ++q) conv_store16(a, p, n0 + cc + 16u * q, v + 16u * q);
             }
             // this accumulator is read: the MMA issuer may fill it again
             tc_fence_before();
