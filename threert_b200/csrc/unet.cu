@@ -5,8 +5,9 @@
 // Tensors are NHWC bf16 with channel counts padded to multiples of 32; a convolution is an implicit GEMM (M = pixels,
 // N = output channels, K = 9 taps x input channels) on the 5th-generation tensor cores (TMA loads, tcgen05.mma into
 // tensor memory, f32 accumulation). The input gradient is the same kernel run on the output gradient with the
-// weights flipped and transposed; the weight gradient is a GEMM over pixels on mma.sync (split across CTAs, summed
-// with f32 atomics). Master weights, gradients and Adam's moments are f32.
+// weights flipped and transposed; the weight and bias gradients are one GEMM over pixels on the same tensor cores
+// (both operands MN-major, split across CTAs, summed with f32 atomics). Master weights, gradients and Adam's moments
+// are f32.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -26,25 +27,7 @@ namespace unet {
 
 typedef __nv_bfloat16 bf16;
 
-// ---- tensor-core fragments of the weight gradient (mma.sync m16n8k16, bf16 in, f32 accumulate) ---------------------
-
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void ldsm_x4(uint32_t& r0, uint32_t& r1, uint32_t& r2, uint32_t& r3, const void* p) {
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];\n"
-                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3) : "r"(smem_addr(p)));
-}
-__device__ __forceinline__ void ldsm_x4_t(uint32_t& r0, uint32_t& r1, uint32_t& r2, uint32_t& r3, const void* p) {
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0, %1, %2, %3}, [%4];\n"
-                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3) : "r"(smem_addr(p)));
-}
-__device__ __forceinline__ void mma16816(float* c, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
-                                         uint32_t b1) {
-    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
-                 "{%0, %1, %2, %3};\n"
-                 : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-                 : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
-}
 
 // ---- convolution (forward; and the input gradient with flipped, transposed weights) -------------------------------
 //
@@ -331,65 +314,193 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ C
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
 }
 
-// ---- weight gradient: dw[t][c][n] += sum over pixels p of x[p + off(t)][c] * dy[p][n] ------------------------------
+// ---- weight and bias gradients: dw[t][c][n] += sum over pixels p of x[p + off(t)][c] * dy[p][n]; db[n] += sum dy ---
+//
+// One GEMM over pixels (K) for every (tap, 32-input-channel block) pair of the layer at once: the pairs fill the
+// 32-row slots of a 128-row accumulator (M), four a group, and one more slot holds all ones, so that its rows are the
+// bias gradient; N is the layer's output channels (32 to 128). A CTA takes one group of slots (blockIdx.y) over a run
+// of 128-pixel tiles (blockIdx.x):
+//  - one thread loads a tile's stage: per slot a TMA box of 32 channels x bw x bh pixels of x, shifted by the slot's
+//    tap (zeros outside the image), and the output gradient's boxes of 32 channels x the same pixels, unshifted; a
+//    box lands as 128 rows (pixels) of 64 bytes with the 64-byte swizzle, which is the canonical MN-major layout
+//    (32-element blocks of M or N one box = 8 KB apart, 8-pixel groups of K 512 bytes apart);
+//  - one thread issues eight tcgen05.mma (M 128, N, K 16, both operands MN-major, f32 accumulate in tensor memory)
+//    a stage and hands the stage back to the loader through an mbarrier;
+//  - after the run the four epilogue warps read the accumulator (warp w: slot w % 4, its lanes the slot's 32 input
+//    channels) and add it into dw, and the ones slot's first row into db, with 16-byte f32 atomics.
+// Slots that no pair fills hold zeros; they and the ones slot are written once, when the CTA starts. Waits are
+// bounded as the convolution's are; after a wait that gave up, the CTA waits (bounded) for its copies and MMAs in
+// flight before it frees its tensor memory.
 
 struct WGrad {
-    const bf16* x; uint32_t x_stride, x_off, cin;
-    const bf16* dy; uint32_t dy_stride, cout;  // cout a multiple of 32
-    float* dw;                                 // [9][cin][co_pad] f32, summed into
+    uint32_t cin, x_off;      // input channels (a multiple of 32) and their first channel in x
+    uint32_t kc, nb, pairs;   // input blocks of 32, output-gradient blocks of 32 (N = 32 nb), 9 kc (the ones slot's index)
+    float* dw;                // [9][cin][co_pad] f32, summed into
+    float* db;                // [co_pad] f32, summed into
     uint32_t co_pad;
-    uint32_t B, H, W, chunk;                   // pixels a CTA
+    uint32_t bw, bh, tiles_x, tiles_y, tiles, chunk;  // 128-pixel tiles (bw x bh) over all images; tiles a CTA
+    uint32_t ts;              // pipeline stages
+    uint32_t* err;
 };
+constexpr uint32_t WG_BOX = 128u * 64u;  // one box: 128 pixels x 32 channels of bf16
+constexpr uint32_t WG_THREADS = 192u;    // loader, MMA, 4 epilogue warps
+constexpr uint32_t WG_SMEM_EXTRA = 1024u + 256u;  // alignment of the stages to 1 KB, the barriers
+constexpr uint32_t WG_SMEM_MAX = 227u * 1024u;
 
-// A CTA: one tap, 32 input x 32 output channels, `chunk` pixels; 4 warps of 16 x 16.
-__global__ void __launch_bounds__(128) k_wgrad(WGrad a) {
-    __shared__ __align__(16) bf16 Xs[32][32 + 8];
-    __shared__ __align__(16) bf16 Ys[32][32 + 8];
+// The canonical MN-major shared-memory matrix with the 64-byte swizzle: 32-element blocks of M (or N) `lbo` bytes
+// apart, 8-row groups of K (rows of 64 bytes) 512 bytes apart; descriptor version 1, layout type 4 (SWIZZLE_64B).
+__device__ __forceinline__ uint64_t umma_desc_mn64(uint32_t saddr, uint32_t lbo) {
+    return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)(512u >> 4) << 32) | (1ull << 46) | (4ull << 61);
+}
+// A wait bounded at about 2^31 cycles that ignores the abort word: the drain of a CTA that gave up.
+__device__ __forceinline__ bool mbar_wait_drain(uint32_t a, uint32_t parity) {
+    long long t0 = clock64();
+    while (!mbar_try_wait(a, parity))
+        if (clock64() - t0 > (1ll << 31)) return false;
+    return true;
+}
+// 32 accumulator columns of this warp's lanes.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
+    uint32_t r[32];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__global__ void __launch_bounds__(WG_THREADS) k_wgrad(const __grid_constant__ CUtensorMap xmap,
+                                                     const __grid_constant__ CUtensorMap dymap, WGrad a) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
-    const uint32_t wm = warp & 1u, wn = warp >> 1;
-    const int tap = (int)blockIdx.y, dy = tap / 3 - 1, dx = tap % 3 - 1;
-    const uint32_t ct = a.cout / 32u, c0 = (blockIdx.z / ct) * 32u, n0 = (blockIdx.z % ct) * 32u;
-    const uint32_t M = a.B * a.H * a.W, hw = a.H * a.W;
-    const uint32_t p_begin = blockIdx.x * a.chunk, p_end = min(M, p_begin + a.chunk);
-    float acc[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
-    const uint32_t lrow = tid >> 2, lpart = tid & 3u;  // 32 rows x 4 parts of 16 bytes
-    for (uint32_t p0 = p_begin; p0 < p_end; p0 += 32) {
-        uint32_t p = p0 + lrow;
-        uint4 xv = make_uint4(0u, 0u, 0u, 0u), yv = make_uint4(0u, 0u, 0u, 0u);
-        if (p < p_end) {
-            uint32_t b = p / hw, y = (p % hw) / a.W, x = p % a.W;
-            int sy = (int)y + dy, sx = (int)x + dx;
-            if (sy >= 0 && sx >= 0 && sy < (int)a.H && sx < (int)a.W) {
-                uint64_t pix = ((uint64_t)b * a.H + (uint32_t)sy) * a.W + (uint32_t)sx;
-                xv = *reinterpret_cast<const uint4*>(a.x + pix * a.x_stride + a.x_off + c0 + lpart * 8u);
-            }
-            yv = *reinterpret_cast<const uint4*>(a.dy + (uint64_t)p * a.dy_stride + n0 + lpart * 8u);
+    const uint32_t sraw = smem_addr(smem_raw), sbase = (sraw + 1023u) & ~1023u;
+    uint8_t* smem = smem_raw + (sbase - sraw);
+    const uint32_t stage = (4u + a.nb) * WG_BOX, sBar = sbase + a.ts * stage;
+    // barriers: full[ts], empty[ts], acc_full; then the tensor-memory address, the abort word and the counts of
+    // stages issued and consumed
+    auto full = [&](uint32_t s) { return sBar + 8u * s; };
+    auto empty = [&](uint32_t s) { return sBar + 8u * (a.ts + s); };
+    const uint32_t acc_full = sBar + 16u * a.ts;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + a.ts * stage + 16u * a.ts + 8u);
+    volatile uint32_t* abort_flag = tslot + 1;
+    volatile uint32_t* counts = tslot + 2;
+    const uint32_t n_cols = 32u * a.nb, ncols = a.nb == 1u ? 32u : a.nb == 2u ? 64u : 128u;
+    const uint32_t slot0 = blockIdx.y * 4u;
+    const uint32_t loaded = slot0 < a.pairs ? min(4u, a.pairs - slot0) : 0u;  // slots 0 .. loaded-1 hold pairs
+    const uint32_t k0 = blockIdx.x * a.chunk, k1 = min(a.tiles, k0 + a.chunk);
+    const uint32_t per_img = a.tiles_x * a.tiles_y;
+
+    // the slots no pair fills: the ones slot (bf16 1.0) and zeros, in every stage
+    for (uint32_t j = loaded; j < 4u; ++j) {
+        const uint32_t v = slot0 + j == a.pairs ? 0x3F803F80u : 0u;
+        for (uint32_t s = 0; s < a.ts; ++s) {
+            uint4* p = reinterpret_cast<uint4*>(smem + s * stage + j * WG_BOX);
+            for (uint32_t i = tid; i < WG_BOX / 16u; i += WG_THREADS) p[i] = make_uint4(v, v, v, v);
         }
-        *reinterpret_cast<uint4*>(&Xs[lrow][lpart * 8u]) = xv;
-        *reinterpret_cast<uint4*>(&Ys[lrow][lpart * 8u]) = yv;
-        __syncthreads();
-#pragma unroll
-        for (uint32_t kk = 0; kk < 32; kk += 16) {
-            // A[m = c][k = p] = Xs[p][c]: transposed 8 x 8 blocks
-            uint32_t a0, a1, a2, a3, b0, b1, b2, b3;
-            ldsm_x4_t(a0, a1, a2, a3,
-                      &Xs[kk + (lane & 7u) + (lane >> 4) * 8u][wm * 16u + ((lane >> 3) & 1u) * 8u]);
-            ldsm_x4_t(b0, b1, b2, b3, &Ys[kk + (lane & 7u) + ((lane >> 3) & 1u) * 8u][wn * 16u + (lane >> 4) * 8u]);
-            mma16816(acc[0], a0, a1, a2, a3, b0, b1);
-            mma16816(acc[1], a0, a1, a2, a3, b2, b3);
-        }
-        __syncthreads();
     }
-    const uint32_t g = lane >> 2, t4 = lane & 3u;
-#pragma unroll
-    for (int nt = 0; nt < 2; ++nt)
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            uint32_t c = c0 + wm * 16u + g + h * 8u, n = n0 + wn * 16u + nt * 8u + t4 * 2u;
-            float* dst = a.dw + ((uint64_t)tap * a.cin + c) * a.co_pad + n;
-            atomicAdd(dst, acc[nt][h * 2]);
-            atomicAdd(dst + 1, acc[nt][h * 2 + 1]);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // visible to the tensor cores
+    if (tid == 0) {
+        for (uint32_t s = 0; s < a.ts; ++s) {
+            mbar_init(full(s), 1);
+            mbar_init(empty(s), 1);
         }
+        mbar_init(acc_full, 1);
+        *abort_flag = 0u;
+        counts[0] = counts[1] = 0u;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tslot)),
+                     "r"(ncols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // the loader: a stage a tile
+            uint32_t it = 0;
+            for (uint32_t t = k0; t < k1; ++t, ++it) {
+                const uint32_t s = it % a.ts;
+                if (it >= a.ts && !mbar_wait(empty(s), ((it / a.ts) - 1u) & 1u, a.err, abort_flag)) break;
+                mbar_expect_tx(full(s), (loaded + a.nb) * WG_BOX);
+                const uint32_t b = t / per_img, r = t % per_img;
+                const int x0 = (int)((r % a.tiles_x) * a.bw), y0 = (int)((r / a.tiles_x) * a.bh);
+                const uint32_t base = sbase + s * stage;
+                for (uint32_t j = 0; j < loaded; ++j) {
+                    const uint32_t pr = slot0 + j, tap = pr / a.kc, cb = pr % a.kc;
+                    tma_load_4d(base + j * WG_BOX, &xmap, (int)(a.x_off + cb * 32u), x0 + (int)(tap % 3u) - 1,
+                                y0 + (int)(tap / 3u) - 1, (int)b, full(s));
+                }
+                for (uint32_t i = 0; i < a.nb; ++i)
+                    tma_load_4d(base + (4u + i) * WG_BOX, &dymap, (int)(i * 32u), x0, y0, (int)b, full(s));
+            }
+            counts[0] = it;
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // the MMA issuer: eight K-16 steps a stage into the one accumulator
+            const uint32_t idesc = umma_idesc(128u, n_cols) | (1u << 15) | (1u << 16);  // A and B MN-major
+            uint32_t it = 0;
+            for (uint32_t t = k0; t < k1; ++t, ++it) {
+                const uint32_t s = it % a.ts;
+                if (!mbar_wait(full(s), (it / a.ts) & 1u, a.err, abort_flag)) break;
+                tc_fence_after();
+                const uint32_t base = sbase + s * stage;
+#pragma unroll
+                for (uint32_t j = 0; j < 8u; ++j) {
+                    const uint64_t ad = umma_desc_mn64(base + j * 1024u, WG_BOX);
+                    const uint64_t bd = umma_desc_mn64(base + 4u * WG_BOX + j * 1024u, WG_BOX);
+                    umma_f16(tmem, ad, bd, idesc, (it | j) != 0u ? 1u : 0u);
+                }
+                umma_commit(empty(s));
+            }
+            counts[1] = it;
+            umma_commit(acc_full);  // every MMA issued is done (after a wait that gave up too)
+        }
+    } else {
+        // the epilogue: warp w reads tensor-memory lanes 32 (w % 4) ..., the rows of slot w % 4
+        const uint32_t quarter = warp & 3u, slot = slot0 + quarter;
+        const bool fin = mbar_wait(acc_full, 0u, a.err, abort_flag);
+        __syncwarp();
+        tc_fence_after();
+        if (fin && (quarter < loaded || slot == a.pairs)) {
+            float* dst = nullptr;
+            if (slot < a.pairs)
+                dst = a.dw + ((uint64_t)(slot / a.kc) * a.cin + (slot % a.kc) * 32u + lane) * a.co_pad;
+            else if (lane == 0)
+                dst = a.db;  // every row of the ones slot is the bias gradient
+            for (uint32_t cc = 0; cc < n_cols; cc += 32u) {
+                float v[32];
+                tmem_ld32(tmem + ((quarter * 32u) << 16) + cc, v);
+                if (dst)
+#pragma unroll
+                    for (uint32_t q = 0; q < 8u; ++q)
+                        atomicAdd(reinterpret_cast<float4*>(dst + cc) + q,
+                                  make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]));
+            }
+        }
+    }
+    __syncwarp();
+    tc_fence_before();
+    __syncthreads();
+    if (*abort_flag && lane == 0) {
+        // a wait gave up: let the copies and MMAs in flight land before the memory they use is released
+        if (warp == 0)
+            for (uint32_t i = counts[1]; i < counts[0]; ++i) mbar_wait_drain(full(i % a.ts), (i / a.ts) & 1u);
+        else if (warp == 1)
+            mbar_wait_drain(acc_full, 0u);
+    }
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 1)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
 }
 
 // ---- the other layers ----------------------------------------------------------------------------------------------
@@ -496,14 +607,6 @@ __global__ void k_loss(const float* pred, const float* target, uint64_t P, bf16*
     }
     for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(~0u, l, o);
     if ((threadIdx.x & 31u) == 0 && l != 0.0f) atomicAdd(loss, l / (float)(P * 3));
-}
-// Bias gradient: db[n] += sum over pixels of dy[p][n].
-__global__ void k_bgrad(const bf16* dy, uint32_t dys, uint32_t C, uint64_t P, float* db) {
-    uint32_t c = threadIdx.x;
-    if (c >= C) return;
-    float s = 0.0f;
-    for (uint64_t p = blockIdx.x; p < P; p += gridDim.x) s += __bfloat162float(dy[p * dys + c]);
-    atomicAdd(&db[c], s);
 }
 // Adam (Kingma & Ba 2015) on the f32 master values, then the bf16 forward copy.
 __global__ void k_adam(float* w, const float* g, float* m, float* v, uint64_t n, float lr, float b1, float b2,
@@ -690,36 +793,55 @@ EncodeTiledFn encode_tiled() {
     return fn;
 }
 
+// The 128-pixel tiles of a W x H image: bw the largest power of two <= 128 that divides the width, bh = 128 / bw.
+void tile_shape(uint32_t W, uint32_t H, uint32_t& bw, uint32_t& bh, uint32_t& tiles_x, uint32_t& tiles_y) {
+    bw = 1;
+    while (bw < 128u && W % (bw * 2u) == 0u) bw *= 2u;
+    bh = 128u / bw;
+    tiles_x = W / bw;
+    tiles_y = (H + bh - 1u) / bh;
+}
+
+// A tensor map of an activation: (channels, x, y, image) with `stride` channels a pixel, boxes of 32 channels x bw x bh
+// pixels landing as 64-byte rows with the 64-byte swizzle; reads outside the tensor are zeros.
+bool act_map(Net* n, CUtensorMap* m, const bf16* p, uint32_t stride, uint32_t B, uint32_t H, uint32_t W, uint32_t bw,
+             uint32_t bh) {
+    EncodeTiledFn enc = encode_tiled();
+    if (!enc) {
+        n->conv_err = "unet: cuTensorMapEncodeTiled is not available";
+        return false;
+    }
+    cuuint64_t d[4] = {stride, W, H, B};
+    cuuint64_t st[3] = {(cuuint64_t)stride * 2u, (cuuint64_t)W * stride * 2u, (cuuint64_t)H * W * stride * 2u};
+    cuuint32_t box[4] = {32u, bw, bh, 1u}, es[4] = {1u, 1u, 1u, 1u};
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16*>(p), d, st, box, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        n->conv_err = "unet: an activation's tensor map was refused (" + std::to_string((int)r) + ")";
+        return false;
+    }
+    return true;
+}
+
 // One convolution: x (NHWC bf16, x_stride channels a pixel, channels [x_off, x_off + cin) read) into y or yf, with
 // w [9][co_pad][cin] (each tap's output channels, their input channels contiguous).
 void conv_run(Net* n, const bf16* x, uint32_t x_stride, uint32_t x_off, uint32_t cin, const bf16* w, uint32_t co_pad,
               const float* bias, bf16* y, uint32_t y_stride, uint32_t y_off, uint32_t cout, float* yf, uint32_t B,
               uint32_t H, uint32_t W, int relu) {
-    uint32_t bw = 1;
-    while (bw < 128u && W % (bw * 2u) == 0u) bw *= 2u;
-    const uint32_t bh = 128u / bw, tiles_x = W / bw, tiles_y = (H + bh - 1u) / bh;
+    uint32_t bw, bh, tiles_x, tiles_y;
+    tile_shape(W, H, bw, bh, tiles_x, tiles_y);
     const uint32_t nt = co_pad % 128u == 0u ? 128u : 64u;  // co_pad: a multiple of 64
-    EncodeTiledFn enc = encode_tiled();
-    if (!enc) {
-        n->conv_err = "unet: cuTensorMapEncodeTiled is not available";
-        return;
-    }
-    // the activations: (channels, x, y, image), boxes of 32 channels x bw x bh; the weights: (input channel, output
-    // channel, tap), boxes of 32 x nt x 1; both 64-byte rows with the 64-byte swizzle
+    // the activations: boxes of 32 channels x bw x bh; the weights: (input channel, output channel, tap), boxes of
+    // 32 x nt x 1; both 64-byte rows with the 64-byte swizzle
     CUtensorMap xmap, wmap;
-    cuuint64_t xd[4] = {x_stride, W, H, B};
-    cuuint64_t xs[3] = {(cuuint64_t)x_stride * 2u, (cuuint64_t)W * x_stride * 2u, (cuuint64_t)H * W * x_stride * 2u};
-    cuuint32_t xb[4] = {32u, bw, bh, 1u}, es[4] = {1u, 1u, 1u, 1u};
+    if (!act_map(n, &xmap, x, x_stride, B, H, W, bw, bh)) return;
     cuuint64_t wd[3] = {cin, co_pad, 9u};
     cuuint64_t ws[2] = {(cuuint64_t)cin * 2u, (cuuint64_t)co_pad * cin * 2u};
-    cuuint32_t wb[3] = {32u, nt, 1u};
-    CUresult r = enc(&xmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16*>(x), xd, xs, xb, es,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r == CUDA_SUCCESS)
-        r = enc(&wmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<bf16*>(w), wd, ws, wb, es,
-                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    cuuint32_t wb[3] = {32u, nt, 1u}, es[3] = {1u, 1u, 1u};
+    CUresult r = encode_tiled()(&wmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<bf16*>(w), wd, ws, wb, es,
+                                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+                                CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
         n->conv_err = "unet: a convolution's tensor map was refused (" + std::to_string((int)r) + ")";
         return;
@@ -743,13 +865,32 @@ void conv_dx(Net* n, int li, const Act& dy, const Act& dx, uint32_t B, uint32_t 
     conv_run(n, dy.p, dy.stride, 0u, r32(L.cout), n->wb[li], r64(L.cin), nullptr, dx.p, dx.stride, 0u, L.cin, nullptr,
              B, H, W, 0);
 }
+// The weight and bias gradients of layer li from its input x (channels [x_off, x_off + cin)) and its output gradient dy
+// (cout rounded to 32 channels), summed into the layer's gradients.
 void wgrad(Net* n, int li, const Act& x, uint32_t x_off, const Act& dy, uint32_t B, uint32_t H, uint32_t W) {
     const Layer& L = LAYERS[li];
-    uint32_t M = B * H * W, chunk = 2048;
-    WGrad a{x.p, x.stride, x_off, L.cin, dy.p, dy.stride, r32(L.cout), n->g + n->off[li], r64(L.cout), B, H, W, chunk};
-    k_wgrad<<<dim3((M + chunk - 1) / chunk, 9, (L.cin / 32) * (r32(L.cout) / 32)), 128, 0, n->stream>>>(a);
-    k_bgrad<<<std::min<uint32_t>(1024, M), 128, 0, n->stream>>>(dy.p, dy.stride, r32(L.cout), M,
-                                                                 n->g + n->off[li] + w_count(L));
+    uint32_t bw, bh, tiles_x, tiles_y;
+    tile_shape(W, H, bw, bh, tiles_x, tiles_y);
+    const uint32_t kc = L.cin / 32u, nb = r32(L.cout) / 32u, pairs = 9u * kc, groups = (pairs + 4u) / 4u;
+    const uint32_t tiles = B * tiles_x * tiles_y, stage = (4u + nb) * WG_BOX;
+    // two stages where two CTAs then fit an SM (228 KB, 1 KB of it reserved a CTA), else as many as one CTA holds
+    uint32_t ts = 2u, per_sm = 2u;
+    if (2u * (ts * stage + WG_SMEM_EXTRA + 1024u) > 228u * 1024u) {
+        ts = std::min<uint32_t>(4u, (WG_SMEM_MAX - WG_SMEM_EXTRA) / stage);
+        per_sm = 1u;
+    }
+    const uint32_t smem = ts * stage + WG_SMEM_EXTRA;
+    // one wave: runs of tiles so that the groups x runs fill the SMs
+    const uint32_t slots = n->sms * per_sm;
+    const uint32_t chunk = std::max<uint32_t>(1u, (tiles * groups + slots - 1u) / slots);
+    const uint32_t chunks = (tiles + chunk - 1u) / chunk;
+    CUtensorMap xmap, dmap;
+    if (!act_map(n, &xmap, x.p, x.stride, B, H, W, bw, bh) || !act_map(n, &dmap, dy.p, dy.stride, B, H, W, bw, bh))
+        return;
+    float* dw = n->g + n->off[li];
+    WGrad a{L.cin, x_off, kc, nb, pairs, dw, dw + w_count(L), r64(L.cout), bw, bh, tiles_x, tiles_y, tiles, chunk, ts,
+            n->dev_err};
+    k_wgrad<<<dim3(chunks, groups), WG_THREADS, smem, n->stream>>>(xmap, dmap, a);
 }
 void relu_back(Net* n, const Act& dy, uint32_t dyo, const Act& y, uint32_t yo, uint32_t C, uint64_t P) {
     k_relu_back<<<blocks(P * C), 256, 0, n->stream>>>(dy.p, dy.stride, dyo, y.p, y.stride, yo, C, P);
@@ -961,6 +1102,8 @@ int trt_unet_create(int device, uint32_t max_batch, uint32_t max_h, uint32_t max
     if (e == cudaSuccess) e = alloc(n, &n->dev_err, 1);
     if (e == cudaSuccess) e = alloc(n, &n->partial, 3 * FEAT_BLOCKS);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CONV_SMEM);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WG_SMEM_MAX);
     if (e == cudaSuccess) {
         int sms = 0;
         e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
