@@ -74,8 +74,11 @@ def test_forward_on_wide_rows_matches_the_oracle():
     wide.close()
 
 
-def test_every_layers_gradient_matches_the_oracle(net):
-    p, feats, tgt = case(seed=5)
+@pytest.mark.parametrize("b,h,w", [(2, 16, 16), (4, 64, 64)])
+def test_every_layers_gradient_matches_the_oracle(net, b, h, w):
+    # 2 x 16 x 16: a 128-pixel tile a CTA; 4 x 64 x 64: the weight gradient's CTAs take runs of two to six tiles at
+    # the two top levels (the accumulator summed over stages, the pipeline's stages reused)
+    p, feats, tgt = case(seed=5, b=b, h=h, w=w)
     net.set_params(p)
     loss, g, _ = net.step(feats, tgt, update=False, grads=True)
     ref_loss, G, _ = R.loss_and_grads(R.unpack(bf16(p).astype(np.float64)), bf16(feats).astype(np.float64), tgt)
@@ -90,6 +93,15 @@ def test_every_layers_gradient_matches_the_oracle(net):
     # the padding's gradients are zero
     flat = R.pack(gp, g)
     assert np.allclose(g[flat == 0], 0.0)
+
+
+def test_gradients_are_the_same_every_step(net):
+    # the weight gradient's CTA partials are summed in a fixed order: no dependence on the CTAs' timing
+    p, feats, tgt = case(seed=10, b=4, h=64, w=64)
+    net.set_params(p)
+    _, g1, _ = net.step(feats, tgt, update=False, grads=True)
+    _, g2, _ = net.step(feats, tgt, update=False, grads=True)
+    assert np.array_equal(g1, g2)
 
 
 def test_training_fits_a_batch(net):

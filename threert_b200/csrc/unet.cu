@@ -6,8 +6,8 @@
 // N = output channels, K = 9 taps x input channels) on the 5th-generation tensor cores (TMA loads, tcgen05.mma into
 // tensor memory, f32 accumulation). The input gradient is the same kernel run on the output gradient with the
 // weights flipped and transposed; the weight and bias gradients are one GEMM over pixels on the same tensor cores
-// (both operands MN-major, split across CTAs, summed with f32 atomics). Master weights, gradients and Adam's moments
-// are f32.
+// (both operands MN-major, split across CTAs whose f32 partials a second kernel sums in a fixed order, so that training
+// is deterministic). Master weights, gradients and Adam's moments are f32.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -327,7 +327,8 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ C
 //  - one thread issues eight tcgen05.mma (M 128, N, K 16, both operands MN-major, f32 accumulate in tensor memory)
 //    a stage and hands the stage back to the loader through an mbarrier;
 //  - after the run the four epilogue warps read the accumulator (warp w: slot w % 4, its lanes the slot's 32 input
-//    channels) and add it into dw, and the ones slot's first row into db, with 16-byte f32 atomics.
+//    channels) and store it as the CTA's f32 partial; k_wgrad_sum adds the partials of a group's runs, in run order,
+//    into dw (and the ones slot's first row into db), so that the sums do not depend on the CTAs' timing.
 // Slots that no pair fills hold zeros; they and the ones slot are written once, when the CTA starts. Waits are
 // bounded as the convolution's are; after a wait that gave up, the CTA waits (bounded) for its copies and MMAs in
 // flight before it frees its tensor memory.
@@ -335,9 +336,7 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ C
 struct WGrad {
     uint32_t cin, x_off;      // input channels (a multiple of 32) and their first channel in x
     uint32_t kc, nb, pairs;   // input blocks of 32, output-gradient blocks of 32 (N = 32 nb), 9 kc (the ones slot's index)
-    float* dw;                // [9][cin][co_pad] f32, summed into
-    float* db;                // [co_pad] f32, summed into
-    uint32_t co_pad;
+    float* part;              // [group][run][128][32 nb] f32: the CTAs' partials
     uint32_t bw, bh, tiles_x, tiles_y, tiles, chunk;  // 128-pixel tiles (bw x bh) over all images; tiles a CTA
     uint32_t ts;              // pipeline stages
     uint32_t* err;
@@ -471,19 +470,13 @@ __global__ void __launch_bounds__(WG_THREADS) k_wgrad(const __grid_constant__ CU
         __syncwarp();
         tc_fence_after();
         if (fin && (quarter < loaded || slot == a.pairs)) {
-            float* dst = nullptr;
-            if (slot < a.pairs)
-                dst = a.dw + ((uint64_t)(slot / a.kc) * a.cin + (slot % a.kc) * 32u + lane) * a.co_pad;
-            else if (lane == 0)
-                dst = a.db;  // every row of the ones slot is the bias gradient
+            float* dst = a.part + (((uint64_t)blockIdx.y * gridDim.x + blockIdx.x) * 128u + quarter * 32u + lane) * n_cols;
             for (uint32_t cc = 0; cc < n_cols; cc += 32u) {
                 float v[32];
                 tmem_ld32(tmem + ((quarter * 32u) << 16) + cc, v);
-                if (dst)
 #pragma unroll
-                    for (uint32_t q = 0; q < 8u; ++q)
-                        atomicAdd(reinterpret_cast<float4*>(dst + cc) + q,
-                                  make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]));
+                for (uint32_t q = 0; q < 8u; ++q)
+                    reinterpret_cast<float4*>(dst + cc)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
             }
         }
     }
@@ -501,6 +494,49 @@ __global__ void __launch_bounds__(WG_THREADS) k_wgrad(const __grid_constant__ CU
     tc_fence_after();
     if (warp == 1)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
+}
+
+// The partials of k_wgrad summed over a group's runs: a block takes 32 outputs (a group's accumulator row and 4
+// columns each, of the slots that hold a pair and the first row of the ones slot) x 8 segments of runs (segment j:
+// runs j, j + 8, ...), the segments then summed in order; every sum is taken in the same order on every call. Added
+// into dw[t][c][n] and db[n].
+constexpr uint32_t WS_SEGS = 8u;
+__global__ void __launch_bounds__(32u * WS_SEGS) k_wgrad_sum(const float* __restrict__ part, uint32_t runs,
+                                                             uint32_t groups, uint32_t n_cols, uint32_t kc,
+                                                             uint32_t pairs, uint32_t cin, uint32_t co_pad, float* dw,
+                                                             float* db) {
+    __shared__ float4 seg[WS_SEGS][32];
+    const uint32_t nq = n_cols / 4u, lane = threadIdx.x & 31u, j = threadIdx.x >> 5;
+    const uint64_t i = (uint64_t)blockIdx.x * 32u + lane;
+    const uint32_t q = (uint32_t)(i % nq), m = (uint32_t)((i / nq) % 128u), g = (uint32_t)(i / (nq * 128u));
+    const uint32_t slot = g * 4u + m / 32u, c = m % 32u;
+    const bool live = i < (uint64_t)groups * 128u * nq && (slot < pairs || (slot == pairs && c == 0u));
+    float4 s = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (live) {
+        const float4* p = reinterpret_cast<const float4*>(part + ((uint64_t)g * runs * 128u + m) * n_cols) + q;
+        const uint64_t run_stride = 128ull * nq;
+        for (uint32_t r = j; r < runs; r += WS_SEGS) {
+            const float4 v = __ldg(p + r * run_stride);
+            s.x += v.x;
+            s.y += v.y;
+            s.z += v.z;
+            s.w += v.w;
+        }
+    }
+    seg[j][lane] = s;
+    __syncthreads();
+    if (j != 0u || !live) return;
+    for (uint32_t k = 1; k < WS_SEGS; ++k) {
+        const float4 v = seg[k][lane];
+        s.x += v.x;
+        s.y += v.y;
+        s.z += v.z;
+        s.w += v.w;
+    }
+    float4* d = reinterpret_cast<float4*>(
+                    slot < pairs ? dw + ((uint64_t)(slot / kc) * cin + (slot % kc) * 32u + c) * co_pad : db) + q;
+    const float4 o = *d;
+    *d = make_float4(o.x + s.x, o.y + s.y, o.z + s.z, o.w + s.w);
 }
 
 // ---- the other layers ----------------------------------------------------------------------------------------------
@@ -608,11 +644,13 @@ __global__ void k_loss(const float* pred, const float* target, uint64_t P, bf16*
     for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(~0u, l, o);
     if ((threadIdx.x & 31u) == 0 && l != 0.0f) atomicAdd(loss, l / (float)(P * 3));
 }
-// Adam (Kingma & Ba 2015) on the f32 master values, then the bf16 forward copy.
-__global__ void k_adam(float* w, const float* g, float* m, float* v, uint64_t n, float lr, float b1, float b2,
-                       float c1, float c2, float eps) {
+// Adam (Kingma & Ba 2015) on the f32 master values, then the bf16 forward copy. `args`: the step's learning rate and
+// bias corrections 1 - b1^t, 1 - b2^t (device memory, so that a captured step reads each step's values).
+__global__ void k_adam(float* w, const float* g, float* m, float* v, uint64_t n, const float* args, float b1, float b2,
+                       float eps) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const float lr = args[0], c1 = args[1], c2 = args[2];
     float gi = g[i];
     float mi = b1 * m[i] + (1.0f - b1) * gi, vi = b2 * v[i] + (1.0f - b2) * gi * gi;
     m[i] = mi;
@@ -749,6 +787,13 @@ struct Net {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     uint32_t* dev_err = nullptr;  // set by a convolution whose pipeline wait gave up
     uint32_t sms = 148;           // the device's SMs (the persistent convolution's grid)
+    float* wpart = nullptr;       // the weight gradient's CTA partials (128 x 128 f32 each)
+    uint32_t wpart_ctas = 0;      // their room, in CTAs
+    // the training step's kernels captured once per batch shape (and with or without the update), replayed after
+    float* adam_args = nullptr;       // device: learning rate, 1 - b1^t, 1 - b2^t
+    float* adam_host = nullptr;       // pinned: the same, written before each replay
+    struct StepGraph { uint32_t B, H, W; int update; cudaGraphExec_t exec; };
+    std::vector<StepGraph> graphs;
     float* partial = nullptr;     // the feature sums' block partials
     std::string conv_err;         // a tensor map that could not be made
 };
@@ -887,10 +932,15 @@ void wgrad(Net* n, int li, const Act& x, uint32_t x_off, const Act& dy, uint32_t
     CUtensorMap xmap, dmap;
     if (!act_map(n, &xmap, x.p, x.stride, B, H, W, bw, bh) || !act_map(n, &dmap, dy.p, dy.stride, B, H, W, bw, bh))
         return;
-    float* dw = n->g + n->off[li];
-    WGrad a{L.cin, x_off, kc, nb, pairs, dw, dw + w_count(L), r64(L.cout), bw, bh, tiles_x, tiles_y, tiles, chunk, ts,
-            n->dev_err};
+    if (chunks * groups > n->wpart_ctas) {  // (at most the SMs' slots + groups, which the room holds)
+        n->conv_err = "unet: the weight gradient's partials exceed their buffer";
+        return;
+    }
+    WGrad a{L.cin, x_off, kc, nb, pairs, n->wpart, bw, bh, tiles_x, tiles_y, tiles, chunk, ts, n->dev_err};
     k_wgrad<<<dim3(chunks, groups), WG_THREADS, smem, n->stream>>>(xmap, dmap, a);
+    float* dw = n->g + n->off[li];
+    k_wgrad_sum<<<groups * 128u * nb * 8u / 32u, 32u * WS_SEGS, 0, n->stream>>>(
+        n->wpart, chunks, groups, 32u * nb, kc, pairs, L.cin, r64(L.cout), dw, dw + w_count(L));
 }
 void relu_back(Net* n, const Act& dy, uint32_t dyo, const Act& y, uint32_t yo, uint32_t C, uint64_t P) {
     k_relu_back<<<blocks(P * C), 256, 0, n->stream>>>(dy.p, dy.stride, dyo, y.p, y.stride, yo, C, P);
@@ -1025,6 +1075,48 @@ void denoise_device(Net* n, const void* accum_device, uint32_t W, uint32_t H) {
     k_unfeat<<<blocks(P * 3), 256, 0, s>>>(n->pred, P, n->sums, n->rgb);
 }
 
+// A training step's kernels, from the staged features and targets to the refreshed weights (Adam's scalars read from
+// adam_args).
+void train_kernels(Net* n, uint32_t B, uint32_t H, uint32_t W, int update) {
+    uint64_t P = (uint64_t)B * H * W;
+    cudaStream_t s = n->stream;
+    k_feat_host<<<blocks(P * 32), 256, 0, s>>>(n->feat, P, n->in0.p);
+    forward(n, B, H, W);
+    cudaMemsetAsync(n->loss, 0, 4, s);
+    cudaMemsetAsync(n->dpred.p, 0, 2 * 32 * P, s);
+    cudaMemsetAsync(n->g, 0, 4 * n->n_params, s);
+    k_loss<<<blocks(P * 3), 256, 0, s>>>(n->pred, n->target, P, n->dpred.p, n->loss);
+    backward(n, B, H, W);
+    if (update) {
+        k_adam<<<blocks(n->n_params), 256, 0, s>>>(n->w, n->g, n->m, n->v, n->n_params, n->adam_args, 0.9f, 0.999f,
+                                                    1e-8f);
+        refresh_weights(n);
+    }
+}
+
+// The training step's graph for this shape: captured from train_kernels on first use (a tensor map refused during
+// the capture leaves no graph and the error in conv_err).
+cudaError_t step_graph(Net* n, uint32_t B, uint32_t H, uint32_t W, int update, cudaGraphExec_t* out) {
+    for (const Net::StepGraph& g : n->graphs)
+        if (g.B == B && g.H == H && g.W == W && g.update == update) {
+            *out = g.exec;
+            return cudaSuccess;
+        }
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(n->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    train_kernels(n, B, H, W, update);
+    e = cudaStreamEndCapture(n->stream, &graph);
+    if (e == cudaSuccess && !n->conv_err.empty()) e = cudaErrorInvalidValue;
+    cudaGraphExec_t exec = nullptr;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return e;
+    n->graphs.push_back({B, H, W, update, exec});
+    *out = exec;
+    return cudaSuccess;
+}
+
 // The end of a call: its stream drained, then what its convolutions reported (a refused tensor map on the host, a
 // pipeline wait that gave up on the device).
 int finish(Net* n, const char* what) {
@@ -1108,7 +1200,11 @@ int trt_unet_create(int device, uint32_t max_batch, uint32_t max_h, uint32_t max
         int sms = 0;
         e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
         if (sms > 0) n->sms = (uint32_t)sms;
+        n->wpart_ctas = 2u * n->sms + 16u;
+        e = alloc(n, &n->wpart, (uint64_t)n->wpart_ctas * 128u * 128u);
     }
+    if (e == cudaSuccess) e = alloc(n, &n->adam_args, 4);
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&n->adam_host, 16);
     if (e == cudaSuccess) e = cudaEventCreate(&n->e0);
     if (e == cudaSuccess) e = cudaEventCreate(&n->e1);
     if (e != cudaSuccess) {
@@ -1124,6 +1220,8 @@ void trt_unet_destroy(trt_unet* n) {
     if (!n) return;
     cudaSetDevice(n->device);
     if (n->stream) cudaStreamSynchronize(n->stream);
+    for (const Net::StepGraph& g : n->graphs) cudaGraphExecDestroy(g.exec);
+    if (n->adam_host) cudaFreeHost(n->adam_host);
     for (void* p : n->allocs) cudaFree(p);
     if (n->e0) cudaEventDestroy(n->e0);
     if (n->e1) cudaEventDestroy(n->e1);
@@ -1177,23 +1275,27 @@ int trt_unet_train_step(trt_unet* n, const float* features, const float* targets
     if (rc) return rc;
     uint64_t P = (uint64_t)B * H * W;
     cudaStream_t s = n->stream;
+    cudaGraphExec_t exec = nullptr;
+    cudaError_t e = step_graph(n, B, H, W, update ? 1 : 0, &exec);
+    if (e != cudaSuccess) {
+        if (!n->conv_err.empty()) {
+            n->err = n->conv_err;
+            n->conv_err.clear();
+            return TRT_ECUDA;
+        }
+        return cuda_check(n, e, "trt_unet_train_step: the step's graph");
+    }
+    if (update) {
+        n->t++;
+        n->adam_host[0] = lr;
+        n->adam_host[1] = 1.0f - std::pow(0.9f, (float)n->t);
+        n->adam_host[2] = 1.0f - std::pow(0.999f, (float)n->t);
+        cudaMemcpyAsync(n->adam_args, n->adam_host, 12, cudaMemcpyHostToDevice, s);
+    }
     cudaMemcpyAsync(n->feat, features, 4ull * N_FEAT * P, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(n->target, targets, 12 * P, cudaMemcpyHostToDevice, s);
     cudaEventRecord(n->e0, s);
-    k_feat_host<<<blocks(P * 32), 256, 0, s>>>(n->feat, P, n->in0.p);
-    forward(n, B, H, W);
-    cudaMemsetAsync(n->loss, 0, 4, s);
-    cudaMemsetAsync(n->dpred.p, 0, 2 * 32 * P, s);
-    cudaMemsetAsync(n->g, 0, 4 * n->n_params, s);
-    k_loss<<<blocks(P * 3), 256, 0, s>>>(n->pred, n->target, P, n->dpred.p, n->loss);
-    backward(n, B, H, W);
-    if (update) {
-        n->t++;
-        const float b1 = 0.9f, b2 = 0.999f;
-        float c1 = 1.0f - std::pow(b1, (float)n->t), c2 = 1.0f - std::pow(b2, (float)n->t);
-        k_adam<<<blocks(n->n_params), 256, 0, s>>>(n->w, n->g, n->m, n->v, n->n_params, lr, b1, b2, c1, c2, 1e-8f);
-        refresh_weights(n);
-    }
+    cudaGraphLaunch(exec, s);
     cudaEventRecord(n->e1, s);
     if (loss) cudaMemcpyAsync(loss, n->loss, 4, cudaMemcpyDeviceToHost, s);
     if (grads) cudaMemcpyAsync(grads, n->g, 4 * n->n_params, cudaMemcpyDeviceToHost, s);
