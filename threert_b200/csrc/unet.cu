@@ -43,7 +43,8 @@ __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)
 //    commits each stage's buffers back to the loader through an mbarrier; TS stages in flight;
 //  - the four warps read the accumulator out of tensor memory (each its 32 lanes = pixels), add the bias, apply the
 //    ReLU and store bf16 (or f32) NHWC.
-// Every mbarrier wait is bounded (about a second); a wait that gives up sets the error word and the CTA finishes.
+// Every mbarrier wait is bounded (about a second); a wait that gives up sets the error word, and the CTA waits
+// (bounded) for its copies and MMAs in flight and finishes.
 
 struct Conv {
     uint32_t cin;             // channels read (a multiple of 32)
@@ -92,6 +93,13 @@ __device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity, uint32_t*
             return false;
         }
     }
+    return true;
+}
+// A wait bounded at about 2^31 cycles that ignores the abort word: the drain of a CTA that gave up.
+__device__ __forceinline__ bool mbar_wait_drain(uint32_t a, uint32_t parity) {
+    long long t0 = clock64();
+    while (!mbar_try_wait(a, parity))
+        if (clock64() - t0 > (1ll << 31)) return false;
     return true;
 }
 __device__ __forceinline__ void tma_load_4d(uint32_t dst, const void* map, int c0, int c1, int c2, int c3,
@@ -186,14 +194,16 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ C
     const uint32_t sraw = smem_addr(smem_raw), sbase = (sraw + 1023u) & ~1023u;
     uint8_t* smem = smem_raw + (sbase - sraw);
     const uint32_t sA = sbase, sB = sbase + TS * A_STAGE, sBar = sbase + TS * (A_STAGE + B_STAGE);
-    // barriers: full[TS], empty[TS] (the stages), acc_full[2], acc_empty[2] (the accumulators); the tensor-memory
-    // address and the abort word after them
+    // barriers: full[TS], empty[TS] (the stages), acc_full[2], acc_empty[2] (the accumulators), mma_done (every MMA
+    // issued); the tensor-memory address, the abort word and the counts of stages issued and consumed after them
     auto full = [&](uint32_t s) { return sBar + 8u * s; };
     auto empty = [&](uint32_t s) { return sBar + 8u * (TS + s); };
     auto acc_full = [&](uint32_t i) { return sBar + 8u * (2u * TS + i); };
     auto acc_empty = [&](uint32_t i) { return sBar + 8u * (2u * TS + 2u + i); };
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + TS * (A_STAGE + B_STAGE) + 8u * (2u * TS + 4u));
+    const uint32_t mma_done = sBar + 8u * (2u * TS + 4u);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + TS * (A_STAGE + B_STAGE) + 8u * (2u * TS + 5u));
     volatile uint32_t* abort_flag = tslot + 1;
+    volatile uint32_t* counts = tslot + 2;
     const uint32_t ncols = 2u * a.nt;  // two accumulators of nt columns: 128 or 256
     const uint32_t per_img = a.tiles_x * a.tiles_y, n_ntiles = a.co_pad / a.nt;
     const uint32_t tiles = a.B * per_img * n_ntiles;
@@ -208,7 +218,9 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ C
             mbar_init(acc_full(i), 1);
             mbar_init(acc_empty(i), CONV_EPI_THREADS);
         }
+        mbar_init(mma_done, 1);
         *abort_flag = 0u;
+        counts[0] = counts[1] = 0u;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 1) {
@@ -251,6 +263,7 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ C
                     tma_load_3d(sB + s * B_STAGE, &wmap, (int)c0, (int)n0, (int)tap, full(s));
                 }
             }
+            counts[0] = it;
         }
     } else if (warp == 1) {
         if (lane == 0) {
@@ -275,8 +288,10 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ C
                     }
                     umma_commit(empty(s));
                 }
-                umma_commit(acc_full(acc));
+                if (ok) umma_commit(acc_full(acc));
             }
+            counts[1] = it;
+            umma_commit(mma_done);  // every MMA issued is done (after a wait that gave up too)
         }
     } else {
         // the epilogue: warp w reads tensor-memory lanes 32 (w % 4) ... (its rows: pixels of the tile)
@@ -310,6 +325,15 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ C
     __syncwarp();
     tc_fence_before();
     __syncthreads();
+    if (*abort_flag && lane == 0) {
+        // a wait gave up: let the copies and MMAs in flight land before the memory they use is released
+        if (warp == 0)
+            for (uint32_t i = counts[1]; i < counts[0]; ++i) mbar_wait_drain(full(i % TS), (i / TS) & 1u);
+        else if (warp == 1)
+            mbar_wait_drain(mma_done, 0u);
+    }
+    __syncthreads();
+    tc_fence_after();
     if (warp == 1)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
 }
@@ -351,13 +375,6 @@ constexpr uint32_t WG_SMEM_MAX = 227u * 1024u;
 __device__ __forceinline__ uint64_t umma_desc_mn64(uint32_t saddr, uint32_t lbo) {
     return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
            ((uint64_t)(512u >> 4) << 32) | (1ull << 46) | (4ull << 61);
-}
-// A wait bounded at about 2^31 cycles that ignores the abort word: the drain of a CTA that gave up.
-__device__ __forceinline__ bool mbar_wait_drain(uint32_t a, uint32_t parity) {
-    long long t0 = clock64();
-    while (!mbar_try_wait(a, parity))
-        if (clock64() - t0 > (1ll << 31)) return false;
-    return true;
 }
 // 32 accumulator columns of this warp's lanes.
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
