@@ -977,7 +977,10 @@ int render_waves(trt_scene* s, const Params& P, uint32_t first_sample, uint32_t 
     if (rc) return rc;
     Walk wk{scene_view(s), s->wide.view(), P.w[P_MOTION + 2], P.w[P_MOTION + 3]};
     uint32_t last = P.w[P_COUNTS + 2];
-    bool sort_rays = (flags & TRT_RENDER_SORT_RAYS) != 0, sort_hits = (flags & TRT_RENDER_UNSORTED_HITS) == 0;
+    // the material table's records (18 vec4 each) between its first row and the lights' first row
+    const uint32_t n_materials = (P.w[P_TABLE_FIRST + 2] - P.w[P_TABLE_FIRST + 1]) / 18u;
+    bool sort_rays = (flags & TRT_RENDER_SORT_RAYS) != 0;
+    bool sort_hits = (flags & TRT_RENDER_UNSORTED_HITS) == 0 && n_materials > TRT_SORT_HITS_MIN_MATERIALS;
     bool sort_shadows = (flags & TRT_RENDER_SORT_SHADOWS) != 0;
     const int blk = 128;
     int g_ext = grid_for((const void*)k_extend<COUNT, WIDE, false>, blk, c->sm_count);
