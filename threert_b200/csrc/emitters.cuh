@@ -90,20 +90,34 @@ __global__ void k_em_weigh(Weigh W) {
     tput(W, (uint64_t)W.entries + id, make_float4(__uint_as_float(e.x), 0.0f, fmaxf(w, 0.0f), area));
 }
 
-// scan_a: each block of 256 entries' running sum, in order; the block's sum.
-__global__ void k_em_scan_a(Weigh W) {
-    uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-    uint32_t nb = (W.n + BLOCK - 1u) / BLOCK;
-    if (b >= nb) return;
-    uint32_t lo = b * BLOCK, hi = min(lo + BLOCK, W.n);
-    float sum = 0.0f;
-    for (uint32_t k = lo; k < hi; ++k) {
-        float4 e = tgetf(W, (uint64_t)W.entries + k);
-        sum += e.z;
-        e.y = sum;
-        tput(W, (uint64_t)W.entries + k, e);
+// scan_a: each block of 256 entries' running sum, in order; the block's sum. A warp a block: its lanes stage the
+// weights in shared memory, one lane adds them up in entry order (the reference's rounding), the lanes write back.
+constexpr uint32_t SCAN_WARPS = 4u;
+__global__ void __launch_bounds__(32u * SCAN_WARPS) k_em_scan_a(Weigh W) {
+    __shared__ float run[SCAN_WARPS][BLOCK];
+    const uint32_t lane = threadIdx.x & 31u, wi = threadIdx.x >> 5;
+    const uint32_t b = blockIdx.x * SCAN_WARPS + wi;
+    const uint32_t nb = (W.n + BLOCK - 1u) / BLOCK;
+    if (b >= nb) return;  // (whole warps)
+    const uint32_t lo = b * BLOCK, cnt = min(BLOCK, W.n - lo);
+    float* r = run[wi];
+    for (uint32_t k = lane; k < cnt; k += 32u) r[k] = tgetf(W, (uint64_t)W.entries + lo + k).z;
+    __syncwarp();
+    if (lane == 0) {
+        float sum = 0.0f;
+#pragma unroll 8
+        for (uint32_t k = 0; k < cnt; ++k) {
+            sum += r[k];
+            r[k] = sum;
+        }
+        W.blocks[b] = make_float4(sum, 0.0f, 0.0f, 0.0f);
     }
-    W.blocks[b] = make_float4(sum, 0.0f, 0.0f, 0.0f);
+    __syncwarp();
+    for (uint32_t k = lane; k < cnt; k += 32u) {
+        float4 e = tgetf(W, (uint64_t)W.entries + lo + k);
+        e.y = r[k];
+        tput(W, (uint64_t)W.entries + lo + k, e);
+    }
 }
 
 // scan_b: the blocks' offsets, in order; after the last, the total. One thread.
@@ -281,7 +295,7 @@ int trt_scene_weigh_emitters(trt_scene* s, const uint32_t* P, uint32_t tree_node
     if (!up.empty()) TRT_CUDA(c, cudaMemcpyAsync(d_levels, up.data(), up.size() * 4, cudaMemcpyHostToDevice, st));
     if (ms) TRT_CUDA(c, cudaEventRecord(c->t0, st));
     k_em_weigh<<<(n + 63) / 64, 64, 0, st>>>(W);
-    k_em_scan_a<<<(nb + 63) / 64, 64, 0, st>>>(W);
+    k_em_scan_a<<<(nb + SCAN_WARPS - 1u) / SCAN_WARPS, 32u * SCAN_WARPS, 0, st>>>(W);
     k_em_scan_b<<<1, 32, 0, st>>>(W);
     k_em_scan_c<<<(n + 63) / 64, 64, 0, st>>>(W);
     k_em_guide<<<(GUIDE / 4u + 1u + 127u) / 128u, 128, 0, st>>>(W);
