@@ -1112,7 +1112,8 @@ void train_kernels(Net* n, uint32_t B, uint32_t H, uint32_t W, int update) {
 }
 
 // The training step's graph for this shape: captured from train_kernels on first use (a tensor map refused during
-// the capture leaves no graph and the error in conv_err).
+// the capture leaves no graph and the error in conv_err); at most MAX_STEP_GRAPHS shapes are kept.
+constexpr size_t MAX_STEP_GRAPHS = 16;
 cudaError_t step_graph(Net* n, uint32_t B, uint32_t H, uint32_t W, int update, cudaGraphExec_t* out) {
     for (const Net::StepGraph& g : n->graphs)
         if (g.B == B && g.H == H && g.W == W && g.update == update) {
@@ -1129,6 +1130,10 @@ cudaError_t step_graph(Net* n, uint32_t B, uint32_t H, uint32_t W, int update, c
     if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
     if (graph) cudaGraphDestroy(graph);
     if (e != cudaSuccess) return e;
+    if (n->graphs.size() >= MAX_STEP_GRAPHS) {  // the oldest shape's graph makes room (its launches have finished:
+        cudaGraphExecDestroy(n->graphs.front().exec);  // every call ends with the stream drained)
+        n->graphs.erase(n->graphs.begin());
+    }
     n->graphs.push_back({B, H, W, update, exec});
     *out = exec;
     return cudaSuccess;
