@@ -224,16 +224,6 @@ __global__ void k_unit_boxes(const uint4* __restrict__ tables, uint32_t t_instan
     T.centre[u] = f4((blo + bhi) * 0.5f, 0.0f);
 }
 
-// Atomic min / max of floats in shared memory, by their bits (non-negative floats order as ints, negative ones in
-// reverse as unsigned).
-__device__ __forceinline__ void atomic_min_f(float* a, float v) {
-    if (__float_as_int(v) >= 0) atomicMin((int*)a, __float_as_int(v));
-    else atomicMax((unsigned*)a, __float_as_uint(v));
-}
-__device__ __forceinline__ void atomic_max_f(float* a, float v) {
-    if (__float_as_int(v) >= 0) atomicMax((int*)a, __float_as_int(v));
-    else atomicMin((unsigned*)a, __float_as_uint(v));
-}
 __device__ __forceinline__ float area3(V3 lo, V3 hi) {
     V3 e = V3{gmax(hi.x - lo.x, 0.0f), gmax(hi.y - lo.y, 0.0f), gmax(hi.z - lo.z, 0.0f)};
     return 2.0f * (e.x * e.y + e.y * e.z + e.z * e.x);
@@ -265,27 +255,58 @@ __device__ __forceinline__ void push_children(const TopBuild& T, uint32_t level,
     }
 }
 
-// total_key is its own inverse (the sign bit is kept): the float of a key.
+// A set of bins in shared memory ([axis][component][bin] boxes, [axis][bin] counts). While the units are added the
+// boxes hold f32::total_cmp keys, joined by integer atomic min / max (exact whatever order the lanes and warps come
+// in); bins_to_floats turns them back into floats for the sweep.
+typedef float BinBoxes[3][TOP_BINS];
 __device__ __forceinline__ float key_float(int32_t k) { return __int_as_float(total_key(__int_as_float(k))); }
-
-// One axis's binning of a warp's units at once (every lane calls it; `valid` lanes hold a unit): the lanes of one bin
-// join their boxes by warp reductions over the boxes' total-order keys, and one of them updates the bin.
-__device__ __forceinline__ void bin_add_warp(float (*blo)[TOP_BINS], float (*bhi)[TOP_BINS], uint32_t* bn, bool valid,
-                                             uint32_t bin, float4 bl, float4 bh) {
-    unsigned grp = __match_any_sync(~0u, valid ? bin : 0xffffffffu);
-    int32_t a0 = __reduce_min_sync(grp, total_key(bl.x)), a1 = __reduce_min_sync(grp, total_key(bl.y));
-    int32_t a2 = __reduce_min_sync(grp, total_key(bl.z));
-    int32_t b0 = __reduce_max_sync(grp, total_key(bh.x)), b1 = __reduce_max_sync(grp, total_key(bh.y));
-    int32_t b2 = __reduce_max_sync(grp, total_key(bh.z));
-    if (valid && (threadIdx.x & 31u) == (uint32_t)(__ffs(grp) - 1)) {
-        atomic_min_f(&blo[0][bin], key_float(a0));
-        atomic_min_f(&blo[1][bin], key_float(a1));
-        atomic_min_f(&blo[2][bin], key_float(a2));
-        atomic_max_f(&bhi[0][bin], key_float(b0));
-        atomic_max_f(&bhi[1][bin], key_float(b1));
-        atomic_max_f(&bhi[2][bin], key_float(b2));
-        atomicAdd(&bn[bin], (uint32_t)__popc(grp));
+__device__ __forceinline__ void bins_clear(BinBoxes* blo, BinBoxes* bhi, uint32_t (*bn)[TOP_BINS], uint32_t i0,
+                                           uint32_t step) {
+    const float lo0 = __int_as_float(total_key(__uint_as_float(0x7f800000u)));
+    const float hi0 = __int_as_float(total_key(__uint_as_float(0xff800000u)));
+    for (uint32_t i = i0; i < 3u * TOP_BINS; i += step) {
+        const uint32_t ax = i / TOP_BINS, b = i % TOP_BINS;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            blo[ax][q][b] = lo0;
+            bhi[ax][q][b] = hi0;
+        }
+        bn[ax][b] = 0u;
     }
+}
+// A unit into the bins its packed bins name (0xff: none on that axis).
+__device__ __forceinline__ void bins_add(BinBoxes* blo, BinBoxes* bhi, uint32_t (*bn)[TOP_BINS], uint32_t packed,
+                                         float4 bl, float4 bh) {
+#pragma unroll
+    for (uint32_t ax = 0; ax < 3; ++ax) {
+        const uint32_t b = (packed >> (8u * ax)) & 0xffu;
+        if (b >= TOP_BINS) continue;
+        atomicMin(reinterpret_cast<int*>(&blo[ax][0][b]), total_key(bl.x));
+        atomicMin(reinterpret_cast<int*>(&blo[ax][1][b]), total_key(bl.y));
+        atomicMin(reinterpret_cast<int*>(&blo[ax][2][b]), total_key(bl.z));
+        atomicMax(reinterpret_cast<int*>(&bhi[ax][0][b]), total_key(bh.x));
+        atomicMax(reinterpret_cast<int*>(&bhi[ax][1][b]), total_key(bh.y));
+        atomicMax(reinterpret_cast<int*>(&bhi[ax][2][b]), total_key(bh.z));
+        atomicAdd(&bn[ax][b], 1u);
+    }
+}
+__device__ __forceinline__ void bins_to_floats(BinBoxes* blo, BinBoxes* bhi, uint32_t i0, uint32_t step) {
+    for (uint32_t i = i0; i < 3u * TOP_BINS; i += step) {
+        const uint32_t ax = i / TOP_BINS, b = i % TOP_BINS;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            blo[ax][q][b] = key_float(__float_as_int(blo[ax][q][b]));
+            bhi[ax][q][b] = key_float(__float_as_int(bhi[ax][q][b]));
+        }
+    }
+}
+// A unit's bins on the three axes, 8 bits each (0xff for an invalid unit or an axis not in use).
+__device__ __forceinline__ uint32_t pack_bins(bool valid, float4 c, V3 clo, const float scale[3], const bool use[3]) {
+    uint32_t p = 0u;
+#pragma unroll
+    for (uint32_t ax = 0; ax < 3; ++ax)
+        p |= (valid && use[ax] ? bin_of(comp(c, ax), comp3(clo, ax), scale[ax]) : 0xffu) << (8u * ax);
+    return p;
 }
 
 // build_sah's sweep over one set of bins (blo / bhi [axis][component][bin], bn [axis][bin]), a warp at once: lane i
@@ -427,25 +448,17 @@ __global__ void __launch_bounds__(TOP_WARPS * 32) k_top_level(TopBuild T, uint32
         V3 ext = chi - clo;
         float scale[3] = {(float)TOP_BINS / ext.x, (float)TOP_BINS / ext.y, (float)TOP_BINS / ext.z};
         bool use[3] = {ext.x > 0.0f, ext.y > 0.0f, ext.z > 0.0f};
-        for (uint32_t i = lane; i < 3u * TOP_BINS; i += 32u) {
-            uint32_t ax = i / TOP_BINS, bn = i % TOP_BINS;
-            for (int q = 0; q < 3; ++q) {
-                s_lo[wib][ax][q][bn] = __uint_as_float(0x7f800000u);
-                s_hi[wib][ax][q][bn] = __uint_as_float(0xff800000u);
-            }
-            s_n[wib][ax][bn] = 0u;
-        }
+        bins_clear(s_lo[wib], s_hi[wib], s_n[wib], lane, 32u);
         __syncwarp();
         for (uint32_t base = start; base < end; base += 32u) {
             uint32_t j = base + lane;
             bool valid = j < end;
             uint32_t k = valid ? order[j] : order[start];
             float4 bl = T.box[2ull * k], bh = T.box[2ull * k + 1], c = T.centre[k];
-            for (uint32_t ax = 0; ax < 3; ++ax)
-                if (use[ax])
-                    bin_add_warp(s_lo[wib][ax], s_hi[wib][ax], s_n[wib][ax], valid,
-                                 bin_of(comp(c, ax), comp3(clo, ax), scale[ax]), bl, bh);
+            bins_add(s_lo[wib], s_hi[wib], s_n[wib], pack_bins(valid, c, clo, scale, use), bl, bh);
         }
+        __syncwarp();
+        bins_to_floats(s_lo[wib], s_hi[wib], lane, 32u);
         __syncwarp();
         float best_cost = 0.0f;
         uint32_t best_axis = 0, best_split = 0, best_left = 0;
@@ -525,11 +538,9 @@ __global__ void __launch_bounds__(BIG_WARPS * 32) k_top_big(TopBuild T, uint32_t
             }
         if (lane == 0)
             for (int q = 0; q < 12; ++q) s_red[w][q] = r[q];
-        for (uint32_t i = tid; i < BIG_WARPS * 3u * TOP_BINS; i += nt) {
-            uint32_t ww = i / (3u * TOP_BINS), ax = (i / TOP_BINS) % 3u, bn = i % TOP_BINS;
-            for (int q = 0; q < 3; ++q) { s_lo[ww][ax][q][bn] = pinf; s_hi[ww][ax][q][bn] = ninf; }
-            s_n[ww][ax][bn] = 0u;
-        }
+        for (uint32_t i = tid; i < BIG_WARPS * 3u * TOP_BINS; i += nt)
+            bins_clear(s_lo[i / (3u * TOP_BINS)], s_hi[i / (3u * TOP_BINS)], s_n[i / (3u * TOP_BINS)],
+                       i % (3u * TOP_BINS), 3u * TOP_BINS);
         __syncthreads();
         for (int q = 0; q < 12; ++q) {
             float v = s_red[0][q];
@@ -541,28 +552,29 @@ __global__ void __launch_bounds__(BIG_WARPS * 32) k_top_big(TopBuild T, uint32_t
         V3 ext = chi - clo;
         float scale[3] = {(float)TOP_BINS / ext.x, (float)TOP_BINS / ext.y, (float)TOP_BINS / ext.z};
         bool use[3] = {ext.x > 0.0f, ext.y > 0.0f, ext.z > 0.0f};
-        for (uint32_t base = start; base < end; base += nt) {
-            uint32_t j = base + tid;
+        for (uint32_t base = start + 32u * w; base < end; base += nt) {
+            uint32_t j = base + lane;
             bool valid = j < end;
             uint32_t k = valid ? order[j] : order[start];
             float4 bl = T.box[2ull * k], bh = T.box[2ull * k + 1], c = T.centre[k];
-            for (uint32_t ax = 0; ax < 3; ++ax)
-                if (use[ax])
-                    bin_add_warp(s_lo[w][ax], s_hi[w][ax], s_n[w][ax], valid,
-                                 bin_of(comp(c, ax), comp3(clo, ax), scale[ax]), bl, bh);
+            bins_add(s_lo[w], s_hi[w], s_n[w], pack_bins(valid, c, clo, scale, use), bl, bh);
         }
         __syncthreads();
-        // The warps' bins joined into warp 0's (min / max and sums do not depend on the order).
+        // The warps' bins joined into warp 0's, on their keys (min / max and sums do not depend on the order).
         for (uint32_t i = tid; i < 3u * TOP_BINS; i += nt) {
             uint32_t ax = i / TOP_BINS, bn = i % TOP_BINS;
             for (uint32_t ww = 1; ww < BIG_WARPS; ++ww) {
                 for (int q = 0; q < 3; ++q) {
-                    s_lo[0][ax][q][bn] = gmin(s_lo[0][ax][q][bn], s_lo[ww][ax][q][bn]);
-                    s_hi[0][ax][q][bn] = gmax(s_hi[0][ax][q][bn], s_hi[ww][ax][q][bn]);
+                    s_lo[0][ax][q][bn] = __int_as_float(
+                        min(__float_as_int(s_lo[0][ax][q][bn]), __float_as_int(s_lo[ww][ax][q][bn])));
+                    s_hi[0][ax][q][bn] = __int_as_float(
+                        max(__float_as_int(s_hi[0][ax][q][bn]), __float_as_int(s_hi[ww][ax][q][bn])));
                 }
                 s_n[0][ax][bn] += s_n[ww][ax][bn];
             }
         }
+        __syncthreads();
+        bins_to_floats(s_lo[0], s_hi[0], tid, nt);
         __syncthreads();
         if (w == 0) {
             float c;
