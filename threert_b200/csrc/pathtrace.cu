@@ -24,9 +24,10 @@
 
 #include "deform.h"
 
-// Resident blocks of 128 an SM the walks and the shading are compiled for (their register budgets: 64, 72 and 80 a
-// thread). Measured on the city frame against 6 / 6 / 4 (72 / 72 / 108 registers, no spills): the extend walk 3 %,
-// the shadow walk 4 % and the shading 11 % faster, a few spilled words notwithstanding.
+// Resident blocks of 128 an SM the walks and the shading are compiled for (their register budgets: 64, 72 and 64 a
+// thread). Measured on the city frame against 6 / 6 / 4 (72 / 72 / 108 registers, no spills): the extend walk 3 %
+// and the shadow walk 4 % faster; the shading, latency-bound, 2.5 % faster at 8 blocks than at 6 (80 registers), its
+// spills notwithstanding, and no faster at 10 (48).
 #ifndef TRT_BLOCKS_EXTEND
 #define TRT_BLOCKS_EXTEND 8
 #endif
@@ -34,7 +35,7 @@
 #define TRT_BLOCKS_SHADOW 7
 #endif
 #ifndef TRT_BLOCKS_SHADE
-#define TRT_BLOCKS_SHADE 6
+#define TRT_BLOCKS_SHADE 8
 #endif
 #include "sky.h"
 #include "unet.h"
