@@ -41,6 +41,8 @@ __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)
 //    K-major layout the MMA reads (8-row atoms of 512 bytes);
 //  - one thread issues two tcgen05.mma (M 128, N, K 16, bf16 in, f32 accumulate in tensor memory) a stage and
 //    commits each stage's buffers back to the loader through an mbarrier; TS stages in flight;
+//  - where the layer reads one 32-channel block into one output tile (cin 32, co_pad = N), the nine taps' weight boxes
+//    (36 KB) are loaded once a CTA into the weight stages' room, and a stage loads the activations alone;
 //  - the four warps read the accumulator out of tensor memory (each its 32 lanes = pixels), add the bias, apply the
 //    ReLU and store bf16 (or f32) NHWC.
 // Every mbarrier wait is bounded (about a second); a wait that gives up sets the error word, and the CTA waits
@@ -58,6 +60,7 @@ struct Conv {
     uint32_t bw, bh, tiles_x, tiles_y;
     int relu;
     uint32_t* err;
+    uint32_t resident;        // 1: every tap's weights loaded once a CTA (one 32-channel block, one output tile)
 };
 
 constexpr uint32_t TS = 5;                  // pipeline stages (82 KB of shared memory: two CTAs an SM)
@@ -195,13 +198,14 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ C
     uint8_t* smem = smem_raw + (sbase - sraw);
     const uint32_t sA = sbase, sB = sbase + TS * A_STAGE, sBar = sbase + TS * (A_STAGE + B_STAGE);
     // barriers: full[TS], empty[TS] (the stages), acc_full[2], acc_empty[2] (the accumulators), mma_done (every MMA
-    // issued); the tensor-memory address, the abort word and the counts of stages issued and consumed after them
+    // issued), wfull (the resident weights); the tensor-memory address, the abort word and the counts of stages issued
+    // and consumed after them
     auto full = [&](uint32_t s) { return sBar + 8u * s; };
     auto empty = [&](uint32_t s) { return sBar + 8u * (TS + s); };
     auto acc_full = [&](uint32_t i) { return sBar + 8u * (2u * TS + i); };
     auto acc_empty = [&](uint32_t i) { return sBar + 8u * (2u * TS + 2u + i); };
-    const uint32_t mma_done = sBar + 8u * (2u * TS + 4u);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + TS * (A_STAGE + B_STAGE) + 8u * (2u * TS + 5u));
+    const uint32_t mma_done = sBar + 8u * (2u * TS + 4u), wfull = sBar + 8u * (2u * TS + 5u);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + TS * (A_STAGE + B_STAGE) + 8u * (2u * TS + 6u));
     volatile uint32_t* abort_flag = tslot + 1;
     volatile uint32_t* counts = tslot + 2;
     const uint32_t ncols = 2u * a.nt;  // two accumulators of nt columns: 128 or 256
@@ -219,6 +223,7 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ C
             mbar_init(acc_empty(i), CONV_EPI_THREADS);
         }
         mbar_init(mma_done, 1);
+        mbar_init(wfull, 1);
         *abort_flag = 0u;
         counts[0] = counts[1] = 0u;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -246,7 +251,13 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ C
 
     if (warp == 0) {
         if (lane == 0) {
-            // the loader: the stages of every tile of this CTA, in order
+            // the loader: the resident weights (the nine taps' boxes, one after another), then the stages of every tile
+            // of this CTA, in order
+            if (a.resident) {
+                mbar_expect_tx(wfull, 9u * a.nt * 64u);
+                for (uint32_t tap = 0; tap < 9u; ++tap)
+                    tma_load_3d(sB + tap * a.nt * 64u, &wmap, 0, 0, (int)tap, wfull);
+            }
             uint32_t it = 0;
             bool ok = true;
             for (uint32_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
@@ -256,11 +267,11 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ C
                 for (uint32_t k = 0; k < nk; ++k, ++it) {
                     const uint32_t s = it % TS;
                     if (it >= TS && !(ok = mbar_wait(empty(s), ((it / TS) - 1u) & 1u, a.err, abort_flag))) break;
-                    mbar_expect_tx(full(s), A_STAGE + a.nt * 64u);
+                    mbar_expect_tx(full(s), A_STAGE + (a.resident ? 0u : a.nt * 64u));
                     const uint32_t tap = k / kc, c0 = (k % kc) * 32u;
                     const int dy = (int)(tap / 3u) - 1, dx = (int)(tap % 3u) - 1;
                     tma_load_4d(sA + s * A_STAGE, &xmap, (int)(a.x_off + c0), x0 + dx, y0 + dy, (int)b, full(s));
-                    tma_load_3d(sB + s * B_STAGE, &wmap, (int)c0, (int)n0, (int)tap, full(s));
+                    if (!a.resident) tma_load_3d(sB + s * B_STAGE, &wmap, (int)c0, (int)n0, (int)tap, full(s));
                 }
             }
             counts[0] = it;
@@ -270,7 +281,7 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ C
             // the MMA issuer: a tile's stages into accumulator (tile count % 2), then that accumulator to the epilogue
             const uint32_t idesc = umma_idesc(128u, a.nt);
             uint32_t it = 0, ti = 0;
-            bool ok = true;
+            bool ok = !a.resident || mbar_wait(wfull, 0u, a.err, abort_flag);
             for (uint32_t t = blockIdx.x; t < tiles && ok; t += gridDim.x, ++ti) {
                 const uint32_t acc = ti & 1u;
                 if (ti >= 2u && !(ok = mbar_wait(acc_empty(acc), ((ti / 2u) - 1u) & 1u, a.err, abort_flag))) break;
@@ -280,10 +291,12 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ C
                     const uint32_t s = it % TS;
                     if (!(ok = mbar_wait(full(s), (it / TS) & 1u, a.err, abort_flag))) break;
                     tc_fence_after();
+                    // (resident weights: one box a tap, kc = 1)
+                    const uint32_t sb = a.resident ? sB + k * a.nt * 64u : sB + s * B_STAGE;
 #pragma unroll
                     for (uint32_t j = 0; j < 2u; ++j) {
                         uint64_t ad = umma_desc_sw64(sA + s * A_STAGE + j * 32u, 512u);
-                        uint64_t bd = umma_desc_sw64(sB + s * B_STAGE + j * 32u, 512u);
+                        uint64_t bd = umma_desc_sw64(sb + j * 32u, 512u);
                         umma_f16(d, ad, bd, idesc, (k | j) != 0u ? 1u : 0u);
                     }
                     umma_commit(empty(s));
@@ -327,10 +340,12 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ C
     __syncthreads();
     if (*abort_flag && lane == 0) {
         // a wait gave up: let the copies and MMAs in flight land before the memory they use is released
-        if (warp == 0)
+        if (warp == 0) {
+            if (a.resident) mbar_wait_drain(wfull, 0u);
             for (uint32_t i = counts[1]; i < counts[0]; ++i) mbar_wait_drain(full(i % TS), (i / TS) & 1u);
-        else if (warp == 1)
+        } else if (warp == 1) {
             mbar_wait_drain(mma_done, 0u);
+        }
     }
     __syncthreads();
     tc_fence_after();
@@ -908,8 +923,11 @@ void conv_run(Net* n, const bf16* x, uint32_t x_stride, uint32_t x_off, uint32_t
         n->conv_err = "unet: a convolution's tensor map was refused (" + std::to_string((int)r) + ")";
         return;
     }
+    // the nine taps' weights stay in the weight stages' room (9 x nt x 64 bytes <= TS x B_STAGE) where the layer
+    // reads one 32-channel block into one output tile
+    const uint32_t resident = cin == 32u && co_pad == nt && 9u * nt * 64u <= TS * B_STAGE ? 1u : 0u;
     Conv a{cin, co_pad, nt, bias, y, y_stride, y_off, cout, yf, B, H, W, x_off, bw, bh, tiles_x, tiles_y, relu,
-           n->dev_err};
+           n->dev_err, resident};
     const uint32_t tiles = B * tiles_x * tiles_y * (co_pad / nt);
     const uint32_t grid = std::min<uint32_t>(tiles, n->sms * CONV_CTAS_PER_SM);
     k_conv<<<grid, CONV_THREADS, CONV_SMEM, n->stream>>>(xmap, wmap, a);
