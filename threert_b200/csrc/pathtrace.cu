@@ -24,18 +24,23 @@
 
 #include "deform.h"
 
-// Resident blocks of 128 an SM the walks and the shading are compiled for (their register budgets: 64, 72 and 64 a
-// thread). Measured on the city frame against 6 / 6 / 4 (72 / 72 / 108 registers, no spills): the extend walk 3 %
-// and the shadow walk 4 % faster; the shading, latency-bound, 2.5 % faster at 8 blocks than at 6 (80 registers), its
-// spills notwithstanding, and no faster at 10 (48).
+// Resident blocks of 128 an SM the walks and the shading are compiled for (their register budgets: 64 a thread each).
+// Measured on the city frame: the extend walk 3 % faster than at 6 blocks (72 registers, no spills) and 6 % faster
+// than at 9 (56); the split shadow walk (trace_binary_split) 5 % faster at 8 than at 7 (67 registers), 3 % faster
+// than at 9 and 9 % faster than at 10; the shading, latency-bound, 2.5 % faster at 8 blocks than at 6 (80
+// registers), its spills notwithstanding, and no faster at 10 (48).
 #ifndef TRT_BLOCKS_EXTEND
 #define TRT_BLOCKS_EXTEND 8
 #endif
 #ifndef TRT_BLOCKS_SHADOW
-#define TRT_BLOCKS_SHADOW 7
+#define TRT_BLOCKS_SHADOW 8
 #endif
 #ifndef TRT_BLOCKS_SHADE
 #define TRT_BLOCKS_SHADE 8
+#endif
+// 1: the closest-hit walk with its loop split too (measured slower on the city; see trace_binary_split).
+#ifndef TRT_SPLIT_CLOSEST
+#define TRT_SPLIT_CLOSEST 0
 #endif
 #include "sky.h"
 #include "unet.h"
@@ -224,10 +229,12 @@ __global__ void k_raygen(const Job* __restrict__ jobs, uint32_t n_jobs, PathBufs
     Q.q[0][at] = p;
 }
 
-template <bool COUNT, bool WIDE>
+// SPLIT: the binary walk with its loop split (trace_binary_split), which the shadow walks use.
+template <bool COUNT, bool WIDE, bool SPLIT = false>
 __device__ __forceinline__ Hit walk(const Walk& wk, const Sections& X, V3 o, V3 d, float tmax, uint32_t mode,
                                     WalkCount* wc, bool* guard) {
     if (WIDE) return trace_wide<COUNT>(wk.S, wk.W, X, o, d, tmax, mode, wc, guard);
+    if (SPLIT) return trace_binary_split<COUNT>(wk.S, X, wk.top, wk.n_units, o, d, tmax, mode, wc, guard);
     return trace_binary<COUNT>(wk.S, X, wk.top, wk.n_units, o, d, tmax, mode, wc, guard);
 }
 
@@ -247,7 +254,7 @@ __global__ void __launch_bounds__(128, TRT_BLOCKS_EXTEND) k_extend(const Job* __
             Sections X(J.P);
             float4 o = B.o[p], d = B.d[p];
             bool guard = false;
-            Hit h = walk<COUNT, WIDE>(J.wk, X, xyz(o), xyz(d), INF, TRACE_CLOSEST, &wc, &guard);
+            Hit h = walk<COUNT, WIDE, TRT_SPLIT_CLOSEST != 0>(J.wk, X, xyz(o), xyz(d), INF, TRACE_CLOSEST, &wc, &guard);
             if (guard) guard_trips++;
             Q.hit_a[p] = make_float4(h.t, h.u, h.v, bf(h.tri));
             Q.hit_b[p] = make_uint2(h.inst, h.part);
@@ -287,7 +294,7 @@ __global__ void __launch_bounds__(128, TRT_BLOCKS_SHADOW) k_shadow(const Job* __
             Sections X(J.P);
             float4 o = Q.so[i], d = Q.sd[i];
             bool guard = false;
-            Hit h = walk<COUNT, WIDE>(J.wk, X, xyz(o), xyz(d), o.w, bu(d.w), &wc, &guard);
+            Hit h = walk<COUNT, WIDE, true>(J.wk, X, xyz(o), xyz(d), o.w, bu(d.w), &wc, &guard);
             if (guard) guard_trips++;
             if (h.tri == MISS) atomicOr(&B.vis[sp >> 3], 1u << (sp & 7u));
         }
