@@ -33,6 +33,13 @@ def trace_parity(gpu, P, flags, n=20000):
     t_own = O.intersect(P.params, rays[differ], got[differ])
     tie = np.abs(t_own / want["t"][differ] - 1) <= 1e-6
     assert (differ.sum() - tie.sum()) <= 1e-4 * both.sum(), (differ.sum(), tie.sum())
+    # Any-hit rays stop at the first triangle the walk meets. The binary walks (the shadow walk's split loop included)
+    # keep the reference's node order, so it is the oracle's own; the wide walk orders a node's children by the ray's
+    # octant, so only its hit or miss is the reference's.
+    if not flags & N.TRT_RENDER_WIDE:
+        anyhit = hit_g & hit_w & (rays["mode"] != 0)
+        same = (got["tri"][anyhit] == want["tri"][anyhit]) & (got["inst"][anyhit] == want["inst"][anyhit])
+        assert same.mean() >= 0.9999, (anyhit.sum(), (~same).sum())
     return both.sum()
 
 

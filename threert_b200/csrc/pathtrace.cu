@@ -723,7 +723,10 @@ __global__ void k_trace(Params P, Walk wk, const trt_ray* rays, uint64_t n, trt_
     if (i < n) {
         trt_ray r = rays[i];
         bool guard = false;
-        Hit h = walk<COUNT, WIDE>(wk, X, V3{r.o[0], r.o[1], r.o[2]}, V3{r.d[0], r.d[1], r.d[2]}, r.tmax, r.mode, &wc, &guard);
+        // (closest-hit rays through the single loop, any-hit rays through the split one: the pass's own walks)
+        const V3 o{r.o[0], r.o[1], r.o[2]}, d{r.d[0], r.d[1], r.d[2]};
+        Hit h = r.mode == TRACE_CLOSEST ? walk<COUNT, WIDE>(wk, X, o, d, r.tmax, r.mode, &wc, &guard)
+                                        : walk<COUNT, WIDE, true>(wk, X, o, d, r.tmax, r.mode, &wc, &guard);
         hits[i] = trt_hit{h.t, h.tri, h.u, h.v, h.inst, h.part};
     }
     if (COUNT) {
