@@ -145,7 +145,8 @@ __device__ Hit trace_binary(const DScene& S, const Sections& X, uint32_t top, ui
 // The same walk with its loop split in two (Aila and Laine's "while-while"): interior nodes in an inner loop until a
 // leaf, then the leaf. A ray's nodes, tests, pops and result are trace_binary's; only the lanes of a warp fall into
 // step differently. Measured on B200 (the city frame): the shadow walks 6 % faster with it (2.49 -> 2.33 ms a
-// frame, compiled for 8 blocks an SM), the closest-hit walk 4.6 % slower, so the shadow walks use this one.
+// frame, compiled for 8 blocks an SM); the closest-hit walk 4.6 % slower with it on every depth but 2 % faster on
+// the depths past the camera's rays, so the shadow walks and the closest-hit walks past depth 0 use this one.
 template <bool COUNT>
 __device__ Hit trace_binary_split(const DScene& S, const Sections& X, uint32_t top, uint32_t n_units, V3 o, V3 d, float tmax,
                             uint32_t mode, WalkCount* wc, bool* guard) {
