@@ -609,7 +609,7 @@ def main():
                          "the learned denoiser (trained, then judged), the atmosphere's sky bake, or the Cornell box")
     ap.add_argument("--scenes", type=int, default=64, help="denoise: procedural cities rendered for training")
     ap.add_argument("--views", type=int, default=16, help="denoise: views of each")
-    ap.add_argument("--train-steps", type=int, default=20000, help="denoise: Adam steps")
+    ap.add_argument("--train-steps", type=int, default=40000, help="denoise: Adam steps")
     ap.add_argument("--save", default="", help="denoise: where to save the trained parameters (.npy)")
     ap.add_argument("--denoiser-params", default="", help="serve: the learned denoiser's parameters (.npy)")
     ap.add_argument("--requests", type=int, default=64, help="serve: requests a stream")
