@@ -1,7 +1,8 @@
 // Software traversal over the reference's own two-level binary trees (renderer/shaders/trace_units.wgsl:44-135):
 // the top tree over the units' world boxes, each unit's mesh tree in its model space, one loop over both levels.
-// This is the exact walk, kept for parity checks and as the first extend kernel; the wide-BVH walk (wide_bvh.cuh)
-// is the fast one.
+// It is the pass's walk (faster on B200 than the wide-BVH walk of wide_bvh.cuh, which TRT_RENDER_WIDE selects), in
+// two forms with the same nodes, tests and results a ray: trace_binary's single loop, and trace_binary_split's loop
+// split into interior nodes and leaves.
 #pragma once
 #include "device_common.cuh"
 
