@@ -25,8 +25,8 @@
 #include "deform.h"
 
 // Resident blocks of 128 an SM the walks and the shading are compiled for (their register budgets: 64 a thread each).
-// Measured on the city frame: the extend walk 3 % faster than at 6 blocks (72 registers, no spills) and 6 % faster
-// than at 9 (56); the split shadow walk (trace_binary_split) 5 % faster at 8 than at 7 (67 registers), 3 % faster
+// Measured on the city frame: the extend walk 3 % faster than at 6 blocks (72 registers, no spills), 2.6 % faster
+// than at 7 (70, no spills; both of its loops compiled in) and 6 % faster than at 9 (56); the split shadow walk (trace_binary_split) 5 % faster at 8 than at 7 (67 registers), 3 % faster
 // than at 9 and 9 % faster than at 10; the shading, latency-bound, 2.5 % faster at 8 blocks than at 6 (80
 // registers), its spills notwithstanding, and no faster at 10 (48).
 #ifndef TRT_BLOCKS_EXTEND
