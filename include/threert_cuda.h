@@ -307,18 +307,22 @@ int trt_server_submit_rgb(trt_server* server, trt_scene* scene, const uint32_t p
 int trt_server_poll(trt_server* server, trt_request_done* done, uint32_t cap, uint32_t* n, uint32_t wait_ms);
 int trt_server_stats_get(trt_server* server, trt_server_stats* out);
 
-/* The render without allocations, for callers that cannot call cudaMalloc: code inside a CUDA graph capture, or a
- * process whose device memory all belongs to one pool (an engine's caching allocator, a hard memory budget). It has
- * no counterpart in the reference. The caller owns every buffer: `dev` holds DEVICE pointers to the scene's buffers
- * (laid out as for trt_scene_upload), `accum_device` w * h Pixel records, `stream` a cudaStream_t (NULL: the legacy
- * default stream); the call is asynchronous on that stream. The wave's working state lives in one file-scope device
- * array of 32 MiB (31.5 MiB used) that every GPU loading the library holds until the process exits; it allocates
- * nothing: no cudaMalloc, no cudaFree, no allocating library routine. Limits: images of at most 65,536 path slots
- * (8 x 4 pixel tiles: 256 x 256), at most 4 directional lights, the binary walk; larger sizes are refused with
- * TRT_EINVAL and a message in `err` (err_len bytes, may be NULL). The first call on a device sets it up (the array's
- * device address, the sampler's tables): make that first call before any stream capture. Every call shares the
- * array, so calls whose work overlaps on the GPU race: run them on one stream, or one at a time. Flags:
- * TRT_RENDER_ACCUMULATE alone. */
+/* The render without allocations. It has no counterpart in the reference. It is for callers that may not call
+ * cudaMalloc: a process whose device memory all belongs to one pool (an engine's caching allocator that reserved the
+ * device up front, or a hard per-process memory budget), where an allocation from outside the pool fails or steals
+ * memory the pool has counted on; and plugin hosts that forbid allocation inside their render callbacks. The caller
+ * owns every buffer: `dev` holds DEVICE pointers to the scene's buffers (laid out as for trt_scene_upload),
+ * `accum_device` w * h Pixel records, `stream` a cudaStream_t (NULL: the legacy default stream). The wave's working
+ * state lives in one file-scope device array of 32 MiB (31.5 MiB used) that every GPU loading the library holds
+ * until the process exits; the call allocates nothing: no cudaMalloc, no cudaFree, no allocating library routine.
+ * Limits: images of at most 65,536 path slots (8 x 4 pixel tiles: 256 x 256), at most 4 directional lights, the
+ * binary walk; larger sizes are refused with TRT_EINVAL before any CUDA call, with a message in `err` (err_len bytes,
+ * may be NULL). The first call on a device sets it up with that device current (the array's device address, the
+ * sampler's tables). The kernels run on `stream`; the call then waits for them and returns TRT_EGUARD if a walk
+ * stopped at its iteration limit. Every call shares the array, which keeps the last call's contents (each call
+ * clears the counters it needs): calls whose work overlaps on the GPU race for it, so run them on one stream, or one
+ * at a time. Flags: TRT_RENDER_ACCUMULATE; TRT_RENDER_UNSORTED_HITS is accepted and changes nothing (the hits are
+ * always shaded unsorted here). */
 int trt_render_noalloc(const trt_scene_desc* dev, const uint32_t params[TRT_PARAMS_WORDS], uint32_t first_sample,
                        uint32_t spp, uint32_t flags, float* accum_device, void* stream, char* err, size_t err_len);
 

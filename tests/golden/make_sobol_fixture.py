@@ -3,15 +3,20 @@
 The reference's kernel sampler (renderer/shaders/sample.wgsl:5-64) unrolls the first 16 bit-reversed direction
 numbers of Sobol dimensions 1-3 as hex literals, and its CPU mirror's test (renderer/src/sample.rs:90-99,
 `the_directions_are_the_shaders`) holds the 32-entry tables to those literals and their last entries to
-0xffffffff, 0xaaaa00a3, 0xc900a00a. This script reads the literals out of the WGSL text (run it where the reference
-is mounted; its output is committed) so the oracle's own recurrence is checked against the reference's numbers.
+0xffffffff, 0xaaaa00a3, 0xc900a00a. This script reads the literals out of the WGSL text so the oracle's own
+recurrence is checked against the reference's numbers. Run it where the reference is mounted, with the path of
+renderer/shaders/sample.wgsl as its one argument; its output is committed.
+
+  python tests/golden/make_sobol_fixture.py <reference>/renderer/shaders/sample.wgsl
 """
 import json
 import re
 import sys
 from pathlib import Path
 
-src = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/renderer/shaders/sample.wgsl").read_text()
+if len(sys.argv) != 2:
+    sys.exit(__doc__)
+src = Path(sys.argv[1]).read_text()
 dims = []
 for name in ("sobol_d1", "sobol_d2", "sobol_d3"):
     body = src.split(f"fn {name}(x: u32) -> u32 {{", 1)[1].split("return r;", 1)[0]

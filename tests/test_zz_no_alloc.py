@@ -1,7 +1,8 @@
-"""The render without allocations (trt_render_noalloc): the entry point for callers that cannot call cudaMalloc
-(inside a CUDA graph capture, or under a pool that owns the device's memory). The caller's own device buffers go in
-through the C ABI, and two calls in a row must give what the allocating entry point (trt_render) gives on the same
-scene. This file sorts last so that a run stopping at its first failure has run every other test first."""
+"""The render without allocations (trt_render_noalloc): the entry point for callers that may not call cudaMalloc,
+such as a process whose device memory all belongs to one pool allocator, or a plugin host that forbids allocation in
+its render callback. The caller's own device buffers go in through the C ABI, and two calls in a row must give what
+the allocating entry point (trt_render) gives on the same scene. This file sorts last so that a run stopping at its
+first failure has run every other test first."""
 import ctypes as C
 
 import numpy as np
@@ -53,5 +54,10 @@ def test_no_alloc_render_refuses_an_image_past_its_array(gpu):
     accum = torch.zeros(16, dtype=torch.float32, device="cuda")
     err = C.create_string_buffer(256)
     rc = L.trt_render_noalloc(C.byref(d), big.ctypes.data_as(C.POINTER(C.c_uint32)), 0, 1, 0, accum.data_ptr(),
+                              torch.cuda.current_stream().cuda_stream, err, 256)
+    assert rc == 1 and b"too large" in err.value
+    # A size whose 32-bit slot count would wrap to zero (2^20 x 2^14 pixels) is refused the same way.
+    huge = prep.params_with(P.params, width=1 << 20, height=1 << 14)
+    rc = L.trt_render_noalloc(C.byref(d), huge.ctypes.data_as(C.POINTER(C.c_uint32)), 0, 1, 0, accum.data_ptr(),
                               torch.cuda.current_stream().cuda_stream, err, 256)
     assert rc == 1 and b"too large" in err.value

@@ -24,6 +24,7 @@ TRT_RENDER_UNSORTED_HITS = 16
 TRT_RENDER_SORT_SHADOWS = 32
 TRT_RENDER_DEPTH = 64
 
+TRT_OK, TRT_EINVAL, TRT_ECUDA, TRT_EGUARD = 0, 1, 2, 3
 ERRORS = {1: "TRT_EINVAL", 2: "TRT_ECUDA", 3: "TRT_EGUARD"}
 
 

@@ -8,6 +8,7 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -57,15 +58,14 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     if not force and not _stale(LIB, cu + cpp + headers + [Path(__file__)]):
         return LIB
     BUILD.mkdir(exist_ok=True)
-    objs = []
-    for src in cu:
-        obj = BUILD / (src.stem + ".o")
-        _run([NVCC, *NVCC_FLAGS, "-I", INCLUDE, "-I", CSRC, "-c", src, "-o", obj], verbose)
-        objs.append(obj)
-    for src in cpp:
-        obj = BUILD / (src.stem + ".o")
-        _run(["g++", *CXX_FLAGS, "-I", INCLUDE, "-I", CSRC, "-c", src, "-o", obj], verbose)
-        objs.append(obj)
+    jobs = [([NVCC, *NVCC_FLAGS, "-I", INCLUDE, "-I", CSRC, "-c", src, "-o", BUILD / (src.stem + ".o")],
+             BUILD / (src.stem + ".o")) for src in cu]
+    jobs += [(["g++", *CXX_FLAGS, "-I", INCLUDE, "-I", CSRC, "-c", src, "-o", BUILD / (src.stem + ".o")],
+              BUILD / (src.stem + ".o")) for src in cpp]
+    # The translation units compile independently: one compiler process each, side by side.
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
+        list(pool.map(lambda j: _run(j[0], verbose), jobs))
+    objs = [obj for _, obj in jobs]
     tmp = LIB.with_suffix(".so.tmp")
     _run([NVCC, *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"], verbose)
     os.replace(tmp, LIB)

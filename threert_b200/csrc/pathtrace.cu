@@ -1600,16 +1600,12 @@ int trt_render_noalloc(const trt_scene_desc* dev, const uint32_t params[TRT_PARA
                        uint32_t spp, uint32_t flags, float* accum_device, void* stream, char* err, size_t err_len) {
     if (err && err_len) err[0] = 0;
     if (!dev || !params || !accum_device) return na_fail(err, err_len, TRT_EINVAL, "a null argument");
+    // (Its hits are always shaded unsorted, so TRT_RENDER_UNSORTED_HITS is accepted and changes nothing.)
     if (flags & ~(TRT_RENDER_ACCUMULATE | TRT_RENDER_UNSORTED_HITS))
-        return na_fail(err, err_len, TRT_EINVAL, "only TRT_RENDER_ACCUMULATE is taken here (its hits are shaded unsorted)");
-    int device = 0;
-    cudaError_t e = cudaGetDevice(&device);
-    if (e != cudaSuccess) return na_fail(err, err_len, TRT_ECUDA, cudaGetErrorString(e));
-    int rc = noalloc_setup(device, err, err_len);
-    if (rc) return rc;
+        return na_fail(err, err_len, TRT_EINVAL, "flags: TRT_RENDER_ACCUMULATE and TRT_RENDER_UNSORTED_HITS only");
     Params P;
     std::memcpy(P.w, params, sizeof(P.w));
-    // The same checks as trt_render's, against the caller's buffers.
+    // The same checks as trt_render's, against the caller's buffers, all before the first CUDA call.
     const uint64_t nb[5] = {dev->vertices_bytes, dev->leaves_bytes, dev->nodes_bytes, dev->tables_bytes, dev->words_bytes};
     const void* ptrs[5] = {dev->vertices, dev->leaves, dev->nodes, dev->tables, dev->words};
     const uint64_t unit[5] = {48, 48, 32, 16, 4};
@@ -1623,11 +1619,13 @@ int trt_render_noalloc(const trt_scene_desc* dev, const uint32_t params[TRT_PARA
         if (P.w[P_WORD_FIRST + k] > nb[4] / 4) return na_fail(err, err_len, TRT_EINVAL, "Params.word_first names a word past the words");
     uint32_t w = P.w[P_SIZE], h = P.w[P_SIZE + 1];
     if (w == 0 || h == 0) return na_fail(err, err_len, TRT_EINVAL, "Params.size: an empty image");
-    uint32_t n_idx = ((w + 7u) / 8u) * ((h + 3u) / 4u) * 32u;
-    if (n_idx > NOALLOC_SLOTS)
+    // Path slots in 64 bits: a size whose 32-bit count would wrap is refused like any other too large.
+    const uint64_t slots64 = ((uint64_t)w + 7u) / 8u * (((uint64_t)h + 3u) / 4u) * 32u;
+    if (slots64 > NOALLOC_SLOTS)
         return na_fail(err, err_len, TRT_EINVAL, "image too large for the no-allocation render: " + std::to_string(w) + " x " +
-                       std::to_string(h) + " needs " + std::to_string(n_idx) + " path slots (8 x 4 tiles), the most is " +
+                       std::to_string(h) + " needs " + std::to_string(slots64) + " path slots (8 x 4 tiles), the most is " +
                        std::to_string(NOALLOC_SLOTS) + " (256 x 256)");
+    const uint32_t n_idx = (uint32_t)slots64;
     if (P.w[P_COUNTS + 2] >= MAX_DEPTH - 1) return na_fail(err, err_len, TRT_EINVAL, "Params.counts.z (max bounces) must be below 63");
     if (P.w[P_COUNTS2] > MAX_DIR_LIGHTS) return na_fail(err, err_len, TRT_EINVAL, "more than 4 directional lights");
     if (P.w[P_COUNTS] != P.w[P_COUNTS2]) return na_fail(err, err_len, TRT_EINVAL, "local lights are not part of this pass");
@@ -1635,6 +1633,11 @@ int trt_render_noalloc(const trt_scene_desc* dev, const uint32_t params[TRT_PARA
         return na_fail(err, err_len, TRT_EINVAL, "Params.motion.z names a node past the nodes");
     if (P.w[P_ENV] == 0x3f800000u && ((uint32_t)bf(P.w[P_ENV + 1]) != dev->env_w || (uint32_t)bf(P.w[P_ENV + 2]) != dev->env_h))
         return na_fail(err, err_len, TRT_EINVAL, "Params.env's size is not the environment's");
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return na_fail(err, err_len, TRT_ECUDA, cudaGetErrorString(e));
+    int rc = noalloc_setup(device, err, err_len);
+    if (rc) return rc;
     cudaStream_t st = (cudaStream_t)stream;
     uint32_t K = std::max(1u, std::min(spp, NOALLOC_SLOTS / n_idx));
     uint32_t slots = n_idx * K;
@@ -1718,7 +1721,14 @@ int trt_render_noalloc(const trt_scene_desc* dev, const uint32_t params[TRT_PARA
         k_tally<<<1, 32, 0, st>>>(Q, last + 1, w * h * k, nullptr);
         e = cudaGetLastError();
     }
+    // The walks' guard trips (the reference's loop guard, gpu.rs:4199-4205): the call waits for its work to read them
+    // (a pageable copy of one word, no allocation).
+    unsigned long long guard_trips = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&guard_trips, Q.totals + T_GUARD, sizeof(guard_trips), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return na_fail(err, err_len, TRT_ECUDA, cudaGetErrorString(e));
+    if (guard_trips)
+        return na_fail(err, err_len, TRT_EGUARD, std::to_string(guard_trips) + " traversals stopped at their iteration limit");
     return TRT_OK;
 }
 
