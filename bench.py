@@ -230,6 +230,62 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+SPLIT_METRIC = "Mrays/s (closest + shadow rays, one city 720p frame of --spp samples split by sample ranges over the GPUs)"
+
+
+def run_split(args, rank, world, local, dist):
+    """One image across the GPUs: each step is one frame of the city at `--spp` samples; rank r renders its range of
+    the samples (threert_b200.split.sample_range) into its accum, copies it into a tensor on its device and one NCCL
+    sum-reduce brings the ranks' Pixel records to rank 0 (strong scaling: the frame's work is fixed as N grows). Each
+    rank's step time is the device time of its render (CUDA events on the pass's stream) plus that of the reduce
+    (CUDA events on torch's stream); the job's is the slowest rank's."""
+    import torch
+    from threert_b200 import Gpu
+    from threert_b200.split import render_split, sample_range
+    P = city_scene()
+    gpu = Gpu(local)
+    name, sms = gpu.device_info()
+    S = gpu.upload(P)
+    acc = torch.zeros(WIDTH * HEIGHT * 20, dtype=torch.float32, device=f"cuda:{local}")
+    frames = [warm for warm in range(args.warmup)] + [args.warmup + i for i in range(args.steps)]
+
+    def step(f):
+        t = time.perf_counter()
+        st = render_split(S, frame_params(P, f), args.spp, rank, world, None, acc)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        if dist:
+            dist.reduce(acc, dst=0, op=dist.ReduceOp.SUM)
+        e1.record()
+        torch.cuda.synchronize()
+        return float(st.device_ms) + e0.elapsed_time(e1), st.closest_rays + st.shadow_rays
+
+    for f in frames[:args.warmup]:
+        step(f)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms, rays = 0.0, 0
+    for f in frames[args.warmup:]:
+        m, r = step(f)
+        ms += m
+        rays += r
+    ms_all, _, rays_all = reduce_over_ranks(dist, ms, ms, float(rays), device=f"cuda:{local}")
+    first, k = sample_range(rank, world, args.spp)
+    line = {"metric": SPLIT_METRIC, "value": rays_all / (ms_all * 1e-3) / 1e6, "unit": "Mrays/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_all / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD.replace("1 spp", f"{args.spp} spp a frame"), "split": "samples",
+                       "samples_per_rank": k, "device": name, "sms": sms,
+                       "parallelism": f"sample ranges x{world}, NCCL sum-reduce of the 80-byte Pixel records"},
+            "e2e": {"value": rays_all / (ms_all * 1e-3) / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": 624,
+                    "d2h_bytes_per_step": 0}}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    S.close()
+    gpu.close()
+
+
 CROWD_DEPTH = 3
 CROWD_METRIC = "Mrays/s (closest + shadow rays, crowd 720p 1 spp depth 3, skin + refit + top rebuild each frame)"
 
@@ -617,6 +673,10 @@ def main():
     ap.add_argument("--rate-720p", type=float, default=60.0, help="serve: the 720p stream's arrival rate")
     ap.add_argument("--rate-small", type=float, default=2000.0, help="serve: the 256^2 stream's arrival rate")
     ap.add_argument("--groups", type=int, default=1, help="crowd: pose groups (skinned copies of the humanoid)")
+    ap.add_argument("--split", default="frames", choices=["frames", "samples"],
+                    help="city on N GPUs: disjoint frames a rank (weak scaling), or one frame's samples split by "
+                         "sample ranges with an NCCL sum-reduce of the accum (strong scaling)")
+    ap.add_argument("--spp", type=int, default=16, help="split samples: samples a frame")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -655,6 +715,11 @@ def main():
         return
     if args.workload == "serve":
         run_serve(args, rank, world, local)
+        if dist:
+            dist.destroy_process_group()
+        return
+    if args.workload == "city" and args.split == "samples":
+        run_split(args, rank, world, local, dist)
         if dist:
             dist.destroy_process_group()
         return

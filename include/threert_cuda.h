@@ -251,6 +251,9 @@ int trt_render(trt_scene* scene, const uint32_t params[TRT_PARAMS_WORDS], uint32
 int trt_accum_device_ptr(trt_scene* scene, void** ptr, uint64_t* bytes);
 /* Copies the accum to host memory. */
 int trt_accum_read(trt_scene* scene, float* accum_host, uint64_t bytes);
+/* Copies the accum into device memory the caller owns (a buffer on the scene's device, bytes = w * h * 80) and waits
+ * for the copy: for a collective that sums the accums of ranks that rendered disjoint sample ranges of one image. */
+int trt_accum_copy(trt_scene* scene, void* dst_device, uint64_t bytes);
 
 /* Casts rays against the scene (trace_units.wgsl:44-135's query) from host arrays: parity and cost tests. */
 int trt_trace(trt_scene* scene, const uint32_t params[TRT_PARAMS_WORDS], const trt_ray* rays, uint64_t n, uint32_t flags,
@@ -325,6 +328,16 @@ int trt_server_stats_get(trt_server* server, trt_server_stats* out);
  * always shaded unsorted here). */
 int trt_render_noalloc(const trt_scene_desc* dev, const uint32_t params[TRT_PARAMS_WORDS], uint32_t first_sample,
                        uint32_t spp, uint32_t flags, float* accum_device, void* stream, char* err, size_t err_len);
+
+/* Diagnostics: the device's single-precision transcendentals, compiled as the pass's shading calls them (cosf, sinf
+ * for sampled angles, acosf and atan2f for the environment's coordinates), over host arrays: out[i] = f(x[i]) or
+ * atan2f(x[i], y[i]). The shading's results differ from a CPU libm's only by these functions' last bits; this lets a
+ * test bound that difference in ulps (the reference leaves WGSL builtins' precision to the GPU driver). */
+#define TRT_MATH_COS 0u
+#define TRT_MATH_SIN 1u
+#define TRT_MATH_ACOS 2u
+#define TRT_MATH_ATAN2 3u
+int trt_math_eval(trt_ctx* ctx, uint32_t fn, const float* x, const float* y, uint64_t n, float* out);
 
 int trt_scene_totals(trt_scene* scene, trt_totals* out);
 void trt_scene_reset_totals(trt_scene* scene);

@@ -85,3 +85,58 @@ def test_two_ranks_render_the_frames_one_rank_renders():
             cam = scenes.city_camera(f, 8, 5, 24, 16, 40.0)
             acc, _ = O.render(prep.set_camera(P.params, cam), 2, threads=1)
             assert np.array_equal(frame_of(acc, 24, 16, 2).color, img)
+
+
+def test_sample_ranges_cover_the_samples_once():
+    from threert_b200.split import sample_range
+    for world in (1, 2, 3, 4, 8):
+        for spp in (0, 1, 5, 16, 64, 67):
+            r = [sample_range(k, world, spp) for k in range(world)]
+            got = [s for first, n in r for s in range(first, first + n)]
+            assert got == list(range(spp)), (world, spp, r)
+    with pytest.raises(ValueError):
+        sample_range(2, 2, 4)
+
+
+def _split_rank(rank, world, port, out):
+    """A rank of the sample-range split: its samples of one frame through the oracle (this rank's stand-in for the
+    device's render, which renders the same samples), its accum summed into rank 0's by gloo."""
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        import torch
+        import oracle
+        from threert_b200 import prep, scenes
+        from threert_b200.split import reduce_accum, sample_range
+        P = prep.prepare(scenes.cornell(24, 16))
+        first, k = sample_range(rank, world, 6)
+        acc, _ = oracle.Oracle(P).render(P.params, k, first_sample=first, threads=1)
+        t = reduce_accum(dist, torch.from_numpy(acc.reshape(-1).copy()))
+        if rank == 0:
+            out.put(t.numpy())
+    finally:
+        dist.destroy_process_group()
+
+
+def test_an_image_split_by_sample_ranges_sums_to_the_one_rank_image():
+    """Two ranks render samples [0, 3) and [3, 6) of the same frame; their accums summed on rank 0 are the one-rank
+    render of samples [0, 6), up to the order of the sums (the sample counts exactly)."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = free_port()
+    procs = [ctx.Process(target=_split_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    try:
+        got = q.get(timeout=240)
+    finally:
+        for p in procs:
+            p.join(timeout=60)
+    assert all(p.exitcode == 0 for p in procs)
+    import oracle
+    from threert_b200 import prep, scenes
+    P = prep.prepare(scenes.cornell(24, 16))
+    want, _ = oracle.Oracle(P).render(P.params, 6, threads=1)
+    got = got.reshape(want.shape)
+    assert np.array_equal(got[:, 3], want[:, 3]) and (want[:, 3] == 6).all()  # sample counts
+    assert np.allclose(got, want, rtol=1e-5, atol=1e-6)

@@ -25,6 +25,7 @@ TRT_RENDER_SORT_SHADOWS = 32
 TRT_RENDER_DEPTH = 64
 
 TRT_OK, TRT_EINVAL, TRT_ECUDA, TRT_EGUARD = 0, 1, 2, 3
+TRT_MATH_COS, TRT_MATH_SIN, TRT_MATH_ACOS, TRT_MATH_ATAN2 = 0, 1, 2, 3
 ERRORS = {1: "TRT_EINVAL", 2: "TRT_ECUDA", 3: "TRT_EGUARD"}
 
 
@@ -196,6 +197,7 @@ SIGNATURES = [
     ("trt_render", C.c_int, [C.c_void_p, P(u32), u32, u32, u32, P(f32), P(Stats)]),
     ("trt_accum_device_ptr", C.c_int, [C.c_void_p, P(C.c_void_p), P(u64)]),
     ("trt_accum_read", C.c_int, [C.c_void_p, P(f32), u64]),
+    ("trt_accum_copy", C.c_int, [C.c_void_p, C.c_void_p, u64]),
     ("trt_trace", C.c_int, [C.c_void_p, P(u32), P(Ray), u64, u32, P(Hit)]),
     ("trt_render_noalloc", C.c_int, [P(SceneDesc), P(u32), u32, u32, u32, C.c_void_p, C.c_void_p, C.c_char_p,
                                      C.c_size_t]),
@@ -214,6 +216,7 @@ SIGNATURES = [
     ("trt_unet_forward", C.c_int, [C.c_void_p, P(f32), u32, u32, u32, P(f32), P(f32)]),
     ("trt_unet_train_step", C.c_int, [C.c_void_p, P(f32), P(f32), u32, u32, u32, f32, C.c_int, P(f32), P(f32), P(f32)]),
     ("trt_unet_denoise_accum", C.c_int, [C.c_void_p, C.c_void_p, u32, u32, P(f32), P(f32)]),
+    ("trt_math_eval", C.c_int, [C.c_void_p, u32, P(f32), P(f32), u64, P(f32)]),
     ("trt_scene_totals", C.c_int, [C.c_void_p, P(Totals)]),
     ("trt_scene_reset_totals", None, [C.c_void_p]),
     ("trt_scene_set_profiling", None, [C.c_void_p, C.c_int]),

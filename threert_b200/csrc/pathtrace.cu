@@ -740,6 +740,22 @@ __global__ void k_trace(Params P, Walk wk, const trt_ray* rays, uint64_t n, trt_
     }
 }
 
+// The device's single-precision transcendentals as the pass calls them (same compile flags): out[i] = f(x[i], y[i]).
+__global__ void k_math_eval(uint32_t fn, const float* __restrict__ x, const float* __restrict__ y, uint64_t n,
+                            float* __restrict__ out) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float a = x[i], b = y ? y[i] : 0.0f, r;
+    switch (fn) {
+        case TRT_MATH_COS: r = cosf(a); break;
+        case TRT_MATH_SIN: r = sinf(a); break;
+        case TRT_MATH_ACOS: r = acosf(a); break;
+        case TRT_MATH_ATAN2: r = atan2f(a, b); break;
+        default: r = __int_as_float(0x7fc00000); break;
+    }
+    out[i] = r;
+}
+
 // The Joe-Kuo direction numbers of Sobol dimensions 1-3, bit-reversed (the recurrence of the primitive polynomials
 // x + 1, x^2 + x + 1, x^3 + x + 1 with initial numbers 1; 1, 3; 1, 3, 1).
 void sobol_directions(uint32_t out[3][16]) {
@@ -1474,6 +1490,16 @@ int trt_accum_read(trt_scene* s, float* accum_host, uint64_t bytes) {
     return TRT_OK;
 }
 
+int trt_accum_copy(trt_scene* s, void* dst_device, uint64_t bytes) {
+    if (!s || !dst_device) return TRT_EINVAL;
+    trt_ctx* c = s->ctx;
+    if (!s->accum || bytes != 80ull * s->accum_w * s->accum_h) return fail(c, TRT_EINVAL, "trt_accum_copy: wrong size");
+    cudaSetDevice(c->device);
+    TRT_CUDA(c, cudaMemcpyAsync(dst_device, s->accum, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    TRT_CUDA(c, cudaStreamSynchronize(c->stream));
+    return TRT_OK;
+}
+
 int trt_trace(trt_scene* s, const uint32_t params[TRT_PARAMS_WORDS], const trt_ray* rays, uint64_t n, uint32_t flags,
               trt_hit* hits) {
     if (!s || !params || (!rays && n) || (!hits && n)) return TRT_EINVAL;
@@ -1515,6 +1541,27 @@ int trt_trace(trt_scene* s, const uint32_t params[TRT_PARAMS_WORDS], const trt_r
     cudaFree(dr);
     cudaFree(dh);
     if (e != cudaSuccess) return cuda_fail(c, e, "trt_trace");
+    return TRT_OK;
+}
+
+int trt_math_eval(trt_ctx* c, uint32_t fn, const float* x, const float* y, uint64_t n, float* out) {
+    if (!c) return TRT_EINVAL;
+    if (fn > TRT_MATH_ATAN2 || (n && (!x || !out)) || (fn == TRT_MATH_ATAN2 && n && !y))
+        return fail(c, TRT_EINVAL, "trt_math_eval: a bad function or a null array");
+    if (n == 0) return TRT_OK;
+    cudaSetDevice(c->device);
+    float* d = nullptr;
+    TRT_CUDA(c, cudaMalloc(&d, 12ull * n));
+    cudaError_t e = cudaMemcpyAsync(d, x, 4ull * n, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess && y) e = cudaMemcpyAsync(d + n, y, 4ull * n, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) {
+        k_math_eval<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(fn, d, y ? d + n : nullptr, n, d + 2 * n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d + 2 * n, 4ull * n, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(d);
+    if (e != cudaSuccess) return cuda_fail(c, e, "trt_math_eval");
     return TRT_OK;
 }
 

@@ -30,7 +30,11 @@ struct WideView {
 };
 
 constexpr uint32_t WIDE_UNIT_BIT = 0x80000000u;
+// The walk's stack: entries of 8 bytes, the first WIDE_SHORT of each thread's in shared memory (a column a thread),
+// the rest in local memory. A kernel that walks the wide BVH runs blocks of at most WIDE_BLOCK threads.
+constexpr int WIDE_SHORT = 8;
 constexpr int WIDE_STACK = 64;
+constexpr uint32_t WIDE_BLOCK = 128;
 
 struct WideBvh {
     uint4* nodes = nullptr;
@@ -59,216 +63,210 @@ __device__ __forceinline__ WideRay wide_ray(V3 o, V3 d, V3 inv) {
     return WideRay{o, d, inv, (inv.x < 0.0f ? 1u : 0u) | (inv.y < 0.0f ? 2u : 0u) | (inv.z < 0.0f ? 4u : 0u)};
 }
 
-// Byte k of w as a float (the conversion runs beside the walk's integer work, which keeps the ALU pipe busy).
-__device__ __forceinline__ float q_float(uint32_t w, int k) { return __uint2float_rn((w >> (8 * k)) & 0xffu); }
-
-// Visit order: slot i is visited k-th for i = k ^ oct. A node's byte arrays (one byte a slot, slots 0-3 in the low word)
-// are put in that order with one byte permute a word: oct bit 0 swaps neighbouring bytes, bit 1 byte pairs, bit 2 the
-// two words.
-__device__ __forceinline__ void visit_order(uint32_t oct, uint32_t a, uint32_t b, uint32_t& x, uint32_t& y) {
-    const uint32_t sel = (oct & 3u) == 0u ? 0x3210u : ((oct & 3u) == 1u ? 0x2301u : ((oct & 3u) == 2u ? 0x1032u : 0x0123u));
-    uint32_t pa = __byte_perm(a, 0u, sel), pb = __byte_perm(b, 0u, sel);
-    x = (oct & 4u) ? pb : pa;
-    y = (oct & 4u) ? pa : pb;
+// Byte k of w as an exact float: one byte permute builds 2^23 + byte (the float 0x4B0000bb), one add removes 2^23.
+// (It keeps the conversion off the XU pipe, whose quarter rate bounded the walk when it used integer-to-float
+// conversions: 48 a node.)
+__device__ __forceinline__ float q_byte(uint32_t w, int k) {
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440u | (uint32_t)k)) - 8388608.0f;
 }
 
-// The eight child boxes of node `nd` against the ray, in visit order: tv[k] is the entry t of slot k ^ r.neg (INF:
-// missed, or past tmax). A slot's plane at q steps is origin + q 2^e: t = q (2^e / d) + (origin - o) / d, one FMA.
-// The near and far planes of each axis are picked once by the ray's signs; an empty slot (q_lo > q_hi) has its near
-// plane past its far one on every axis, so it misses whatever the signs.
-__device__ __forceinline__ void wide_children(const uint4 nd[5], const WideRay& r, float tmax, float tv[8]) {
-    uint32_t eb = nd[0].w;
-    float Sx = bf((eb & 0xffu) << 23) * r.inv.x, Sy = bf(((eb >> 8) & 0xffu) << 23) * r.inv.y,
-          Sz = bf(((eb >> 16) & 0xffu) << 23) * r.inv.z;
-    float Bx = (bf(nd[0].x) - r.o.x) * r.inv.x, By = (bf(nd[0].y) - r.o.y) * r.inv.y, Bz = (bf(nd[0].z) - r.o.z) * r.inv.z;
+// The eight child boxes of node `nd` against the ray: bit i of the result is set when slot i's box is entered before
+// tmax. A slot's plane at q steps is origin + q 2^e: t = q (2^e / d) + (origin - o) / d, one FMA. The near and far
+// planes of each axis are picked once by the ray's signs; an empty slot (q_lo > q_hi) has its near plane past its far
+// one on every axis, so it misses whatever the signs.
+__device__ __forceinline__ uint32_t wide_hits(const uint4 nd[5], const WideRay& r, float tmax) {
+    const uint32_t eb = nd[0].w;
+    const float Sx = __uint_as_float((eb & 0xffu) << 23) * r.inv.x;
+    const float Sy = __uint_as_float(((eb >> 8) & 0xffu) << 23) * r.inv.y;
+    const float Sz = __uint_as_float(((eb >> 16) & 0xffu) << 23) * r.inv.z;
+    const float Bx = (bf(nd[0].x) - r.o.x) * r.inv.x, By = (bf(nd[0].y) - r.o.y) * r.inv.y,
+                Bz = (bf(nd[0].z) - r.o.z) * r.inv.z;
     // q_lo x: nd[2].x,y; y: nd[2].z,w; z: nd[3].x,y. q_hi x: nd[3].z,w; y: nd[4].x,y; z: nd[4].z,w.
-    bool nx = r.neg & 1u, ny = r.neg & 2u, nz = r.neg & 4u;
-    uint32_t nearx[2], farx[2], neary[2], fary[2], nearz[2], farz[2];
-    visit_order(r.neg, nx ? nd[3].z : nd[2].x, nx ? nd[3].w : nd[2].y, nearx[0], nearx[1]);
-    visit_order(r.neg, nx ? nd[2].x : nd[3].z, nx ? nd[2].y : nd[3].w, farx[0], farx[1]);
-    visit_order(r.neg, ny ? nd[4].x : nd[2].z, ny ? nd[4].y : nd[2].w, neary[0], neary[1]);
-    visit_order(r.neg, ny ? nd[2].z : nd[4].x, ny ? nd[2].w : nd[4].y, fary[0], fary[1]);
-    visit_order(r.neg, nz ? nd[4].z : nd[3].x, nz ? nd[4].w : nd[3].y, nearz[0], nearz[1]);
-    visit_order(r.neg, nz ? nd[3].x : nd[4].z, nz ? nd[3].y : nd[4].w, farz[0], farz[1]);
+    const bool nx = r.neg & 1u, ny = r.neg & 2u, nz = r.neg & 4u;
+    const uint32_t nearx[2] = {nx ? nd[3].z : nd[2].x, nx ? nd[3].w : nd[2].y};
+    const uint32_t farx[2] = {nx ? nd[2].x : nd[3].z, nx ? nd[2].y : nd[3].w};
+    const uint32_t neary[2] = {ny ? nd[4].x : nd[2].z, ny ? nd[4].y : nd[2].w};
+    const uint32_t fary[2] = {ny ? nd[2].z : nd[4].x, ny ? nd[2].w : nd[4].y};
+    const uint32_t nearz[2] = {nz ? nd[4].z : nd[3].x, nz ? nd[4].w : nd[3].y};
+    const uint32_t farz[2] = {nz ? nd[3].x : nd[4].z, nz ? nd[3].y : nd[4].w};
+    uint32_t hits = 0;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        int h = k >> 2, j = k & 3;
-        float x0 = fmaf(q_float(nearx[h], j), Sx, Bx), x1 = fmaf(q_float(farx[h], j), Sx, Bx);
-        float y0 = fmaf(q_float(neary[h], j), Sy, By), y1 = fmaf(q_float(fary[h], j), Sy, By);
-        float z0 = fmaf(q_float(nearz[h], j), Sz, Bz), z1 = fmaf(q_float(farz[h], j), Sz, Bz);
-        float tnear = fmaxf(fmaxf(x0, y0), fmaxf(z0, 0.0f));
-        float tfar = fminf(fminf(x1, y1), fminf(z1, tmax));
-        tv[k] = tnear <= tfar ? tnear : INF;
+    for (int i = 0; i < 8; ++i) {
+        const int h = i >> 2, k = i & 3;
+        const float x0 = fmaf(q_byte(nearx[h], k), Sx, Bx), x1 = fmaf(q_byte(farx[h], k), Sx, Bx);
+        const float y0 = fmaf(q_byte(neary[h], k), Sy, By), y1 = fmaf(q_byte(fary[h], k), Sy, By);
+        const float z0 = fmaf(q_byte(nearz[h], k), Sz, Bz), z1 = fmaf(q_byte(farz[h], k), Sz, Bz);
+        const float tnear = fmaxf(fmaxf(x0, y0), fmaxf(z0, 0.0f));
+        const float tfar = fminf(fminf(x1, y1), fminf(z1, tmax));
+        hits |= (tnear <= tfar ? 1u : 0u) << i;
     }
+    return hits;
 }
 
-// Ascending sort of eight keys (a sorting network of 19 compare-exchanges).
-__device__ __forceinline__ void cas(uint32_t& a, uint32_t& b) {
-    uint32_t lo = min(a, b), hi = max(a, b);
-    a = lo;
-    b = hi;
-}
-__device__ __forceinline__ void sort8(uint32_t k[8]) {
-    cas(k[0], k[2]); cas(k[1], k[3]); cas(k[4], k[6]); cas(k[5], k[7]);
-    cas(k[0], k[4]); cas(k[1], k[5]); cas(k[2], k[6]); cas(k[3], k[7]);
-    cas(k[0], k[1]); cas(k[2], k[3]); cas(k[4], k[5]); cas(k[6], k[7]);
-    cas(k[2], k[4]); cas(k[3], k[5]);
-    cas(k[1], k[4]); cas(k[3], k[6]);
-    cas(k[1], k[2]); cas(k[3], k[4]); cas(k[5], k[6]);
+// An 8-bit slot mask in visit order: bit k is slot k ^ oct's. The builder places children in slots by octant (slot
+// bit a: the upper half along axis a), so the ray's sign bits as oct make the lowest visit bit the nearest octant.
+__device__ __forceinline__ uint32_t visit_mask(uint32_t m, uint32_t oct) {
+    m = (oct & 1u) ? (((m & 0x55u) << 1) | ((m >> 1) & 0x55u)) : m;
+    m = (oct & 2u) ? (((m & 0x33u) << 2) | ((m >> 2) & 0x33u)) : m;
+    m = (oct & 4u) ? (((m & 0x0fu) << 4) | ((m >> 4) & 0x0fu)) : m;
+    return m;
 }
 
-// The walk over both levels: the top tree's hit leaves are units, entered (the ray in the unit's space, as
-// trace_units.wgsl:86-105) when popped; a unit's walk ends when the stack is back to where it was entered. Entries
-// carry the t they were hit at and are skipped once a closer hit is known.
+// Slot i's items in a node's leaf list: (first item, count). (A node's items number at most 8 x 16: the byte-wise
+// running sum does not carry.)
+__device__ __forceinline__ uint2 slot_items(uint32_t leaf_base, uint32_t c_lo, uint32_t c_hi, uint32_t slot) {
+    const uint64_t counts = ((uint64_t)c_hi << 32) | c_lo;
+    const uint32_t cnt = (uint32_t)(counts >> (8 * slot)) & 0xffu;
+    const uint32_t upto = (uint32_t)((counts * 0x0101010101010101ull) >> (8 * slot)) & 0xffu;  // slots 0..slot
+    return make_uint2(leaf_base + upto - cnt, cnt);
+}
+
+// The walk over both levels by node groups (Ylitie, Karras and Laine, "Efficient incoherent ray traversal on GPUs
+// through compressed wide BVHs", HPG 2017): opening a node tests its eight children at once and leaves its hit
+// interior children as one group, (first child's index, hit mask in visit order | interior mask), from which the walk
+// takes the nearest child next; what is left of a group goes onto the stack as one 8-byte entry when the walk
+// descends. No child is sorted or pushed on its own. A node's hit leaf slots are done before its children: a mesh's
+// triangles are tested on the spot (the reference's Moller-Trumbore on the unit-space ray, pathtrace.wgsl:742-761),
+// and a top-tree node's hit units become a unit group entry (node, slots in visit order, item cursor) that enters
+// them one at a time, the ray taken into each unit's space as trace_units.wgsl:86-105 does; a unit's walk ends when
+// the stack is back to where it was entered. Shadow rays (TRACE_SHADOW) skip units that cast no shadow, and any-hit
+// rays stop at the first triangle hit. The first WIDE_SHORT entries of a thread's stack are in shared memory; more
+// than WIDE_STACK end the walk with the guard set.
 template <bool COUNT>
 __device__ Hit trace_wide(const DScene& S, const WideView& W, const Sections& X, V3 o, V3 d, float tmax, uint32_t mode,
                           WalkCount* wc, bool* guard) {
     Hit hit{tmax, MISS, 0.0f, 0.0f, NO_INST, 0u};
     if (W.n_units == 0) return hit;
-    V3 inv_d = safe_inv(d);
-    WideRay r = wide_ray(o, d, inv_d);
-    uint32_t stack_ref[WIDE_STACK];
-    float stack_t[WIDE_STACK];
+    __shared__ uint2 short_stack[WIDE_SHORT * WIDE_BLOCK];
+    if (blockDim.x > WIDE_BLOCK) { *guard = true; return hit; }
+    const uint32_t tid = threadIdx.x;
+    uint2 spill[WIDE_STACK - WIDE_SHORT];
     int sp = 0;
-#define STACK_PUSH(ref, tt)                                   \
-    do {                                                      \
-        if (sp < WIDE_STACK) {                                \
-            stack_ref[sp] = (ref);                            \
-            stack_t[sp] = (tt);                               \
-            sp++;                                             \
-        }                                                     \
+#define WIDE_PUSH(X_, Y_)                                                                    \
+    do {                                                                                     \
+        if (sp >= WIDE_STACK) { *guard = true; return hit; }                                 \
+        if (sp < WIDE_SHORT) short_stack[sp * WIDE_BLOCK + tid] = make_uint2((X_), (Y_));   \
+        else spill[sp - WIDE_SHORT] = make_uint2((X_), (Y_));                                \
+        ++sp;                                                                                \
     } while (0)
-    uint32_t cur = W.top_root;  // the node to open next (NO_INST: pop)
+    constexpr uint32_t ENTRY_UNITS = 0x80000000u;  // in y: a unit group (x: its node)
+    const V3 inv_d = safe_inv(d);
+    WideRay r = wide_ray(o, d, inv_d);
+    uint32_t node = W.top_root;       // the node to open next
+    uint32_t g_base = 0, g_bits = 0;  // the current group: first child's index; hit mask (visit order) << 8 | imask
     uint32_t rec = NO_INST;
     int base = 0;
     for (uint32_t iter = 0;; ++iter) {
-        if (iter >= WALK_GUARD) { *guard = true; break; }
-        if (cur != NO_INST) {
-            if (cur >= W.n_nodes) { *guard = true; break; }
-            const uint4* np = W.nodes + 5ull * cur;
-            uint4 nd[5];
+        if (iter >= WALK_GUARD || node >= W.n_nodes) { *guard = true; return hit; }
+        const uint4* np = W.nodes + 5ull * node;
+        uint4 nd[5];
 #pragma unroll
-            for (int k = 0; k < 5; ++k) nd[k] = __ldg(np + k);
-            if (COUNT) wc->nodes++;
-            float tn[8];
-            wide_children(nd, r, hit.t, tn);
-            uint32_t imask = nd[0].w >> 24;
-            uint32_t child_base = nd[1].x, leaf_base = nd[1].y;
-            uint64_t counts = ((uint64_t)nd[1].w << 32) | nd[1].z;
-            uint64_t prefix = counts * 0x0101010101010101ull;  // byte i: the items of slots 0..i
-            // The visit order: for closest hits the hit slots sorted by their entry t; for any-hit rays (shadow
-            // rays stop at the first hit, whichever) the octant order k ^ (the ray's signs), nearly front to back
-            // as the builder put children by octant. order[j]: visit index of the j-th slot to visit (9: none).
-            uint32_t oct = r.neg;
-            uint32_t key[8];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) key[k] = tn[k] >= hit.t ? 0xffffffffu : ((bu(tn[k]) & ~7u) | (uint32_t)k);
-            if (mode == TRACE_CLOSEST) {
-                uint32_t hits = 0;
-#pragma unroll
-                for (int k = 0; k < 8; ++k) hits += key[k] != 0xffffffffu;
-                if (hits > 1) sort8(key);
-                else if (hits == 1) {
-                    // (One hit: move it first.)
-                    uint32_t m = key[0];
-#pragma unroll
-                    for (int k = 1; k < 8; ++k) m = min(m, key[k]);
-                    key[0] = m;
-#pragma unroll
-                    for (int k = 1; k < 8; ++k) key[k] = 0xffffffffu;
-                }
-            }
-            // Leaves first (their hits cull the farther entries), then the other entries pushed farthest first,
-            // so the nearest is on top.
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                if (key[j] == 0xffffffffu) continue;
-                uint32_t i = (key[j] & 7u) ^ oct;
-                if (imask & (1u << i)) continue;
-                if (bf(key[j] & ~7u) >= hit.t) continue;
-                uint32_t cnt = (uint32_t)(counts >> (8 * i)) & 0xffu;
-                if (cnt == 0 || rec == NO_INST) continue;  // (top-tree leaves are units: entries, below)
-                uint32_t item = leaf_base + ((uint32_t)(prefix >> (8 * i)) & 0xffu) - cnt;
-                for (uint32_t q = 0; q < cnt; ++q) {
-                    uint32_t ti = item + q;
-                    if (ti >= W.n_tris) { *guard = true; return hit; }
-                    const float4* tp = W.tris + 3ull * ti;
-                    float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
-                    if (COUNT) wc->tris++;
-                    // pathtrace.wgsl:742-761 intersect_tri, on the copy of the reference's leaf record.
-                    V3 v0 = xyz(a), e1 = xyz(b), e2 = xyz(c);
-                    V3 pv = cross(r.d, e2);
-                    float det = dot(e1, pv);
-                    if (fabsf(det) < 1e-12f) continue;
-                    float inv = 1.0f / det;
-                    V3 tv = r.o - v0;
-                    float u = dot(tv, pv) * inv;
-                    if (u < 0.0f || u > 1.0f) continue;
-                    V3 qv = cross(tv, e1);
-                    float v = dot(r.d, qv) * inv;
-                    if (v < 0.0f || u + v > 1.0f) continue;
-                    float t = dot(e2, qv) * inv;
-                    if (t <= 0.0f || t >= hit.t) continue;
-                    hit = Hit{t, bu(c.w), u, v, rec, bu(a.w)};
-                    if (mode != TRACE_CLOSEST) return hit;
-                }
-            }
-#pragma unroll
-            for (int j = 7; j >= 0; --j) {
-                if (key[j] == 0xffffffffu) continue;
-                float t = bf(key[j] & ~7u);
-                if (t >= hit.t) continue;
-                uint32_t i = (key[j] & 7u) ^ oct;
-                if (imask & (1u << i)) {
-                    STACK_PUSH(child_base + (uint32_t)__popc(imask & ((1u << i) - 1u)), t);
-                } else if (rec == NO_INST) {
-                    uint32_t cnt = (uint32_t)(counts >> (8 * i)) & 0xffu;
-                    uint32_t item = leaf_base + ((uint32_t)(prefix >> (8 * i)) & 0xffu) - cnt;
-                    if (COUNT) wc->units += cnt;
-                    for (uint32_t q = 0; q < cnt; ++q) {
-                        if (item + q >= W.n_units) { *guard = true; return hit; }
-                        uint32_t u = __ldg(W.units + item + q);
-                        if (mode == TRACE_SHADOW && !(u & WIDE_UNIT_BIT)) continue;
-                        STACK_PUSH(u | WIDE_UNIT_BIT, t);
+        for (int k = 0; k < 5; ++k) nd[k] = __ldg(np + k);
+        if (COUNT) wc->nodes++;
+        const uint32_t hm = wide_hits(nd, r, hit.t);
+        const uint32_t imask = nd[0].w >> 24;
+        g_base = nd[1].x;
+        g_bits = (visit_mask(hm & imask, r.neg) << 8) | imask;
+        uint32_t leaf = hm & ~imask;
+        if (leaf != 0u) {
+            if (rec == NO_INST) {
+                // Units: the group of this node's hit unit slots goes on top of what is left of its children.
+                if (g_bits >> 8) WIDE_PUSH(g_base, g_bits);
+                g_bits = 0;
+                WIDE_PUSH(node, ENTRY_UNITS | (visit_mask(leaf, r.neg) << 8));
+            } else {
+                do {
+                    const uint32_t slot = (uint32_t)__ffs(leaf) - 1u;
+                    leaf &= leaf - 1u;
+                    const uint2 it = slot_items(nd[1].y, nd[1].z, nd[1].w, slot);
+                    for (uint32_t q = 0; q < it.y; ++q) {
+                        const uint32_t ti = it.x + q;
+                        if (ti >= W.n_tris) { *guard = true; return hit; }
+                        const float4* tp = W.tris + 3ull * ti;
+                        const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+                        if (COUNT) wc->tris++;
+                        // pathtrace.wgsl:742-761 intersect_tri, on the copy of the reference's leaf record.
+                        const V3 v0 = xyz(a), e1 = xyz(b), e2 = xyz(c);
+                        const V3 pv = cross(r.d, e2);
+                        const float det = dot(e1, pv);
+                        if (fabsf(det) < 1e-12f) continue;
+                        const float inv = 1.0f / det;
+                        const V3 tv = r.o - v0;
+                        const float u = dot(tv, pv) * inv;
+                        if (u < 0.0f || u > 1.0f) continue;
+                        const V3 qv = cross(tv, e1);
+                        const float v = dot(r.d, qv) * inv;
+                        if (v < 0.0f || u + v > 1.0f) continue;
+                        const float t = dot(e2, qv) * inv;
+                        if (t <= 0.0f || t >= hit.t) continue;
+                        hit = Hit{t, bu(c.w), u, v, rec, bu(a.w)};
+                        if (mode != TRACE_CLOSEST) return hit;
                     }
-                }
+                } while (leaf != 0u);
             }
         }
-        // Pop: the nearest pending entry still in front of the closest hit.
+        // The next node: the nearest child left in the group, else the stack's top (a group, or the next unit of a
+        // unit group, entered).
         for (;;) {
-            if (rec != NO_INST && sp == base) {
+            if (g_bits >> 8) {
+                const uint32_t k = (uint32_t)__ffs(g_bits >> 8) - 1u;
+                g_bits &= ~(1u << (k + 8u));
+                const uint32_t slot = k ^ r.neg;
+                node = g_base + (uint32_t)__popc(g_bits & ((1u << slot) - 1u) & 0xffu);
+                if (g_bits >> 8) WIDE_PUSH(g_base, g_bits);
+                break;
+            }
+            if (rec != NO_INST && sp == base) {  // the unit's walk is over: back to the world's ray
                 rec = NO_INST;
                 r = wide_ray(o, d, inv_d);
             }
             if (sp == 0) return hit;
             --sp;
-            if (stack_t[sp] < hit.t) break;
-        }
-        uint32_t e = stack_ref[sp];
-        if (e & WIDE_UNIT_BIT) {
-            uint32_t u = e & ~WIDE_UNIT_BIT;
-            uint32_t b = X.t_instances + u * 10u;
-            if (u >= W.n_records || (uint64_t)b + 10u > S.n_table_vec4) { *guard = true; break; }
-            float4 m0 = tab(S, b), m1 = tab(S, b + 1), m2 = tab(S, b + 2);
-            float4 n0 = tab(S, b + 3), n1 = tab(S, b + 4), n2 = tab(S, b + 5);
+            const uint2 e = sp < WIDE_SHORT ? short_stack[sp * WIDE_BLOCK + tid] : spill[sp - WIDE_SHORT];
+            if (!(e.y & ENTRY_UNITS)) {
+                g_base = e.x;
+                g_bits = e.y;
+                continue;
+            }
+            // The next unit of a unit group (its slots in the world ray's visit order, a cursor in the first).
+            if (e.x >= W.n_nodes) { *guard = true; return hit; }
+            const uint4 n1 = __ldg(W.nodes + 5ull * e.x + 1);
+            uint32_t um = (e.y >> 8) & 0xffu;
+            const uint32_t cursor = e.y & 0xffu;
+            const uint32_t slot = ((uint32_t)__ffs(um) - 1u) ^ r.neg;
+            const uint2 it = slot_items(n1.y, n1.z, n1.w, slot);
+            const uint32_t item = it.x + cursor;
+            if (cursor + 1u < it.y) {
+                WIDE_PUSH(e.x, ENTRY_UNITS | (um << 8) | (cursor + 1u));
+            } else {
+                um &= um - 1u;
+                if (um) WIDE_PUSH(e.x, ENTRY_UNITS | (um << 8));
+            }
+            if (cursor >= it.y || item >= W.n_units) { *guard = true; return hit; }
+            const uint32_t uu = __ldg(W.units + item);
+            if (mode == TRACE_SHADOW && !(uu & WIDE_UNIT_BIT)) continue;
+            const uint32_t u = uu & ~WIDE_UNIT_BIT;
+            const uint32_t b = X.t_instances + u * 10u;
+            if (u >= W.n_records || (uint64_t)b + 10u > S.n_table_vec4) { *guard = true; return hit; }
+            if (COUNT) wc->units++;
+            const float4 m0 = tab(S, b), m1 = tab(S, b + 1), m2 = tab(S, b + 2);
+            const float4 n0 = tab(S, b + 3), nn1 = tab(S, b + 4), n2 = tab(S, b + 5);
             rec = u;
             V3 ro = o - V3{m0.w, m1.w, m2.w};
-            V3 rd = d;
-            V3 rinv = inv_d;
-            if ((bu(n1.w) & UNIT_SHIFTED) == 0) {
-                ro = proc_dir(n0, n1, n2, ro);
-                rd = proc_dir(n0, n1, n2, d);
+            V3 rd = d, rinv = inv_d;
+            if ((bu(nn1.w) & UNIT_SHIFTED) == 0) {
+                ro = proc_dir(n0, nn1, n2, ro);
+                rd = proc_dir(n0, nn1, n2, d);
                 rinv = safe_inv(rd);
             }
             r = wide_ray(ro, rd, rinv);
             base = sp;
-            cur = __ldg(W.unit_root + u);
-        } else {
-            cur = e;
+            g_bits = 0;
+            node = __ldg(W.unit_root + u);
+            break;
         }
     }
-    return hit;
-#undef STACK_PUSH
+#undef WIDE_PUSH
 }
 
 }  // namespace trt

@@ -93,6 +93,10 @@ class Scene:
         self.gpu._check(rc, "trt_render")
         return acc, st
 
+    def accum_copy(self, dst_device_ptr: int, nbytes: int):
+        """trt_accum_copy: the accum into caller-owned device memory (e.g. a torch tensor's data_ptr()), waited for."""
+        self.gpu._check(N.lib().trt_accum_copy(self.handle, C.c_void_p(dst_device_ptr), nbytes), "trt_accum_copy")
+
     def trace(self, params: np.ndarray, rays: np.ndarray, flags: int = 0) -> np.ndarray:
         L = N.lib()
         rays = np.ascontiguousarray(rays, dtype=RAY_DTYPE)
@@ -235,6 +239,15 @@ class Gpu:
                 scene.close()
         w, h = int(base[16]), int(base[17])
         return frame_of(acc, w, h, spp)
+
+    def math_eval(self, fn: int, x: np.ndarray, y: np.ndarray | None = None) -> np.ndarray:
+        """trt_math_eval: the device's cosf / sinf / acosf / atan2f (N.TRT_MATH_*) over float32 arrays."""
+        x = np.ascontiguousarray(x, np.float32)
+        yy = None if y is None else np.ascontiguousarray(y, np.float32)
+        out = np.zeros_like(x)
+        fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float)) if a is not None else None
+        self._check(N.lib().trt_math_eval(self.ctx, fn, fp(x), fp(yy), x.size, fp(out)), "trt_math_eval")
+        return out
 
     def timer_start(self):
         self._check(N.lib().trt_timer_start(self.ctx), "trt_timer_start")
