@@ -39,6 +39,7 @@ WORKLOAD = ("procedural city 1984402 tris / 4002 units, 1280x720, 1 spp, depth 4
 METRIC = "Mrays/s (closest + shadow rays, city 720p 1 spp depth 4)"
 # Algorithmic bytes a walk reads: a node record, a triangle's leaf record, the part of a unit record the walk reads.
 NODE_BYTES, LEAF_BYTES, UNIT_BYTES = 32, 48, 64
+WIDE_NODE_BYTES = 80  # a wide node: five 16-byte loads
 
 
 def log(*a):
@@ -73,18 +74,19 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """DRAM bytes per extend launch from the committed ncu summary of this workload, if there is one."""
-    p = ROOT / "profiles" / "extend_city720p.md"
+def walk_profile(walk: str):
+    """The ncu figures of the two walks on this workload, from the committed summary: per kernel, averaged over the
+    depths of one frame: DRAM bytes a launch, L1 / L2 hit rates, issue active, lanes active a warp instruction."""
+    p = ROOT / "profiles" / f"walks_{walk}_city720p.md"
     if not p.exists():
-        return None
+        return {}
     for line in p.read_text().splitlines():
-        if line.startswith("dram_bytes_per_launch:"):
+        if line.startswith("figures:"):
             try:
-                return float(line.split(":", 1)[1].split()[0])
+                return json.loads(line.split(":", 1)[1])
             except ValueError:
-                return None
-    return None
+                return {}
+    return {}
 
 
 class ClockSampler:
@@ -648,6 +650,85 @@ def run_sky(args, rank, world, local):
     gpu.close()
 
 
+TRUTH_SPP = 4096
+
+
+def run_extras(gpu, S, P, frame: int, args, flags: int) -> dict:
+    """The rest of the headline metric on the benched frame (rank 0): ΔE against a 4096-spp render of the same frame
+    (renderer/src/compare.rs, as threert_b200.metrics computes it) for the plain path at 1, 4 and 64 spp and for the
+    learned denoiser at 4 spp, the denoiser trained here first on pairs the pass renders (small procedural cities of
+    other seeds, 128 x 128, 1-4 spp against 256 spp); the plain path at the denoiser's device time (ΔE at equal ms);
+    and serving: 720p 1-spp denoised requests of the city's spline frames through the library's server, a saturated
+    burst for its capacity, then a Poisson stream at 70 % of it for p50 / p99, against one request at a time."""
+    from threert_b200 import metrics, prep, unet
+    from threert_b200 import denoise_train as DT
+    from threert_b200 import serve as SV
+    from threert_b200 import _native as N
+    from threert_b200.gpu import frame_of
+    out = {}
+    params = frame_params(P, frame)
+    t0 = time.perf_counter()
+    truth_acc, st_t = S.render_raw(prep.params_with(params, seed=0xACE), TRUTH_SPP, flags=flags)
+    truth = frame_of(truth_acc, WIDTH, HEIGHT, TRUTH_SPP).color
+    log(f"extras: truth {TRUTH_SPP} spp in {st_t.device_ms / 1e3:.1f} s")
+    de = lambda img: metrics.delta_e(truth, img)["mean"]
+    plain = {}
+    for spp in (1, 4, 64):
+        acc, st = S.render_raw(params, spp, flags=flags)
+        plain[spp] = {"delta_e": de(frame_of(acc, WIDTH, HEIGHT, spp).color), "ms": float(st.device_ms)}
+    # The learned denoiser, trained on the device by the library's own kernels.
+    t1 = time.perf_counter()
+    F, T = DT.make_dataset(gpu, range(100, 100 + args.extras_scenes), 16, 128, 128, 256)
+    t_data = time.perf_counter() - t1
+    net = unet.UNet(0, max_batch=16, max_h=HEIGHT, max_w=WIDTH)
+    net.set_params(unet.init_params(0))
+    t1 = time.perf_counter()
+    losses = DT.train(net, F, T, args.extras_train_steps, batch=16, lr=1e-3, seed=0)
+    t_train = time.perf_counter() - t1
+    del F, T
+    acc, st = S.render_raw(params, 4, flags=flags | N.TRT_RENDER_DEPTH)
+    den, ms_net = net.denoise(S)
+    at, ms_at = S.denoise_atrous(4)
+    ms_den = float(st.device_ms) + ms_net
+    # The plain path at the denoised frame's device time: as many samples as that time renders (a sample's time from
+    # the 64-sample render, where the per-call overhead is spread thin).
+    spp_eq = max(1, int(round(ms_den / max(plain[64]["ms"] / 64.0, 1e-6))))
+    acc_eq, st_eq = S.render_raw(params, spp_eq, flags=flags)
+    learned = {"delta_e": de(den), "ms": ms_den, "network_ms": ms_net}
+    out["delta_e"] = {
+        "truth_spp": TRUTH_SPP, "frame": frame, "metric": "mean ΔE (CIE76) of 8-bit sRGB at a fixed exposure",
+        "plain_1spp": plain[1], "plain_4spp": plain[4], "plain_64spp": plain[64],
+        "atrous_4spp": {"delta_e": de(at), "ms": float(st.device_ms) + ms_at},
+        "learned_4spp": learned,
+        "plain_at_equal_ms": {"spp": spp_eq, "delta_e": de(frame_of(acc_eq, WIDTH, HEIGHT, spp_eq).color),
+                              "ms": float(st_eq.device_ms)},
+        "target_met": bool(learned["delta_e"] <= plain[64]["delta_e"] and ms_den <= 0.25 * plain[64]["ms"]),
+        "training": {"pairs": 16 * args.extras_scenes, "steps": args.extras_train_steps, "dataset_s": t_data,
+                     "train_s": t_train, "first_loss": float(np.mean(losses[:100])),
+                     "last_loss": float(np.mean(losses[-100:]))},
+        "held_out": "trained on small procedural cities of seeds 100+, judged on the benched city (seed 1)"}
+    # Serving 720p 1-spp denoised requests on the resident city.
+    reqs = lambda n, off: [SV.Request(0, frame_params(P, off + 3 * k), 1, denoise=True) for k in range(n)]
+    srv = SV.Server(gpu, denoiser=net)
+    try:
+        SV.run_stream(srv, [S], reqs(8, 100), rate=0.0, keep=False)  # warm-up: pools, graphs
+        sat = SV.run_stream(srv, [S], reqs(64, 1), rate=0.0, keep=False)
+        cap = 64 / sat["span_s"]
+        at_rate = SV.run_stream(srv, [S], reqs(128, 2), rate=0.7 * cap, seed=7, keep=False)
+    finally:
+        srv.close()
+    serial = SV.run_serial(gpu, [S], reqs(64, 1), denoiser=net)
+    out["serve_720p"] = {
+        "requests": "1280x720, 1 spp, depth 4, denoised by the learned U-Net on the device, image read back",
+        "capacity_req_per_s": cap, "rate_req_per_s": 0.7 * cap, "p50_ms": at_rate["p50_ms"],
+        "p99_ms": at_rate["p99_ms"], "mrays_per_s_at_rate": at_rate["mrays_per_s"],
+        "mrays_per_s_saturated": sat["mrays_per_s"], "serial_mrays_per_s": serial["mrays_per_s"],
+        "serial_p50_ms": serial["p50_ms"], "speedup_over_serial": sat["mrays_per_s"] / serial["mrays_per_s"]}
+    net.close()
+    log(f"extras: {time.perf_counter() - t0:.1f} s")
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -660,6 +741,11 @@ def main():
                     help="coherence sorts on the device: 'none', or a comma list of rays, hits, shadows "
                          "(hits by material is the pass's default; the other two measured slower here)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="city: skip the image-quality and serving figures (ΔE against 4096 spp, the learned "
+                         "denoiser at equal ms, 720p serving latency)")
+    ap.add_argument("--extras-train-steps", type=int, default=20000, help="city extras: the denoiser's Adam steps")
+    ap.add_argument("--extras-scenes", type=int, default=32, help="city extras: procedural cities for training")
     ap.add_argument("--workload", default="city", choices=["city", "crowd", "serve", "denoise", "sky", "cornell"],
                     help="city (the headline workload), the crowd with its per-frame deformation, the serving mix, "
                          "the learned denoiser (trained, then judged), the atmosphere's sky bake, or the Cornell box")
@@ -795,14 +881,48 @@ def main():
     for f in frames:
         S.render_raw(params[f], SPP, flags=flags | N.TRT_RENDER_COUNT, read=False, stats=False)
     cnt = S.totals()
-    ext_bytes = (cnt["node_visits"] * NODE_BYTES + cnt["tri_tests"] * LEAF_BYTES + cnt["unit_entries"] * UNIT_BYTES)
+    node_bytes = WIDE_NODE_BYTES if args.walk == "wide" else NODE_BYTES
+    ext_bytes = (cnt["node_visits"] * node_bytes + cnt["tri_tests"] * LEAF_BYTES + cnt["unit_entries"] * UNIT_BYTES)
+    sha_bytes = (cnt["shadow_node_visits"] * node_bytes + cnt["shadow_tri_tests"] * LEAF_BYTES
+                 + cnt["shadow_unit_entries"] * UNIT_BYTES)
+    per_ray = lambda k, n: cnt[k] / max(1, n)
+    walk_counts = {
+        "closest": {"rays": int(cnt["closest_rays"]), "nodes": per_ray("node_visits", cnt["closest_rays"]),
+                    "tris": per_ray("tri_tests", cnt["closest_rays"]),
+                    "units": per_ray("unit_entries", cnt["closest_rays"])},
+        "shadow": {"rays": int(cnt["shadow_rays"]), "nodes": per_ray("shadow_node_visits", cnt["shadow_rays"]),
+                   "tris": per_ray("shadow_tri_tests", cnt["shadow_rays"]),
+                   "units": per_ray("shadow_unit_entries", cnt["shadow_rays"])},
+        "node_bytes": node_bytes}
     ext_bytes_per_launch = ext_bytes / max(1, cnt["extend_launches"])
+    sha_bytes_per_launch = sha_bytes / max(1, cnt["shadow_launches"])
+    sha_avg_ms = tot["shadow_ms"] / max(1, tot["shadow_launches"])
 
     ms, e2e_ms, rays_all = reduce_over_ranks(dist, ms, e2e_ms, float(rays), device="cuda")
 
     peak, peak_kind = measured_peaks()
-    achieved = ext_bytes_per_launch / (ext_avg_ms * 1e-3) / 1e9 if ext_avg_ms > 0 else None
-    traffic = profile_traffic()
+    prof = walk_profile(args.walk)
+
+    def roof(kernel, bytes_per_launch, launch_ms, rays_walked):
+        """Algorithmic bytes a launch (node records, leaf records, unit records the walk reads, counted by the
+        walk itself) over the launch's device time, against the measured HBM copy bandwidth. The walks' reads are
+        mostly L1 / L2 hits: the profile's DRAM traffic and lane figures say what bounds them."""
+        achieved = bytes_per_launch / (launch_ms * 1e-3) / 1e9 if launch_ms > 0 else None
+        pf = prof.get(kernel, {})
+        traffic = pf.get("dram_bytes_per_launch")
+        return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "traffic": traffic, "kernel": kernel,
+                "peak_kind": f"{peak_kind} hbm_gbs", "bytes_per_launch": bytes_per_launch, "launch_ms": launch_ms,
+                "bytes_per_ray": bytes_per_launch * (cnt["extend_launches"] if kernel == "k_extend"
+                                                     else cnt["shadow_launches"]) / max(1, rays_walked),
+                "dram_frac_of_peak": (traffic / (launch_ms * 1e-3) / 1e9 / peak) if traffic and launch_ms else None,
+                "l1_hit_pct": pf.get("l1_hit_pct"), "l2_hit_pct": pf.get("l2_hit_pct"),
+                "issue_active_pct": pf.get("issue_active_pct"), "lanes_active_of_32": pf.get("lanes"),
+                "limiter": pf.get("limiter"), "profile": f"profiles/walks_{args.walk}_city720p.md" if pf else None}
+
+    rooflines = {"k_extend": roof("k_extend", ext_bytes_per_launch, ext_avg_ms, cnt["closest_rays"]),
+                 "k_shadow": roof("k_shadow", sha_bytes_per_launch, sha_avg_ms, cnt["shadow_rays"])}
+    dominant = "k_shadow" if tot["shadow_ms"] >= tot["extend_ms"] else "k_extend"
     line = {
         "metric": METRIC, "value": rays_all / (ms * 1e-3) / 1e6, "unit": "Mrays/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -813,17 +933,20 @@ def main():
         "e2e": {"value": rays_all / (e2e_ms * 1e-3) / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": 624,
                 "d2h_bytes_per_step": WIDTH * HEIGHT * 80},
         "gpu_launches": int(launches),
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                     "kernel": "k_extend (closest-hit walk)", "peak_kind": f"{peak_kind} hbm_gbs",
-                     "bytes_per_launch": ext_bytes_per_launch, "launch_ms": ext_avg_ms,
-                     "bytes_per_ray": ext_bytes / max(1, tot["closest_rays"])},
+        "roofline": rooflines[dominant],
+        "rooflines": rooflines,
         "clocks": clk,
         "rays_per_path": rays / max(1, tot["paths"]),
+        "walk_counts": walk_counts,
         "paths_per_s": tot["paths"] * world / (ms * 1e-3),
         "stage_ms_per_step": {"extend": tot["extend_ms"] / args.steps, "shadow": tot["shadow_ms"] / args.steps,
                               "shade": tot["shade_ms"] / args.steps, "sort": tot["sort_ms"] / args.steps},
     }
+    if rank == 0 and not args.no_extras:
+        try:
+            line.update(run_extras(gpu, S, P, frames[0], args, flags))
+        except Exception as e:  # (the throughput line stands without them)
+            line["extras_error"] = f"{type(e).__name__}: {e}"
     if rank == 0 and world == 1 and not args.no_cpu:
         v, cores, sample = cpu_sample(P, frames[:4], 20.0)
         line["cpu_baseline"] = {"value": v / 1e6, "unit": "Mrays/s", "cores": cores, "kind": "port",

@@ -70,11 +70,23 @@ __device__ __forceinline__ float q_byte(uint32_t w, int k) {
     return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440u | (uint32_t)k)) - 8388608.0f;
 }
 
+// Three-input minimum and maximum (one instruction each on sm_100; exact, like two fminf / fmaxf).
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
 // The eight child boxes of node `nd` against the ray: bit i of the result is set when slot i's box is entered before
-// tmax. A slot's plane at q steps is origin + q 2^e: t = q (2^e / d) + (origin - o) / d, one FMA. The near and far
-// planes of each axis are picked once by the ray's signs; an empty slot (q_lo > q_hi) has its near plane past its far
-// one on every axis, so it misses whatever the signs.
-__device__ __forceinline__ uint32_t wide_hits(const uint4 nd[5], const WideRay& r, float tmax) {
+// tmax; *tmin is the nearest hit slot's entry t (INF: none). A slot's plane at q steps is origin + q 2^e:
+// t = q (2^e / d) + (origin - o) / d, one FMA. The near and far planes of each axis are picked once by the ray's signs;
+// an empty slot (q_lo > q_hi) has its near plane past its far one on every axis, so it misses whatever the signs.
+__device__ __forceinline__ uint32_t wide_hits(const uint4 nd[5], const WideRay& r, float tmax, float* tmin) {
     const uint32_t eb = nd[0].w;
     const float Sx = __uint_as_float((eb & 0xffu) << 23) * r.inv.x;
     const float Sy = __uint_as_float(((eb >> 8) & 0xffu) << 23) * r.inv.y;
@@ -90,16 +102,20 @@ __device__ __forceinline__ uint32_t wide_hits(const uint4 nd[5], const WideRay& 
     const uint32_t nearz[2] = {nz ? nd[4].z : nd[3].x, nz ? nd[4].w : nd[3].y};
     const uint32_t farz[2] = {nz ? nd[3].x : nd[4].z, nz ? nd[3].y : nd[4].w};
     uint32_t hits = 0;
+    float tm = INF;
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
         const int h = i >> 2, k = i & 3;
         const float x0 = fmaf(q_byte(nearx[h], k), Sx, Bx), x1 = fmaf(q_byte(farx[h], k), Sx, Bx);
         const float y0 = fmaf(q_byte(neary[h], k), Sy, By), y1 = fmaf(q_byte(fary[h], k), Sy, By);
         const float z0 = fmaf(q_byte(nearz[h], k), Sz, Bz), z1 = fmaf(q_byte(farz[h], k), Sz, Bz);
-        const float tnear = fmaxf(fmaxf(x0, y0), fmaxf(z0, 0.0f));
-        const float tfar = fminf(fminf(x1, y1), fminf(z1, tmax));
-        hits |= (tnear <= tfar ? 1u : 0u) << i;
+        const float tnear = max3f(x0, y0, fmaxf(z0, 0.0f));
+        const float tfar = min3f(x1, y1, fminf(z1, tmax));
+        const bool hit = tnear <= tfar;
+        hits |= (hit ? 1u : 0u) << i;
+        tm = fminf(tm, hit ? tnear : INF);
     }
+    *tmin = tm;
     return hits;
 }
 
@@ -125,148 +141,198 @@ __device__ __forceinline__ uint2 slot_items(uint32_t leaf_base, uint32_t c_lo, u
 // through compressed wide BVHs", HPG 2017): opening a node tests its eight children at once and leaves its hit
 // interior children as one group, (first child's index, hit mask in visit order | interior mask), from which the walk
 // takes the nearest child next; what is left of a group goes onto the stack as one 8-byte entry when the walk
-// descends. No child is sorted or pushed on its own. A node's hit leaf slots are done before its children: a mesh's
-// triangles are tested on the spot (the reference's Moller-Trumbore on the unit-space ray, pathtrace.wgsl:742-761),
-// and a top-tree node's hit units become a unit group entry (node, slots in visit order, item cursor) that enters
-// them one at a time, the ray taken into each unit's space as trace_units.wgsl:86-105 does; a unit's walk ends when
-// the stack is back to where it was entered. Shadow rays (TRACE_SHADOW) skip units that cast no shadow, and any-hit
-// rays stop at the first triangle hit. The first WIDE_SHORT entries of a thread's stack are in shared memory; more
-// than WIDE_STACK end the walk with the guard set.
-template <bool COUNT>
-__device__ Hit trace_wide(const DScene& S, const WideView& W, const Sections& X, V3 o, V3 d, float tmax, uint32_t mode,
-                          WalkCount* wc, bool* guard) {
-    Hit hit{tmax, MISS, 0.0f, 0.0f, NO_INST, 0u};
-    if (W.n_units == 0) return hit;
+// descends. No child is sorted or pushed on its own. A node's hit leaf slots are done before its children, in visit
+// order: a mesh's triangles are tested on the spot (the reference's Moller-Trumbore on the unit-space ray,
+// pathtrace.wgsl:742-761), and a top-tree node's hit units become a unit group entry (node, slots in visit order, item
+// cursor) that enters them one at a time, the ray taken into each unit's space as trace_units.wgsl:86-105 does; a
+// unit's walk ends when the stack is back to where it was entered. Each entry carries a lower bound of its group's
+// nearest entry distance, and a group that lies past the closest hit is dropped unopened. Shadow rays (TRACE_SHADOW)
+// skip units that cast no shadow, and any-hit rays stop at the first triangle hit. The first WIDE_SHORT entries of a
+// thread's stack are in shared memory (wide_smem, a column a thread); more than WIDE_STACK end the walk with the
+// guard set.
+//
+// The walk is a state (WideWalk) advanced one node at a time (wide_step). (Measured on the city frame: giving a lane
+// whose ray is done the next ray between steps, while its warp's other lanes walk on, gained 3 % at best against a
+// warp that takes 32 new rays when all are done, and the state kept across steps cost more than that in spills.)
+struct WideWalk {
+    V3 o, d, inv_d;          // the world's ray
+    WideRay r;               // the ray in the current level's space
+    Hit hit;
+    uint32_t node;           // the node to open next
+    uint32_t g_base, g_bits; // the current node group (entry layout)
+    uint32_t rec, iter, mode;
+    int sp, base;            // stack depth; the depth at which the current unit was entered
+};
+
+__device__ __forceinline__ uint2* wide_smem() {
     __shared__ uint2 short_stack[WIDE_SHORT * WIDE_BLOCK];
-    if (blockDim.x > WIDE_BLOCK) { *guard = true; return hit; }
+    return short_stack;
+}
+
+// Starts a walk; false when there is nothing to walk (w.hit is then the miss).
+__device__ __forceinline__ bool wide_begin(WideWalk& w, const WideView& W, V3 o, V3 d, float tmax, uint32_t mode) {
+    w.hit = Hit{tmax, MISS, 0.0f, 0.0f, NO_INST, 0u};
+    if (W.n_units == 0) return false;
+    w.o = o;
+    w.d = d;
+    w.inv_d = safe_inv(d);
+    w.r = wide_ray(o, d, w.inv_d);
+    w.node = W.top_root;
+    w.g_base = w.g_bits = 0;
+    w.rec = NO_INST;
+    w.iter = 0;
+    w.mode = mode;
+    w.sp = w.base = 0;
+    return true;
+}
+
+// One node of the walk: opens w.node, tests its hit leaves, takes the next node. Returns false when the walk is over
+// (w.hit is its result; *guard set when it gave up on a tree that is not one).
+template <bool COUNT>
+__device__ __forceinline__ bool wide_step(WideWalk& w, const DScene& S, const WideView& W, const Sections& X,
+                                          uint2* short_stack, uint2* spill, WalkCount* wc, bool* guard) {
     const uint32_t tid = threadIdx.x;
-    uint2 spill[WIDE_STACK - WIDE_SHORT];
-    int sp = 0;
-#define WIDE_PUSH(X_, Y_)                                                                    \
-    do {                                                                                     \
-        if (sp >= WIDE_STACK) { *guard = true; return hit; }                                 \
-        if (sp < WIDE_SHORT) short_stack[sp * WIDE_BLOCK + tid] = make_uint2((X_), (Y_));   \
-        else spill[sp - WIDE_SHORT] = make_uint2((X_), (Y_));                                \
-        ++sp;                                                                                \
+#define WIDE_PUSH(X_, Y_)                                                                      \
+    do {                                                                                       \
+        if (w.sp >= WIDE_STACK) { *guard = true; return false; }                               \
+        if (w.sp < WIDE_SHORT) short_stack[w.sp * WIDE_BLOCK + tid] = make_uint2((X_), (Y_)); \
+        else spill[w.sp - WIDE_SHORT] = make_uint2((X_), (Y_));                                \
+        ++w.sp;                                                                                \
     } while (0)
-    constexpr uint32_t ENTRY_UNITS = 0x80000000u;  // in y: a unit group (x: its node)
-    const V3 inv_d = safe_inv(d);
-    WideRay r = wide_ray(o, d, inv_d);
-    uint32_t node = W.top_root;       // the node to open next
-    uint32_t g_base = 0, g_bits = 0;  // the current group: first child's index; hit mask (visit order) << 8 | imask
-    uint32_t rec = NO_INST;
-    int base = 0;
-    for (uint32_t iter = 0;; ++iter) {
-        if (iter >= WALK_GUARD || node >= W.n_nodes) { *guard = true; return hit; }
-        const uint4* np = W.nodes + 5ull * node;
+    // An entry: a node group, x its first child's index, y = imask | hits (visit order) << 8 | t << 16; or a unit
+    // group, x its node | ENTRY_UNITS, y = item cursor | slots (visit order) << 8 | t << 16. t: the top 16 bits of
+    // the group's nearest entry distance (truncated: a lower bound).
+    constexpr uint32_t ENTRY_UNITS = 0x80000000u;
+    const auto t_of = [](uint32_t y) { return __uint_as_float(y & 0xffff0000u); };
+    if (w.iter++ >= WALK_GUARD || w.node >= W.n_nodes) { *guard = true; return false; }
+    {
+        const uint4* np = W.nodes + 5ull * w.node;
         uint4 nd[5];
 #pragma unroll
         for (int k = 0; k < 5; ++k) nd[k] = __ldg(np + k);
         if (COUNT) wc->nodes++;
-        const uint32_t hm = wide_hits(nd, r, hit.t);
+        float tmin;
+        const uint32_t hm = wide_hits(nd, w.r, w.hit.t, &tmin);
         const uint32_t imask = nd[0].w >> 24;
-        g_base = nd[1].x;
-        g_bits = (visit_mask(hm & imask, r.neg) << 8) | imask;
-        uint32_t leaf = hm & ~imask;
+        const uint32_t t16 = __float_as_uint(tmin) & 0xffff0000u;
+        w.g_base = nd[1].x;
+        w.g_bits = (visit_mask(hm & imask, w.r.neg) << 8) | imask | t16;
+        uint32_t leaf = visit_mask(hm & ~imask, w.r.neg);
         if (leaf != 0u) {
-            if (rec == NO_INST) {
+            if (w.rec == NO_INST) {
                 // Units: the group of this node's hit unit slots goes on top of what is left of its children.
-                if (g_bits >> 8) WIDE_PUSH(g_base, g_bits);
-                g_bits = 0;
-                WIDE_PUSH(node, ENTRY_UNITS | (visit_mask(leaf, r.neg) << 8));
+                if (w.g_bits & 0xff00u) WIDE_PUSH(w.g_base, w.g_bits);
+                w.g_bits = 0;
+                WIDE_PUSH(w.node | ENTRY_UNITS, (leaf << 8) | t16);
             } else {
                 do {
-                    const uint32_t slot = (uint32_t)__ffs(leaf) - 1u;
+                    const uint32_t slot = ((uint32_t)__ffs(leaf) - 1u) ^ w.r.neg;
                     leaf &= leaf - 1u;
                     const uint2 it = slot_items(nd[1].y, nd[1].z, nd[1].w, slot);
                     for (uint32_t q = 0; q < it.y; ++q) {
                         const uint32_t ti = it.x + q;
-                        if (ti >= W.n_tris) { *guard = true; return hit; }
+                        if (ti >= W.n_tris) { *guard = true; return false; }
                         const float4* tp = W.tris + 3ull * ti;
                         const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
                         if (COUNT) wc->tris++;
                         // pathtrace.wgsl:742-761 intersect_tri, on the copy of the reference's leaf record.
                         const V3 v0 = xyz(a), e1 = xyz(b), e2 = xyz(c);
-                        const V3 pv = cross(r.d, e2);
+                        const V3 pv = cross(w.r.d, e2);
                         const float det = dot(e1, pv);
                         if (fabsf(det) < 1e-12f) continue;
                         const float inv = 1.0f / det;
-                        const V3 tv = r.o - v0;
+                        const V3 tv = w.r.o - v0;
                         const float u = dot(tv, pv) * inv;
                         if (u < 0.0f || u > 1.0f) continue;
                         const V3 qv = cross(tv, e1);
-                        const float v = dot(r.d, qv) * inv;
+                        const float v = dot(w.r.d, qv) * inv;
                         if (v < 0.0f || u + v > 1.0f) continue;
                         const float t = dot(e2, qv) * inv;
-                        if (t <= 0.0f || t >= hit.t) continue;
-                        hit = Hit{t, bu(c.w), u, v, rec, bu(a.w)};
-                        if (mode != TRACE_CLOSEST) return hit;
+                        if (t <= 0.0f || t >= w.hit.t) continue;
+                        w.hit = Hit{t, bu(c.w), u, v, w.rec, bu(a.w)};
+                        if (w.mode != TRACE_CLOSEST) return false;
                     }
                 } while (leaf != 0u);
             }
         }
-        // The next node: the nearest child left in the group, else the stack's top (a group, or the next unit of a
-        // unit group, entered).
-        for (;;) {
-            if (g_bits >> 8) {
-                const uint32_t k = (uint32_t)__ffs(g_bits >> 8) - 1u;
-                g_bits &= ~(1u << (k + 8u));
-                const uint32_t slot = k ^ r.neg;
-                node = g_base + (uint32_t)__popc(g_bits & ((1u << slot) - 1u) & 0xffu);
-                if (g_bits >> 8) WIDE_PUSH(g_base, g_bits);
-                break;
-            }
-            if (rec != NO_INST && sp == base) {  // the unit's walk is over: back to the world's ray
-                rec = NO_INST;
-                r = wide_ray(o, d, inv_d);
-            }
-            if (sp == 0) return hit;
-            --sp;
-            const uint2 e = sp < WIDE_SHORT ? short_stack[sp * WIDE_BLOCK + tid] : spill[sp - WIDE_SHORT];
-            if (!(e.y & ENTRY_UNITS)) {
-                g_base = e.x;
-                g_bits = e.y;
-                continue;
-            }
-            // The next unit of a unit group (its slots in the world ray's visit order, a cursor in the first).
-            if (e.x >= W.n_nodes) { *guard = true; return hit; }
-            const uint4 n1 = __ldg(W.nodes + 5ull * e.x + 1);
-            uint32_t um = (e.y >> 8) & 0xffu;
-            const uint32_t cursor = e.y & 0xffu;
-            const uint32_t slot = ((uint32_t)__ffs(um) - 1u) ^ r.neg;
-            const uint2 it = slot_items(n1.y, n1.z, n1.w, slot);
-            const uint32_t item = it.x + cursor;
-            if (cursor + 1u < it.y) {
-                WIDE_PUSH(e.x, ENTRY_UNITS | (um << 8) | (cursor + 1u));
-            } else {
-                um &= um - 1u;
-                if (um) WIDE_PUSH(e.x, ENTRY_UNITS | (um << 8));
-            }
-            if (cursor >= it.y || item >= W.n_units) { *guard = true; return hit; }
-            const uint32_t uu = __ldg(W.units + item);
-            if (mode == TRACE_SHADOW && !(uu & WIDE_UNIT_BIT)) continue;
-            const uint32_t u = uu & ~WIDE_UNIT_BIT;
-            const uint32_t b = X.t_instances + u * 10u;
-            if (u >= W.n_records || (uint64_t)b + 10u > S.n_table_vec4) { *guard = true; return hit; }
-            if (COUNT) wc->units++;
-            const float4 m0 = tab(S, b), m1 = tab(S, b + 1), m2 = tab(S, b + 2);
-            const float4 n0 = tab(S, b + 3), nn1 = tab(S, b + 4), n2 = tab(S, b + 5);
-            rec = u;
-            V3 ro = o - V3{m0.w, m1.w, m2.w};
-            V3 rd = d, rinv = inv_d;
-            if ((bu(nn1.w) & UNIT_SHIFTED) == 0) {
-                ro = proc_dir(n0, nn1, n2, ro);
-                rd = proc_dir(n0, nn1, n2, d);
-                rinv = safe_inv(rd);
-            }
-            r = wide_ray(ro, rd, rinv);
-            base = sp;
-            g_bits = 0;
-            node = __ldg(W.unit_root + u);
-            break;
+    }
+    // The next node: the nearest child left in the group, else the stack's top (a group, or the next unit of a unit
+    // group, entered); groups whose nearest entry lies past the closest hit are dropped.
+    for (;;) {
+        if ((w.g_bits & 0xff00u) && t_of(w.g_bits) < w.hit.t) {
+            const uint32_t k = (uint32_t)__ffs(w.g_bits >> 8) - 1u;
+            w.g_bits &= ~(1u << (k + 8u));
+            const uint32_t slot = k ^ w.r.neg;
+            w.node = w.g_base + (uint32_t)__popc(w.g_bits & ((1u << slot) - 1u) & 0xffu);
+            if (w.g_bits & 0xff00u) WIDE_PUSH(w.g_base, w.g_bits);
+            return true;
         }
+        if (w.rec != NO_INST && w.sp == w.base) {  // the unit's walk is over: back to the world's ray
+            w.rec = NO_INST;
+            w.r = wide_ray(w.o, w.d, w.inv_d);
+        }
+        if (w.sp == 0) return false;
+        --w.sp;
+        const uint2 e = w.sp < WIDE_SHORT ? short_stack[w.sp * WIDE_BLOCK + tid] : spill[w.sp - WIDE_SHORT];
+        w.g_bits = 0;
+        if (t_of(e.y) >= w.hit.t) continue;
+        if (!(e.x & ENTRY_UNITS)) {
+            w.g_base = e.x;
+            w.g_bits = e.y;
+            continue;
+        }
+        // The next unit of a unit group (its slots in the world ray's visit order, a cursor in the first).
+        const uint32_t un = e.x & ~ENTRY_UNITS;
+        if (un >= W.n_nodes) { *guard = true; return false; }
+        const uint4 n1 = __ldg(W.nodes + 5ull * un + 1);
+        uint32_t um = (e.y >> 8) & 0xffu;
+        const uint32_t cursor = e.y & 0xffu;
+        const uint32_t slot = ((uint32_t)__ffs(um) - 1u) ^ w.r.neg;
+        const uint2 it = slot_items(n1.y, n1.z, n1.w, slot);
+        const uint32_t item = it.x + cursor;
+        if (cursor + 1u < it.y) {
+            WIDE_PUSH(e.x, (e.y & 0xffff0000u) | (um << 8) | (cursor + 1u));
+        } else {
+            um &= um - 1u;
+            if (um) WIDE_PUSH(e.x, (e.y & 0xffff0000u) | (um << 8));
+        }
+        if (cursor >= it.y || item >= W.n_units) { *guard = true; return false; }
+        const uint32_t uu = __ldg(W.units + item);
+        if (w.mode == TRACE_SHADOW && !(uu & WIDE_UNIT_BIT)) continue;
+        const uint32_t u = uu & ~WIDE_UNIT_BIT;
+        const uint32_t b = X.t_instances + u * 10u;
+        if (u >= W.n_records || (uint64_t)b + 10u > S.n_table_vec4) { *guard = true; return false; }
+        if (COUNT) wc->units++;
+        const float4 m0 = tab(S, b), m1 = tab(S, b + 1), m2 = tab(S, b + 2);
+        const float4 n0 = tab(S, b + 3), nn1 = tab(S, b + 4), n2 = tab(S, b + 5);
+        w.rec = u;
+        V3 ro = w.o - V3{m0.w, m1.w, m2.w};
+        V3 rd = w.d, rinv = w.inv_d;
+        if ((bu(nn1.w) & UNIT_SHIFTED) == 0) {
+            ro = proc_dir(n0, nn1, n2, ro);
+            rd = proc_dir(n0, nn1, n2, w.d);
+            rinv = safe_inv(rd);
+        }
+        w.r = wide_ray(ro, rd, rinv);
+        w.base = w.sp;
+        w.node = __ldg(W.unit_root + u);
+        return true;
     }
 #undef WIDE_PUSH
+}
+
+// The whole walk of one ray (trt_trace's queries): the steps until it is over. A block has at most WIDE_BLOCK threads.
+template <bool COUNT>
+__device__ Hit trace_wide(const DScene& S, const WideView& W, const Sections& X, V3 o, V3 d, float tmax, uint32_t mode,
+                          WalkCount* wc, bool* guard) {
+    WideWalk w;
+    if (blockDim.x > WIDE_BLOCK) { *guard = true; return Hit{tmax, MISS, 0.0f, 0.0f, NO_INST, 0u}; }
+    if (!wide_begin(w, W, o, d, tmax, mode)) return w.hit;
+    uint2 spill[WIDE_STACK - WIDE_SHORT];
+    uint2* sh = wide_smem();
+    while (wide_step<COUNT>(w, S, W, X, sh, spill, wc, guard)) {
+    }
+    return w.hit;
 }
 
 }  // namespace trt
