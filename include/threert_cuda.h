@@ -167,6 +167,15 @@ int trt_scene_set_sky(trt_scene* scene, const trt_atmosphere* atm, int32_t sun_l
 int trt_scene_weigh_emitters(trt_scene* scene, const uint32_t params[TRT_PARAMS_WORDS], uint32_t tree_nodes,
                              const float* lod, const float* cull, float* ms);
 
+/* The light tree built again on the device (renderer/src/ltree.rs:405-470 build: the emitters of positive power that
+ * are neither nominal nor moving, one a leaf, median splits along the widest axis of their centroids; lib.rs:393-418:
+ * the emitter table put in the tree's leaf order, the others after it, each triangle's code) from the emitter records
+ * as the tables hold them now: after emitters moved (their records written). params: its light-tree words are set
+ * (the tree's entries; the candidates resampled at camera hits); *tree_nodes: the tree's nodes (0: no tree, below 256
+ * such emitters). Then trt_scene_weigh_emitters(scene, params, *tree_nodes, ...) makes the nodes' powers, the CDF and
+ * the header. At most 16,384 emitters in the tree; ms (may be NULL): device time. */
+int trt_scene_build_light_tree(trt_scene* scene, uint32_t params[TRT_PARAMS_WORDS], uint32_t* tree_nodes, float* ms);
+
 /* ---- The learned denoiser (no counterpart in the reference, whose learned denoiser is the external OIDN library,
  * renderer/src/denoise.rs:80-103): a 4-level U-Net (32 / 64 / 96 / 128 channels, 3 x 3 convolutions, 2 x 2 average
  * pooling, nearest upsampling, skip concatenations) on bf16 tensor cores with f32 accumulation; its training (forward,

@@ -12,12 +12,13 @@ def luma(c):
     return 0.2126 * c[..., 0] + 0.7152 * c[..., 1] + 0.0722 * c[..., 2]
 
 
-def small_city(seed=3, n_objects=80, width=64, height=36, n_emitters=140, max_depth=4, sky="gradient"):
+def small_city(seed=3, n_objects=80, width=64, height=36, n_emitters=140, max_depth=4, sky="gradient",
+               emitter_offset=(0.0, 0.0, 0.0)):
     """A city small enough for the oracle: boxes turned about y (units with normal rows), spheres placed by a
     translation alone (UNIT_SHIFTED), a ground, emissive quads past the light tree's 256 triangles."""
     return scenes.city(n_objects=n_objects, width=width, height=height, seed=seed, extent=60.0, n_emitters=n_emitters,
                        box_segments=2, sphere_slices=10, sphere_stacks=8, max_depth=max_depth, sky_size=(64, 32),
-                       sky=sky)
+                       sky=sky, emitter_offset=emitter_offset)
 
 
 def scaled_units_scene():

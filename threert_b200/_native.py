@@ -191,6 +191,7 @@ SIGNATURES = [
     ("trt_denoise_atrous", C.c_int, [C.c_void_p, u32, P(f32), P(f32)]),
     ("trt_sky_bake", C.c_int, [C.c_void_p, P(Atmosphere), P(f32), P(f32), P(SkyResult)]),
     ("trt_scene_weigh_emitters", C.c_int, [C.c_void_p, P(u32), u32, P(f32), P(f32), P(f32)]),
+    ("trt_scene_build_light_tree", C.c_int, [C.c_void_p, P(u32), P(u32), P(f32)]),
     ("trt_scene_set_sky", C.c_int, [C.c_void_p, P(Atmosphere), C.c_int32, f32, P(u32), P(SkyResult)]),
     ("trt_deform_setup", C.c_int, [C.c_void_p, P(DeformDesc)]),
     ("trt_deform", C.c_int, [C.c_void_p, P(u32), P(f32), u32, u32, P(DeformStats)]),

@@ -1783,3 +1783,4 @@ int trt_render_noalloc(const trt_scene_desc* dev, const uint32_t params[TRT_PARA
 
 #include "serve.cuh"
 #include "emitters.cuh"
+#include "ltree.cuh"

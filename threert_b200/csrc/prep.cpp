@@ -609,8 +609,15 @@ struct LightTree {
             for (int k = 1; k < 3; ++k)
                 if ((chi[k] - clo[k]) >= (chi[axis] - clo[axis])) axis = k;
             size_t mid = len / 2;
+            // (ltree.rs orders by the centroid's coordinate under f32::total_cmp; equal ones here by their emitter's
+            // index, so that the split does not depend on the selection's order of equals and the device build, which
+            // orders them so, makes the same tree.)
+            auto key = [&](const LtItem& p) {
+                uint32_t b = bu(p.c[axis]);
+                return ((uint64_t)((b & 0x80000000u) ? ~b : (b | 0x80000000u)) << 32) | p.e;
+            };
             std::nth_element(items.begin() + t.a, items.begin() + t.a + mid, items.begin() + t.b,
-                             [&](const LtItem& p, const LtItem& q) { return p.c[axis] < q.c[axis]; });
+                             [&](const LtItem& p, const LtItem& q) { return key(p) < key(q); });
             size_t left = nodes.size();
             nodes.push_back({0, 0, 0, 0});
             nodes.push_back({0, 0, 0, 0});
@@ -1044,7 +1051,9 @@ int trt_prep_build(const trt_scene_spec* spec, trt_prepared** out) {
                 for (int k = 0; k < 3; ++k) {
                     it.lo[k] = std::min(std::min(std::min(std::numeric_limits<float>::max(), vs[0][k]), vs[1][k]), vs[2][k]);
                     it.hi[k] = std::max(std::max(std::max(std::numeric_limits<float>::lowest(), vs[0][k]), vs[1][k]), vs[2][k]);
-                    it.c[k] = etris[i].c[k];
+                    // The centroid of the record's vertices (the reference takes the world vertices' before the record
+                    // rounds them to v0, e1, e2: the same point to an ulp). A device build has only the record.
+                    it.c[k] = (vs[0][k] + vs[1][k] + vs[2][k]) / 3.0f;
                 }
                 it.w = w;
                 fixed.push_back(it);

@@ -16,14 +16,26 @@ __device__ __forceinline__ Node node_at(const DScene& S, uint32_t i) {
     return {{bf(a.x), bf(a.y), bf(a.z)}, a.w, {bf(b.x), bf(b.y), bf(b.z)}, b.w};
 }
 
-// pathtrace.wgsl:732-739 ray_aabb
+// Three-input minimum and maximum (one instruction each on sm_100; exact, like two fminf / fmaxf).
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
+// pathtrace.wgsl:732-739 ray_aabb (min and max are exact, so grouping them three at a time rounds nothing)
 __device__ __forceinline__ float ray_aabb(V3 o, V3 inv_d, V3 bmin, V3 bmax, float tmax) {
     V3 t0 = (bmin - o) * inv_d;
     V3 t1 = (bmax - o) * inv_d;
     V3 tmin_v = vmin(t0, t1);
     V3 tmax_v = vmax(t0, t1);
-    float tn = fmaxf(fmaxf(tmin_v.x, tmin_v.y), fmaxf(tmin_v.z, 0.0f));
-    float tf = fminf(fminf(tmax_v.x, tmax_v.y), fminf(tmax_v.z, tmax));
+    float tn = max3f(tmin_v.x, tmin_v.y, fmaxf(tmin_v.z, 0.0f));
+    float tf = min3f(tmax_v.x, tmax_v.y, fminf(tmax_v.z, tmax));
     return tn <= tf ? tn : INF;
 }
 

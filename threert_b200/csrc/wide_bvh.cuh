@@ -70,18 +70,6 @@ __device__ __forceinline__ float q_byte(uint32_t w, int k) {
     return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440u | (uint32_t)k)) - 8388608.0f;
 }
 
-// Three-input minimum and maximum (one instruction each on sm_100; exact, like two fminf / fmaxf).
-__device__ __forceinline__ float max3f(float a, float b, float c) {
-    float r;
-    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
-    return r;
-}
-__device__ __forceinline__ float min3f(float a, float b, float c) {
-    float r;
-    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
-    return r;
-}
-
 // The eight child boxes of node `nd` against the ray: bit i of the result is set when slot i's box is entered before
 // tmax; *tmin is the nearest hit slot's entry t (INF: none). A slot's plane at q steps is origin + q 2^e:
 // t = q (2^e / d) + (origin - o) / d, one FMA. The near and far planes of each axis are picked once by the ray's signs;

@@ -132,6 +132,17 @@ class Scene:
                         "trt_scene_weigh_emitters")
         return float(ms.value)
 
+    def build_light_tree(self, params: np.ndarray) -> tuple[int, float]:
+        """The light tree built again on the device from the emitter records as they are now
+        (trt_scene_build_light_tree); `params` (uint32 (156,), C-contiguous) gets its tree words. Returns (the tree's
+        nodes, device ms); then weigh_emitters(params, nodes) makes the powers, the CDF and the header."""
+        if params.dtype != np.uint32 or not params.flags.c_contiguous:
+            raise ValueError("build_light_tree: params must be a C-contiguous uint32 array")
+        nodes, ms = C.c_uint32(), C.c_float()
+        self.gpu._check(N.lib().trt_scene_build_light_tree(self.handle, params.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                                           C.byref(nodes), C.byref(ms)), "trt_scene_build_light_tree")
+        return int(nodes.value), float(ms.value)
+
     def read(self, which: int, offset: int, nbytes: int, dtype=np.uint8) -> np.ndarray:
         """Bytes [offset, offset + nbytes) of buffer `which` (0 vertices, 1 leaves, 2 nodes, 3 tables, 4 words, 5 the
         environment's RGBA16F texels)."""

@@ -166,13 +166,14 @@ def city_camera(frame: int, frames: int, seed: int, width: int, height: int, ext
 def city(n_objects: int = 4000, width: int = 1280, height: int = 720, max_depth: int = 4, seed: int = 1,
          extent: float = 500.0, n_emitters: int = 200, box_segments: int = 4, sphere_slices: int = 20,
          sphere_stacks: int = 21, frame: int = 0, frames: int = 240, sky_size=(1024, 512),
-         sky: str = "atmosphere") -> SceneDescription:
+         sky: str = "atmosphere", emitter_offset=(0.0, 0.0, 0.0)) -> SceneDescription:
     """Config 1: `n_objects` seeded boxes (faces split 4 x 4: 192 triangles) and UV spheres (20 x 21: 800 triangles),
     half each, on a 1 km grid: 1,984,000 triangles at 4,000, one mesh and one unit each. GGX materials with roughness
     U(0.05, 1), metallic Bernoulli(0.3) and base colour uniform in sRGB. 200 emissive quads (400 triangles, a light
     tree) of log-uniform 10-1000 nits, a 90,000-lux sun at 28 degrees elevation, and the sky: the physical atmosphere
     lit by that sun (sky.rs:643 bake_atmosphere, baked on the device at 1024 x 512; its sun light tinted by the
-    atmosphere's transmittance), or with sky="gradient" a gradient sky (sky.rs:941) that the host prep bakes."""
+    atmosphere's transmittance), or with sky="gradient" a gradient sky (sky.rs:941) that the host prep bakes.
+    emitter_offset moves every emissive quad (the same quads elsewhere: scenes whose emitters moved)."""
     rng = np.random.default_rng(seed)
     meshes, materials, instances = [], [], []
     side = int(math.ceil(math.sqrt(n_objects)))
@@ -211,7 +212,7 @@ def city(n_objects: int = 4000, width: int = 1280, height: int = 720, max_depth:
             a = rng.uniform(0, 2 * math.pi)
             u = np.array([math.cos(a), 0.0, math.sin(a)]) * w_ / 2
             v = np.array([0.0, h_ / 2, 0.0])
-            c = np.array([cx, cy, cz])
+            c = np.array([cx, cy, cz]) + np.asarray(emitter_offset, np.float64)
             t, n = quad([c - u - v, c + u - v, c + u + v, c - u + v])
             tris.append(t)
             nrm.append(n)
