@@ -202,6 +202,10 @@ int trt_unet_train_step(trt_unet* net, const float* features, const float* targe
 /* Denoises a rendered accum in device memory (w * h Pixel records with TRT_RENDER_DEPTH's depth; trt_accum_device_ptr)
  * into w * h RGB floats: features, network and output transform all on the device. */
 int trt_unet_denoise_accum(trt_unet* net, const void* accum_device, uint32_t w, uint32_t h, float* rgb_host, float* ms);
+/* For tests of the error path: the next convolution of the next trt_unet_forward or trt_unet_denoise_accum withholds
+ * one of its copies, so that the pipeline's bounded wait (about a second) runs out. That call returns TRT_ECUDA with
+ * the message of a wait that gave up, and the network stays usable. */
+int trt_unet_hold_next_load(trt_unet* net);
 
 /* ---- Scenes that move: the per-frame deformation, on the device ----
  * The reference poses skinned meshes with two shaders (renderer/shaders/skin.wgsl, leaf_gather.wgsl), refits their

@@ -128,3 +128,22 @@ def test_inference_on_the_device_is_the_host_path(gpu, net):
     assert ms > 0
     assert np.linalg.norm(got - want) / np.linalg.norm(want) < 0.02
     S.close()
+
+
+def test_a_withheld_copy_ends_the_forward_with_an_error_and_the_network_stays_usable():
+    """The convolution's pipeline waits are bounded (about a second): a copy that never lands (one activation box
+    withheld by trt_unet_hold_next_load) ends its wait, the call reports it (TRT_ECUDA, "gave up") instead of hanging,
+    and the next forward on the same network gives the same output as before."""
+    from threert_b200 import RenderError
+    n = unet.UNet(0, max_batch=1, max_h=64, max_w=64)
+    try:
+        n.set_params(unet.init_params(3))
+        f = np.random.default_rng(9).normal(0, 1, (1, 64, 64, unet.N_FEAT)).astype(np.float32)
+        want, _ = n.forward(f)
+        n.hold_next_load()
+        with pytest.raises(RenderError, match="gave up"):
+            n.forward(f)
+        got, _ = n.forward(f)
+        assert np.array_equal(got, want)
+    finally:
+        n.close()

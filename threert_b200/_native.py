@@ -217,6 +217,7 @@ SIGNATURES = [
     ("trt_unet_forward", C.c_int, [C.c_void_p, P(f32), u32, u32, u32, P(f32), P(f32)]),
     ("trt_unet_train_step", C.c_int, [C.c_void_p, P(f32), P(f32), u32, u32, u32, f32, C.c_int, P(f32), P(f32), P(f32)]),
     ("trt_unet_denoise_accum", C.c_int, [C.c_void_p, C.c_void_p, u32, u32, P(f32), P(f32)]),
+    ("trt_unet_hold_next_load", C.c_int, [C.c_void_p]),
     ("trt_math_eval", C.c_int, [C.c_void_p, u32, P(f32), P(f32), u64, P(f32)]),
     ("trt_scene_totals", C.c_int, [C.c_void_p, P(Totals)]),
     ("trt_scene_reset_totals", None, [C.c_void_p]),

@@ -61,6 +61,8 @@ struct Conv {
     int relu;
     uint32_t* err;
     uint32_t resident;        // 1: every tap's weights loaded once a CTA (one 32-channel block, one output tile)
+    uint32_t hold;            // 1: CTA 0 withholds its first activation box (trt_unet_hold_next_load: a test of the
+                              // bounded waits), so that the stage's wait runs out
 };
 
 constexpr uint32_t TS = 5;                  // pipeline stages (82 KB of shared memory: two CTAs an SM)
@@ -270,7 +272,8 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ C
                     mbar_expect_tx(full(s), A_STAGE + (a.resident ? 0u : a.nt * 64u));
                     const uint32_t tap = k / kc, c0 = (k % kc) * 32u;
                     const int dy = (int)(tap / 3u) - 1, dx = (int)(tap % 3u) - 1;
-                    tma_load_4d(sA + s * A_STAGE, &xmap, (int)(a.x_off + c0), x0 + dx, y0 + dy, (int)b, full(s));
+                    if (!(a.hold && blockIdx.x == 0 && it == 0))
+                        tma_load_4d(sA + s * A_STAGE, &xmap, (int)(a.x_off + c0), x0 + dx, y0 + dy, (int)b, full(s));
                     if (!a.resident) tma_load_3d(sB + s * B_STAGE, &wmap, (int)c0, (int)n0, (int)tap, full(s));
                 }
             }
@@ -818,6 +821,7 @@ struct Net {
     std::vector<void*> allocs;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     uint32_t* dev_err = nullptr;  // set by a convolution whose pipeline wait gave up
+    bool hold_next = false;       // the next convolution launched outside a graph withholds one copy (a test)
     uint32_t sms = 148;           // the device's SMs (the persistent convolution's grid)
     float* wpart = nullptr;       // the weight gradient's CTA partials (128 x 128 f32 each)
     uint32_t wpart_ctas = 0;      // their room, in CTAs
@@ -927,7 +931,8 @@ void conv_run(Net* n, const bf16* x, uint32_t x_stride, uint32_t x_off, uint32_t
     // reads one 32-channel block into one output tile
     const uint32_t resident = cin == 32u && co_pad == nt && 9u * nt * 64u <= TS * B_STAGE ? 1u : 0u;
     Conv a{cin, co_pad, nt, bias, y, y_stride, y_off, cout, yf, B, H, W, x_off, bw, bh, tiles_x, tiles_y, relu,
-           n->dev_err, resident};
+           n->dev_err, resident, n->hold_next ? 1u : 0u};
+    n->hold_next = false;
     const uint32_t tiles = B * tiles_x * tiles_y * (co_pad / nt);
     const uint32_t grid = std::min<uint32_t>(tiles, n->sms * CONV_CTAS_PER_SM);
     k_conv<<<grid, CONV_THREADS, CONV_SMEM, n->stream>>>(xmap, wmap, a);
@@ -1307,9 +1312,16 @@ int trt_unet_forward(trt_unet* n, const float* features, uint32_t B, uint32_t H,
     return rc;
 }
 
+int trt_unet_hold_next_load(trt_unet* n) {
+    if (!n) return TRT_EINVAL;
+    n->hold_next = true;
+    return TRT_OK;
+}
+
 int trt_unet_train_step(trt_unet* n, const float* features, const float* targets, uint32_t B, uint32_t H, uint32_t W,
                         float lr, int update, float* loss, float* grads, float* ms) {
     if (!n || !features || !targets) return TRT_EINVAL;
+    n->hold_next = false;  // (the step is captured in a graph: a withheld copy is for direct launches only)
     cudaSetDevice(n->device);
     int rc = check_size(n, B, H, W);
     if (rc) return rc;

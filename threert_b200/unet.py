@@ -122,6 +122,11 @@ class UNet:
                                                 C.byref(ms)), "train_step")
         return loss.value, g, ms.value
 
+    def hold_next_load(self):
+        """trt_unet_hold_next_load: the next forward's first convolution withholds a copy, so that its bounded
+        pipeline wait runs out and the call fails (a test of the error path)."""
+        self._check(N.lib().trt_unet_hold_next_load(self.handle), "hold_next_load")
+
     def denoise(self, scene: Scene) -> tuple[np.ndarray, float]:
         """The scene's last accum (rendered with TRT_RENDER_DEPTH) denoised on the device: (h, w, 3), device ms."""
         ptr, nbytes = C.c_void_p(), C.c_uint64()
