@@ -723,7 +723,9 @@ def run_extras(gpu, S, P, frame: int, args, flags: int) -> dict:
         "capacity_req_per_s": cap, "rate_req_per_s": 0.7 * cap, "p50_ms": at_rate["p50_ms"],
         "p99_ms": at_rate["p99_ms"], "mrays_per_s_at_rate": at_rate["mrays_per_s"],
         "mrays_per_s_saturated": sat["mrays_per_s"], "serial_mrays_per_s": serial["mrays_per_s"],
-        "serial_p50_ms": serial["p50_ms"], "speedup_over_serial": sat["mrays_per_s"] / serial["mrays_per_s"]}
+        "serial_p50_ms": serial["p50_ms"], "speedup_over_serial": sat["mrays_per_s"] / serial["mrays_per_s"],
+        "serial_gpu_busy_frac": serial["gpu_busy_frac"],
+        "speedup_bound": 1.0 / max(serial["gpu_busy_frac"], 1e-9)}
     net.close()
     log(f"extras: {time.perf_counter() - t0:.1f} s")
     return out

@@ -213,20 +213,25 @@ def run_serial(gpu: Gpu, scenes: list[Scene], requests: list[Request], denoiser=
         px = int(r.params[16]) * int(r.params[17])
         if px not in bufs:
             bufs[px] = pinned_buffer(px, keep)
+    busy_ms = 0.0
     t0 = time.perf_counter()
     for r in requests:
         t = time.perf_counter()
         S = scenes[r.scene]
         if r.denoise:
             _, st = S.render_raw(r.params, r.spp, flags=N.TRT_RENDER_DEPTH, read=False)
-            denoiser.denoise(S)
+            _, ms_net = denoiser.denoise(S)
+            busy_ms += ms_net
         else:
             acc, st = S.render_raw(r.params, r.spp, out=bufs[int(r.params[16]) * int(r.params[17])])
+        busy_ms += float(st.device_ms)
         lat.append((time.perf_counter() - t) * 1e3)
         rays += st.closest_rays + st.shadow_rays
     span = time.perf_counter() - t0
+    # The share of the span the device was busy with the requests' kernels: 1 / it bounds what batching can gain.
     return {"requests": len(requests), "span_s": span, "rays": int(rays), "mrays_per_s": rays / span / 1e6,
-            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))}
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "gpu_busy_frac": busy_ms * 1e-3 / span}
 
 
 def autotune(gpu: Gpu, scenes: list[Scene], requests: list[Request], candidates=(1 << 20, 2 << 20, 4 << 20),
