@@ -94,6 +94,10 @@ typedef struct { float t; uint32_t tri; float u; float v; uint32_t inst; uint32_
  * the offline reference leaves zero: the denoisers' depth guide (mean = x / count). */
 #define TRT_RENDER_DEPTH         64u
 #define TRT_RENDER_SORT_SHADOWS  32u
+/* With accum_host: the call returns once the render is queued, and the accum's copy to accum_host (which must be
+ * pinned memory, left untouched until then) runs on the context's copy stream while the next render, into the scene's
+ * other accum, runs; trt_synchronize (or trt_timer_stop) waits for the copies too. Not with TRT_RENDER_ACCUMULATE. */
+#define TRT_RENDER_ASYNC_READBACK 128u
 
 int trt_create(const trt_options* opts, trt_ctx** out);
 /* Frees the context and every scene still uploaded through it (their handles are then invalid). */
@@ -360,7 +364,9 @@ void trt_scene_set_profiling(trt_scene* scene, int on);
 /* Device-time brackets on the context's stream: start records an event, stop records one, synchronises and returns
  * the milliseconds between them. */
 int trt_timer_start(trt_ctx* ctx);
+/* (waits for the asynchronous read-backs queued on the context's copy stream as well) */
 int trt_timer_stop(trt_ctx* ctx, float* ms);
+/* Waits for the context's stream and its copy stream. */
 int trt_synchronize(trt_ctx* ctx);
 
 #ifdef __cplusplus

@@ -92,25 +92,36 @@ def up_back(dy):
     return dy.reshape(B, H // 2, 2, W // 2, 2, C).sum((2, 4))
 
 
-def forward(p, feats):
-    """feats (B, H, W, k <= 32): the prediction (B, H, W, 3) and the activations the backward pass needs."""
+def bf16_round(a):
+    """Values rounded to bfloat16 (to nearest, ties to even), as float64."""
+    u = np.asarray(a, np.float32).view(np.uint32).astype(np.uint64)
+    u = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return u.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def forward(p, feats, act=None):
+    """feats (B, H, W, k <= 32): the prediction (B, H, W, 3) and the activations the backward pass needs. act: None, or
+    a rounding applied where the device stores an activation (each hidden layer's output and each pooling's, as bf16:
+    bf16_round), so that the device's outputs can be held to the accumulation's rounding alone."""
     B, H, W, k = feats.shape
     x = np.zeros((B, H, W, 32))
     x[..., :k] = feats
     A = {"in": x}
     relu = lambda v: np.maximum(v, 0.0)
+    keep = act if act is not None else (lambda v: v)
 
     def L(name, inp):
         W_, b_ = p[name]
         pre = conv(inp, W_, b_)
-        out = relu(pre) if name != "out" else pre
+        out = keep(relu(pre)) if name != "out" else pre
         A[name] = out
         return out
 
+    pl = lambda v: keep(pool(v))
     e0 = L("e0b", L("e0a", x))
-    e1 = L("e1b", L("e1a", pool(e0)))
-    e2 = L("e2b", L("e2a", pool(e1)))
-    e3 = L("e3b", L("e3a", pool(e2)))
+    e1 = L("e1b", L("e1a", pl(e0)))
+    e2 = L("e2b", L("e2a", pl(e1)))
+    e3 = L("e3b", L("e3a", pl(e2)))
     A["cat2"] = np.concatenate([up(e3), e2], -1)
     u2 = L("d2b", L("d2a", A["cat2"]))
     A["cat1"] = np.concatenate([up(u2), e1], -1)

@@ -154,3 +154,28 @@ def test_a_cycle_in_the_tree_trips_the_guard(gpu):
     S = gpu.upload(P)
     with pytest.raises(RenderError, match="TRT_EGUARD"):
         S.render_raw(P.params, 1)
+
+
+def test_asynchronous_readback_gives_each_frame_its_accum(gpu):
+    """TRT_RENDER_ASYNC_READBACK: three renders queued back to back, each copied to its own pinned buffer while the
+    next renders into the scene's other accum; after trt_synchronize each buffer holds its frame's accum, bit for bit
+    the synchronous render's. It does not combine with TRT_RENDER_ACCUMULATE."""
+    import ctypes as C
+    import torch
+    P = prep.prepare(scenes.cornell(48, 48))
+    S = gpu.upload(P)
+    params = [np.ascontiguousarray(prep.params_with(P.params, seed=sd), np.uint32) for sd in (1, 2, 3)]
+    want = [S.render_raw(p, 2)[0].copy() for p in params]
+    bufs = [torch.zeros((48 * 48, N.PIXEL_FLOATS), dtype=torch.float32, pin_memory=True) for _ in params]
+    L = N.lib()
+    for p, b in zip(params, bufs):
+        rc = L.trt_render(S.handle, p.ctypes.data_as(C.POINTER(C.c_uint32)), 0, 2, N.TRT_RENDER_ASYNC_READBACK,
+                          C.cast(b.data_ptr(), C.POINTER(C.c_float)), None)
+        assert rc == 0
+    gpu.synchronize()
+    for w, b in zip(want, bufs):
+        assert np.array_equal(b.numpy(), w)
+    assert np.array_equal(S.render_raw(params[1], 2)[0], want[1])  # a synchronous render after them
+    with pytest.raises(RenderError, match="TRT_EINVAL"):
+        S.render_raw(params[0], 2, flags=N.TRT_RENDER_ASYNC_READBACK | N.TRT_RENDER_ACCUMULATE)
+    S.close()

@@ -50,6 +50,21 @@ def test_forward_matches_the_oracle(net):
     assert ms > 0
 
 
+def test_forward_matches_the_oracle_rounding_as_the_device_does(net):
+    """With the oracle's activations stored as bf16 where the device stores them (each hidden layer's output, each
+    pooling's), what is left between the two is the f32 accumulation against float64: 2e-3 relative over the image,
+    and no output off by more than 2 % of the output's scale."""
+    for seed, (b, h, w) in ((3, (2, 16, 16)), (11, (1, 40, 72))):
+        p, feats, _ = case(seed=seed, b=b, h=h, w=w)
+        net.set_params(p)
+        got, _ = net.forward(feats)
+        want, _ = R.forward(R.unpack(bf16(p).astype(np.float64)), bf16(feats).astype(np.float64), act=R.bf16_round)
+        err = np.linalg.norm(got - want) / np.linalg.norm(want)
+        worst = np.abs(got - want).max() / np.abs(want).max()
+        print(f"forward {b}x{h}x{w}: relative error {err:.2e}, worst output {worst:.2e}")
+        assert err < 2e-3 and worst < 0.02, (err, worst)
+
+
 def test_forward_on_ragged_tiles_matches_the_oracle(net):
     # 72 x 40: tiles of 8 x 16 pixels at the top level (the last row of tiles half outside the image), 4 x 32,
     # 2 x 64, then 1 x 128 over a 9 x 5 level

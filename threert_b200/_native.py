@@ -23,6 +23,7 @@ TRT_RENDER_SORT_RAYS = 8
 TRT_RENDER_UNSORTED_HITS = 16
 TRT_RENDER_SORT_SHADOWS = 32
 TRT_RENDER_DEPTH = 64
+TRT_RENDER_ASYNC_READBACK = 128
 
 TRT_OK, TRT_EINVAL, TRT_ECUDA, TRT_EGUARD = 0, 1, 2, 3
 TRT_MATH_COS, TRT_MATH_SIN, TRT_MATH_ACOS, TRT_MATH_ATAN2 = 0, 1, 2, 3

@@ -797,6 +797,8 @@ struct trt_ctx {
     std::string err;
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     SkyState* sky = nullptr;  // the sky bake's tables and texels (trt_sky_bake, trt_scene_set_sky)
+    cudaStream_t copy_stream = nullptr;  // asynchronous read-backs (TRT_RENDER_ASYNC_READBACK)
+    cudaEvent_t copy_mark = nullptr;     // the copy stream's point the timer and synchronisation wait for
 };
 
 namespace trt {
@@ -821,6 +823,11 @@ struct trt_scene {
     WideBvh wide;
     float4* accum = nullptr;
     uint32_t accum_w = 0, accum_h = 0;
+    // Asynchronous read-backs: a second accum, so that a render writes one while the other's copy to the host runs
+    // on the context's copy stream; each buffer's event marks its last copy done (accum's and accum_alt's, swapped
+    // with them). accum is always the last rendered.
+    float4* accum_alt = nullptr;
+    cudaEvent_t copied = nullptr, copied_alt = nullptr;
     Wave wave;  // the render's wave state
     void* dn = nullptr;  // the denoiser's buffers, for dn_w x dn_h pixels
     uint32_t dn_w = 0, dn_h = 0;
@@ -1170,10 +1177,13 @@ int trt_create(const trt_options* opts, trt_ctx** out) {
     }
     if (e == cudaSuccess) e = cudaEventCreate(&c->t0);
     if (e == cudaSuccess) e = cudaEventCreate(&c->t1);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->copy_mark, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         // (No context to hold the message: the caller gets the code.)
         std::fprintf(stderr, "trt_create: %s\n", cudaGetErrorString(e));
         if (c->stream) cudaStreamDestroy(c->stream);
+        if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
         delete c;
         return TRT_ECUDA;
     }
@@ -1188,6 +1198,8 @@ void trt_destroy(trt_ctx* c) {
     sky_free(c->sky);
     if (c->t0) cudaEventDestroy(c->t0);
     if (c->t1) cudaEventDestroy(c->t1);
+    if (c->copy_mark) cudaEventDestroy(c->copy_mark);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -1244,10 +1256,14 @@ void trt_scene_free(trt_scene* s) {
     live.erase(std::remove(live.begin(), live.end(), s), live.end());
     cudaSetDevice(s->ctx->device);
     cudaStreamSynchronize(s->ctx->stream);
+    cudaStreamSynchronize(s->ctx->copy_stream);
     for (void* b : s->buf)
         if (b) cudaFree(b);
     if (s->env) cudaFree(s->env);
     if (s->accum) cudaFree(s->accum);
+    if (s->accum_alt) cudaFree(s->accum_alt);
+    if (s->copied) cudaEventDestroy(s->copied);
+    if (s->copied_alt) cudaEventDestroy(s->copied_alt);
     if (s->wave.work) cudaFree(s->wave.work);
     if (s->dn) cudaFree(s->dn);
     if (s->totals) cudaFree(s->totals);
@@ -1427,14 +1443,30 @@ int trt_render(trt_scene* s, const uint32_t params[TRT_PARAMS_WORDS], uint32_t f
     Params P;
     std::memcpy(P.w, params, sizeof(P.w));
     uint32_t w = P.w[P_SIZE], h = P.w[P_SIZE + 1];
+    const bool async_back = (flags & TRT_RENDER_ASYNC_READBACK) != 0 && accum_host != nullptr;
+    if (async_back && (flags & TRT_RENDER_ACCUMULATE))
+        return fail(c, TRT_EINVAL, "TRT_RENDER_ASYNC_READBACK renders into a second accum: it cannot accumulate");
     if (!s->accum || s->accum_w != w || s->accum_h != h) {
+        // (a size change waits for the read-backs in flight from the old buffers)
+        TRT_CUDA(c, cudaStreamSynchronize(c->copy_stream));
         if (s->accum) cudaFree(s->accum);
-        s->accum = nullptr;
+        if (s->accum_alt) cudaFree(s->accum_alt);
+        s->accum = s->accum_alt = nullptr;
         TRT_CUDA(c, cudaMalloc(&s->accum, 80ull * w * h));
         s->accum_w = w;
         s->accum_h = h;
         flags &= ~TRT_RENDER_ACCUMULATE;
     }
+    if (async_back) {
+        // Render into the other buffer, once its own last read-back is done; it becomes the accum.
+        if (!s->accum_alt) TRT_CUDA(c, cudaMalloc(&s->accum_alt, 80ull * w * h));
+        if (!s->copied) TRT_CUDA(c, cudaEventCreateWithFlags(&s->copied, cudaEventDisableTiming));
+        if (!s->copied_alt) TRT_CUDA(c, cudaEventCreateWithFlags(&s->copied_alt, cudaEventDisableTiming));
+        std::swap(s->accum, s->accum_alt);
+        std::swap(s->copied, s->copied_alt);
+    }
+    // The accum may still be read back to the host by an earlier asynchronous render: wait for it on the device.
+    if (s->copied) TRT_CUDA(c, cudaStreamWaitEvent(c->stream, s->copied, 0));
     if (!(flags & TRT_RENDER_ACCUMULATE)) TRT_CUDA(c, cudaMemsetAsync(s->accum, 0, 80ull * w * h, c->stream));
     unsigned long long before[T_COUNT] = {0};
     if (stats) {
@@ -1451,8 +1483,15 @@ int trt_render(trt_scene* s, const uint32_t params[TRT_PARAMS_WORDS], uint32_t f
         if (rc) return rc;
     }
     s->renders++;
-    if (accum_host)
+    if (async_back) {
+        // The read-back on the copy stream, after the render; the next render writes the other buffer meanwhile.
+        TRT_CUDA(c, cudaEventRecord(c->copy_mark, c->stream));
+        TRT_CUDA(c, cudaStreamWaitEvent(c->copy_stream, c->copy_mark, 0));
+        TRT_CUDA(c, cudaMemcpyAsync(accum_host, s->accum, 80ull * w * h, cudaMemcpyDeviceToHost, c->copy_stream));
+        TRT_CUDA(c, cudaEventRecord(s->copied, c->copy_stream));
+    } else if (accum_host) {
         TRT_CUDA(c, cudaMemcpyAsync(accum_host, s->accum, 80ull * w * h, cudaMemcpyDeviceToHost, c->stream));
+    }
     if (stats) {
         unsigned long long after[T_COUNT];
         TRT_CUDA(c, cudaEventRecord(c->t1, c->stream));
@@ -1467,7 +1506,7 @@ int trt_render(trt_scene* s, const uint32_t params[TRT_PARAMS_WORDS], uint32_t f
         stats->device_ms = ms;
         stats->launches = (uint32_t)(s->launches - launches0);
         if (stats->guard_trips) return fail(c, TRT_EGUARD, "a traversal stopped at its iteration limit");
-    } else if (accum_host) {
+    } else if (accum_host && !async_back) {
         TRT_CUDA(c, cudaStreamSynchronize(c->stream));
     }
     return TRT_OK;
@@ -1631,6 +1670,9 @@ int trt_timer_start(trt_ctx* c) {
 
 int trt_timer_stop(trt_ctx* c, float* ms) {
     if (!c || !ms) return TRT_EINVAL;
+    // (after the read-backs still running on the copy stream, too)
+    TRT_CUDA(c, cudaEventRecord(c->copy_mark, c->copy_stream));
+    TRT_CUDA(c, cudaStreamWaitEvent(c->stream, c->copy_mark, 0));
     TRT_CUDA(c, cudaEventRecord(c->t1, c->stream));
     TRT_CUDA(c, cudaEventSynchronize(c->t1));
     TRT_CUDA(c, cudaEventElapsedTime(ms, c->t0, c->t1));
@@ -1640,6 +1682,7 @@ int trt_timer_stop(trt_ctx* c, float* ms) {
 int trt_synchronize(trt_ctx* c) {
     if (!c) return TRT_EINVAL;
     TRT_CUDA(c, cudaStreamSynchronize(c->stream));
+    TRT_CUDA(c, cudaStreamSynchronize(c->copy_stream));
     return TRT_OK;
 }
 
