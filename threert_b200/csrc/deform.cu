@@ -100,36 +100,26 @@ __device__ __forceinline__ void store_box(uint4* nodes, uint32_t i, V3 lo, V3 hi
 }
 
 // A distinct tree shape: its leaves in triangle order, then its interior nodes a level at a time, deepest first
-// (level_start[levels_first .. levels_first + n_levels] are offsets into its interior nodes); its leaves in chunks of
-// consecutive leaves (chunks[chunks_first .. chunks_first + n_chunks]).
-struct Shape { uint32_t leaves_first, n_leaves, interior_first, levels_first, n_levels, chunks_first, n_chunks; };
-// A run of consecutive leaves of a shape and the triangles they hold (which follow one another: the leaves in
-// triangle order cover each of the mesh's triangles once), at most CHUNK_LEAVES leaves and CHUNK_TRIS triangles.
-struct Chunk { uint32_t leaf_first, n_leaves, tri_first, n_tris; };
-constexpr uint32_t CHUNK_LEAVES = 64u, CHUNK_TRIS = 1024u;
+// (level_start[levels_first .. levels_first + n_levels] are offsets into its interior nodes).
+struct Shape { uint32_t leaves_first, n_leaves, interior_first, levels_first, n_levels; };
 
-// The leaves of every deforming mesh at once, a CTA a chunk of consecutive leaves (blockIdx.x the chunk, blockIdx.y
-// the mesh). First a thread a triangle, in triangle order (coalesced): its corners gathered again from the vertices
-// (leaf_gather.wgsl:41-51: (v0, keep w), (e1, keep w), (e2, 0)) and the box of its finite corners, into shared memory;
-// then a thread a leaf folds its triangles' boxes in triangle order. min and max keep the last of equal operands, as a
-// fold over every corner in order does, so a leaf's box is the per-corner fold's to the bit.
-__global__ void __launch_bounds__(256) k_refit_leaves(const DMesh* __restrict__ meshes, const uint32_t* __restrict__ shape_of,
-                                                      uint32_t n_meshes, const Shape* __restrict__ shapes,
-                                                      const Chunk* __restrict__ chunks,
-                                                      const uint32_t* __restrict__ level_nodes,
-                                                      const float4* __restrict__ vertices,
-                                                      const uint32_t* __restrict__ words, uint32_t w_indices,
-                                                      float4* leaves, uint4* nodes, uint32_t* err) {
-    __shared__ float tb[6][CHUNK_TRIS];
+// The leaves of every deforming mesh at once (one thread a leaf, blockIdx.y a mesh), neighbours in triangle order on
+// neighbouring threads, whose corners they share.
+__global__ void k_refit_leaves(const DMesh* __restrict__ meshes, const uint32_t* __restrict__ shape_of,
+                               uint32_t n_meshes, const Shape* __restrict__ shapes,
+                               const uint32_t* __restrict__ level_nodes, const float4* __restrict__ vertices,
+                               const uint32_t* __restrict__ words, uint32_t w_indices, float4* leaves, uint4* nodes,
+                               uint32_t* err) {
     for (uint32_t m = blockIdx.y; m < n_meshes; m += gridDim.y) {
-        const DMesh M = meshes[m];
-        const Shape sh = shapes[shape_of[m]];
-        for (uint32_t ci = blockIdx.x; ci < sh.n_chunks; ci += gridDim.x) {
-            const Chunk ch = chunks[sh.chunks_first + ci];
-            for (uint32_t k = threadIdx.x; k < ch.n_tris; k += blockDim.x) {
-                const uint32_t t = M.first_tri + ch.tri_first + k;
+        DMesh M = meshes[m];
+        Shape sh = shapes[shape_of[m]];
+        for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < sh.n_leaves; j += gridDim.x * blockDim.x) {
+            uint32_t i = M.root + level_nodes[sh.leaves_first + j];
+            uint4 na = nodes[2ull * i], nb = nodes[2ull * i + 1];
+            V3 lo = v3(__uint_as_float(0x7f800000u)), hi = v3(__uint_as_float(0xff800000u));
+            for (uint32_t k = na.w; k < na.w + nb.w; ++k) {
+                uint32_t t = M.first_tri + k;
                 V3 p[3];
-                V3 lo = v3(__uint_as_float(0x7f800000u)), hi = v3(__uint_as_float(0xff800000u));
                 for (uint32_t c = 0; c < 3; ++c) {
                     p[c] = corner(vertices, words, w_indices, M, t, c, err);
                     if (finite1(p[c].x) && finite1(p[c].y) && finite1(p[c].z)) {
@@ -137,28 +127,13 @@ __global__ void __launch_bounds__(256) k_refit_leaves(const DMesh* __restrict__ 
                         hi = V3{gmax(hi.x, p[c].x), gmax(hi.y, p[c].y), gmax(hi.z, p[c].z)};
                     }
                 }
-                const uint64_t q = 3ull * t;
-                const float w0 = leaves[q].w, w1 = leaves[q + 1].w;
-                leaves[q] = f4(p[0], w0);
-                leaves[q + 1] = f4(p[1] - p[0], w1);
+                uint64_t q = 3ull * t;
+                leaves[q] = f4(p[0], leaves[q].w);
+                leaves[q + 1] = f4(p[1] - p[0], leaves[q + 1].w);
                 leaves[q + 2] = f4(p[2] - p[0], 0.0f);
-                tb[0][k] = lo.x; tb[1][k] = lo.y; tb[2][k] = lo.z;
-                tb[3][k] = hi.x; tb[4][k] = hi.y; tb[5][k] = hi.z;
             }
-            __syncthreads();
-            for (uint32_t j = threadIdx.x; j < ch.n_leaves; j += blockDim.x) {
-                const uint32_t i = M.root + level_nodes[sh.leaves_first + ch.leaf_first + j];
-                const uint4 na = nodes[2ull * i], nb = nodes[2ull * i + 1];
-                V3 lo = v3(__uint_as_float(0x7f800000u)), hi = v3(__uint_as_float(0xff800000u));
-                // (the setup put each leaf's triangles inside its chunk's)
-                for (uint32_t k = na.w - ch.tri_first; k < na.w - ch.tri_first + nb.w; ++k) {
-                    lo = V3{gmin(lo.x, tb[0][k]), gmin(lo.y, tb[1][k]), gmin(lo.z, tb[2][k])};
-                    hi = V3{gmax(hi.x, tb[3][k]), gmax(hi.y, tb[4][k]), gmax(hi.z, tb[5][k])};
-                }
-                if (lo.x > hi.x) { lo = v3(0.0f); hi = v3(0.0f); }  // a leaf of nothing finite: a point
-                store_box(nodes, i, lo, hi, na.w, nb.w);
-            }
-            __syncthreads();
+            if (lo.x > hi.x) { lo = v3(0.0f); hi = v3(0.0f); }  // a leaf of nothing finite: a point
+            store_box(nodes, i, lo, hi, na.w, nb.w);
         }
     }
 }
@@ -665,8 +640,6 @@ struct DeformState {
     Shape* shapes = nullptr;
     uint32_t* level_start = nullptr;
     uint32_t* level_nodes = nullptr;
-    Chunk* chunks = nullptr;
-    uint32_t max_chunks = 0;
     uint32_t* err = nullptr;
     float4* palette = nullptr;
     uint32_t palette_cap = 0;
@@ -730,8 +703,7 @@ dim3 mesh_grid(uint32_t per_mesh, uint32_t n_meshes) {
 void deform_free(DeformState* st) {
     if (!st) return;
     for (void* p : {(void*)st->meshes, (void*)st->corners, (void*)st->shape_of, (void*)st->shapes,
-                    (void*)st->level_start, (void*)st->level_nodes, (void*)st->chunks, (void*)st->err,
-                    (void*)st->palette, st->top})
+                    (void*)st->level_start, (void*)st->level_nodes, (void*)st->err, (void*)st->palette, st->top})
         if (p) cudaFree(p);
     for (auto& e : st->ev)
         if (e) cudaEventDestroy(e);
@@ -751,7 +723,6 @@ int deform_setup(DeformState** out, const SceneBuffers& sb, const trt_deform_des
     // Distinct tree shapes (the links and counts of a tree's nodes), each with its nodes by level, deepest first.
     std::unordered_map<std::string, uint32_t> shape_ids;
     std::vector<Shape> shapes;
-    std::vector<Chunk> chunks;
     std::vector<uint32_t> shape_of(d->n_meshes), level_start, level_nodes;
     for (uint32_t m = 0; m < d->n_meshes; ++m) {
         const DMesh& M = st->host_meshes[m];
@@ -798,33 +769,16 @@ int deform_setup(DeformState** out, const SceneBuffers& sb, const trt_deform_des
             if (deepest >= 64) return fail(at + "a tree deeper than 64 levels");
             // The shape: its leaves by first triangle, then its interior nodes by level, deepest first
             // (n_levels + 1 offsets into them from level_start[levels_first]).
-            Shape sh{(uint32_t)level_nodes.size(), 0, 0, (uint32_t)level_start.size(), deepest + 1,
-                     (uint32_t)chunks.size(), 0};
+            Shape sh{(uint32_t)level_nodes.size(), 0, 0, (uint32_t)level_start.size(), deepest + 1};
             std::vector<std::pair<uint32_t, uint32_t>> by_tri;
-            std::vector<uint32_t> count_of(M.n_nodes, 0);
             for (uint32_t k = 0; k < M.n_nodes; ++k) {
                 uint32_t w[8];
                 host_node(hn, M.root + k, w);
                 if (w[7] > 0) by_tri.push_back({w[3], k});
-                count_of[k] = w[7];
             }
             std::sort(by_tri.begin(), by_tri.end());
             for (auto& pr : by_tri) level_nodes.push_back(pr.second);
             sh.n_leaves = (uint32_t)by_tri.size();
-            // The leaves in chunks for the leaf refit: consecutive leaves (whose triangles follow one another) up to
-            // CHUNK_LEAVES leaves and CHUNK_TRIS triangles.
-            for (uint32_t j = 0; j < sh.n_leaves;) {
-                Chunk c{j, 0, by_tri[j].first, 0};
-                while (j < sh.n_leaves && c.n_leaves < CHUNK_LEAVES &&
-                       c.n_tris + count_of[by_tri[j].second] <= CHUNK_TRIS) {
-                    c.n_tris += count_of[by_tri[j].second];
-                    c.n_leaves++;
-                    j++;
-                }
-                if (c.n_leaves == 0) return fail(at + "a leaf of more than 1,024 triangles");
-                chunks.push_back(c);
-                sh.n_chunks++;
-            }
             sh.interior_first = (uint32_t)level_nodes.size();
             level_start.push_back(0);
             for (uint32_t l = deepest + 1; l-- > 0;) {
@@ -850,7 +804,6 @@ int deform_setup(DeformState** out, const SceneBuffers& sb, const trt_deform_des
         st->max_tris = std::max(st->max_tris, M.n_tris);
         st->max_nodes = std::max(st->max_nodes, M.n_nodes);
         st->max_leaves = std::max(st->max_leaves, shapes[shape_of[m]].n_leaves);
-        st->max_chunks = std::max(st->max_chunks, shapes[shape_of[m]].n_chunks);
     }
     cudaError_t e = cudaSuccess;
     auto upload = [&](auto** dst, const void* src, uint64_t bytes) {
@@ -863,7 +816,6 @@ int deform_setup(DeformState** out, const SceneBuffers& sb, const trt_deform_des
     upload(&st->shapes, shapes.data(), sizeof(Shape) * shapes.size());
     upload(&st->level_start, level_start.data(), 4ull * level_start.size());
     upload(&st->level_nodes, level_nodes.data(), 4ull * level_nodes.size());
-    upload(&st->chunks, chunks.data(), sizeof(Chunk) * chunks.size());
     if (e == cudaSuccess) e = cudaMalloc(&st->err, 4);
     if (e == cudaSuccess) e = cudaMemsetAsync(st->err, 0, 4, sb.stream);
     for (auto& ev : st->ev)
@@ -923,9 +875,9 @@ int deform_run(DeformState* st, const SceneBuffers& sb, const uint32_t* P, const
         // A CTA a mesh; few meshes get wide CTAs so that a single tree's levels still fill many warps.
         uint32_t threads = n_meshes < 296u ? 1024u : 256u;
         uint32_t blocks = std::min(n_meshes, 148u * (2048u / threads) * 4u);
-        dim3 g(std::max(1u, std::min(st->max_chunks, 1024u)), std::max(1u, std::min(n_meshes, 65535u)));
-        k_refit_leaves<<<g, 256, 0, s>>>(st->meshes, st->shape_of, n_meshes, st->shapes, st->chunks, st->level_nodes,
-                                         vertices, words, w_indices, leaves, nodes, st->err);
+        k_refit_leaves<<<mesh_grid(st->max_leaves, n_meshes), 256, 0, s>>>(st->meshes, st->shape_of, n_meshes, st->shapes,
+                                                                            st->level_nodes, vertices, words, w_indices,
+                                                                            leaves, nodes, st->err);
         k_refit<<<blocks, threads, 0, s>>>(st->meshes, st->shape_of, n_meshes, st->shapes, st->level_start,
                                            st->level_nodes, nodes);
     }

@@ -69,35 +69,12 @@ __device__ __forceinline__ V3 safe_inv(V3 d) {
 
 struct WalkCount { uint32_t nodes, tris, units; };
 
-// The binary walks' stack: 64 entries a ray, the first WALK_SHORT in shared memory (a column a thread, so that a
-// warp's lanes at the same depth hit distinct banks), the rest in local memory. A kernel that walks runs blocks of at
-// most WALK_BLOCK threads.
-#ifndef TRT_WALK_SHORT
-#define TRT_WALK_SHORT 16
-#endif
-constexpr uint32_t WALK_SHORT = TRT_WALK_SHORT, WALK_STACK = 64u, WALK_BLOCK = 128u;
-struct WalkStack {
-    uint32_t* sh;                              // this thread's column of the block's shared stack
-    uint32_t spill[WALK_STACK - WALK_SHORT];
-    __device__ __forceinline__ void put(uint32_t at, uint32_t v) {
-        if (WALK_SHORT > 0 && at < WALK_SHORT) sh[at * WALK_BLOCK] = v;
-        else spill[at - WALK_SHORT] = v;
-    }
-    __device__ __forceinline__ uint32_t get(uint32_t at) const {
-        return (WALK_SHORT > 0 && at < WALK_SHORT) ? sh[at * WALK_BLOCK] : spill[at - WALK_SHORT];
-    }
-};
-__device__ __forceinline__ uint32_t* walk_smem() {
-    __shared__ uint32_t short_stack[(WALK_SHORT > 0 ? WALK_SHORT : 1) * WALK_BLOCK];
-    return short_stack + threadIdx.x;
-}
-
 // The loop guard (renderer/src/gpu.rs:1214-1285 guard_loops): a walk that has not ended after this many nodes stops,
 // sets *guard and returns what it has; the render then reports an error instead of hanging on trees that are not
 // trees.
 constexpr uint32_t WALK_GUARD = 1u << 20;
 
-// trace_units.wgsl:44-135, with a 64-entry stack of its own (WalkStack). Returns the hit (tri MISS for none).
+// trace_units.wgsl:44-135, with a 64-entry stack of its own. Returns the hit (tri MISS for none).
 template <bool COUNT>
 __device__ Hit trace_binary(const DScene& S, const Sections& X, uint32_t top, uint32_t n_units, V3 o, V3 d, float tmax,
                             uint32_t mode, WalkCount* wc, bool* guard) {
@@ -108,9 +85,7 @@ __device__ Hit trace_binary(const DScene& S, const Sections& X, uint32_t top, ui
     Node whole = node_at(S, top);
     if (COUNT) wc->nodes++;
     if (ray_aabb(o, inv_d, whole.bmin, whole.bmax, hit.t) == INF) return hit;
-    if (blockDim.x > WALK_BLOCK) { *guard = true; return hit; }
-    WalkStack stack;
-    stack.sh = walk_smem();
+    uint32_t stack[64];
     uint32_t sp = 0, node = top, rec = NO_INST;
     V3 ro = o, rd = d, rinv = inv_d;
     uint32_t off = top, first = 0, base = 0;
@@ -130,7 +105,7 @@ __device__ Hit trace_binary(const DScene& S, const Sections& X, uint32_t top, ui
                 uint32_t nearn = l, farn = r;
                 if (tr < tl) { nearn = r; farn = l; float tmp = tl; tl = tr; tr = tmp; }
                 node = nearn;
-                if (tr != INF && sp < WALK_STACK) stack.put(sp++, farn);
+                if (tr != INF && sp < 64) stack[sp++] = farn;
                 continue;
             }
         } else if (rec == NO_INST) {
@@ -175,7 +150,7 @@ __device__ Hit trace_binary(const DScene& S, const Sections& X, uint32_t top, ui
         }
         if (sp == 0) break;
         sp--;
-        node = stack.get(sp);
+        node = stack[sp];
     }
     return hit;
 }
@@ -195,9 +170,7 @@ __device__ Hit trace_binary_split(const DScene& S, const Sections& X, uint32_t t
     Node whole = node_at(S, top);
     if (COUNT) wc->nodes++;
     if (ray_aabb(o, inv_d, whole.bmin, whole.bmax, hit.t) == INF) return hit;
-    if (blockDim.x > WALK_BLOCK) { *guard = true; return hit; }
-    WalkStack stack;
-    stack.sh = walk_smem();
+    uint32_t stack[64];
     uint32_t sp = 0, node = top, rec = NO_INST;
     V3 ro = o, rd = d, rinv = inv_d;
     uint32_t off = top, first = 0, base = 0;
@@ -208,7 +181,7 @@ __device__ Hit trace_binary_split(const DScene& S, const Sections& X, uint32_t t
     (((rec != NO_INST && sp == base)          \
           ? (rec = NO_INST, ro = o, rd = d, rinv = inv_d, off = top, 0) \
           : 0),                               \
-     sp == 0 ? false : (node = stack.get(--sp), true))
+     sp == 0 ? false : (node = stack[--sp], true))
     for (;;) {
         // Interior nodes first, until a leaf (a unit's record or a mesh's triangles); the nodes, tests and pops are
         // the single loop's, in the same order.
@@ -229,7 +202,7 @@ __device__ Hit trace_binary_split(const DScene& S, const Sections& X, uint32_t t
                 uint32_t nearn = l, farn = r;
                 if (tr < tl) { nearn = r; farn = l; float tmp = tl; tl = tr; tr = tmp; }
                 node = nearn;
-                if (tr != INF && sp < WALK_STACK) stack.put(sp++, farn);
+                if (tr != INF && sp < 64) stack[sp++] = farn;
                 continue;
             }
             if (!TRT_WALK_POP()) return hit;
