@@ -799,6 +799,9 @@ struct trt_ctx {
     SkyState* sky = nullptr;  // the sky bake's tables and texels (trt_sky_bake, trt_scene_set_sky)
     cudaStream_t copy_stream = nullptr;  // asynchronous read-backs (TRT_RENDER_ASYNC_READBACK)
     cudaEvent_t copy_mark = nullptr;     // the copy stream's point the timer and synchronisation wait for
+    // A render's second stream: each depth's shadow walk runs on it beside the next depth's closest-hit walk.
+    cudaStream_t aux_stream = nullptr;
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
 };
 
 namespace trt {
@@ -1024,11 +1027,17 @@ int render_waves(trt_scene* s, const Params& P, uint32_t first_sample, uint32_t 
     int g_ext = grid_for((const void*)k_extend<COUNT, WIDE, false>, blk, c->sm_count);
     int g_sha = grid_for((const void*)k_shadow<COUNT, WIDE, false>, blk, c->sm_count);
     std::vector<uint32_t> host_cnt(MAX_DEPTH * CNT_STRIDE + CNT_STRIDE, 0);
-    auto mark = [&](std::vector<std::pair<cudaEvent_t, cudaEvent_t>>& v, bool begin) {
+    auto mark = [&](std::vector<std::pair<cudaEvent_t, cudaEvent_t>>& v, bool begin, cudaStream_t on = nullptr) {
         if (!s->profiling) return;
-        if (begin) { v.push_back(take_events(s)); cudaEventRecord(v.back().first, st); }
-        else cudaEventRecord(v.back().second, st);
+        if (!on) on = st;
+        if (begin) { v.push_back(take_events(s)); cudaEventRecord(v.back().first, on); }
+        else cudaEventRecord(v.back().second, on);
     };
+    // Each depth's shadow walk on the second stream beside the next depth's closest-hit walk: both read what the
+    // depth's shading wrote and write apart (visibility bits; hit records), so their tails overlap. (Not with the ray
+    // sort, whose output buffer is the previous depth's shading order, which that depth's resolve still reads.)
+    const bool overlap = !sort_rays;
+    cudaStream_t aux = c->aux_stream;
     for (uint32_t s0 = 0; s0 < spp; s0 += K) {
         uint32_t k = std::min(K, spp - s0);
         TRT_CUDA(c, cudaMemcpyAsync(s->wave.Q.cnt, host_cnt.data(), host_cnt.size() * 4, cudaMemcpyHostToDevice, st));
@@ -1048,9 +1057,11 @@ int render_waves(trt_scene* s, const Params& P, uint32_t first_sample, uint32_t 
                 mark(s->ev_sort, false);
                 ext_q = s->wave.Q.qx;
             }
-            mark(s->ev_extend, true);
-            k_extend<COUNT, WIDE, false><<<g_ext, blk, 0, st>>>(s->wave.jobs, job, s->wave.B, s->wave.Q, depth, ext_q);
-            mark(s->ev_extend, false);
+            if (!overlap || depth == 0u) {  // (past depth 0 with the overlap, launched beside the last shadow walk)
+                mark(s->ev_extend, true);
+                k_extend<COUNT, WIDE, false><<<g_ext, blk, 0, st>>>(s->wave.jobs, job, s->wave.B, s->wave.Q, depth, ext_q);
+                mark(s->ev_extend, false);
+            }
             uint32_t* shade_q = ext_q;
             if (sort_hits) {
                 shade_q = ext_q == raw ? s->wave.Q.qx : raw;
@@ -1068,9 +1079,25 @@ int render_waves(trt_scene* s, const Params& P, uint32_t first_sample, uint32_t 
                 mark(s->ev_sort, false);
                 perm = s->wave.Q.perm;
             }
-            mark(s->ev_shadow, true);
-            k_shadow<COUNT, WIDE, false><<<g_sha, blk, 0, st>>>(s->wave.jobs, job, s->wave.B, s->wave.Q, depth, perm);
-            mark(s->ev_shadow, false);
+            if (overlap) {
+                TRT_CUDA(c, cudaEventRecord(c->fork_ev, st));
+                TRT_CUDA(c, cudaStreamWaitEvent(aux, c->fork_ev, 0));
+                mark(s->ev_shadow, true, aux);
+                k_shadow<COUNT, WIDE, false><<<g_sha, blk, 0, aux>>>(s->wave.jobs, job, s->wave.B, s->wave.Q, depth, perm);
+                mark(s->ev_shadow, false, aux);
+                if (depth < last) {
+                    mark(s->ev_extend, true);
+                    k_extend<COUNT, WIDE, false><<<g_ext, blk, 0, st>>>(s->wave.jobs, job, s->wave.B, s->wave.Q,
+                                                                        depth + 1u, next);
+                    mark(s->ev_extend, false);
+                }
+                TRT_CUDA(c, cudaEventRecord(c->join_ev, aux));
+                TRT_CUDA(c, cudaStreamWaitEvent(st, c->join_ev, 0));
+            } else {
+                mark(s->ev_shadow, true);
+                k_shadow<COUNT, WIDE, false><<<g_sha, blk, 0, st>>>(s->wave.jobs, job, s->wave.B, s->wave.Q, depth, perm);
+                mark(s->ev_shadow, false);
+            }
             k_resolve<false><<<(n + blk - 1) / blk, blk, 0, st>>>(s->wave.jobs, job, s->wave.B, s->wave.Q, depth, shade_q);
             s->launches += 4;
             s->extend_launches++;
@@ -1179,11 +1206,15 @@ int trt_create(const trt_options* opts, trt_ctx** out) {
     if (e == cudaSuccess) e = cudaEventCreate(&c->t1);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->copy_mark, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->aux_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->join_ev, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         // (No context to hold the message: the caller gets the code.)
         std::fprintf(stderr, "trt_create: %s\n", cudaGetErrorString(e));
         if (c->stream) cudaStreamDestroy(c->stream);
         if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+        if (c->aux_stream) cudaStreamDestroy(c->aux_stream);
         delete c;
         return TRT_ECUDA;
     }
@@ -1200,6 +1231,9 @@ void trt_destroy(trt_ctx* c) {
     if (c->t1) cudaEventDestroy(c->t1);
     if (c->copy_mark) cudaEventDestroy(c->copy_mark);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+    if (c->fork_ev) cudaEventDestroy(c->fork_ev);
+    if (c->join_ev) cudaEventDestroy(c->join_ev);
+    if (c->aux_stream) cudaStreamDestroy(c->aux_stream);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
