@@ -162,6 +162,7 @@ struct Job {
     uint32_t slot_first, n_idx, K, first_sample;
     uint32_t idx_first;  // the earlier jobs' n_idx summed: its pixels' place in a pass over every job's pixels
     uint32_t depth;      // 1: accumulate the first hit's distance into the Pixel's fourth vec4 (TRT_RENDER_DEPTH)
+    uint32_t pix_first;  // the first of the image's pixel indices (8 x 4 tiles) the job's n_idx slots a sample take
 };
 // What a wave of a server step holds, in device memory ahead of its job table, so that the step's launches (and a
 // graph captured from them) do not change from step to step.
@@ -205,7 +206,8 @@ __global__ void k_raygen(const Job* __restrict__ jobs, uint32_t n_jobs, PathBufs
         while (j + 1 < n_jobs && p >= jobs[j + 1].slot_first) ++j;  // jobs lie in slot order
         const Job& J = jobs[j];
         uint32_t local = p - J.slot_first;
-        if (local < J.n_idx * J.K) valid = slot_pixel(local % J.n_idx, J.P.w[P_SIZE], J.P.w[P_SIZE + 1], gx, gy);
+        if (local < J.n_idx * J.K)
+            valid = slot_pixel(local % J.n_idx + J.pix_first, J.P.w[P_SIZE], J.P.w[P_SIZE + 1], gx, gy);
     }
     uint32_t at = warp_append(&Q.cnt[0], valid);
     if (!valid) return;
@@ -671,7 +673,7 @@ __device__ __forceinline__ void accumulate_one(const Job& J, const PathBufs& B, 
     float4* accum = J.accum;
     uint32_t w = J.P.w[P_SIZE], h = J.P.w[P_SIZE + 1];
     uint32_t gx, gy;
-    if (idx >= n_idx || !slot_pixel(idx, w, h, gx, gy)) return;
+    if (idx >= n_idx || !slot_pixel(idx + J.pix_first, w, h, gx, gy)) return;
     uint32_t pix = gy * w + gx;
     float4 c = accum[pix * 5], a = accum[pix * 5 + 1], nn = accum[pix * 5 + 2];
     float dsum = 0.0f;
@@ -802,6 +804,10 @@ struct trt_ctx {
     // A render's second stream: each depth's shadow walk runs on it beside the next depth's closest-hit walk.
     cudaStream_t aux_stream = nullptr;
     cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+    // A render's second half-wave: its own stream pair, so that one half's shading shares the SMs with the other
+    // half's walks.
+    cudaStream_t half_stream = nullptr, half_aux = nullptr;
+    cudaEvent_t half_fork = nullptr, half_join = nullptr, half_fork2 = nullptr, half_join2 = nullptr;
 };
 
 namespace trt {
@@ -832,6 +838,7 @@ struct trt_scene {
     float4* accum_alt = nullptr;
     cudaEvent_t copied = nullptr, copied_alt = nullptr;
     Wave wave;  // the render's wave state
+    Wave wave2; // the second half-wave's
     void* dn = nullptr;  // the denoiser's buffers, for dn_w x dn_h pixels
     uint32_t dn_w = 0, dn_h = 0;
     DenoiseBufs D{};
@@ -968,10 +975,6 @@ int wave_ensure(Wave& w, uint32_t slots, uint32_t n_dir, unsigned long long* tot
     return TRT_OK;
 }
 
-int ensure_work(trt_scene* s, uint32_t slots, uint32_t n_dir) {
-    return wave_ensure(s->wave, slots, n_dir, s->totals, s->ctx->stream, s->ctx->err);
-}
-
 std::pair<cudaEvent_t, cudaEvent_t> take_events(trt_scene* s) {
     if (!s->ev_free.empty()) {
         auto e = s->ev_free.back();
@@ -998,12 +1001,101 @@ uint32_t chunk_shift(uint32_t cap) {
 }
 
 template <uint32_t KIND>
-void launch_sort(trt_scene* s, const uint32_t* in, uint32_t* out, uint32_t depth, uint32_t cap, cudaStream_t st) {
+void launch_sort(trt_scene* s, Wave& W, const uint32_t* in, uint32_t* out, uint32_t depth, uint32_t cap, cudaStream_t st) {
     uint32_t shift = chunk_shift(cap);
-    k_sort_count<KIND><<<(cap + SORT_ITEMS - 1u) / SORT_ITEMS, SORT_THREADS, 0, st>>>(s->wave.jobs, s->wave.B, s->wave.Q, in, depth, shift);
-    k_sort_scatter<KIND><<<(cap + 255u) / 256u, 256, 0, st>>>(s->wave.Q, in, out, depth);
+    k_sort_count<KIND><<<(cap + SORT_ITEMS - 1u) / SORT_ITEMS, SORT_THREADS, 0, st>>>(W.jobs, W.B, W.Q, in, depth, shift);
+    k_sort_scatter<KIND><<<(cap + 255u) / 256u, 256, 0, st>>>(W.Q, in, out, depth);
     s->launches += 2;
 }
+
+// A wave's launches on a stream pair (st, aux): ray generation, then each depth's walks, sorts, shading and resolve,
+// then the accumulation. g_ext / g_sha: the persistent walks' grids.
+template <bool COUNT, bool WIDE>
+void launch_wave(trt_scene* s, Wave& W, const Job& job, uint32_t n, uint32_t last, uint32_t flags_eff,
+                 cudaStream_t st, cudaStream_t aux, cudaEvent_t fork_ev, cudaEvent_t join_ev, int g_ext, int g_sha) {
+    const bool sort_rays = (flags_eff & TRT_RENDER_SORT_RAYS) != 0;
+    const bool sort_hits = (flags_eff & TRT_RENDER_UNSORTED_HITS) == 0;
+    const bool sort_shadows = (flags_eff & TRT_RENDER_SORT_SHADOWS) != 0;
+    const int blk = 128;
+    auto mark = [&](std::vector<std::pair<cudaEvent_t, cudaEvent_t>>& v, bool begin, cudaStream_t on) {
+        if (!s->profiling) return;
+        if (begin) { v.push_back(take_events(s)); cudaEventRecord(v.back().first, on); }
+        else cudaEventRecord(v.back().second, on);
+    };
+    // Each depth's shadow walk on the second stream beside the next depth's closest-hit walk: both read what the
+    // depth's shading wrote and write apart (visibility bits; hit records), so their tails overlap. (Not with the ray
+    // sort, whose output buffer is the previous depth's shading order, which that depth's resolve still reads.)
+    const bool overlap = !sort_rays;
+    k_put_job<<<1, 128, 0, st>>>(job, W.jobs, 0u);
+    k_raygen<<<(n + blk - 1) / blk, blk, 0, st>>>(W.jobs, 1u, W.B, W.Q, n, nullptr);
+    s->launches += 2;
+    for (uint32_t depth = 0; depth <= last; ++depth) {
+        // The depth's queue (raw), the order extend walks it in, the order shade takes the hits in.
+        uint32_t* raw = W.Q.q[depth & 1u];
+        uint32_t* next = W.Q.q[(depth + 1u) & 1u];
+        uint32_t* ext_q = raw;
+        if (sort_rays && depth > 0u) {
+            mark(s->ev_sort, true, st);
+            launch_sort<SORT_RAYS>(s, W, raw, W.Q.qx, depth, n, st);
+            mark(s->ev_sort, false, st);
+            ext_q = W.Q.qx;
+        }
+        if (!overlap || depth == 0u) {  // (past depth 0 with the overlap, launched beside the last shadow walk)
+            mark(s->ev_extend, true, st);
+            k_extend<COUNT, WIDE, false><<<g_ext, blk, 0, st>>>(W.jobs, job, W.B, W.Q, depth, ext_q);
+            mark(s->ev_extend, false, st);
+        }
+        uint32_t* shade_q = ext_q;
+        if (sort_hits) {
+            shade_q = ext_q == raw ? W.Q.qx : raw;
+            mark(s->ev_sort, true, st);
+            launch_sort<SORT_HITS>(s, W, ext_q, shade_q, depth, n, st);
+            mark(s->ev_sort, false, st);
+        }
+        mark(s->ev_shade, true, st);
+        k_shade<false><<<(n + blk - 1) / blk, blk, 0, st>>>(W.jobs, job, W.B, W.Q, depth, shade_q, next);
+        mark(s->ev_shade, false, st);
+        const uint32_t* perm = nullptr;
+        if (sort_shadows) {
+            mark(s->ev_sort, true, st);
+            launch_sort<SORT_SHADOWS>(s, W, nullptr, W.Q.perm, depth, W.Q.shadow_cap, st);
+            mark(s->ev_sort, false, st);
+            perm = W.Q.perm;
+        }
+        if (overlap) {
+            cudaEventRecord(fork_ev, st);
+            cudaStreamWaitEvent(aux, fork_ev, 0);
+            mark(s->ev_shadow, true, aux);
+            k_shadow<COUNT, WIDE, false><<<g_sha, blk, 0, aux>>>(W.jobs, job, W.B, W.Q, depth, perm);
+            mark(s->ev_shadow, false, aux);
+            if (depth < last) {
+                mark(s->ev_extend, true, st);
+                k_extend<COUNT, WIDE, false><<<g_ext, blk, 0, st>>>(W.jobs, job, W.B, W.Q, depth + 1u, next);
+                mark(s->ev_extend, false, st);
+            }
+            cudaEventRecord(join_ev, aux);
+            cudaStreamWaitEvent(st, join_ev, 0);
+        } else {
+            mark(s->ev_shadow, true, st);
+            k_shadow<COUNT, WIDE, false><<<g_sha, blk, 0, st>>>(W.jobs, job, W.B, W.Q, depth, perm);
+            mark(s->ev_shadow, false, st);
+        }
+        k_resolve<false><<<(n + blk - 1) / blk, blk, 0, st>>>(W.jobs, job, W.B, W.Q, depth, shade_q);
+        s->launches += 4;
+        s->extend_launches++;
+        s->shadow_launches++;
+    }
+    k_accumulate<<<dim3((job.n_idx + blk - 1) / blk, 1), blk, 0, st>>>(W.jobs, W.B);
+    s->launches++;
+}
+
+// A wave of at least this many paths runs as two half-waves (their own queues and stream pairs): one half's shading,
+// latency-bound, then shares the SMs with the other half's walks, issue-bound. Each half's persistent walks are sized
+// for the whole GPU (measured on the city frame: 1,134 Mrays/s, against 1,125 with half the grid each and 1,118 in
+// one wave; the Cornell box 3,099, 3,228 and 3,048).
+#ifndef TRT_HALF_WAVE_MIN
+#define TRT_HALF_WAVE_MIN (1u << 19)
+#endif
 
 template <bool COUNT, bool WIDE>
 int render_waves(trt_scene* s, const Params& P, uint32_t first_sample, uint32_t spp, uint32_t flags) {
@@ -1014,98 +1106,50 @@ int render_waves(trt_scene* s, const Params& P, uint32_t first_sample, uint32_t 
     // Samples a wave: enough paths to fill the GPU (about two million), at most spp.
     uint32_t K = std::max(1u, std::min(spp, (2u << 20) / std::max(1u, n_idx)));
     uint32_t n_dir = P.w[P_COUNTS2];
-    int rc = ensure_work(s, n_idx * K, n_dir);
+    // Two half-waves: the image's pixel indices (8 x 4 tiles of 32) split at a tile.
+    const bool halves = (uint64_t)n_idx * K >= TRT_HALF_WAVE_MIN && n_idx >= 64u;
+    const uint32_t n_idx_a = halves ? (n_idx / 2u) / 32u * 32u : n_idx, n_idx_b = n_idx - n_idx_a;
+    int rc = wave_ensure(s->wave, n_idx_a * K, n_dir, s->totals, st, c->err);
     if (rc) return rc;
+    if (halves) {
+        rc = wave_ensure(s->wave2, n_idx_b * K, n_dir, s->totals, st, c->err);
+        if (rc) return rc;
+    }
     Walk wk{scene_view(s), s->wide.view(), P.w[P_MOTION + 2], P.w[P_MOTION + 3]};
     uint32_t last = P.w[P_COUNTS + 2];
     // the material table's records (18 vec4 each) between its first row and the lights' first row
     const uint32_t n_materials = (P.w[P_TABLE_FIRST + 2] - P.w[P_TABLE_FIRST + 1]) / 18u;
-    bool sort_rays = (flags & TRT_RENDER_SORT_RAYS) != 0;
-    bool sort_hits = (flags & TRT_RENDER_UNSORTED_HITS) == 0 && n_materials > TRT_SORT_HITS_MIN_MATERIALS;
-    bool sort_shadows = (flags & TRT_RENDER_SORT_SHADOWS) != 0;
+    const bool sort_hits = (flags & TRT_RENDER_UNSORTED_HITS) == 0 && n_materials > TRT_SORT_HITS_MIN_MATERIALS;
+    const uint32_t flags_eff = (flags & ~TRT_RENDER_UNSORTED_HITS) | (sort_hits ? 0u : TRT_RENDER_UNSORTED_HITS);
     const int blk = 128;
     int g_ext = grid_for((const void*)k_extend<COUNT, WIDE, false>, blk, c->sm_count);
     int g_sha = grid_for((const void*)k_shadow<COUNT, WIDE, false>, blk, c->sm_count);
     std::vector<uint32_t> host_cnt(MAX_DEPTH * CNT_STRIDE + CNT_STRIDE, 0);
-    auto mark = [&](std::vector<std::pair<cudaEvent_t, cudaEvent_t>>& v, bool begin, cudaStream_t on = nullptr) {
-        if (!s->profiling) return;
-        if (!on) on = st;
-        if (begin) { v.push_back(take_events(s)); cudaEventRecord(v.back().first, on); }
-        else cudaEventRecord(v.back().second, on);
-    };
-    // Each depth's shadow walk on the second stream beside the next depth's closest-hit walk: both read what the
-    // depth's shading wrote and write apart (visibility bits; hit records), so their tails overlap. (Not with the ray
-    // sort, whose output buffer is the previous depth's shading order, which that depth's resolve still reads.)
-    const bool overlap = !sort_rays;
-    cudaStream_t aux = c->aux_stream;
     for (uint32_t s0 = 0; s0 < spp; s0 += K) {
         uint32_t k = std::min(K, spp - s0);
+        const uint32_t depth_flag = (flags & TRT_RENDER_DEPTH) ? 1u : 0u;
+        Job job_a{P, wk, s->accum, 0u, n_idx_a, k, first_sample + s0, 0u, depth_flag, 0u};
         TRT_CUDA(c, cudaMemcpyAsync(s->wave.Q.cnt, host_cnt.data(), host_cnt.size() * 4, cudaMemcpyHostToDevice, st));
-        uint32_t n = n_idx * k;
-        Job job{P, wk, s->accum, 0u, n_idx, k, first_sample + s0, 0u, (flags & TRT_RENDER_DEPTH) ? 1u : 0u};
-        k_put_job<<<1, 128, 0, st>>>(job, s->wave.jobs, 0u);
-        k_raygen<<<(n + blk - 1) / blk, blk, 0, st>>>(s->wave.jobs, 1u, s->wave.B, s->wave.Q, n, nullptr);
-        s->launches += 2;
-        for (uint32_t depth = 0; depth <= last; ++depth) {
-            // The depth's queue (raw), the order extend walks it in, the order shade takes the hits in.
-            uint32_t* raw = s->wave.Q.q[depth & 1u];
-            uint32_t* next = s->wave.Q.q[(depth + 1u) & 1u];
-            uint32_t* ext_q = raw;
-            if (sort_rays && depth > 0u) {
-                mark(s->ev_sort, true);
-                launch_sort<SORT_RAYS>(s, raw, s->wave.Q.qx, depth, n, st);
-                mark(s->ev_sort, false);
-                ext_q = s->wave.Q.qx;
-            }
-            if (!overlap || depth == 0u) {  // (past depth 0 with the overlap, launched beside the last shadow walk)
-                mark(s->ev_extend, true);
-                k_extend<COUNT, WIDE, false><<<g_ext, blk, 0, st>>>(s->wave.jobs, job, s->wave.B, s->wave.Q, depth, ext_q);
-                mark(s->ev_extend, false);
-            }
-            uint32_t* shade_q = ext_q;
-            if (sort_hits) {
-                shade_q = ext_q == raw ? s->wave.Q.qx : raw;
-                mark(s->ev_sort, true);
-                launch_sort<SORT_HITS>(s, ext_q, shade_q, depth, n, st);
-                mark(s->ev_sort, false);
-            }
-            mark(s->ev_shade, true);
-            k_shade<false><<<(n + blk - 1) / blk, blk, 0, st>>>(s->wave.jobs, job, s->wave.B, s->wave.Q, depth, shade_q, next);
-            mark(s->ev_shade, false);
-            const uint32_t* perm = nullptr;
-            if (sort_shadows) {
-                mark(s->ev_sort, true);
-                launch_sort<SORT_SHADOWS>(s, nullptr, s->wave.Q.perm, depth, s->wave.Q.shadow_cap, st);
-                mark(s->ev_sort, false);
-                perm = s->wave.Q.perm;
-            }
-            if (overlap) {
-                TRT_CUDA(c, cudaEventRecord(c->fork_ev, st));
-                TRT_CUDA(c, cudaStreamWaitEvent(aux, c->fork_ev, 0));
-                mark(s->ev_shadow, true, aux);
-                k_shadow<COUNT, WIDE, false><<<g_sha, blk, 0, aux>>>(s->wave.jobs, job, s->wave.B, s->wave.Q, depth, perm);
-                mark(s->ev_shadow, false, aux);
-                if (depth < last) {
-                    mark(s->ev_extend, true);
-                    k_extend<COUNT, WIDE, false><<<g_ext, blk, 0, st>>>(s->wave.jobs, job, s->wave.B, s->wave.Q,
-                                                                        depth + 1u, next);
-                    mark(s->ev_extend, false);
-                }
-                TRT_CUDA(c, cudaEventRecord(c->join_ev, aux));
-                TRT_CUDA(c, cudaStreamWaitEvent(st, c->join_ev, 0));
-            } else {
-                mark(s->ev_shadow, true);
-                k_shadow<COUNT, WIDE, false><<<g_sha, blk, 0, st>>>(s->wave.jobs, job, s->wave.B, s->wave.Q, depth, perm);
-                mark(s->ev_shadow, false);
-            }
-            k_resolve<false><<<(n + blk - 1) / blk, blk, 0, st>>>(s->wave.jobs, job, s->wave.B, s->wave.Q, depth, shade_q);
-            s->launches += 4;
-            s->extend_launches++;
-            s->shadow_launches++;
+        if (halves) {
+            // The second half on its own stream pair, after what the main stream holds so far; joined at the end.
+            Job job_b{P, wk, s->accum, 0u, n_idx_b, k, first_sample + s0, 0u, depth_flag, n_idx_a};
+            TRT_CUDA(c, cudaEventRecord(c->half_fork, st));
+            TRT_CUDA(c, cudaStreamWaitEvent(c->half_stream, c->half_fork, 0));
+            TRT_CUDA(c, cudaMemcpyAsync(s->wave2.Q.cnt, host_cnt.data(), host_cnt.size() * 4, cudaMemcpyHostToDevice,
+                                        c->half_stream));
+            launch_wave<COUNT, WIDE>(s, s->wave, job_a, n_idx_a * k, last, flags_eff, st, c->aux_stream, c->fork_ev,
+                                     c->join_ev, g_ext, g_sha);
+            launch_wave<COUNT, WIDE>(s, s->wave2, job_b, n_idx_b * k, last, flags_eff, c->half_stream, c->half_aux,
+                                     c->half_fork2, c->half_join2, g_ext, g_sha);
+            k_tally<<<1, 32, 0, c->half_stream>>>(s->wave2.Q, last + 1, 0u, nullptr);
+            TRT_CUDA(c, cudaEventRecord(c->half_join, c->half_stream));
+            TRT_CUDA(c, cudaStreamWaitEvent(st, c->half_join, 0));
+        } else {
+            launch_wave<COUNT, WIDE>(s, s->wave, job_a, n_idx_a * k, last, flags_eff, st, c->aux_stream, c->fork_ev,
+                                     c->join_ev, g_ext, g_sha);
         }
-        k_accumulate<<<dim3((n_idx + blk - 1) / blk, 1), blk, 0, st>>>(s->wave.jobs, s->wave.B);
         k_tally<<<1, 32, 0, st>>>(s->wave.Q, last + 1, w * h * k, nullptr);
-        s->launches += 2;
+        s->launches += halves ? 2 : 1;
     }
     TRT_CUDA(c, cudaGetLastError());
     return TRT_OK;
@@ -1209,12 +1253,18 @@ int trt_create(const trt_options* opts, trt_ctx** out) {
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->aux_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->join_ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->half_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->half_aux, cudaStreamNonBlocking);
+    for (cudaEvent_t* ev : {&c->half_fork, &c->half_join, &c->half_fork2, &c->half_join2})
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         // (No context to hold the message: the caller gets the code.)
         std::fprintf(stderr, "trt_create: %s\n", cudaGetErrorString(e));
         if (c->stream) cudaStreamDestroy(c->stream);
         if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
         if (c->aux_stream) cudaStreamDestroy(c->aux_stream);
+        if (c->half_stream) cudaStreamDestroy(c->half_stream);
+        if (c->half_aux) cudaStreamDestroy(c->half_aux);
         delete c;
         return TRT_ECUDA;
     }
@@ -1234,6 +1284,10 @@ void trt_destroy(trt_ctx* c) {
     if (c->fork_ev) cudaEventDestroy(c->fork_ev);
     if (c->join_ev) cudaEventDestroy(c->join_ev);
     if (c->aux_stream) cudaStreamDestroy(c->aux_stream);
+    for (cudaEvent_t ev : {c->half_fork, c->half_join, c->half_fork2, c->half_join2})
+        if (ev) cudaEventDestroy(ev);
+    if (c->half_stream) cudaStreamDestroy(c->half_stream);
+    if (c->half_aux) cudaStreamDestroy(c->half_aux);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -1299,6 +1353,7 @@ void trt_scene_free(trt_scene* s) {
     if (s->copied) cudaEventDestroy(s->copied);
     if (s->copied_alt) cudaEventDestroy(s->copied_alt);
     if (s->wave.work) cudaFree(s->wave.work);
+    if (s->wave2.work) cudaFree(s->wave2.work);
     if (s->dn) cudaFree(s->dn);
     if (s->totals) cudaFree(s->totals);
     deform_free(s->deform);
@@ -1765,7 +1820,7 @@ int trt_render_noalloc(const trt_scene_desc* dev, const uint32_t params[TRT_PARA
     cudaStream_t st = (cudaStream_t)stream;
     uint32_t K = std::max(1u, std::min(spp, NOALLOC_SLOTS / n_idx));
     uint32_t slots = n_idx * K;
-    // The array's parts, as ensure_work lays out an allocation.
+    // The array's parts, as wave_ensure lays out an allocation.
     uint8_t* b = g_noalloc_ptr[device];
     uint64_t at = 0;
     auto take = [&](uint64_t bytes) { uint8_t* p = b + at; at += na_round(bytes); return p; };
