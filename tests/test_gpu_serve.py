@@ -120,3 +120,20 @@ def test_denoised_requests_are_the_denoise_of_their_render_alone(gpu, resident):
         else:
             assert np.array_equal(r.accum, S[r.scene].render_raw(r.params, r.spp)[0])
     net.close()
+
+
+def test_a_720p_frame_rendered_in_two_half_waves_is_the_servers_one_wave(gpu, resident):
+    """trt_render runs a wave of 2^19 paths or more as two half-waves (each with its first pixel index); the server
+    renders the same request in one wave. Both give the same accum, bit for bit: a path's pixel, sample and random
+    numbers do not depend on which half-wave it is in."""
+    Ps, S = resident
+    params = params_with(Ps[1].params, width=1280, height=720)
+    alone, _ = S[1].render_raw(params, 1)  # 921,600 paths: two half-waves
+    srv = Server(gpu, wave_slots=1 << 21)
+    try:
+        r = Request(1, params, 1)
+        res = run_stream(srv, S, [r], rate=0.0)
+    finally:
+        srv.close()
+    assert res["failed"] == 0
+    assert np.array_equal(r.accum, alone)
