@@ -319,13 +319,15 @@ def run_crowd(args, rank, world, local, dist):
         inputs[f] = (prep.set_camera(P.params, cam), np.ascontiguousarray(crowd.frame_records(P, c, t)),
                      np.ascontiguousarray(crowd.palettes(t, c.phase, c.scale).reshape(-1, 12)))
     L = N.lib()
+    # --walk wide: the wide BVH (built once, before the frames) is refit by each trt_deform on the device
+    rflags = N.TRT_RENDER_WIDE if args.walk == "wide" else 0
 
     def frame(f, acc_ptr=None):
         params, rec, pal = inputs[f]
         gpu._check(L.trt_scene_update(S.handle, 3, t_inst * 16, rec.ctypes.data, rec.nbytes), "trt_scene_update")
         p = params.ctypes.data_as(C.POINTER(C.c_uint32))
         gpu._check(L.trt_deform(S.handle, p, pal.ctypes.data_as(C.POINTER(C.c_float)), len(pal), 0, None), "trt_deform")
-        gpu._check(L.trt_render(S.handle, p, 0, SPP, 0, acc_ptr, None), "trt_render")
+        gpu._check(L.trt_render(S.handle, p, 0, SPP, rflags, acc_ptr, None), "trt_render")
 
     def barrier():
         if dist:
@@ -356,7 +358,7 @@ def run_crowd(args, rank, world, local, dist):
     rays = tot["closest_rays"] + tot["shadow_rays"]
     # The deformation's own stages, frame by frame, untimed above.
     ds = [S.deform(inputs[f][0], inputs[f][2], stats=True) for f in frames[:8]]
-    deform = {k: float(np.mean([d[k] for d in ds])) for k in ("device_ms", "skin_ms", "refit_ms", "top_ms")}
+    deform = {k: float(np.mean([d[k] for d in ds])) for k in ("device_ms", "skin_ms", "refit_ms", "top_ms", "wide_ms")}
     # End to end: the same frames with the accum read back into pinned memory.
     acc = torch.empty((WIDTH * HEIGHT, N.PIXEL_FLOATS), dtype=torch.float32, pin_memory=True)
     acc_ptr = C.cast(acc.data_ptr(), C.POINTER(C.c_float))
@@ -375,8 +377,9 @@ def run_crowd(args, rank, world, local, dist):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"crowd: 5000 walkers x 20160 tris in {args.groups} pose groups "
                                f"({P.info['n_tris']} tris), 49928-tri ground, 1280x720, 1 spp, depth 3",
-                   "frames_per_rank": args.steps, "pose_groups": args.groups,
-                   "per_step": "records + palette H2D, trt_deform (skin, leaf gather, refit, top rebuild), render",
+                   "frames_per_rank": args.steps, "pose_groups": args.groups, "walk": args.walk,
+                   "per_step": "records + palette H2D, trt_deform (skin, leaf gather, refit, top rebuild"
+                               + (", wide BVH refit" if rflags else "") + "), render",
                    "device": name, "sms": sms, "parallelism": f"replicas x{world}"},
         "e2e": {"value": rays_all / (e2e_ms * 1e-3) / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": rec_bytes,
                 "d2h_bytes_per_step": WIDTH * HEIGHT * 80},

@@ -246,15 +246,17 @@ typedef struct {
 } trt_deform_desc;
 
 /* Device times of one deformation (filled when stats is given: the call then waits for it) and the errors the device
- * found (a tree that is not one, a top tree that came out deeper than TOP_DEPTH). */
-typedef struct { float device_ms, skin_ms, gather_ms, refit_ms, top_ms; uint32_t errors; } trt_deform_stats;
+ * found (a tree that is not one, a top tree that came out deeper than TOP_DEPTH; bit 16: the wide BVH's refit met an
+ * index out of its buffers). wide_ms: the wide BVH's refit (0 when the scene has none built), after device_ms. */
+typedef struct { float device_ms, skin_ms, gather_ms, refit_ms, top_ms, wide_ms; uint32_t errors; } trt_deform_stats;
 
 /* Uploads the skinned models' corners and the deforming meshes, checks each mesh's tree (on the host copy taken at
  * upload) and links every node to its parent. Again replaces what was set up. */
 int trt_deform_setup(trt_scene* scene, const trt_deform_desc* desc);
 /* One frame: palette_rows holds n_matrices matrices of 3 rows (x, y, z, translation) each; every mesh's palette
- * indices must fall inside it. Asynchronous unless stats is given. After it the scene walks the binary trees only
- * (the wide BVH is built from host copies the deformation does not update). flags: 0. */
+ * indices must fall inside it. Asynchronous unless stats is given. A wide BVH (TRT_RENDER_WIDE) follows on the device:
+ * its mesh trees' nodes quantised again over the refit boxes, its triangle copies gathered again, the rebuilt top tree
+ * collapsed again (at once when one is built, else when the first wide walk builds it). flags: 0. */
 int trt_deform(trt_scene* scene, const uint32_t params[TRT_PARAMS_WORDS], const float* palette_rows,
                uint32_t n_matrices, uint32_t flags, trt_deform_stats* stats);
 

@@ -153,12 +153,13 @@ def test_city_frame_at_720p_matches_the_oracle(gpu, city, flags):
     assert close1 >= 0.9 and close >= 0.85, (close1, close)
 
 
-@pytest.mark.parametrize("groups", [1, 5000])
-def test_crowd_trace_after_deform_matches_the_oracle(gpu, groups):
+@pytest.mark.parametrize("groups,flags", [(1, 0), (1, N.TRT_RENDER_WIDE), (5000, 0)])
+def test_crowd_trace_after_deform_matches_the_oracle(gpu, groups, flags):
     """Config 2 at full size (5,000 walkers of 20,160 triangles on a 49,928-triangle ground; one pose group: 70,488
     triangles, 5,000 pose groups: 100,850,328): one frame's records and palettes, trt_deform on the device (skin, leaf
-    gather, refit, top rebuild), then the walk against the oracle's on the deformed buffers read back from the device.
-    (The deformation itself is checked bit for bit against the oracle's in test_gpu_deform.py.)"""
+    gather, refit, top rebuild), then the walk against the oracle's on the deformed buffers read back from the device:
+    the binary walk, and in one pose group the wide walk too (its BVH refit on the device, its top tree of 5,000 units
+    collapsed again). (The deformation itself is checked bit for bit against the oracle's in test_gpu_deform.py.)"""
     c = crowd.crowd(n=5000, groups=groups, width=CITY_W, height=CITY_H, max_depth=3)
     P = prep.prepare(c.desc)
     corners, jobs = crowd.deform_jobs(P, c)
@@ -178,12 +179,13 @@ def test_crowd_trace_after_deform_matches_the_oracle(gpu, groups):
     want_scene = dataclasses.replace(P, vertices=vertices, leaves=leaves, nodes=nodes, tables=tables, params=params)
     rays = np.concatenate([camera_rays(params, CITY_W, CITY_H)[::3],
                            random_rays(want_scene, 200000, seed=13, spread=5.0)])
-    got = S.trace(params, rays)
+    got = S.trace(params, rays, flags=flags)
     S.close()
     O = oracle.Oracle(want_scene)
     want, _ = O.trace(params, rays)
     both = check_hits(O, params, rays, got, want, min_both=100000)
-    print(f"crowd ({groups} pose groups, {P.info['n_tris']} tris): {len(rays)} rays, {both.sum()} closest hits")
+    print(f"crowd ({groups} pose groups, {P.info['n_tris']} tris, {'wide' if flags else 'binary'}): {len(rays)} rays, "
+          f"{both.sum()} closest hits")
 
 
 def ulps(got32, truth64):

@@ -105,10 +105,59 @@ def test_render_after_deform_matches_the_oracle(gpu, scene):
     assert both.sum() > 1000
     assert np.abs(got["t"][both] / ref["t"][both] - 1).max() <= 1e-6
     assert ((got["tri"] == ref["tri"]) | ~both).mean() >= 0.9999
-    # the wide walk is built from host copies the deformation did not update: refused
-    with pytest.raises(RenderError):
-        S.render_raw(P.params, 1, flags=N.TRT_RENDER_WIDE)
+    # the wide walk, built now from the uploaded copies and brought to the deformed buffers on the device
+    check_walk(S.trace(P.params, rays, flags=N.TRT_RENDER_WIDE), ref, rays)
     S.close()
+
+
+def check_walk(got, ref, rays):
+    """Hit or miss on >= 99.99 % of rays, t within 1e-6, the same triangle on >= 99.99 % of closest hits."""
+    hg, hw = got["tri"] != 0xFFFFFFFF, ref["tri"] != 0xFFFFFFFF
+    assert (hg == hw).mean() >= 0.9999, (hg != hw).sum()
+    both = hg & hw & (rays["mode"] == 0)
+    assert both.sum() > 1000
+    assert np.abs(got["t"][both] / ref["t"][both] - 1).max() <= 1e-6
+    assert ((got["tri"] == ref["tri"]) | ~both).mean() >= 0.9999
+
+
+@pytest.mark.parametrize("n", [160, 700])
+def test_wide_walk_follows_each_deformation(gpu, n):
+    """A wide BVH in use is refit by each trt_deform on the device (its mesh nodes quantised again over the refit
+    boxes, its triangle copies gathered again, the rebuilt top tree collapsed again): three frames in a row, each
+    walked against the oracle on the frame's buffers; a wide BVH first built after the deformations (from the uploaded
+    copies, then refit) gives the same hits bit for bit."""
+    c, P, corners, jobs = make_scene(n)
+    S = gpu.upload(P)
+    S.deform_setup(corners, jobs)
+    probe = random_rays(P, 1000, seed=1, spread=2.0)
+    S.trace(P.params, probe, flags=N.TRT_RENDER_WIDE)  # built before the first deformation
+    for i, t in enumerate((0.4, 1.3, 2.2)):
+        recs, pal, st = run_frame(S, P, c, t)
+        assert st["errors"] == 0 and st["wide_ms"] > 0, st
+        want = oracle_frame(P, c, corners, jobs, recs, pal)
+        rays = random_rays(want, 20000, seed=20 + i, spread=2.0)
+        ref, _ = oracle.Oracle(want).trace(P.params, rays)
+        got = S.trace(P.params, rays, flags=N.TRT_RENDER_WIDE)
+        check_walk(got, ref, rays)
+        binary = S.trace(P.params, rays)
+        same = (got["tri"] != 0xFFFFFFFF) == (binary["tri"] != 0xFFFFFFFF)
+        assert same.mean() >= 0.9999
+    # the same three frames on a second scene whose wide BVH is built only after them
+    S2 = gpu.upload(P)
+    S2.deform_setup(corners, jobs)
+    for t in (0.4, 1.3, 2.2):
+        _, _, st = run_frame(S2, P, c, t)
+        assert st["wide_ms"] == 0
+    got2 = S2.trace(P.params, rays, flags=N.TRT_RENDER_WIDE)
+    for f in ("tri", "inst", "t"):
+        assert np.array_equal(got2[f], got[f]), f
+    # a frame rendered with the wide walk: first-hit albedo and normals as the binary walk's
+    acc_w = S2.render_raw(P.params, 1, flags=N.TRT_RENDER_WIDE)[0]
+    acc_b = S2.render_raw(P.params, 1)[0]
+    same = np.isclose(acc_w[:, 4:7], acc_b[:, 4:7], rtol=1e-4, atol=1e-5).all(1)
+    assert same.mean() >= 0.999, (~same).sum()
+    S.close()
+    S2.close()
 
 
 def test_deform_refuses_what_it_cannot_do(gpu, scene):

@@ -129,7 +129,7 @@ class DeformDesc(C.Structure):
 
 class DeformStats(C.Structure):
     _fields_ = [("device_ms", f32), ("skin_ms", f32), ("gather_ms", f32), ("refit_ms", f32), ("top_ms", f32),
-                ("errors", u32)]
+                ("wide_ms", f32), ("errors", u32)]
 
 
 TRT_CORNER_NORMAL = 1

@@ -915,6 +915,8 @@ int deform_run(DeformState* st, const SceneBuffers& sb, const uint32_t* P, const
     return TRT_OK;
 }
 
+uint32_t* deform_error_word(DeformState* st) { return st->err; }
+
 int deform_errors(DeformState* st, cudaStream_t stream, uint32_t* errors) {
     uint32_t e = 0;
     if (cudaMemcpyAsync(&e, st->err, 4, cudaMemcpyDeviceToHost, stream) != cudaSuccess) return TRT_ECUDA;

@@ -28,6 +28,9 @@ int deform_run(DeformState* st, const SceneBuffers& sb, const uint32_t* params, 
                uint32_t n_matrices, uint32_t flags, trt_deform_stats* stats, std::string& err);
 // Errors the device recorded since the last call (bad trees, a top tree deeper than it may be); resets them.
 int deform_errors(DeformState* st, cudaStream_t stream, uint32_t* errors);
+// The device word the errors are recorded in; DEFORM_E_WIDE is the bit the wide BVH's refit sets in it.
+uint32_t* deform_error_word(DeformState* st);
+constexpr uint32_t DEFORM_E_WIDE = 16u;
 void deform_free(DeformState* st);
 
 }  // namespace trt

@@ -853,7 +853,8 @@ struct trt_scene {
     void* em = nullptr;  // the emitter re-weigh's scratch (trt_scene_weigh_emitters)
     uint64_t em_bytes = 0;
     bool deform_stale = false;  // the nodes were written after setup: its tree checks no longer hold
-    bool deformed = false;      // a deformation ran: the host copies (and a wide BVH built from them) are old
+    bool deformed = false;      // a deformation ran: the host copies are old (a wide BVH built from them is refit)
+    uint64_t deform_gen = 0;    // deformations run (WideBvh::refit_gen: the one the wide trees were brought to)
 };
 
 namespace {
@@ -1364,6 +1365,34 @@ void trt_scene_free(trt_scene* s) {
     delete s;
 }
 
+namespace {
+
+// The wide BVH brought to the deformed buffers on the device (WideBvh::refit); errors go to the deformation's word.
+int refit_wide(trt_scene* s, const uint32_t* params) {
+    trt_ctx* c = s->ctx;
+    if (s->wide.refit(params, s->buf[2], s->bytes[2] / 32, s->buf[1], s->bytes[1] / 48, s->buf[3], s->bytes[3] / 16,
+                      deform_error_word(s->deform), DEFORM_E_WIDE, c->stream) != 0)
+        return fail(c, TRT_ECUDA, s->wide.error);
+    s->wide.refit_gen = s->deform_gen;
+    return TRT_OK;
+}
+
+// The wide BVH for a walk: built from the host copies (the scene as uploaded and edited), then, on a deformed scene,
+// brought to the device's buffers; a refit here waits for its error word.
+int ensure_wide(trt_scene* s, const uint32_t* params) {
+    trt_ctx* c = s->ctx;
+    if (s->wide.ensure(params, s->host, c->stream) != 0) return fail(c, TRT_EINVAL, s->wide.error);
+    if (!s->deformed || s->wide.refit_gen == s->deform_gen) return TRT_OK;
+    int rc = refit_wide(s, params);
+    if (rc) return rc;
+    uint32_t errors = 0;
+    if (deform_errors(s->deform, c->stream, &errors) != TRT_OK) return fail(c, TRT_ECUDA, "reading the deformation's errors");
+    if (errors) return fail(c, TRT_EGUARD, "the deformation or the wide BVH's refit met a bad tree (error bits " + std::to_string(errors) + ")");
+    return TRT_OK;
+}
+
+}  // namespace
+
 int trt_scene_update(trt_scene* s, uint32_t which, uint64_t offset, const void* src, uint64_t bytes) {
     if (!s) return TRT_EINVAL;
     trt_ctx* c = s->ctx;
@@ -1372,8 +1401,12 @@ int trt_scene_update(trt_scene* s, uint32_t which, uint64_t offset, const void* 
     cudaSetDevice(c->device);
     TRT_CUDA(c, cudaMemcpyAsync((char*)s->buf[which] + offset, src, bytes, cudaMemcpyHostToDevice, c->stream));
     if (which >= 1 && which <= 3) {
+        // The wide BVH is rebuilt from the edited buffers at the next render; of the tables it reads only the units'
+        // mesh roots, first triangles and shadow bits, so an edit that leaves those alone (units moved by their
+        // transforms) keeps it.
+        if (which != 3 || s->wide.reads_edit(s->host[3].data(), offset, static_cast<const uint8_t*>(src), bytes))
+            s->wide.invalidate();
         std::memcpy(s->host[which].data() + offset, src, bytes);
-        s->wide.invalidate();  // rebuilt from the edited buffers at the next render
     }
     if (which == 2 && s->deform) s->deform_stale = true;
     return TRT_OK;
@@ -1516,9 +1549,24 @@ int trt_deform(trt_scene* s, const uint32_t params[TRT_PARAMS_WORDS], const floa
                     {s->bytes[0], s->bytes[1], s->bytes[2], s->bytes[3], s->bytes[4]}, c->stream, s->host};
     std::string err;
     s->deformed = true;
-    s->wide.invalidate();
+    s->deform_gen++;
     rc = deform_run(s->deform, sb, params, palette_rows, n_matrices, flags, stats, err);
     if (rc) return fail(c, rc, err);
+    if (s->wide.ready() && s->wide.key_matches(params)) {
+        // A wide BVH in use follows the deformation at once (one built later is refit when it is built).
+        if (stats) TRT_CUDA(c, cudaEventRecord(c->t0, c->stream));
+        rc = refit_wide(s, params);
+        if (rc) return rc;
+        if (stats) {
+            TRT_CUDA(c, cudaEventRecord(c->t1, c->stream));
+            TRT_CUDA(c, cudaEventSynchronize(c->t1));
+            cudaEventElapsedTime(&stats->wide_ms, c->t0, c->t1);
+            uint32_t errors = 0;
+            if (deform_errors(s->deform, c->stream, &errors) != TRT_OK) return fail(c, TRT_ECUDA, "trt_deform: reading the errors");
+            stats->errors |= errors;
+            if (errors) return fail(c, TRT_EGUARD, "trt_deform: the wide BVH's refit met an index out of its buffers");
+        }
+    }
     return TRT_OK;
 }
 
@@ -1564,8 +1612,10 @@ int trt_render(trt_scene* s, const uint32_t params[TRT_PARAMS_WORDS], uint32_t f
     }
     uint64_t launches0 = s->launches;
     bool count = (flags & TRT_RENDER_COUNT) != 0, binary = (flags & TRT_RENDER_WIDE) == 0;
-    if (!binary && s->deformed) return fail(c, TRT_EINVAL, "a deformed scene walks the binary trees (the wide BVH is built from host copies)");
-    if (!binary && s->wide.ensure(params, s->host, c->stream) != 0) return fail(c, TRT_EINVAL, s->wide.error);
+    if (!binary) {
+        rc = ensure_wide(s, params);
+        if (rc) return rc;
+    }
     if (spp > 0) {
         if (count) rc = binary ? render_waves<true, false>(s, P, first_sample, spp, flags) : render_waves<true, true>(s, P, first_sample, spp, flags);
         else rc = binary ? render_waves<false, false>(s, P, first_sample, spp, flags) : render_waves<false, true>(s, P, first_sample, spp, flags);
@@ -1646,10 +1696,13 @@ int trt_trace(trt_scene* s, const uint32_t params[TRT_PARAMS_WORDS], const trt_r
     e = cudaMemcpyAsync(dr, rays, sizeof(trt_ray) * n, cudaMemcpyHostToDevice, c->stream);
     bool binary = (flags & TRT_RENDER_WIDE) == 0;
     bool count = (flags & TRT_RENDER_COUNT) != 0;
-    if (e == cudaSuccess && !binary && (s->deformed || s->wide.ensure(params, s->host, c->stream) != 0)) {
-        cudaFree(dr);
-        cudaFree(dh);
-        return fail(c, TRT_EINVAL, s->deformed ? "a deformed scene walks the binary trees" : s->wide.error);
+    if (e == cudaSuccess && !binary) {
+        rc = ensure_wide(s, params);
+        if (rc) {
+            cudaFree(dr);
+            cudaFree(dh);
+            return rc;
+        }
     }
     DScene S = scene_view(s);
     Walk wk{S, s->wide.view(), P.w[P_MOTION + 2], P.w[P_MOTION + 3]};

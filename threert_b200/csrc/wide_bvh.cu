@@ -33,55 +33,19 @@ struct Builder {
     std::vector<WNode> out;
     std::string error;
 
-    // Quantises the child boxes of one wide node (wide_bvh.cuh's layout) and writes its header.
+    // Quantises the child boxes of one wide node (wide_encode) and writes its header.
     void encode(WNode& W, const std::vector<const BinNode*>& ch, const std::vector<bool>& interior, uint32_t child_base,
                 uint32_t leaf_base, const std::vector<uint32_t>& counts, float tree_pad) {
-        std::memset(&W, 0, sizeof(W));
-        float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-        for (const BinNode* c : ch)
-            if (c)
-                for (int k = 0; k < 3; ++k) { lo[k] = std::min(lo[k], c->bmin[k]); hi[k] = std::max(hi[k], c->bmax[k]); }
-        float origin[3];
-        int ex[3];
-        for (int k = 0; k < 3; ++k) {
-            float ext = hi[k] - lo[k];
-            float mag = std::max(std::fabs(lo[k]), std::fabs(hi[k]));
-            // A step's margin on every side is added per child; this pad keeps the widened boxes inside 0..255 and
-            // gives flat boxes a width of some 2^-16 of their coordinates.
-            float pad = ext * (1.0f / 253.0f) + mag * (1.0f / 65536.0f) + tree_pad + 1e-20f;
-            origin[k] = lo[k] - pad;
-            float range = (hi[k] + pad) - origin[k];
-            int e;
-            std::frexp(range / 255.0f, &e);  // range / 255 < 2^e
-            while (std::ldexp(255.0f, e) < range) ++e;
-            ex[k] = std::max(-126, std::min(127, e));
-        }
-        uint8_t qlo[3][8], qhi[3][8];
-        for (int i = 0; i < 8; ++i)
-            for (int k = 0; k < 3; ++k) { qlo[k][i] = 255; qhi[k][i] = 0; }
-        for (size_t i = 0; i < ch.size(); ++i) {
+        float bmin[8][3], bmax[8][3];
+        uint32_t present = 0, imask = 0, cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (size_t i = 0; i < ch.size() && i < 8; ++i) {
             if (!ch[i]) continue;
-            for (int k = 0; k < 3; ++k) {
-                float s = std::ldexp(1.0f, ex[k]);
-                double a = std::floor((double)(ch[i]->bmin[k] - origin[k]) / s) - 1.0;
-                double b = std::ceil((double)(ch[i]->bmax[k] - origin[k]) / s) + 1.0;
-                qlo[k][i] = (uint8_t)std::max(0.0, std::min(255.0, a));
-                qhi[k][i] = (uint8_t)std::max(0.0, std::min(255.0, b));
-            }
-        }
-        uint32_t imask = 0;
-        for (size_t i = 0; i < ch.size(); ++i)
+            present |= 1u << i;
+            for (int k = 0; k < 3; ++k) { bmin[i][k] = ch[i]->bmin[k]; bmax[i][k] = ch[i]->bmax[k]; }
             if (interior[i]) imask |= 1u << i;
-        std::memcpy(&W.w[0], origin, 12);
-        W.w[3] = (uint32_t)(ex[0] + 127) | ((uint32_t)(ex[1] + 127) << 8) | ((uint32_t)(ex[2] + 127) << 16) | (imask << 24);
-        W.w[4] = child_base;
-        W.w[5] = leaf_base;
-        uint8_t cnt[8] = {0};
-        for (size_t i = 0; i < ch.size(); ++i) cnt[i] = (interior[i] || !ch[i]) ? 0 : (uint8_t)counts[i];
-        std::memcpy(&W.w[6], cnt, 8);
-        uint8_t* q = reinterpret_cast<uint8_t*>(&W.w[8]);
-        for (int k = 0; k < 3; ++k) std::memcpy(q + 8 * k, qlo[k], 8);
-        for (int k = 0; k < 3; ++k) std::memcpy(q + 24 + 8 * k, qhi[k], 8);
+            else cnt[i] = counts[i];
+        }
+        wide_encode(W.w, bmin, bmax, present, imask, child_base, leaf_base, cnt, tree_pad);
     }
 
     // The children in slots by octant: slot s (bit k set: the upper half along axis k) takes the child whose centre
@@ -116,8 +80,12 @@ struct Builder {
 
     // Collapses the binary tree rooted at `root` (child indices from `root`); `leaf(node, items)` appends a binary
     // leaf's items and returns their count. Returns the wide root's index, or UINT32_MAX on a malformed tree.
+    // What a refit reads (WideBvh::slot_host, pad_host), by wide node.
+    std::vector<uint32_t> slots;
+    std::vector<float> pads;
+
     template <class Leaf>
-    uint32_t collapse(uint32_t root, Leaf&& leaf, uint32_t max_leaf_items) {
+    uint32_t collapse(uint32_t root, Leaf&& leaf, uint32_t max_leaf_items, bool top_tree) {
         if (root >= n_nodes) { error = "a tree's root is past the nodes"; return UINT32_MAX; }
         // A slab test rounds with the distance to the box: a box far from the ray's origin but small (a few
         // millimetres of a 10 m mesh seen from 1 km) needs more margin than its own size gives, so every box of a
@@ -191,6 +159,12 @@ struct Builder {
             }
             if (leaf_base == UINT32_MAX) leaf_base = 0;
             encode(out[w], cp, interior, child_base, leaf_base, counts, pad_of_tree);
+            if (slots.size() < 8 * out.size()) {
+                slots.resize(8 * out.size(), WIDE_SLOT_EMPTY);
+                pads.resize(out.size(), 0.0f);
+            }
+            for (int i = 0; i < 8; ++i) slots[8ull * w + i] = top_tree ? WIDE_SLOT_TOP : ch[i];
+            pads[w] = pad_of_tree;
 
         }
         return wroot;
@@ -199,18 +173,366 @@ struct Builder {
 
 constexpr uint32_t P_MOTION_Z = 70, P_MOTION_W = 71, P_T_INSTANCES = 124 + 7, P_W_INDICES = 136 + 4;
 
+// ---- the refit after a deformation --------------------------------------------------------------------------------
+
+// A binary node (the reference's GpuNode, two vec4s): its box, left_or_first and count.
+__device__ __forceinline__ void bin_node(const uint4* __restrict__ bin, uint32_t i, float mn[3], float mx[3],
+                                         uint32_t* lof, uint32_t* count) {
+    const uint4 a = bin[2ull * i], b = bin[2ull * i + 1];
+    mn[0] = __uint_as_float(a.x); mn[1] = __uint_as_float(a.y); mn[2] = __uint_as_float(a.z);
+    mx[0] = __uint_as_float(b.x); mx[1] = __uint_as_float(b.y); mx[2] = __uint_as_float(b.z);
+    *lof = a.w;
+    *count = b.w;
+}
+
+__device__ __forceinline__ void put_node(uint4* __restrict__ wn, uint32_t w, const uint32_t W[20]) {
+#pragma unroll
+    for (int j = 0; j < 5; ++j) wn[5ull * w + j] = make_uint4(W[4 * j], W[4 * j + 1], W[4 * j + 2], W[4 * j + 3]);
+}
+
+// Every built node of a mesh tree quantised again over its slots' binary boxes (the topology, its child and leaf
+// indices and counts are the build's). A thread a node; the top tree's nodes are skipped.
+__global__ void k_wide_refit(const uint4* __restrict__ bin, uint64_t n_bin, const uint32_t* __restrict__ slots,
+                             const float* __restrict__ pads, uint4* wn, uint32_t n_nodes, uint32_t* err, uint32_t err_bit) {
+    for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < n_nodes; w += gridDim.x * blockDim.x) {
+        const uint32_t* sl = slots + 8ull * w;
+        if (sl[0] == WIDE_SLOT_TOP) continue;
+        uint32_t W[20];
+#pragma unroll
+        for (int j = 0; j < 5; ++j) {
+            const uint4 q = wn[5ull * w + j];
+            W[4 * j] = q.x; W[4 * j + 1] = q.y; W[4 * j + 2] = q.z; W[4 * j + 3] = q.w;
+        }
+        float bmin[8][3], bmax[8][3];
+        uint32_t present = 0, counts[8];
+        bool bad = false;
+        for (int i = 0; i < 8; ++i) {
+            counts[i] = (W[6 + (i >> 2)] >> (8 * (i & 3))) & 0xffu;
+            const uint32_t b = sl[i];
+            if (b == WIDE_SLOT_EMPTY) continue;
+            if (b >= n_bin) { bad = true; continue; }
+            uint32_t lof, cnt;
+            bin_node(bin, b, bmin[i], bmax[i], &lof, &cnt);
+            present |= 1u << i;
+        }
+        if (bad) { atomicOr(err, err_bit); continue; }
+        uint32_t out[20];
+        wide_encode(out, bmin, bmax, present, W[3] >> 24, W[4], W[5], counts, pads[w]);
+        put_node(wn, w, out);
+    }
+}
+
+// The wide triangle copies gathered again from the deformed leaves (each copy keeps its reference index in the third
+// vec4's w).
+__global__ void k_wide_tris(const float4* __restrict__ leaves, uint64_t n_leaf_tris, float4* tris, uint32_t n_tris,
+                            uint32_t* err, uint32_t err_bit) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_tris; i += gridDim.x * blockDim.x) {
+        const uint32_t ti = __float_as_uint(tris[3ull * i + 2].w);
+        if (ti >= n_leaf_tris) { atomicOr(err, err_bit); continue; }
+        float4 c = leaves[3ull * ti + 2];
+        c.w = __uint_as_float(ti);
+        tris[3ull * i] = leaves[3ull * ti];
+        tris[3ull * i + 1] = leaves[3ull * ti + 1];
+        tris[3ull * i + 2] = c;
+    }
+}
+
+struct TopCollapse {
+    const uint4* bin;
+    uint64_t n_bin;
+    uint32_t top;           // the binary top tree's root; its children are at top + left_or_first
+    const uint4* tables;
+    uint64_t n_table_vec4;
+    uint32_t t_instances;   // the units' records, 10 vec4s each
+    uint4* wn;
+    uint32_t base, cap;     // the top region: nodes [base, base + cap)
+    uint32_t* items;        // the top tree's leaf items (unit record | shadow bit)
+    uint32_t n_items;
+    uint2* front;           // two frontiers of cap entries
+    uint32_t* err;
+    uint32_t err_bit;
+};
+
+constexpr uint32_t TOP_THREADS = 256, TOP_WARPS_C = TOP_THREADS / 32;
+
+// Exclusive prefix of v over the block, and the block's total; `part` is TOP_WARPS_C words of shared memory.
+__device__ __forceinline__ uint32_t block_prefix(uint32_t v, uint32_t* total, uint32_t* part) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+        if (lane >= (uint32_t)d) x += y;
+    }
+    if (lane == 31) part[warp] = x;
+    __syncthreads();
+    uint32_t before = 0, all = 0;
+    for (uint32_t k = 0; k < TOP_WARPS_C; ++k) {
+        before += k < warp ? part[k] : 0u;
+        all += part[k];
+    }
+    *total = all;
+    return before + x - v;
+}
+
+// One binary node of the top tree opened into a wide node's children as the host build opens it (the child of
+// largest surface area first, up to eight; a leaf stays whole), then placed in slots by octant (the greedy assignment
+// of (child, slot) pairs by score, ties to the lower child and slot). False on a malformed tree.
+__device__ bool top_slots(const TopCollapse& T, uint32_t b, uint32_t slot[8]) {
+    uint32_t ch[8], n;
+    float mn[3], mx[3];
+    uint32_t lof, cnt;
+    bin_node(T.bin, b, mn, mx, &lof, &cnt);
+    if (cnt > 0) {
+        ch[0] = b;
+        n = 1;
+    } else {
+        const uint32_t l = T.top + lof;
+        if (l <= b || (uint64_t)l + 1 >= T.n_bin) return false;
+        ch[0] = l;
+        ch[1] = l + 1;
+        n = 2;
+        while (n < 8) {
+            int best = -1;
+            float best_area = -1.0f;
+            for (uint32_t i = 0; i < n; ++i) {
+                bin_node(T.bin, ch[i], mn, mx, &lof, &cnt);
+                float e[3];
+                for (int k = 0; k < 3; ++k) e[k] = wmax(mx[k] - mn[k], 0.0f);
+                const float area = 2.0f * (e[0] * e[1] + e[1] * e[2] + e[2] * e[0]);
+                if (cnt == 0 && area > best_area) { best_area = area; best = (int)i; }
+            }
+            if (best < 0) break;
+            bin_node(T.bin, ch[best], mn, mx, &lof, &cnt);
+            const uint32_t cl = T.top + lof;
+            if (cl <= ch[best] || (uint64_t)cl + 1 >= T.n_bin) return false;
+            for (uint32_t i = n; i > (uint32_t)best + 1; --i) ch[i] = ch[i - 1];
+            ch[best] = cl;
+            ch[best + 1] = cl + 1;
+            ++n;
+        }
+    }
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    float v[8][3];
+    for (uint32_t j = 0; j < n; ++j) {
+        bin_node(T.bin, ch[j], mn, mx, &lof, &cnt);
+        for (int k = 0; k < 3; ++k) { lo[k] = wmin(lo[k], mn[k]); hi[k] = wmax(hi[k], mx[k]); }
+    }
+    for (uint32_t j = 0; j < n; ++j) {
+        bin_node(T.bin, ch[j], mn, mx, &lof, &cnt);
+        for (int k = 0; k < 3; ++k) {
+            const float e = wmax(hi[k] - lo[k], 1e-30f);
+            v[j][k] = ((mn[k] + mx[k]) - (lo[k] + hi[k])) / e;
+        }
+    }
+    for (int i = 0; i < 8; ++i) slot[i] = WIDE_SLOT_EMPTY;
+    uint32_t placed = 0, taken = 0;
+    for (uint32_t round = 0; round < n; ++round) {
+        int bj = -1, bs = -1;
+        float bsc = 0.0f;
+        for (uint32_t j = 0; j < n; ++j) {
+            if (placed >> j & 1u) continue;
+            for (int sl = 0; sl < 8; ++sl) {
+                if (taken >> sl & 1u) continue;
+                float sc = 0.0f;
+                for (int k = 0; k < 3; ++k) sc += (sl >> k & 1) ? v[j][k] : -v[j][k];
+                if (bj < 0 || sc > bsc) { bj = (int)j; bs = sl; bsc = sc; }
+            }
+        }
+        slot[bs] = ch[bj];
+        placed |= 1u << bj;
+        taken |= 1u << bs;
+    }
+    return true;
+}
+
+// The rebuilt top tree collapsed again into the top region, one CTA, a level of wide nodes at a time: each thread
+// opens a frontier node, the block's prefix sums give its children's nodes and its leaf items their places (a node's
+// interior children consecutive, its leaf items consecutive in slot order), and the children form the next frontier.
+__global__ void __launch_bounds__(TOP_THREADS) k_wide_top(TopCollapse T) {
+    __shared__ uint32_t part_n[TOP_WARPS_C], part_i[TOP_WARPS_C];
+    __shared__ uint32_t next_free, items_next, next_count, failed;
+    const uint32_t tid = threadIdx.x;
+    if (T.top >= T.n_bin || T.cap == 0) {
+        if (tid == 0) atomicOr(T.err, T.err_bit);
+        return;
+    }
+    float mn[3], mx[3];
+    uint32_t lof, cnt;
+    bin_node(T.bin, T.top, mn, mx, &lof, &cnt);
+    float ext = 0.0f;
+    for (int k = 0; k < 3; ++k) ext = wmax(ext, mx[k] - mn[k]);
+    const float tree_pad = isfinite(ext) ? ext * (1.0f / 16384.0f) : 0.0f;
+    if (tid == 0) {
+        T.front[0] = make_uint2(T.top, T.base);
+        next_free = 1;
+        items_next = 0;
+        failed = 0;
+    }
+    __syncthreads();
+    uint2* cur = T.front;
+    uint2* nxt = T.front + T.cap;
+    uint32_t count = 1;
+    for (uint32_t level = 0; count > 0; ++level) {
+        if (level >= 64) {
+            if (tid == 0) atomicOr(T.err, T.err_bit);
+            return;
+        }
+        if (tid == 0) next_count = 0;
+        __syncthreads();
+        for (uint32_t chunk = 0; chunk < count; chunk += TOP_THREADS) {
+            const uint32_t i = chunk + tid;
+            uint32_t slot[8], n_int = 0, n_items = 0;
+            uint2 item = make_uint2(0, 0);
+            bool ok = i < count;
+            if (ok) {
+                item = cur[i];
+                ok = top_slots(T, item.x, slot);
+                if (!ok) failed = 1;
+            }
+            if (ok)
+                for (int s = 0; s < 8; ++s) {
+                    if (slot[s] == WIDE_SLOT_EMPTY) continue;
+                    bin_node(T.bin, slot[s], mn, mx, &lof, &cnt);
+                    if (cnt == 0) n_int++;
+                    else if (cnt > 16) { ok = false; failed = 1; }
+                    else n_items += cnt;
+                }
+            if (!ok) n_int = n_items = 0;
+            uint32_t tot_n, tot_i;
+            const uint32_t pn = block_prefix(n_int, &tot_n, part_n);
+            const uint32_t pi = block_prefix(n_items, &tot_i, part_i);
+            const uint32_t nf = next_free, it0 = items_next, nc = next_count;
+            const bool room = nf + tot_n <= T.cap && it0 + tot_i <= T.n_items;
+            if (ok && room) {
+                const uint32_t child_base = T.base + nf + pn, leaf_base = it0 + pi;
+                float bmin[8][3], bmax[8][3];
+                uint32_t present = 0, imask = 0, counts[8], k = 0, off = 0;
+                for (int s = 0; s < 8; ++s) {
+                    counts[s] = 0;
+                    if (slot[s] == WIDE_SLOT_EMPTY) continue;
+                    bin_node(T.bin, slot[s], bmin[s], bmax[s], &lof, &cnt);
+                    present |= 1u << s;
+                    if (cnt == 0) {
+                        imask |= 1u << s;
+                        nxt[nc + pn + k] = make_uint2(slot[s], child_base + k);
+                        ++k;
+                    } else {
+                        counts[s] = cnt;
+                        for (uint32_t j = 0; j < cnt; ++j) {
+                            const uint32_t rec = lof + j;
+                            const uint64_t r = (uint64_t)T.t_instances + 10ull * rec;
+                            uint32_t bits = 0;
+                            if (r + 10 > T.n_table_vec4) failed = 1;
+                            else bits = T.tables[r + 4].w;
+                            T.items[leaf_base + off++] = rec | ((bits & UNIT_SHADOW) ? WIDE_UNIT_BIT : 0u);
+                        }
+                    }
+                }
+                uint32_t W[20];
+                wide_encode(W, bmin, bmax, present, imask, child_base, n_items ? leaf_base : 0u, counts, tree_pad);
+                put_node(T.wn, item.y, W);
+            }
+            __syncthreads();
+            if (tid == 0) {
+                if (!room) failed = 1;
+                next_free = nf + tot_n;
+                items_next = it0 + tot_i;
+                next_count = nc + tot_n;
+            }
+            __syncthreads();
+            if (failed) {
+                if (tid == 0) atomicOr(T.err, T.err_bit);
+                return;
+            }
+        }
+        count = next_count;
+        uint2* t = cur;
+        cur = nxt;
+        nxt = t;
+        __syncthreads();
+    }
+}
+
 }  // namespace
 
+int WideBvh::refit(const uint32_t* P, const void* bin_nodes, uint64_t n_bin, const void* leaves, uint64_t n_leaf_tris,
+                   const void* tables, uint64_t n_table_vec4, uint32_t* err, uint32_t err_bit, cudaStream_t st) {
+    if (!built) { error = "the wide BVH is not built"; return 1; }
+    cudaError_t e = cudaSuccess;
+    if (!slot_dev) {
+        e = cudaMalloc(&slot_dev, std::max<size_t>(slot_host.size() * 4, 16));
+        if (e == cudaSuccess) e = cudaMalloc(&pad_dev, std::max<size_t>(pad_host.size() * 4, 16));
+        if (e == cudaSuccess && top_cap) e = cudaMalloc(&frontier, 2ull * top_cap * sizeof(uint2));
+        if (e == cudaSuccess) e = cudaMemcpyAsync(slot_dev, slot_host.data(), slot_host.size() * 4, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(pad_dev, pad_host.data(), pad_host.size() * 4, cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) { error = std::string("wide BVH refit: ") + cudaGetErrorString(e); return 1; }
+    }
+    const uint4* bin = static_cast<const uint4*>(bin_nodes);
+    if (n_built) {
+        unsigned g = (unsigned)std::min<uint64_t>((n_built + 255) / 256, 148ull * 8);
+        k_wide_refit<<<g, 256, 0, st>>>(bin, n_bin, slot_dev, pad_dev, nodes, n_built, err, err_bit);
+    }
+    if (v.n_tris) {
+        unsigned g = (unsigned)std::min<uint64_t>((v.n_tris + 255) / 256, 148ull * 8);
+        k_wide_tris<<<g, 256, 0, st>>>(static_cast<const float4*>(leaves), n_leaf_tris, tris, v.n_tris, err, err_bit);
+    }
+    if (top_cap && v.n_units) {
+        TopCollapse T{bin, n_bin, P[P_MOTION_Z], static_cast<const uint4*>(tables), n_table_vec4, P[P_T_INSTANCES],
+                      nodes, n_built, top_cap, units, v.n_units, frontier, err, err_bit};
+        k_wide_top<<<1, TOP_THREADS, 0, st>>>(T);
+        v.top_root = n_built;
+        v.n_nodes = n_built + top_cap;
+    }
+    e = cudaGetLastError();
+    if (e != cudaSuccess) { error = std::string("wide BVH refit: ") + cudaGetErrorString(e); return 1; }
+    return 0;
+}
+
 void WideBvh::release() {
-    if (nodes) cudaFree(nodes);
-    if (tris) cudaFree(tris);
-    if (units) cudaFree(units);
-    if (unit_root) cudaFree(unit_root);
+    for (void* p : {(void*)nodes, (void*)tris, (void*)units, (void*)unit_root, (void*)slot_dev, (void*)pad_dev, (void*)frontier})
+        if (p) cudaFree(p);
     nodes = nullptr;
     tris = nullptr;
     units = nullptr;
     unit_root = nullptr;
+    slot_dev = nullptr;
+    pad_dev = nullptr;
+    frontier = nullptr;
+    slot_host.clear();
+    pad_host.clear();
+    n_built = top_cap = 0;
+    refit_gen = 0;
     built = false;
+}
+
+bool WideBvh::key_matches(const uint32_t* P) const {
+    const uint32_t k[6] = {P[P_MOTION_Z], P[P_MOTION_W], P[P_T_INSTANCES], P[P_W_INDICES], 0, 0};
+    return std::memcmp(k, key, sizeof(k)) == 0;
+}
+
+bool WideBvh::reads_edit(const uint8_t* old_tables, uint64_t offset, const uint8_t* src, uint64_t bytes) const {
+    if (!built || bytes == 0) return false;
+    const uint64_t t_inst = key[2], n_units = key[1], end = offset + bytes;
+    const uint64_t first = t_inst * 16, last = (t_inst + 10 * n_units) * 16;  // the unit records' bytes
+    if (end <= first || offset >= last) return false;
+    const uint64_t r0 = (std::max(offset, first) - first) / 160, r1 = std::min(n_units, (end - first + 159) / 160);
+    // A record's words the build reads: vec4 3's w (the mesh root), vec4 6's x (the first triangle), and of vec4 4's
+    // w (the bits) the shadow bit.
+    const uint64_t words[3] = {3 * 16 + 12, 6 * 16, 4 * 16 + 12};
+    const uint32_t masks[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, UNIT_SHADOW};
+    for (uint64_t r = r0; r < r1; ++r)
+        for (int j = 0; j < 3; ++j) {
+            const uint64_t a = first + 160 * r + words[j];
+            uint8_t now[4];
+            std::memcpy(now, old_tables + a, 4);
+            for (uint64_t b = std::max(a, offset); b < std::min(a + 4, end); ++b) now[b - a] = src[b - offset];
+            uint32_t was, is;
+            std::memcpy(&was, old_tables + a, 4);
+            std::memcpy(&is, now, 4);
+            if ((was ^ is) & masks[j]) return true;
+        }
+    return false;
 }
 
 int WideBvh::ensure(const uint32_t* P, const std::vector<uint8_t>* host, cudaStream_t st) {
@@ -262,7 +584,7 @@ int WideBvh::ensure(const uint32_t* P, const std::vector<uint8_t>* host, cudaStr
                         }
                         return f;
                     };
-                    wr = B.collapse(root, tri_leaf, 16);
+                    wr = B.collapse(root, tri_leaf, 16, false);
                     if (wr == UINT32_MAX) return UINT32_MAX;
                     mesh_root.emplace(key2, wr);
                 } else {
@@ -274,22 +596,25 @@ int WideBvh::ensure(const uint32_t* P, const std::vector<uint8_t>* host, cudaStr
             return first;
         };
         // Collapse the top tree with its unit leaves (mesh trees are collapsed as their units are met).
-        top_root = B.collapse(top, unit_leaf, 16);
+        top_root = B.collapse(top, unit_leaf, 16, true);
         if (top_root == UINT32_MAX) {
             error = B.error;
             return 1;
         }
     }
     uint32_t n_wn = (uint32_t)B.out.size();
+    // Room after the built nodes for the top tree collapsed again after a deformation: at most a node a unit.
+    uint32_t cap = n_units > 0 ? n_units + 1u : 0u;
     cudaError_t e = cudaSuccess;
-    auto upload = [&](void** dst, const void* src, size_t bytes) {
+    auto upload = [&](void** dst, const void* src, size_t bytes, size_t room = 0) {
         if (e != cudaSuccess) return;
-        e = cudaMalloc(dst, std::max<size_t>(bytes, 16));
+        e = cudaMalloc(dst, std::max<size_t>(bytes + room, 16));
         if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess && room) e = cudaMemsetAsync((char*)*dst + bytes, 0, room, st);
     };
     if (top_items.empty()) top_items.push_back(0);
     if (unit_roots.empty()) unit_roots.push_back(0);
-    upload((void**)&nodes, B.out.data(), B.out.size() * sizeof(WNode));
+    upload((void**)&nodes, B.out.data(), B.out.size() * sizeof(WNode), (size_t)cap * sizeof(WNode));
     upload((void**)&tris, wtris.data(), wtris.size() * 4);
     upload((void**)&units, top_items.data(), top_items.size() * 4);
     upload((void**)&unit_root, unit_roots.data(), unit_roots.size() * 4);
@@ -302,6 +627,13 @@ int WideBvh::ensure(const uint32_t* P, const std::vector<uint8_t>* host, cudaStr
     v = WideView{nodes, tris, units, unit_root, top_root, n_wn, (uint32_t)(wtris.size() / 12),
                  (uint32_t)top_items.size(), (uint32_t)unit_roots.size()};
     if (n_units == 0) v.n_units = 0;
+    slot_host = std::move(B.slots);
+    pad_host = std::move(B.pads);
+    slot_host.resize(8ull * n_wn, WIDE_SLOT_EMPTY);
+    pad_host.resize(n_wn, 0.0f);
+    n_built = n_wn;
+    top_cap = cap;
+    refit_gen = 0;
     std::memcpy(key, k, sizeof(k));
     built = true;
     build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();

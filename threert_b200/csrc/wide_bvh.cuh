@@ -13,6 +13,8 @@
 // Leaf items: in a mesh tree, triangles (a copy of the reference's leaf record, three vec4s, with the reference's
 // triangle index in the third's w); in the top tree, unit records (bit 31: the unit casts shadows).
 #pragma once
+#include <cmath>
+#include <cstring>
 #include <string>
 #include <vector>
 
@@ -36,8 +38,71 @@ constexpr int WIDE_SHORT = 8;
 constexpr int WIDE_STACK = 64;
 constexpr uint32_t WIDE_BLOCK = 128;
 
+// std::min / std::max on floats as the host build calls them (the second operand when it compares smaller / larger,
+// else the first), so that the device refit rounds and picks as the host build does.
+__host__ __device__ __forceinline__ float wmin(float a, float b) { return b < a ? b : a; }
+__host__ __device__ __forceinline__ float wmax(float a, float b) { return a < b ? b : a; }
+
+// Writes wide node W (the layout above) over child boxes bmin / bmax by slot: `present` the occupied slots, `imask`
+// the interior ones, counts[i] a leaf slot's items (0 otherwise). The node's own box is the children's, widened by a
+// pad (a 253rd of its extent, 2^-16 of its coordinates' magnitude and the tree's pad) so that the widened boxes stay
+// within 0..255 steps; each axis's step is the power of two that covers the padded extent in 255 steps, and each child
+// box is rounded outwards and widened by a step on every side. Shared by the host build and the device refit.
+__host__ __device__ inline void wide_encode(uint32_t W[20], const float bmin[8][3], const float bmax[8][3],
+                                            uint32_t present, uint32_t imask, uint32_t child_base, uint32_t leaf_base,
+                                            const uint32_t counts[8], float tree_pad) {
+    for (int i = 0; i < 20; ++i) W[i] = 0u;
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int i = 0; i < 8; ++i)
+        if (present >> i & 1u)
+            for (int k = 0; k < 3; ++k) { lo[k] = wmin(lo[k], bmin[i][k]); hi[k] = wmax(hi[k], bmax[i][k]); }
+    float origin[3];
+    int ex[3];
+    for (int k = 0; k < 3; ++k) {
+        const float ext = hi[k] - lo[k];
+        const float mag = wmax(fabsf(lo[k]), fabsf(hi[k]));
+        const float pad = ext * (1.0f / 253.0f) + mag * (1.0f / 65536.0f) + tree_pad + 1e-20f;
+        origin[k] = lo[k] - pad;
+        const float range = (hi[k] + pad) - origin[k];
+        int e;
+        frexpf(range / 255.0f, &e);  // range / 255 < 2^e
+        for (int guard = 0; guard < 512 && ldexpf(255.0f, e) < range; ++guard) ++e;
+        ex[k] = e < -126 ? -126 : (e > 127 ? 127 : e);
+    }
+    uint32_t q[12] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};  // q_lo x, y, z then q_hi x, y, z: 8 bytes each
+    for (int i = 0; i < 8; ++i)
+        for (int k = 0; k < 3; ++k) {
+            uint32_t a = 255u, b = 0u;  // an empty slot: q_lo > q_hi
+            if (present >> i & 1u) {
+                const double s = (double)ldexpf(1.0f, ex[k]);
+                const double fa = floor((double)(bmin[i][k] - origin[k]) / s) - 1.0;
+                const double fb = ceil((double)(bmax[i][k] - origin[k]) / s) + 1.0;
+                const double ca = fa < 255.0 ? fa : 255.0, cb = fb < 255.0 ? fb : 255.0;
+                a = (uint32_t)(0.0 < ca ? ca : 0.0);
+                b = (uint32_t)(0.0 < cb ? cb : 0.0);
+            }
+            q[2 * k + (i >> 2)] |= a << (8 * (i & 3));
+            q[6 + 2 * k + (i >> 2)] |= b << (8 * (i & 3));
+        }
+    for (int k = 0; k < 3; ++k) {
+        float o = origin[k];
+        uint32_t u;
+        memcpy(&u, &o, 4);
+        W[k] = u;
+    }
+    W[3] = (uint32_t)(ex[0] + 127) | ((uint32_t)(ex[1] + 127) << 8) | ((uint32_t)(ex[2] + 127) << 16) | (imask << 24);
+    W[4] = child_base;
+    W[5] = leaf_base;
+    for (int i = 0; i < 8; ++i) W[6 + (i >> 2)] |= (counts[i] & 0xffu) << (8 * (i & 3));
+    for (int j = 0; j < 12; ++j) W[8 + j] = q[j];
+}
+
+// A slot of the build's record: no child, or (for every slot of a node of the units' top tree) not refit in place:
+// the top tree is built again by each deformation, so its wide nodes are collapsed again instead.
+constexpr uint32_t WIDE_SLOT_EMPTY = 0xFFFFFFFFu, WIDE_SLOT_TOP = 0xFFFFFFFEu;
+
 struct WideBvh {
-    uint4* nodes = nullptr;
+    uint4* nodes = nullptr;  // the built nodes, then room for a collapsed-again top tree
     float4* tris = nullptr;
     uint32_t* units = nullptr;
     uint32_t* unit_root = nullptr;
@@ -45,12 +110,33 @@ struct WideBvh {
     bool built = false;
     uint32_t key[6] = {0, 0, 0, 0, 0, 0};  // the Params words the build read (it is redone when they change)
     double build_ms = 0.0;
+    // What a refit needs: for each built node the binary node each slot was collapsed from (8 a node) and its tree's
+    // pad, on the host from the build, on the device from the first refit on.
+    std::vector<uint32_t> slot_host;
+    std::vector<float> pad_host;
+    uint32_t* slot_dev = nullptr;
+    float* pad_dev = nullptr;
+    uint2* frontier = nullptr;   // the top collapse's two frontiers of (binary node, wide node), top_cap each
+    uint32_t n_built = 0;        // nodes of the build; the top region starts here
+    uint32_t top_cap = 0;        // the top region's nodes: a collapsed top tree has at most one a unit
+    uint64_t refit_gen = 0;      // the deformation the wide trees were last brought to (0: the scene as uploaded)
     bool ready() const { return built; }
     WideView view() const { return v; }
     std::string error;
     // Builds (or keeps) the wide trees for the scene as `params` lays it out, from host copies of the scene's nodes,
     // leaves and tables (host[2], host[1], host[3]). 0, or 1 with `error` set.
     int ensure(const uint32_t* params, const std::vector<uint8_t>* host, cudaStream_t st);
+    // Brings built wide trees to the scene's device buffers after a deformation (units.rs:251-275 refit, then the top
+    // tree's collapse): every mesh tree's node quantised again over its binary children's refit boxes, the triangle
+    // copies gathered again from the leaves, the rebuilt top tree collapsed again into the top region. Asynchronous on
+    // `st`; an index out of its buffer sets err_bit in *err (the kernels skip the access). 0, or 1 with `error` set.
+    int refit(const uint32_t* params, const void* bin_nodes, uint64_t n_bin, const void* leaves, uint64_t n_leaf_tris,
+              const void* tables, uint64_t n_table_vec4, uint32_t* err, uint32_t err_bit, cudaStream_t st);
+    // Whether `params` lays the scene out as the build read it.
+    bool key_matches(const uint32_t* params) const;
+    // Whether writing src[0, bytes) at byte `offset` of the tables (old: the host copy before it) changes a word the
+    // build read: a unit record's mesh root, first triangle or bits.
+    bool reads_edit(const uint8_t* old_tables, uint64_t offset, const uint8_t* src, uint64_t bytes) const;
     void release();
     void invalidate() { built = false; }
 };
