@@ -677,7 +677,7 @@ def run_extras(gpu, S, P, frame: int, args, flags: int) -> dict:
     de = lambda img: metrics.delta_e(truth, img)["mean"]
     plain = {}
     for spp in (1, 4, 64):
-        acc, st = S.render_raw(params, spp, flags=flags)
+        acc, st = S.render_timed(params, spp, flags=flags)
         plain[spp] = {"delta_e": de(frame_of(acc, WIDTH, HEIGHT, spp).color), "ms": float(st.device_ms)}
     # The learned denoiser, trained on the device by the library's own kernels.
     t1 = time.perf_counter()
@@ -689,17 +689,18 @@ def run_extras(gpu, S, P, frame: int, args, flags: int) -> dict:
     losses = DT.train(net, F, T, args.extras_train_steps, batch=16, lr=1e-3, seed=0)
     t_train = time.perf_counter() - t1
     del F, T
-    acc, st = S.render_raw(params, 4, flags=flags | N.TRT_RENDER_DEPTH)
+    acc, st = S.render_timed(params, 4, flags=flags | N.TRT_RENDER_DEPTH)
     den, ms_net = net.denoise(S)
     at, ms_at = S.denoise_atrous(4)
     ms_den = float(st.device_ms) + ms_net
     # The plain path at the denoised frame's device time: as many samples as that time renders (a sample's time from
     # the 64-sample render, where the per-call overhead is spread thin).
     spp_eq = max(1, int(round(ms_den / max(plain[64]["ms"] / 64.0, 1e-6))))
-    acc_eq, st_eq = S.render_raw(params, spp_eq, flags=flags)
+    acc_eq, st_eq = S.render_timed(params, spp_eq, flags=flags)
     learned = {"delta_e": de(den), "ms": ms_den, "network_ms": ms_net}
     out["delta_e"] = {
         "truth_spp": TRUTH_SPP, "frame": frame, "metric": "mean ΔE (CIE76) of 8-bit sRGB at a fixed exposure",
+        "ms": "device time of the render (and the filter), its accum left on the device",
         "plain_1spp": plain[1], "plain_4spp": plain[4], "plain_64spp": plain[64],
         "atrous_4spp": {"delta_e": de(at), "ms": float(st.device_ms) + ms_at},
         "learned_4spp": learned,

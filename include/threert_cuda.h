@@ -325,6 +325,14 @@ int trt_server_submit(trt_server* server, trt_scene* scene, const uint32_t param
  * denoiser, above denoise_max_spp samples, or at a size the network does not take. */
 int trt_server_submit_rgb(trt_server* server, trt_scene* scene, const uint32_t params[TRT_PARAMS_WORDS], uint32_t spp,
                           float* accum_host, float* rgb_host, uint64_t* id);
+/* The server's clock: ms since it was created (the clock of trt_request_done's times). */
+int trt_server_clock(trt_server* server, double* now_ms);
+/* trt_server_submit_rgb (accum_host, rgb_host: either may be NULL, not both; rgb_host needs the denoiser) for a request
+ * that arrives at at_ms on the server's clock: the worker admits it no earlier, and its submit_ms is at_ms, so that an
+ * open-loop stream of arrivals is handed over at once, with no host thread timing it. A time not after now (or
+ * negative: now) arrives at once. No counterpart in the reference, whose serve loop reads jobs as they come. */
+int trt_server_submit_at(trt_server* server, trt_scene* scene, const uint32_t params[TRT_PARAMS_WORDS], uint32_t spp,
+                         float* accum_host, float* rgb_host, double at_ms, uint64_t* id);
 /* Up to cap finished requests since the last call, waiting up to wait_ms for one if none is ready. */
 int trt_server_poll(trt_server* server, trt_request_done* done, uint32_t cap, uint32_t* n, uint32_t wait_ms);
 int trt_server_stats_get(trt_server* server, trt_server_stats* out);

@@ -71,6 +71,30 @@ def test_requests_that_arrive_during_a_run_join_it(gpu, resident):
         assert np.array_equal(r.accum, S[r.scene].render_raw(r.params, r.spp)[0])
 
 
+def test_scheduled_arrivals_wait_for_their_time(gpu, resident):
+    """trt_server_submit_at: requests handed over at once with arrival times 40 ms apart are started no earlier than
+    their arrival (their submit_ms), in arrival order, and give the accum each gets alone."""
+    Ps, S = resident
+    reqs = the_mix(Ps, seed=9)[:6]
+    srv = Server(gpu, wave_slots=16384, max_active=4)
+    try:
+        t = srv.clock() + 20.0
+        at = [t + 40.0 * i for i in range(len(reqs))]
+        for r, a in zip(reqs[::-1], at[::-1]):  # handed over last-first: the arrival times set the order
+            srv.submit(S[r.scene], r, at_ms=a)
+        done = []
+        while len(done) < len(reqs):
+            done += srv.poll(wait_ms=50)
+    finally:
+        srv.close()
+    for r, a in zip(reqs, at):
+        assert r.done["status"] == 0 and r.done["submit_ms"] == a
+        assert r.done["start_ms"] >= a, (r.done["start_ms"], a)
+        assert np.array_equal(r.accum, S[r.scene].render_raw(r.params, r.spp)[0])
+    starts = [r.done["start_ms"] for r in reqs]
+    assert starts == sorted(starts)
+
+
 def test_what_cannot_be_served_is_refused(gpu, resident):
     Ps, S = resident
     srv = Server(gpu, wave_slots=4096)

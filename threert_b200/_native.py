@@ -207,6 +207,8 @@ SIGNATURES = [
     ("trt_server_destroy", None, [C.c_void_p]),
     ("trt_server_submit", C.c_int, [C.c_void_p, C.c_void_p, P(u32), u32, P(f32), P(u64)]),
     ("trt_server_submit_rgb", C.c_int, [C.c_void_p, C.c_void_p, P(u32), u32, P(f32), P(f32), P(u64)]),
+    ("trt_server_clock", C.c_int, [C.c_void_p, P(C.c_double)]),
+    ("trt_server_submit_at", C.c_int, [C.c_void_p, C.c_void_p, P(u32), u32, P(f32), P(f32), C.c_double, P(u64)]),
     ("trt_server_poll", C.c_int, [C.c_void_p, P(RequestDone), u32, P(u32), u32]),
     ("trt_server_stats_get", C.c_int, [C.c_void_p, P(ServerStats)]),
     ("trt_unet_create", C.c_int, [C.c_int, u32, u32, u32, P(C.c_void_p)]),

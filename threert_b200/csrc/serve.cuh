@@ -56,6 +56,7 @@ struct trt_server {
     std::condition_variable cv_work, cv_done;
     bool stop = false;
     std::deque<trt::ServeRequest*> pending;
+    std::multimap<double, trt::ServeRequest*> scheduled;  // requests that arrive later (trt_server_submit_at), by time
     std::vector<trt::ServeRequest*> active;
     std::vector<trt_request_done> done;
     std::vector<trt::ServeRequest*> copying;  // read-backs queued on the copy stream, not yet seen complete
@@ -91,8 +92,16 @@ float4* serve_take_accum(trt_server* s, uint64_t bytes) {
     return p;
 }
 
-// Moves waiting requests into the active set while there is room (with the lock held).
+// Moves waiting requests into the active set while there is room (with the lock held); scheduled requests whose
+// time has come join the waiting ones first, in arrival order.
 void serve_admit(trt_server* s) {
+    if (!s->scheduled.empty()) {
+        const double now = serve_now(s);
+        while (!s->scheduled.empty() && s->scheduled.begin()->first <= now) {
+            s->pending.push_back(s->scheduled.begin()->second);
+            s->scheduled.erase(s->scheduled.begin());
+        }
+    }
     while (!s->pending.empty() && s->active.size() < s->opt.max_active) {
         ServeRequest* r = s->pending.front();
         float4* a = serve_take_accum(s, r->accum_bytes);
@@ -311,9 +320,12 @@ void serve_loop(trt_server* s) {
         bool have = false;
         for (ServeRequest* r : s->active) have |= r->issued < r->spp;
         if (have) continue;
-        if (s->stop && s->active.empty() && s->pending.empty()) break;
-        // (A request that waits for device memory is retried when a request finishes or 1 ms passes.)
-        s->cv_work.wait_for(lk, std::chrono::milliseconds(1));
+        if (s->stop && s->active.empty() && s->pending.empty() && s->scheduled.empty()) break;
+        // (A request that waits for device memory is retried when a request finishes or 1 ms passes; the wait ends
+        // early at the next scheduled arrival.)
+        double wait_ms = 1.0;
+        if (!s->scheduled.empty()) wait_ms = std::min(wait_ms, s->scheduled.begin()->first - serve_now(s));
+        if (wait_ms > 0.0) s->cv_work.wait_for(lk, std::chrono::microseconds((int64_t)(wait_ms * 1000.0) + 1));
     }
     for (auto& st : steps) {
         cudaEventDestroy(st.t0);
@@ -382,6 +394,8 @@ void trt_server_destroy(trt_server* s) {
             s->pending.pop_front();
             serve_finish(s, r, TRT_EINVAL);
         }
+        for (auto& pr : s->scheduled) serve_finish(s, pr.second, TRT_EINVAL);
+        s->scheduled.clear();
     }
     s->cv_work.notify_all();
     if (s->worker.joinable()) s->worker.join();
@@ -410,7 +424,18 @@ int trt_server_submit(trt_server* s, trt_scene* scene, const uint32_t params[TRT
 
 int trt_server_submit_rgb(trt_server* s, trt_scene* scene, const uint32_t params[TRT_PARAMS_WORDS], uint32_t spp,
                           float* accum_host, float* rgb_host, uint64_t* id) {
-    if (!s || !scene || !params || (!accum_host && !rgb_host) || spp == 0) return TRT_EINVAL;
+    return trt_server_submit_at(s, scene, params, spp, accum_host, rgb_host, -1.0, id);
+}
+
+int trt_server_clock(trt_server* s, double* now_ms) {
+    if (!s || !now_ms) return TRT_EINVAL;
+    *now_ms = serve_now(s);
+    return TRT_OK;
+}
+
+int trt_server_submit_at(trt_server* s, trt_scene* scene, const uint32_t params[TRT_PARAMS_WORDS], uint32_t spp,
+                         float* accum_host, float* rgb_host, double at_ms, uint64_t* id) {
+    if (!s || !scene || !params || (!accum_host && !rgb_host) || spp == 0 || at_ms != at_ms) return TRT_EINVAL;
     if (rgb_host) {
         uint32_t w = params[P_SIZE], h = params[P_SIZE + 1];
         uint32_t most = s->opt.denoise_max_spp ? s->opt.denoise_max_spp : 4u;
@@ -442,8 +467,14 @@ int trt_server_submit_rgb(trt_server* s, trt_scene* scene, const uint32_t params
     {
         std::lock_guard<std::mutex> lk(s->mu);
         r->id = s->next_id++;
-        r->t_submit = serve_now(s);
-        s->pending.push_back(r);
+        const double now = serve_now(s);
+        if (at_ms > now) {
+            r->t_submit = at_ms;
+            s->scheduled.emplace(at_ms, r);
+        } else {
+            r->t_submit = at_ms >= 0.0 ? at_ms : now;
+            s->pending.push_back(r);
+        }
         if (id) *id = r->id;
     }
     s->cv_work.notify_all();
@@ -474,7 +505,7 @@ int trt_server_stats_get(trt_server* s, trt_server_stats* out) {
     out->closest_rays = t[T_CLOSEST];
     out->shadow_rays = t[T_SHADOW];
     out->active = (uint32_t)s->active.size();
-    out->pending = (uint32_t)s->pending.size();
+    out->pending = (uint32_t)(s->pending.size() + s->scheduled.size());
     return TRT_OK;
 }
 

@@ -95,13 +95,13 @@ def judge(gpu: Gpu, net: UNet, seeds, width: int, height: int, spp_net: int, spp
             truth_acc, _ = S.render_raw(prep.params_with(params, seed=0xACE), spp_truth)
             truth = frame_of(truth_acc, width, height, spp_truth).color
             r = {}
-            acc, st = S.render_raw(prep.params_with(params, seed=k + 1), spp_net, flags=N.TRT_RENDER_DEPTH)
+            acc, st = S.render_timed(prep.params_with(params, seed=k + 1), spp_net, flags=N.TRT_RENDER_DEPTH)
             den, ms_net = net.denoise(S)
             r["net"] = (metrics.delta_e(truth, den)["mean"], st.device_ms + ms_net)
             at, ms_at = S.denoise_atrous(4)
             r["atrous_low"] = (metrics.delta_e(truth, at)["mean"], st.device_ms + ms_at)
             r["plain_low"] = (metrics.delta_e(truth, frame_of(acc, width, height, spp_net).color)["mean"], st.device_ms)
-            acc, st = S.render_raw(prep.params_with(params, seed=k + 1), spp_plain)
+            acc, st = S.render_timed(prep.params_with(params, seed=k + 1), spp_plain)
             r["plain_high"] = (metrics.delta_e(truth, frame_of(acc, width, height, spp_plain).color)["mean"], st.device_ms)
             at, ms_at = S.denoise_atrous(4)
             r["atrous_high"] = (metrics.delta_e(truth, at)["mean"], st.device_ms + ms_at)

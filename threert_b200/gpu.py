@@ -93,6 +93,19 @@ class Scene:
         self.gpu._check(rc, "trt_render")
         return acc, st
 
+    def read_accum(self, out: np.ndarray | None = None) -> np.ndarray:
+        """The accum of the last render (trt_accum_read), as (w*h, 20) float32."""
+        w, h = self.last_size
+        acc = out if out is not None else np.empty((w * h, N.PIXEL_FLOATS), np.float32)
+        self.gpu._check(N.lib().trt_accum_read(self.handle, acc.ctypes.data_as(C.POINTER(C.c_float)), acc.nbytes),
+                        "trt_accum_read")
+        return acc
+
+    def render_timed(self, params: np.ndarray, spp: int, flags: int = 0):
+        """render_raw whose Stats' device_ms is the render's alone (the accum read back after the timed call)."""
+        _, st = self.render_raw(params, spp, flags=flags, read=False)
+        return self.read_accum(), st
+
     def accum_copy(self, dst_device_ptr: int, nbytes: int):
         """trt_accum_copy: the accum into caller-owned device memory (e.g. a torch tensor's data_ptr()), waited for."""
         self.gpu._check(N.lib().trt_accum_copy(self.handle, C.c_void_p(dst_device_ptr), nbytes), "trt_accum_copy")

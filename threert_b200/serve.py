@@ -8,7 +8,6 @@ others run joins the next wave. Each result is the accum `Scene.render_raw` make
 from __future__ import annotations
 
 import ctypes as C
-import threading
 import time
 from dataclasses import dataclass, field
 
@@ -78,21 +77,26 @@ class Server:
                 self.pool.setdefault(a.shape, []).append(a)
                 setattr(req, name, None)
 
-    def submit(self, scene: Scene, req: Request) -> int:
+    def clock(self) -> float:
+        """The server's clock (ms since it was created), the one request times are on."""
+        now = C.c_double()
+        self.gpu._check(N.lib().trt_server_clock(self.handle, C.byref(now)), "trt_server_clock")
+        return now.value
+
+    def submit(self, scene: Scene, req: Request, at_ms: float | None = None) -> int:
+        """Queues the request now, or (at_ms) for its arrival at that time on the server's clock."""
         p = np.ascontiguousarray(req.params, dtype=np.uint32)
         px = int(p[16]) * int(p[17])
         rid = C.c_uint64()
         fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float)) if a is not None else None
         if req.denoise:
             req.accum, req.rgb = None, self._buffer(px, 3)
-            self.gpu._check(N.lib().trt_server_submit_rgb(self.handle, scene.handle,
-                                                          p.ctypes.data_as(C.POINTER(C.c_uint32)), req.spp, None,
-                                                          fp(req.rgb), C.byref(rid)), "trt_server_submit_rgb")
         else:
-            req.accum = self._buffer(px)
-            self.gpu._check(N.lib().trt_server_submit(self.handle, scene.handle,
-                                                      p.ctypes.data_as(C.POINTER(C.c_uint32)), req.spp, fp(req.accum),
-                                                      C.byref(rid)), "trt_server_submit")
+            req.accum, req.rgb = self._buffer(px), None
+        self.gpu._check(N.lib().trt_server_submit_at(self.handle, scene.handle,
+                                                     p.ctypes.data_as(C.POINTER(C.c_uint32)), req.spp, fp(req.accum),
+                                                     fp(req.rgb), -1.0 if at_ms is None else float(at_ms),
+                                                     C.byref(rid)), "trt_server_submit_at")
         req.id = rid.value
         self.live[req.id] = req
         return req.id
@@ -156,40 +160,25 @@ def mix_requests(bases: list[np.ndarray], n: int, seed: int = 0, resolutions=RES
 
 
 def run_stream(server: Server, scenes: list[Scene], requests: list[Request], rate: float, seed: int = 1,
-               timeout_s: float = 600.0, keep: bool = True) -> dict:
-    """Submits the requests at Poisson arrival times of `rate` a second (open loop, from a thread of its own) and
-    waits for every one: latencies (done - submit, ms), the span from the first submit to the last completion, rays."""
+               timeout_s: float = 600.0, keep: bool = True, lead_ms: float = 5.0) -> dict:
+    """Hands the requests to the server at once with Poisson arrival times of `rate` a second on its clock, the first
+    `lead_ms` from now (an open loop the library's worker paces: no host thread times the arrivals), and waits for
+    every one: latencies (done - arrival, ms), the span from the first arrival to the last completion, rays."""
     rng = np.random.default_rng(seed)
     gaps = rng.exponential(1.0 / rate, len(requests)) if rate > 0 else np.zeros(len(requests))
     server.reserve(requests)
     before = server.stats()
     done: list[Request] = []
-    errors: list[BaseException] = []
-
-    def feed():
-        try:
-            t = time.perf_counter()
-            for r, g in zip(requests, gaps):
-                t += g
-                dt = t - time.perf_counter()
-                if dt > 0:
-                    time.sleep(dt)
-                server.submit(scenes[r.scene], r)
-        except BaseException as e:  # surfaced below
-            errors.append(e)
-
-    th = threading.Thread(target=feed, daemon=True)
     t0 = time.perf_counter()
-    th.start()
-    while len(done) < len(requests) and time.perf_counter() - t0 < timeout_s and not errors:
+    at = server.clock() + lead_ms + np.cumsum(gaps) * 1e3
+    for r, a in zip(requests, at):
+        server.submit(scenes[r.scene], r, at_ms=float(a))
+    while len(done) < len(requests) and time.perf_counter() - t0 < timeout_s:
         got = server.poll(wait_ms=20)
         if not keep:
             for r in got:
                 server.release(r)
         done += got
-    th.join()
-    if errors:
-        raise errors[0]
     if len(done) < len(requests):
         raise TimeoutError(f"{len(done)} of {len(requests)} requests done in {timeout_s} s")
     after = server.stats()
