@@ -90,6 +90,37 @@ def test_forward_on_wide_rows_matches_the_oracle():
     wide.close()
 
 
+def test_halo_row_tiles_match_the_oracle():
+    """Images at least 128 wide: the full-resolution layers that read one 32-channel block (and the second level's
+    first, at 256) run the halo kernel, a row tile of 128 pixels read once with its halo and the nine taps as shifted
+    descriptors into it; at 200 the second tile of each row is ragged (72 pixels inside the image). The forward as
+    tight as the 2-D tiles' (activations rounded to bf16 where the device stores them), and every layer's gradient,
+    whose input gradient runs the same kernel with the flipped weights."""
+    wide = unet.UNet(0, max_batch=1, max_h=24, max_w=256)
+    try:
+        for seed, w in ((12, 200), (13, 256)):
+            p, feats, tgt = case(seed=seed, b=1, h=24, w=w)
+            wide.set_params(p)
+            got, _ = wide.forward(feats)
+            want, _ = R.forward(R.unpack(bf16(p).astype(np.float64)), bf16(feats).astype(np.float64), act=R.bf16_round)
+            err = np.linalg.norm(got - want) / np.linalg.norm(want)
+            worst = np.abs(got - want).max() / np.abs(want).max()
+            print(f"halo forward 1x24x{w}: relative error {err:.2e}, worst output {worst:.2e}")
+            assert err < 1e-2 and worst < 0.02, (w, err, worst)
+            loss, g, _ = wide.step(feats, tgt, update=False, grads=True)
+            ref_loss, G, _ = R.loss_and_grads(R.unpack(bf16(p).astype(np.float64)), bf16(feats).astype(np.float64), tgt)
+            assert abs(loss / ref_loss - 1) < 0.02
+            gp = R.unpack(g.astype(np.float64))
+            for name in R.NAMES:
+                for k in range(2):
+                    a, b = gp[name][k].ravel(), G[name][k].ravel()
+                    cos = a @ b / (np.linalg.norm(a) * np.linalg.norm(b) + 1e-30)
+                    ratio = np.linalg.norm(a) / (np.linalg.norm(b) + 1e-30)
+                    assert cos > 0.98 and abs(ratio - 1) < 0.1, (w, name, k, cos, ratio)
+    finally:
+        wide.close()
+
+
 @pytest.mark.parametrize("b,h,w", [(2, 16, 16), (4, 64, 64)])
 def test_every_layers_gradient_matches_the_oracle(net, b, h, w):
     # 2 x 16 x 16: a 128-pixel tile a CTA; 4 x 64 x 64: the weight gradient's CTAs take runs of two to six tiles at
@@ -146,15 +177,16 @@ def test_inference_on_the_device_is_the_host_path(gpu, net):
     S.close()
 
 
-def test_a_withheld_copy_ends_the_forward_with_an_error_and_the_network_stays_usable():
-    """The convolution's pipeline waits are bounded (about a second): a copy that never lands (one activation box
+@pytest.mark.parametrize("h,w", [(64, 64), (32, 256)])  # the first layer on 2-D tiles; on halo row tiles
+def test_a_withheld_copy_ends_the_forward_with_an_error_and_the_network_stays_usable(h, w):
+    """The convolution's pipeline waits are bounded (about a second): a copy that never lands (one activation stage
     withheld by trt_unet_hold_next_load) ends its wait, the call reports it (TRT_ECUDA, "gave up") instead of hanging,
     and the next forward on the same network gives the same output as before."""
     from threert_b200 import RenderError
-    n = unet.UNet(0, max_batch=1, max_h=64, max_w=64)
+    n = unet.UNet(0, max_batch=1, max_h=h, max_w=w)
     try:
         n.set_params(unet.init_params(3))
-        f = np.random.default_rng(9).normal(0, 1, (1, 64, 64, unet.N_FEAT)).astype(np.float32)
+        f = np.random.default_rng(9).normal(0, 1, (1, h, w, unet.N_FEAT)).astype(np.float32)
         want, _ = n.forward(f)
         n.hold_next_load()
         with pytest.raises(RenderError, match="gave up"):

@@ -68,6 +68,15 @@ struct Conv {
 constexpr uint32_t TS = 5;                  // pipeline stages (82 KB of shared memory: two CTAs an SM)
 constexpr uint32_t A_STAGE = 128u * 32u * 2u, B_STAGE = 128u * 32u * 2u;
 constexpr uint32_t CONV_SMEM = TS * (A_STAGE + B_STAGE) + 256u + 1024u;  // + room to align the stages to 1 KB
+// The halo variant (a row tile of 128 pixels read once with its halo, the taps as shifted descriptors): a stage is a
+// 32-channel block as four planes of 8 channels x 3 rows x 130 pixels (16 bytes a pixel, each plane padded to a
+// multiple of 128 bytes), the weights resident.
+constexpr uint32_t HALO_W = 130u, HALO_ROWS = 3u;
+constexpr uint32_t HALO_PLANE = (HALO_ROWS * HALO_W * 16u + 127u) / 128u * 128u;  // 6,272 bytes
+constexpr uint32_t HALO_STAGE = 4u * HALO_PLANE, HALO_TS = 3u;
+constexpr uint32_t HALO_W_OFF = (HALO_TS * HALO_STAGE + 1023u) / 1024u * 1024u;  // the resident weights, 1 KB aligned
+constexpr uint32_t HALO_WEIGHTS = 9u * 64u * 64u;                                // nine taps x 64 outputs x 32 inputs
+constexpr uint32_t CONV_SMEM_HALO = HALO_W_OFF + HALO_WEIGHTS + 256u + 1024u;
 constexpr uint32_t CONV_EPI_THREADS = 128u, CONV_THREADS = 64u + CONV_EPI_THREADS;  // loader, MMA, 4 epilogue warps
 constexpr uint32_t CONV_CTAS_PER_SM = 2u;
 
@@ -128,6 +137,13 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const void* map, int c
 __device__ __forceinline__ uint64_t umma_desc_sw64(uint32_t saddr, uint32_t sbo) {
     return (uint64_t)((saddr & 0x3FFFFu) >> 4) | (1ull << 16) | ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) |
            (1ull << 46) | (4ull << 61);
+}
+// The canonical K-major shared-memory matrix without swizzle: core matrices of 8 rows x 16 bytes, rows 16 bytes
+// apart, `sbo` bytes between core matrices along M / N and `lbo` bytes between the two along K (8 elements each);
+// descriptor version 1, layout type 0. The start may be any 16-byte boundary.
+__device__ __forceinline__ uint64_t umma_desc_plain(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 // kind::f16 instruction descriptor: f32 accumulator, bf16 A and B, both K-major, M x N.
 __host__ __device__ constexpr uint32_t umma_idesc(uint32_t M, uint32_t N) {
@@ -192,31 +208,40 @@ __device__ __forceinline__ void conv_store16(const Conv& a, uint64_t p, uint32_t
     }
 }
 
+// HALO: tiles of 128 x 1 pixels, the weights resident (one 32-channel block, one output tile of 64), and a stage is
+// the tile's activations with their halo (four TMA boxes of 8 channels x 130 pixels x 3 rows, no swizzle) from which
+// the nine taps' A operands are read by descriptors shifted (dy x 130 + dx) rows of 16 bytes: one load a tile instead
+// of nine. The taps' MMAs read rows [dy x 130 + dx, + 128) of each plane, inside the box.
+template <bool HALO>
 __global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ CUtensorMap xmap,
                                                        const __grid_constant__ CUtensorMap wmap, Conv a) {
+    constexpr uint32_t NS = HALO ? HALO_TS : TS;  // stages
+    constexpr uint32_t A_BYTES = HALO ? HALO_STAGE : A_STAGE;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
     const uint32_t sraw = smem_addr(smem_raw), sbase = (sraw + 1023u) & ~1023u;
     uint8_t* smem = smem_raw + (sbase - sraw);
-    const uint32_t sA = sbase, sB = sbase + TS * A_STAGE, sBar = sbase + TS * (A_STAGE + B_STAGE);
-    // barriers: full[TS], empty[TS] (the stages), acc_full[2], acc_empty[2] (the accumulators), mma_done (every MMA
+    constexpr uint32_t B_OFF = HALO ? HALO_W_OFF : TS * A_STAGE;
+    constexpr uint32_t BAR_OFF = HALO ? HALO_W_OFF + HALO_WEIGHTS : TS * (A_STAGE + B_STAGE);
+    const uint32_t sA = sbase, sB = sbase + B_OFF, sBar = sbase + BAR_OFF;
+    // barriers: full[NS], empty[NS] (the stages), acc_full[2], acc_empty[2] (the accumulators), mma_done (every MMA
     // issued), wfull (the resident weights); the tensor-memory address, the abort word and the counts of stages issued
     // and consumed after them
     auto full = [&](uint32_t s) { return sBar + 8u * s; };
-    auto empty = [&](uint32_t s) { return sBar + 8u * (TS + s); };
-    auto acc_full = [&](uint32_t i) { return sBar + 8u * (2u * TS + i); };
-    auto acc_empty = [&](uint32_t i) { return sBar + 8u * (2u * TS + 2u + i); };
-    const uint32_t mma_done = sBar + 8u * (2u * TS + 4u), wfull = sBar + 8u * (2u * TS + 5u);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + TS * (A_STAGE + B_STAGE) + 8u * (2u * TS + 6u));
+    auto empty = [&](uint32_t s) { return sBar + 8u * (NS + s); };
+    auto acc_full = [&](uint32_t i) { return sBar + 8u * (2u * NS + i); };
+    auto acc_empty = [&](uint32_t i) { return sBar + 8u * (2u * NS + 2u + i); };
+    const uint32_t mma_done = sBar + 8u * (2u * NS + 4u), wfull = sBar + 8u * (2u * NS + 5u);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + BAR_OFF + 8u * (2u * NS + 6u));
     volatile uint32_t* abort_flag = tslot + 1;
     volatile uint32_t* counts = tslot + 2;
     const uint32_t ncols = 2u * a.nt;  // two accumulators of nt columns: 128 or 256
     const uint32_t per_img = a.tiles_x * a.tiles_y, n_ntiles = a.co_pad / a.nt;
     const uint32_t tiles = a.B * per_img * n_ntiles;
-    const uint32_t kc = a.cin / 32u, nk = 9u * kc;
+    const uint32_t kc = a.cin / 32u, nk = HALO ? kc : 9u * kc;
 
     if (tid == 0) {
-        for (uint32_t s = 0; s < TS; ++s) {
+        for (uint32_t s = 0; s < NS; ++s) {
             mbar_init(full(s), 1);
             mbar_init(empty(s), 1);
         }
@@ -267,14 +292,24 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ C
                 int x0, y0;
                 tile_of(t, b, x0, y0, n0);
                 for (uint32_t k = 0; k < nk; ++k, ++it) {
-                    const uint32_t s = it % TS;
-                    if (it >= TS && !(ok = mbar_wait(empty(s), ((it / TS) - 1u) & 1u, a.err, abort_flag))) break;
-                    mbar_expect_tx(full(s), A_STAGE + (a.resident ? 0u : a.nt * 64u));
-                    const uint32_t tap = k / kc, c0 = (k % kc) * 32u;
-                    const int dy = (int)(tap / 3u) - 1, dx = (int)(tap % 3u) - 1;
-                    if (!(a.hold && blockIdx.x == 0 && it == 0))
-                        tma_load_4d(sA + s * A_STAGE, &xmap, (int)(a.x_off + c0), x0 + dx, y0 + dy, (int)b, full(s));
-                    if (!a.resident) tma_load_3d(sB + s * B_STAGE, &wmap, (int)c0, (int)n0, (int)tap, full(s));
+                    const uint32_t s = it % NS;
+                    if (it >= NS && !(ok = mbar_wait(empty(s), ((it / NS) - 1u) & 1u, a.err, abort_flag))) break;
+                    const bool withhold = a.hold && blockIdx.x == 0 && it == 0;
+                    if constexpr (HALO) {
+                        // the tile's rows y0 - 1 .. y0 + 1, pixels x0 - 1 .. x0 + 128, one box a plane of 8 channels
+                        mbar_expect_tx(full(s), 4u * HALO_ROWS * HALO_W * 16u);
+                        if (!withhold)
+                            for (uint32_t pl = 0; pl < 4u; ++pl)
+                                tma_load_4d(sA + s * A_BYTES + pl * HALO_PLANE, &xmap, (int)(a.x_off + k * 32u + pl * 8u),
+                                            x0 - 1, y0 - 1, (int)b, full(s));
+                    } else {
+                        mbar_expect_tx(full(s), A_STAGE + (a.resident ? 0u : a.nt * 64u));
+                        const uint32_t tap = k / kc, c0 = (k % kc) * 32u;
+                        const int dy = (int)(tap / 3u) - 1, dx = (int)(tap % 3u) - 1;
+                        if (!withhold)
+                            tma_load_4d(sA + s * A_STAGE, &xmap, (int)(a.x_off + c0), x0 + dx, y0 + dy, (int)b, full(s));
+                        if (!a.resident) tma_load_3d(sB + s * B_STAGE, &wmap, (int)c0, (int)n0, (int)tap, full(s));
+                    }
                 }
             }
             counts[0] = it;
@@ -291,16 +326,30 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ C
                 tc_fence_after();
                 const uint32_t d = tmem + acc * a.nt;
                 for (uint32_t k = 0; k < nk; ++k, ++it) {
-                    const uint32_t s = it % TS;
-                    if (!(ok = mbar_wait(full(s), (it / TS) & 1u, a.err, abort_flag))) break;
+                    const uint32_t s = it % NS;
+                    if (!(ok = mbar_wait(full(s), (it / NS) & 1u, a.err, abort_flag))) break;
                     tc_fence_after();
-                    // (resident weights: one box a tap, kc = 1)
-                    const uint32_t sb = a.resident ? sB + k * a.nt * 64u : sB + s * B_STAGE;
+                    if constexpr (HALO) {
+                        // tap (dy, dx): rows from (dy + 1) x 130 + dx + 1 of planes 2j, 2j + 1 (K 16 each MMA)
+                        for (uint32_t tap = 0; tap < 9u; ++tap) {
+                            const uint32_t row = (tap / 3u) * HALO_W + tap % 3u;
 #pragma unroll
-                    for (uint32_t j = 0; j < 2u; ++j) {
-                        uint64_t ad = umma_desc_sw64(sA + s * A_STAGE + j * 32u, 512u);
-                        uint64_t bd = umma_desc_sw64(sb + j * 32u, 512u);
-                        umma_f16(d, ad, bd, idesc, (k | j) != 0u ? 1u : 0u);
+                            for (uint32_t j = 0; j < 2u; ++j) {
+                                uint64_t ad = umma_desc_plain(sA + s * A_BYTES + 2u * j * HALO_PLANE + row * 16u,
+                                                              HALO_PLANE, 128u);
+                                uint64_t bd = umma_desc_sw64(sB + tap * a.nt * 64u + j * 32u, 512u);
+                                umma_f16(d, ad, bd, idesc, (k | tap | j) != 0u ? 1u : 0u);
+                            }
+                        }
+                    } else {
+                        // (resident weights: one box a tap, kc = 1)
+                        const uint32_t sb = a.resident ? sB + k * a.nt * 64u : sB + s * B_STAGE;
+#pragma unroll
+                        for (uint32_t j = 0; j < 2u; ++j) {
+                            uint64_t ad = umma_desc_sw64(sA + s * A_STAGE + j * 32u, 512u);
+                            uint64_t bd = umma_desc_sw64(sb + j * 32u, 512u);
+                            umma_f16(d, ad, bd, idesc, (k | j) != 0u ? 1u : 0u);
+                        }
                     }
                     umma_commit(empty(s));
                 }
@@ -345,7 +394,7 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ C
         // a wait gave up: let the copies and MMAs in flight land before the memory they use is released
         if (warp == 0) {
             if (a.resident) mbar_wait_drain(wfull, 0u);
-            for (uint32_t i = counts[1]; i < counts[0]; ++i) mbar_wait_drain(full(i % TS), (i / TS) & 1u);
+            for (uint32_t i = counts[1]; i < counts[0]; ++i) mbar_wait_drain(full(i % NS), (i / NS) & 1u);
         } else if (warp == 1) {
             mbar_wait_drain(mma_done, 0u);
         }
@@ -884,9 +933,10 @@ void tile_shape(uint32_t W, uint32_t H, uint32_t& bw, uint32_t& bh, uint32_t& ti
 }
 
 // A tensor map of an activation: (channels, x, y, image) with `stride` channels a pixel, boxes of 32 channels x bw x bh
-// pixels landing as 64-byte rows with the 64-byte swizzle; reads outside the tensor are zeros.
+// pixels landing as 64-byte rows with the 64-byte swizzle (halo: boxes of 8 channels x bw x bh pixels, 16 bytes a
+// pixel, no swizzle); reads outside the tensor are zeros.
 bool act_map(Net* n, CUtensorMap* m, const bf16* p, uint32_t stride, uint32_t B, uint32_t H, uint32_t W, uint32_t bw,
-             uint32_t bh) {
+             uint32_t bh, bool halo = false) {
     EncodeTiledFn enc = encode_tiled();
     if (!enc) {
         n->conv_err = "unet: cuTensorMapEncodeTiled is not available";
@@ -894,10 +944,10 @@ bool act_map(Net* n, CUtensorMap* m, const bf16* p, uint32_t stride, uint32_t B,
     }
     cuuint64_t d[4] = {stride, W, H, B};
     cuuint64_t st[3] = {(cuuint64_t)stride * 2u, (cuuint64_t)W * stride * 2u, (cuuint64_t)H * W * stride * 2u};
-    cuuint32_t box[4] = {32u, bw, bh, 1u}, es[4] = {1u, 1u, 1u, 1u};
+    cuuint32_t box[4] = {halo ? 8u : 32u, bw, bh, 1u}, es[4] = {1u, 1u, 1u, 1u};
     CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16*>(p), d, st, box, es,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, halo ? CU_TENSOR_MAP_SWIZZLE_NONE : CU_TENSOR_MAP_SWIZZLE_64B,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
         n->conv_err = "unet: an activation's tensor map was refused (" + std::to_string((int)r) + ")";
         return false;
@@ -913,10 +963,24 @@ void conv_run(Net* n, const bf16* x, uint32_t x_stride, uint32_t x_off, uint32_t
     uint32_t bw, bh, tiles_x, tiles_y;
     tile_shape(W, H, bw, bh, tiles_x, tiles_y);
     const uint32_t nt = co_pad % 128u == 0u ? 128u : 64u;  // co_pad: a multiple of 64
+    // the nine taps' weights stay in the weight stages' room (9 x nt x 64 bytes <= TS x B_STAGE) where the layer
+    // reads one 32-channel block into one output tile
+    const uint32_t resident = cin == 32u && co_pad == nt && 9u * nt * 64u <= TS * B_STAGE ? 1u : 0u;
+    // ... and such a layer on an image at least 128 wide reads its activations once a tile, with the halo: row tiles
+    // of 128 pixels (the last of a row ragged), boxes of 8 channels x 130 x 3
+    const bool halo = resident && W >= 128u && (x_off % 8u) == 0u;
+    if (halo) {
+        bw = 128u;
+        bh = 1u;
+        tiles_x = (W + 127u) / 128u;
+        tiles_y = H;
+    }
     // the activations: boxes of 32 channels x bw x bh; the weights: (input channel, output channel, tap), boxes of
     // 32 x nt x 1; both 64-byte rows with the 64-byte swizzle
     CUtensorMap xmap, wmap;
-    if (!act_map(n, &xmap, x, x_stride, B, H, W, bw, bh)) return;
+    if (!(halo ? act_map(n, &xmap, x, x_stride, B, H, W, HALO_W, HALO_ROWS, true)
+               : act_map(n, &xmap, x, x_stride, B, H, W, bw, bh)))
+        return;
     cuuint64_t wd[3] = {cin, co_pad, 9u};
     cuuint64_t ws[2] = {(cuuint64_t)cin * 2u, (cuuint64_t)co_pad * cin * 2u};
     cuuint32_t wb[3] = {32u, nt, 1u}, es[3] = {1u, 1u, 1u};
@@ -927,15 +991,13 @@ void conv_run(Net* n, const bf16* x, uint32_t x_stride, uint32_t x_off, uint32_t
         n->conv_err = "unet: a convolution's tensor map was refused (" + std::to_string((int)r) + ")";
         return;
     }
-    // the nine taps' weights stay in the weight stages' room (9 x nt x 64 bytes <= TS x B_STAGE) where the layer
-    // reads one 32-channel block into one output tile
-    const uint32_t resident = cin == 32u && co_pad == nt && 9u * nt * 64u <= TS * B_STAGE ? 1u : 0u;
     Conv a{cin, co_pad, nt, bias, y, y_stride, y_off, cout, yf, B, H, W, x_off, bw, bh, tiles_x, tiles_y, relu,
            n->dev_err, resident, n->hold_next ? 1u : 0u};
     n->hold_next = false;
     const uint32_t tiles = B * tiles_x * tiles_y * (co_pad / nt);
     const uint32_t grid = std::min<uint32_t>(tiles, n->sms * CONV_CTAS_PER_SM);
-    k_conv<<<grid, CONV_THREADS, CONV_SMEM, n->stream>>>(xmap, wmap, a);
+    if (halo) k_conv<true><<<grid, CONV_THREADS, CONV_SMEM_HALO, n->stream>>>(xmap, wmap, a);
+    else k_conv<false><<<grid, CONV_THREADS, CONV_SMEM, n->stream>>>(xmap, wmap, a);
 }
 
 void conv(Net* n, int li, const Act& x, uint32_t x_off, const Act& y, uint32_t y_off, uint32_t B, uint32_t H, uint32_t W,
@@ -1238,7 +1300,9 @@ int trt_unet_create(int device, uint32_t max_batch, uint32_t max_h, uint32_t max
     if (e == cudaSuccess) e = alloc(n, &n->sums, 4);
     if (e == cudaSuccess) e = alloc(n, &n->dev_err, 1);
     if (e == cudaSuccess) e = alloc(n, &n->partial, 3 * FEAT_BLOCKS);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CONV_SMEM);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_conv<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CONV_SMEM);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_conv<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CONV_SMEM_HALO);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WG_SMEM_MAX);
     if (e == cudaSuccess) {
