@@ -91,21 +91,24 @@ def test_forward_on_wide_rows_matches_the_oracle():
 
 
 def test_halo_row_tiles_match_the_oracle():
-    """Images at least 128 wide: the full-resolution layers that read one 32-channel block (and the second level's
-    first, at 256) run the halo kernel, a row tile of 128 pixels read once with its halo and the nine taps as shifted
-    descriptors into it; at 200 the second tile of each row is ragged (72 pixels inside the image). The forward as
-    tight as the 2-D tiles' (activations rounded to bf16 where the device stores them), and every layer's gradient,
-    whose input gradient runs the same kernel with the flipped weights."""
-    wide = unet.UNet(0, max_batch=1, max_h=24, max_w=256)
+    """Images at least 128 wide: a layer of one output tile whose weights fit in shared memory (up to four 32-channel
+    blocks at 64 outputs, two at 128) runs the halo kernel on every level at least 128 wide, a row tile of 128 pixels
+    read once a block with its halo and the nine taps as shifted descriptors into it: at 256 the full-resolution
+    layers (one and three blocks) and the second level's 32 -> 64 and 64 -> 64; at 512 also the third level's
+    64 -> 96 (two blocks, 128 outputs); at 1000 the last tile of each row is ragged on three levels (104, 116 and 122
+    of its 128 pixels inside the image). The
+    forward as tight as the 2-D tiles' (activations rounded to bf16 where the device stores them), and every layer's
+    gradient, whose input gradient runs the same kernel with the flipped weights."""
+    wide = unet.UNet(0, max_batch=1, max_h=24, max_w=1000)
     try:
-        for seed, w in ((12, 200), (13, 256)):
-            p, feats, tgt = case(seed=seed, b=1, h=24, w=w)
+        for seed, h, w in ((12, 16, 1000), (13, 24, 256), (14, 16, 512)):
+            p, feats, tgt = case(seed=seed, b=1, h=h, w=w)
             wide.set_params(p)
             got, _ = wide.forward(feats)
             want, _ = R.forward(R.unpack(bf16(p).astype(np.float64)), bf16(feats).astype(np.float64), act=R.bf16_round)
             err = np.linalg.norm(got - want) / np.linalg.norm(want)
             worst = np.abs(got - want).max() / np.abs(want).max()
-            print(f"halo forward 1x24x{w}: relative error {err:.2e}, worst output {worst:.2e}")
+            print(f"halo forward 1x{h}x{w}: relative error {err:.2e}, worst output {worst:.2e}")
             assert err < 1e-2 and worst < 0.02, (w, err, worst)
             loss, g, _ = wide.step(feats, tgt, update=False, grads=True)
             ref_loss, G, _ = R.loss_and_grads(R.unpack(bf16(p).astype(np.float64)), bf16(feats).astype(np.float64), tgt)

@@ -75,8 +75,13 @@ constexpr uint32_t HALO_W = 130u, HALO_ROWS = 3u;
 constexpr uint32_t HALO_PLANE = (HALO_ROWS * HALO_W * 16u + 127u) / 128u * 128u;  // 6,272 bytes
 constexpr uint32_t HALO_STAGE = 4u * HALO_PLANE, HALO_TS = 3u;
 constexpr uint32_t HALO_W_OFF = (HALO_TS * HALO_STAGE + 1023u) / 1024u * 1024u;  // the resident weights, 1 KB aligned
-constexpr uint32_t HALO_WEIGHTS = 9u * 64u * 64u;                                // nine taps x 64 outputs x 32 inputs
-constexpr uint32_t CONV_SMEM_HALO = HALO_W_OFF + HALO_WEIGHTS + 256u + 1024u;
+constexpr uint32_t SMEM_MAX = 227u * 1024u;                                      // dynamic shared memory a CTA
+// The halo variant's shared memory: the stages, then every (32-channel block, tap) weight box of the output tile
+// (nt rows of 64 bytes each), then the barriers.
+__host__ __device__ constexpr uint32_t halo_weights(uint32_t kc, uint32_t nt) { return 9u * kc * nt * 64u; }
+__host__ __device__ constexpr uint32_t conv_smem_halo(uint32_t kc, uint32_t nt) {
+    return HALO_W_OFF + halo_weights(kc, nt) + 256u + 1024u;
+}
 constexpr uint32_t CONV_EPI_THREADS = 128u, CONV_THREADS = 64u + CONV_EPI_THREADS;  // loader, MMA, 4 epilogue warps
 constexpr uint32_t CONV_CTAS_PER_SM = 2u;
 
@@ -208,8 +213,8 @@ __device__ __forceinline__ void conv_store16(const Conv& a, uint64_t p, uint32_t
     }
 }
 
-// HALO: tiles of 128 x 1 pixels, the weights resident (one 32-channel block, one output tile of 64), and a stage is
-// the tile's activations with their halo (four TMA boxes of 8 channels x 130 pixels x 3 rows, no swizzle) from which
+// HALO: tiles of 128 x 1 pixels, the weights resident (every 32-channel block of one output tile), and a stage is one
+// block of the tile's activations with their halo (four TMA boxes of 8 channels x 130 pixels x 3 rows, no swizzle) from which
 // the nine taps' A operands are read by descriptors shifted (dy x 130 + dx) rows of 16 bytes: one load a tile instead
 // of nine. The taps' MMAs read rows [dy x 130 + dx, + 128) of each plane, inside the box.
 template <bool HALO>
@@ -221,8 +226,9 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ C
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
     const uint32_t sraw = smem_addr(smem_raw), sbase = (sraw + 1023u) & ~1023u;
     uint8_t* smem = smem_raw + (sbase - sraw);
+    const uint32_t kc = a.cin / 32u, nk = HALO ? kc : 9u * kc;
     constexpr uint32_t B_OFF = HALO ? HALO_W_OFF : TS * A_STAGE;
-    constexpr uint32_t BAR_OFF = HALO ? HALO_W_OFF + HALO_WEIGHTS : TS * (A_STAGE + B_STAGE);
+    const uint32_t BAR_OFF = HALO ? HALO_W_OFF + halo_weights(kc, a.nt) : TS * (A_STAGE + B_STAGE);
     const uint32_t sA = sbase, sB = sbase + B_OFF, sBar = sbase + BAR_OFF;
     // barriers: full[NS], empty[NS] (the stages), acc_full[2], acc_empty[2] (the accumulators), mma_done (every MMA
     // issued), wfull (the resident weights); the tensor-memory address, the abort word and the counts of stages issued
@@ -238,7 +244,6 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ C
     const uint32_t ncols = 2u * a.nt;  // two accumulators of nt columns: 128 or 256
     const uint32_t per_img = a.tiles_x * a.tiles_y, n_ntiles = a.co_pad / a.nt;
     const uint32_t tiles = a.B * per_img * n_ntiles;
-    const uint32_t kc = a.cin / 32u, nk = HALO ? kc : 9u * kc;
 
     if (tid == 0) {
         for (uint32_t s = 0; s < NS; ++s) {
@@ -280,10 +285,13 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ C
         if (lane == 0) {
             // the loader: the resident weights (the nine taps' boxes, one after another), then the stages of every tile
             // of this CTA, in order
+            // (halo: every 32-channel block's nine boxes, block-major)
             if (a.resident) {
-                mbar_expect_tx(wfull, 9u * a.nt * 64u);
-                for (uint32_t tap = 0; tap < 9u; ++tap)
-                    tma_load_3d(sB + tap * a.nt * 64u, &wmap, 0, 0, (int)tap, wfull);
+                const uint32_t blocks = HALO ? kc : 1u;
+                mbar_expect_tx(wfull, 9u * blocks * a.nt * 64u);
+                for (uint32_t k = 0; k < blocks; ++k)
+                    for (uint32_t tap = 0; tap < 9u; ++tap)
+                        tma_load_3d(sB + (k * 9u + tap) * a.nt * 64u, &wmap, (int)(k * 32u), 0, (int)tap, wfull);
             }
             uint32_t it = 0;
             bool ok = true;
@@ -337,7 +345,7 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ C
                             for (uint32_t j = 0; j < 2u; ++j) {
                                 uint64_t ad = umma_desc_plain(sA + s * A_BYTES + 2u * j * HALO_PLANE + row * 16u,
                                                               HALO_PLANE, 128u);
-                                uint64_t bd = umma_desc_sw64(sB + tap * a.nt * 64u + j * 32u, 512u);
+                                uint64_t bd = umma_desc_sw64(sB + (k * 9u + tap) * a.nt * 64u + j * 32u, 512u);
                                 umma_f16(d, ad, bd, idesc, (k | tap | j) != 0u ? 1u : 0u);
                             }
                         }
@@ -965,11 +973,20 @@ void conv_run(Net* n, const bf16* x, uint32_t x_stride, uint32_t x_off, uint32_t
     const uint32_t nt = co_pad % 128u == 0u ? 128u : 64u;  // co_pad: a multiple of 64
     // the nine taps' weights stay in the weight stages' room (9 x nt x 64 bytes <= TS x B_STAGE) where the layer
     // reads one 32-channel block into one output tile
-    const uint32_t resident = cin == 32u && co_pad == nt && 9u * nt * 64u <= TS * B_STAGE ? 1u : 0u;
-    // ... and such a layer on an image at least 128 wide reads its activations once a tile, with the halo: row tiles
-    // of 128 pixels (the last of a row ragged), boxes of 8 channels x 130 x 3
-    const bool halo = resident && W >= 128u && (x_off % 8u) == 0u;
+    uint32_t resident = cin == 32u && co_pad == nt && 9u * nt * 64u <= TS * B_STAGE ? 1u : 0u;
+    // A layer of one output tile whose weights fit in shared memory beside three halo stages (up to four 32-channel
+    // blocks at 64 outputs, two at 128), on an image at least 128 wide, reads its activations once a tile with the
+    // halo: row tiles of 128 pixels (the last of a row ragged), boxes of 8 channels x 130 x 3, the weights resident.
+    // (Row tiles that would leave more than an eighth of their pixels outside the image keep the 2-D tiles: at
+    // 320 x 180 the row tiles measured 24.2 against 20.8 us.)
+    const uint32_t kc = cin / 32u, row_tiles = (W + 127u) / 128u;
+    const bool halo = co_pad == nt && cin % 32u == 0u && conv_smem_halo(kc, nt) <= SMEM_MAX && W >= 128u &&
+                      row_tiles * 128u - W <= row_tiles * 16u && (x_off % 8u) == 0u;
+    const uint32_t smem = halo ? conv_smem_halo(kc, nt) : CONV_SMEM;
+    // two CTAs an SM where their shared memory fits (228 KB an SM, 1 KB of it kept a CTA), else one
+    const uint32_t per_sm = 2u * (smem + 1024u) <= 228u * 1024u ? CONV_CTAS_PER_SM : 1u;
     if (halo) {
+        resident = 1u;
         bw = 128u;
         bh = 1u;
         tiles_x = (W + 127u) / 128u;
@@ -995,8 +1012,8 @@ void conv_run(Net* n, const bf16* x, uint32_t x_stride, uint32_t x_off, uint32_t
            n->dev_err, resident, n->hold_next ? 1u : 0u};
     n->hold_next = false;
     const uint32_t tiles = B * tiles_x * tiles_y * (co_pad / nt);
-    const uint32_t grid = std::min<uint32_t>(tiles, n->sms * CONV_CTAS_PER_SM);
-    if (halo) k_conv<true><<<grid, CONV_THREADS, CONV_SMEM_HALO, n->stream>>>(xmap, wmap, a);
+    const uint32_t grid = std::min<uint32_t>(tiles, n->sms * per_sm);
+    if (halo) k_conv<true><<<grid, CONV_THREADS, smem, n->stream>>>(xmap, wmap, a);
     else k_conv<false><<<grid, CONV_THREADS, CONV_SMEM, n->stream>>>(xmap, wmap, a);
 }
 
@@ -1302,7 +1319,7 @@ int trt_unet_create(int device, uint32_t max_batch, uint32_t max_h, uint32_t max
     if (e == cudaSuccess) e = alloc(n, &n->partial, 3 * FEAT_BLOCKS);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_conv<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CONV_SMEM);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_conv<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CONV_SMEM_HALO);
+        e = cudaFuncSetAttribute(k_conv<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WG_SMEM_MAX);
     if (e == cudaSuccess) {
