@@ -43,6 +43,10 @@ struct trt_server {
     trt_ctx* ctx = nullptr;
     trt_server_options opt{};
     cudaStream_t stream = nullptr, copy = nullptr;
+    // each depth's shadow walk on `aux` beside the next depth's closest-hit walk (forked and joined by events, inside
+    // the step's graph)
+    cudaStream_t aux = nullptr;
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     Wave wave;
     unsigned long long* totals = nullptr;
     // The step's table on the device: a StepHead, then at TABLE_JOBS the jobs; pinned staging copies alternate.
@@ -138,10 +142,13 @@ void serve_enqueue(trt_server* s, uint32_t last, uint32_t size, cudaStream_t st)
     cudaMemsetAsync(W.Q.cnt, 0, 4ull * (MAX_DEPTH * CNT_STRIDE + CNT_STRIDE), st);
     k_raygen<<<grid, blk, 0, st>>>(tj, 0u, W.B, W.Q, size, head);
     bool sort_hits = (s->opt.flags & TRT_RENDER_UNSORTED_HITS) == 0;
+    // Each depth's shadow walk runs on the second stream beside the next depth's closest-hit walk, as trt_render
+    // runs them: both read what the depth's shading wrote and write apart (visibility bits; hit records), and the
+    // depth's resolve waits for the shadow walk (the join) before the next depth's hit sort rewrites its order.
+    k_extend<false, false, true><<<s->g_ext, blk, 0, st>>>(tj, none, W.B, W.Q, 0u, W.Q.q[0]);
     for (uint32_t depth = 0; depth <= last; ++depth) {
         uint32_t* raw = W.Q.q[depth & 1u];
         uint32_t* next = W.Q.q[(depth + 1u) & 1u];
-        k_extend<false, false, true><<<s->g_ext, blk, 0, st>>>(tj, none, W.B, W.Q, depth, raw);
         uint32_t* shade_q = raw;
         if (sort_hits) {
             shade_q = W.Q.qx;
@@ -150,7 +157,12 @@ void serve_enqueue(trt_server* s, uint32_t last, uint32_t size, cudaStream_t st)
             k_sort_scatter<SORT_HITS><<<(size + 255u) / 256u, 256, 0, st>>>(W.Q, raw, shade_q, depth);
         }
         k_shade<true><<<grid, blk, 0, st>>>(tj, none, W.B, W.Q, depth, shade_q, next);
-        k_shadow<false, false, true><<<s->g_sha, blk, 0, st>>>(tj, none, W.B, W.Q, depth, nullptr);
+        cudaEventRecord(s->fork_ev, st);
+        cudaStreamWaitEvent(s->aux, s->fork_ev, 0);
+        k_shadow<false, false, true><<<s->g_sha, blk, 0, s->aux>>>(tj, none, W.B, W.Q, depth, nullptr);
+        if (depth < last) k_extend<false, false, true><<<s->g_ext, blk, 0, st>>>(tj, none, W.B, W.Q, depth + 1u, next);
+        cudaEventRecord(s->join_ev, s->aux);
+        cudaStreamWaitEvent(st, s->join_ev, 0);
         k_resolve<true><<<grid, blk, 0, st>>>(tj, none, W.B, W.Q, depth, shade_q);
     }
     k_accumulate_flat<<<grid, blk, 0, st>>>(tj, head, W.B, size);
@@ -352,11 +364,17 @@ int trt_server_create(trt_ctx* c, const trt_server_options* opts, trt_server** o
         c->err = std::string("trt_server_create: ") + what + ": " + cudaGetErrorString(e);
         if (s->stream) cudaStreamDestroy(s->stream);
         if (s->copy) cudaStreamDestroy(s->copy);
+        if (s->aux) cudaStreamDestroy(s->aux);
+        if (s->fork_ev) cudaEventDestroy(s->fork_ev);
+        if (s->join_ev) cudaEventDestroy(s->join_ev);
         delete s;
         return TRT_ECUDA;
     };
     cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->fork_ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->join_ev, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaMalloc(&s->totals, sizeof(unsigned long long) * T_COUNT);
     if (e == cudaSuccess) e = cudaMemsetAsync(s->totals, 0, sizeof(unsigned long long) * T_COUNT, s->stream);
     if (e == cudaSuccess) e = cudaMalloc(&s->table, TABLE_BYTES);
@@ -371,6 +389,9 @@ int trt_server_create(trt_ctx* c, const trt_server_options* opts, trt_server** o
         c->err = "trt_server_create: " + werr;
         if (s->stream) cudaStreamDestroy(s->stream);
         if (s->copy) cudaStreamDestroy(s->copy);
+        if (s->aux) cudaStreamDestroy(s->aux);
+        if (s->fork_ev) cudaEventDestroy(s->fork_ev);
+        if (s->join_ev) cudaEventDestroy(s->join_ev);
         delete s;
         return TRT_ECUDA;
     }
@@ -413,6 +434,9 @@ void trt_server_destroy(trt_server* s) {
     }
     cudaStreamDestroy(s->stream);
     cudaStreamDestroy(s->copy);
+    cudaStreamDestroy(s->aux);
+    cudaEventDestroy(s->fork_ev);
+    cudaEventDestroy(s->join_ev);
     delete s;
 }
 
