@@ -43,8 +43,8 @@ __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)
 //    commits each stage's buffers back to the loader through an mbarrier; TS stages in flight;
 //  - where the layer reads one 32-channel block into one output tile (cin 32, co_pad = N), the nine taps' weight boxes
 //    (36 KB) are loaded once a CTA into the weight stages' room, and a stage loads the activations alone;
-//  - the four warps read the accumulator out of tensor memory (each its 32 lanes = pixels), add the bias, apply the
-//    ReLU and store bf16 (or f32) NHWC.
+//  - eight warps read the accumulator out of tensor memory (two a 32-lane quarter = 32 pixels, each half of the
+//    columns), add the bias, apply the ReLU and store bf16 (or f32) NHWC.
 // Every mbarrier wait is bounded (about a second); a wait that gives up sets the error word, and the CTA waits
 // (bounded) for its copies and MMAs in flight and finishes.
 
@@ -82,7 +82,7 @@ __host__ __device__ constexpr uint32_t halo_weights(uint32_t kc, uint32_t nt) { 
 __host__ __device__ constexpr uint32_t conv_smem_halo(uint32_t kc, uint32_t nt) {
     return HALO_W_OFF + halo_weights(kc, nt) + 256u + 1024u;
 }
-constexpr uint32_t CONV_EPI_THREADS = 128u, CONV_THREADS = 64u + CONV_EPI_THREADS;  // loader, MMA, 4 epilogue warps
+constexpr uint32_t CONV_EPI_THREADS = 256u, CONV_THREADS = 64u + CONV_EPI_THREADS;  // loader, MMA, 8 epilogue warps
 constexpr uint32_t CONV_CTAS_PER_SM = 2u;
 
 __device__ __forceinline__ void mbar_init(uint32_t a, uint32_t count) {
@@ -177,6 +177,17 @@ __device__ __forceinline__ void tmem_ld64(uint32_t taddr, float* v) {
     for (int i = 0; i < 64; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// 32 accumulator columns of this warp's lanes.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
+    uint32_t r[32];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
 // The epilogue of one accumulator row (a pixel) and 16 columns from `c`: bias, ReLU, bf16 NHWC (or the f32 output).
 __device__ __forceinline__ void conv_store16(const Conv& a, uint64_t p, uint32_t c, float* v) {
     if (a.bias) {
@@ -218,7 +229,7 @@ __device__ __forceinline__ void conv_store16(const Conv& a, uint64_t p, uint32_t
 // the nine taps' A operands are read by descriptors shifted (dy x 130 + dx) rows of 16 bytes: one load a tile instead
 // of nine. The taps' MMAs read rows [dy x 130 + dx, + 128) of each plane, inside the box.
 template <bool HALO>
-__global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ CUtensorMap xmap,
+__global__ void __launch_bounds__(CONV_THREADS, 2) k_conv(const __grid_constant__ CUtensorMap xmap,
                                                        const __grid_constant__ CUtensorMap wmap, Conv a) {
     constexpr uint32_t NS = HALO ? HALO_TS : TS;  // stages
     constexpr uint32_t A_BYTES = HALO ? HALO_STAGE : A_STAGE;
@@ -367,9 +378,10 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ C
             umma_commit(mma_done);  // every MMA issued is done (after a wait that gave up too)
         }
     } else {
-        // the epilogue: warp w reads tensor-memory lanes 32 (w % 4) ... (its rows: pixels of the tile)
-        const uint32_t quarter = warp & 3u;
-        const uint32_t m = quarter * 32u + lane;
+        // the epilogue, eight warps, two a tensor-memory lane quarter: warp w reads lanes 32 (w % 4) ... (its rows:
+        // pixels of the tile) and half of the tile's columns, (w - 2) / 4 which
+        const uint32_t quarter = warp & 3u, half = (warp - 2u) >> 2;
+        const uint32_t m = quarter * 32u + lane, cols = a.nt / 2u, c_first = half * cols;
         uint32_t ti = 0;
         for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x, ++ti) {
             const uint32_t acc = ti & 1u;
@@ -382,12 +394,14 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(const __grid_constant__ C
             const int px = x0 + (int)(m % a.bw), py = y0 + (int)(m / a.bw);
             const bool valid = fin && px < (int)a.W && py < (int)a.H;
             const uint64_t p = ((uint64_t)b * a.H + (uint32_t)py) * a.W + (uint32_t)px;
-            for (uint32_t cc = 0; cc < a.nt; cc += 64u) {
-                float v[64];
-                tmem_ld64(tmem + ((quarter * 32u) << 16) + acc * a.nt + cc, v);
-                if (valid)
-#pragma unroll
-                    for (uint32_t q = 0; q < 4u; ++q) conv_store16(a, p, n0 + cc + 16u * q, v + 16u * q);
+            for (uint32_t cc = c_first; cc < c_first + cols; cc += 32u) {
+                if (n0 + cc >= a.cout) break;  // (columns past the layer's outputs: padding, not stored)
+                float v[32];
+                tmem_ld32(tmem + ((quarter * 32u) << 16) + acc * a.nt + cc, v);
+                if (valid) {
+                    conv_store16(a, p, n0 + cc, v);
+                    conv_store16(a, p, n0 + cc + 16u, v + 16u);
+                }
             }
             // this accumulator is read: the MMA issuer may fill it again
             tc_fence_before();
@@ -451,17 +465,6 @@ __device__ __forceinline__ uint64_t umma_desc_mn64(uint32_t saddr, uint32_t lbo)
     return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
            ((uint64_t)(512u >> 4) << 32) | (1ull << 46) | (4ull << 61);
 }
-// 32 accumulator columns of this warp's lanes.
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
-    uint32_t r[32];
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-                 : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
-}
-
 __global__ void __launch_bounds__(WG_THREADS) k_wgrad(const __grid_constant__ CUtensorMap xmap,
                                                      const __grid_constant__ CUtensorMap dymap, WGrad a) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
