@@ -988,16 +988,15 @@ std::pair<cudaEvent_t, cudaEvent_t> take_events(trt_scene* s) {
     return e;
 }
 
-// The walks and the shading live on L1 hits (node records, the walks' stacks, triangle and material records) and use
-// no shared memory: they ask for the whole of the SM's L1 / shared-memory split as L1, also when they share an SM with
-// kernels that use shared memory (measured on the city: 1,138 -> 1,141 Mrays/s; the Cornell box 3,088-3,111 ->
-// 3,116).
+// The binary walks and the shading live on L1 hits (node records, the walks' stacks, triangle and material records)
+// and use no shared memory: they ask for the whole of the SM's L1 / shared-memory split as L1, also when they share an
+// SM with kernels that use shared memory (measured on the city: 1,138 -> 1,141 Mrays/s; the Cornell box 3,088-3,111 ->
+// 3,116). Not the wide walks: their stacks' first entries live in shared memory, and a split that leaves it the least
+// the driver may give a block would hold few of their blocks (the wide walk fell from 912-944 to 336 Mrays/s).
 void prefer_l1() {
     const void* fns[] = {(const void*)k_extend<false, false, false>, (const void*)k_extend<true, false, false>,
-                         (const void*)k_extend<false, true, false>,  (const void*)k_extend<true, true, false>,
                          (const void*)k_extend<false, false, true>,  (const void*)k_shadow<false, false, false>,
-                         (const void*)k_shadow<true, false, false>,  (const void*)k_shadow<false, true, false>,
-                         (const void*)k_shadow<true, true, false>,   (const void*)k_shadow<false, false, true>,
+                         (const void*)k_shadow<true, false, false>,  (const void*)k_shadow<false, false, true>,
                          (const void*)k_shade<false>,                (const void*)k_shade<true>};
     for (const void* f : fns) cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
     cudaGetLastError();  // (a hint: a device that refuses it runs the kernels as they are)
