@@ -336,7 +336,10 @@ __global__ void __launch_bounds__(CONV_THREADS, 2) k_conv(const __grid_constant_
     } else if (warp == 1) {
         if (lane == 0) {
             // the MMA issuer: a tile's stages into accumulator (tile count % 2), then that accumulator to the epilogue
-            const uint32_t idesc = umma_idesc(128u, a.nt);
+            // (a layer of one 64-column output tile with at most 32 outputs: the MMAs' N covers the outputs only, 32
+            // or 16 of the tile's rows of weights; the epilogue reads no column past the outputs)
+            const uint32_t n_mma = a.co_pad == a.nt && a.nt == 64u && a.cout <= 32u ? (a.cout <= 16u ? 16u : 32u) : a.nt;
+            const uint32_t idesc = umma_idesc(128u, n_mma);
             uint32_t it = 0, ti = 0;
             bool ok = !a.resident || mbar_wait(wfull, 0u, a.err, abort_flag);
             for (uint32_t t = blockIdx.x; t < tiles && ok; t += gridDim.x, ++ti) {
