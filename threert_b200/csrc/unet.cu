@@ -63,6 +63,7 @@ struct Conv {
     uint32_t resident;        // 1: every tap's weights loaded once a CTA (one 32-channel block, one output tile)
     uint32_t hold;            // 1: CTA 0 withholds its first activation box (trt_unet_hold_next_load: a test of the
                               // bounded waits), so that the stage's wait runs out
+    uint32_t stages;          // the halo variant's stages (HALO_TS with resident weights; 2 or 3 streaming them)
 };
 
 constexpr uint32_t TS = 5;                  // pipeline stages (82 KB of shared memory: two CTAs an SM)
@@ -75,6 +76,7 @@ constexpr uint32_t HALO_W = 130u, HALO_ROWS = 3u;
 constexpr uint32_t HALO_PLANE = (HALO_ROWS * HALO_W * 16u + 127u) / 128u * 128u;  // 6,272 bytes
 constexpr uint32_t HALO_STAGE = 4u * HALO_PLANE, HALO_TS = 3u;
 constexpr uint32_t HALO_W_OFF = (HALO_TS * HALO_STAGE + 1023u) / 1024u * 1024u;  // the resident weights, 1 KB aligned
+constexpr uint32_t HALO_A_ALIGNED = (HALO_STAGE + 1023u) / 1024u * 1024u;  // a streaming stage's weights start here
 constexpr uint32_t SMEM_MAX = 227u * 1024u;                                      // dynamic shared memory a CTA
 // The halo variant's shared memory: the stages, then every (32-channel block, tap) weight box of the output tile
 // (nt rows of 64 bytes each), then the barriers.
@@ -231,15 +233,18 @@ __device__ __forceinline__ void conv_store16(const Conv& a, uint64_t p, uint32_t
 template <bool HALO>
 __global__ void __launch_bounds__(CONV_THREADS, 2) k_conv(const __grid_constant__ CUtensorMap xmap,
                                                        const __grid_constant__ CUtensorMap wmap, Conv a) {
-    constexpr uint32_t NS = HALO ? HALO_TS : TS;  // stages
-    constexpr uint32_t A_BYTES = HALO ? HALO_STAGE : A_STAGE;
+    // stages, and a stage's bytes: the halo variant's activations, and where the weights are not resident the nine
+    // taps' weight boxes of the stage's 32-channel block after them
+    const uint32_t NS = HALO ? a.stages : TS;
+    const uint32_t A_BYTES = HALO ? (a.resident ? HALO_STAGE : HALO_A_ALIGNED + 9u * a.nt * 64u) : A_STAGE;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
     const uint32_t sraw = smem_addr(smem_raw), sbase = (sraw + 1023u) & ~1023u;
     uint8_t* smem = smem_raw + (sbase - sraw);
     const uint32_t kc = a.cin / 32u, nk = HALO ? kc : 9u * kc;
     constexpr uint32_t B_OFF = HALO ? HALO_W_OFF : TS * A_STAGE;
-    const uint32_t BAR_OFF = HALO ? HALO_W_OFF + halo_weights(kc, a.nt) : TS * (A_STAGE + B_STAGE);
+    const uint32_t BAR_OFF = HALO ? (a.resident ? HALO_W_OFF + halo_weights(kc, a.nt) : NS * A_BYTES)
+                                  : TS * (A_STAGE + B_STAGE);
     const uint32_t sA = sbase, sB = sbase + B_OFF, sBar = sbase + BAR_OFF;
     // barriers: full[NS], empty[NS] (the stages), acc_full[2], acc_empty[2] (the accumulators), mma_done (every MMA
     // issued), wfull (the resident weights); the tensor-memory address, the abort word and the counts of stages issued
@@ -316,11 +321,15 @@ __global__ void __launch_bounds__(CONV_THREADS, 2) k_conv(const __grid_constant_
                     const bool withhold = a.hold && blockIdx.x == 0 && it == 0;
                     if constexpr (HALO) {
                         // the tile's rows y0 - 1 .. y0 + 1, pixels x0 - 1 .. x0 + 128, one box a plane of 8 channels
-                        mbar_expect_tx(full(s), 4u * HALO_ROWS * HALO_W * 16u);
+                        mbar_expect_tx(full(s), 4u * HALO_ROWS * HALO_W * 16u + (a.resident ? 0u : 9u * a.nt * 64u));
                         if (!withhold)
                             for (uint32_t pl = 0; pl < 4u; ++pl)
                                 tma_load_4d(sA + s * A_BYTES + pl * HALO_PLANE, &xmap, (int)(a.x_off + k * 32u + pl * 8u),
                                             x0 - 1, y0 - 1, (int)b, full(s));
+                        if (!a.resident)
+                            for (uint32_t tap = 0; tap < 9u; ++tap)
+                                tma_load_3d(sA + s * A_BYTES + HALO_A_ALIGNED + tap * a.nt * 64u, &wmap, (int)(k * 32u),
+                                            (int)n0, (int)tap, full(s));
                     } else {
                         mbar_expect_tx(full(s), A_STAGE + (a.resident ? 0u : a.nt * 64u));
                         const uint32_t tap = k / kc, c0 = (k % kc) * 32u;
@@ -359,7 +368,9 @@ __global__ void __launch_bounds__(CONV_THREADS, 2) k_conv(const __grid_constant_
                             for (uint32_t j = 0; j < 2u; ++j) {
                                 uint64_t ad = umma_desc_plain(sA + s * A_BYTES + 2u * j * HALO_PLANE + row * 16u,
                                                               HALO_PLANE, 128u);
-                                uint64_t bd = umma_desc_sw64(sB + (k * 9u + tap) * a.nt * 64u + j * 32u, 512u);
+                                const uint32_t wb = a.resident ? sB + (k * 9u + tap) * a.nt * 64u
+                                                               : sA + s * A_BYTES + HALO_A_ALIGNED + tap * a.nt * 64u;
+                                uint64_t bd = umma_desc_sw64(wb + j * 32u, 512u);
                                 umma_f16(d, ad, bd, idesc, (k | tap | j) != 0u ? 1u : 0u);
                             }
                         }
@@ -986,13 +997,19 @@ void conv_run(Net* n, const bf16* x, uint32_t x_stride, uint32_t x_off, uint32_t
     // (Row tiles that would leave more than an eighth of their pixels outside the image keep the 2-D tiles: at
     // 320 x 180 the row tiles measured 24.2 against 20.8 us.)
     const uint32_t kc = cin / 32u, row_tiles = (W + 127u) / 128u;
-    const bool halo = co_pad == nt && cin % 32u == 0u && conv_smem_halo(kc, nt) <= SMEM_MAX && W >= 128u &&
-                      row_tiles * 128u - W <= row_tiles * 16u && (x_off % 8u) == 0u;
-    const uint32_t smem = halo ? conv_smem_halo(kc, nt) : CONV_SMEM;
+    const bool rows_ok = cin % 32u == 0u && W >= 128u && row_tiles * 128u - W <= row_tiles * 16u && (x_off % 8u) == 0u;
+    const bool halo_res = rows_ok && co_pad == nt && conv_smem_halo(kc, nt) <= SMEM_MAX;
+    // Other layers on such levels stream each stage's nine weight boxes beside its activations, one CTA an SM: as
+    // many stages (up to three) as fit.
+    const uint32_t stream_stage = HALO_A_ALIGNED + 9u * nt * 64u;
+    const uint32_t stream_ns = std::min(HALO_TS, (SMEM_MAX - 1280u) / stream_stage);
+    const bool halo = halo_res || (rows_ok && stream_ns >= 2u);
+    const uint32_t stages = halo_res ? HALO_TS : stream_ns;
+    const uint32_t smem = halo_res ? conv_smem_halo(kc, nt) : halo ? stages * stream_stage + 1280u : CONV_SMEM;
     // two CTAs an SM where their shared memory fits (228 KB an SM, 1 KB of it kept a CTA), else one
     const uint32_t per_sm = 2u * (smem + 1024u) <= 228u * 1024u ? CONV_CTAS_PER_SM : 1u;
     if (halo) {
-        resident = 1u;
+        resident = halo_res ? 1u : 0u;
         bw = 128u;
         bh = 1u;
         tiles_x = (W + 127u) / 128u;
@@ -1015,7 +1032,7 @@ void conv_run(Net* n, const bf16* x, uint32_t x_stride, uint32_t x_off, uint32_t
         return;
     }
     Conv a{cin, co_pad, nt, bias, y, y_stride, y_off, cout, yf, B, H, W, x_off, bw, bh, tiles_x, tiles_y, relu,
-           n->dev_err, resident, n->hold_next ? 1u : 0u};
+           n->dev_err, resident, n->hold_next ? 1u : 0u, stages};
     n->hold_next = false;
     const uint32_t tiles = B * tiles_x * tiles_y * (co_pad / nt);
     const uint32_t grid = std::min<uint32_t>(tiles, n->sms * per_sm);
