@@ -226,7 +226,8 @@ __device__ __forceinline__ void conv_store16(const Conv& a, uint64_t p, uint32_t
     }
 }
 
-// HALO: tiles of 128 x 1 pixels, the weights resident (every 32-channel block of one output tile), and a stage is one
+// HALO: tiles of 128 x 1 pixels, the weights resident (every 32-channel block of one output tile) or, where they do
+// not fit, streamed with the activations (a stage then also holds its block's nine weight boxes), and a stage is one
 // block of the tile's activations with their halo (four TMA boxes of 8 channels x 130 pixels x 3 rows, no swizzle) from which
 // the nine taps' A operands are read by descriptors shifted (dy x 130 + dx) rows of 16 bytes: one load a tile instead
 // of nine. The taps' MMAs read rows [dy x 130 + dx, + 128) of each plane, inside the box.
