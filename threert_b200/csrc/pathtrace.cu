@@ -1419,7 +1419,8 @@ int trt_scene_update(trt_scene* s, uint32_t which, uint64_t offset, const void* 
         // The wide BVH is rebuilt from the edited buffers at the next render; of the tables it reads only the units'
         // mesh roots, first triangles and shadow bits, so an edit that leaves those alone (units moved by their
         // transforms) keeps it.
-        if (which != 3 || s->wide.reads_edit(s->host[3].data(), offset, static_cast<const uint8_t*>(src), bytes))
+        if (which != 3 ||
+            s->wide.reads_edit(s->host[3].data(), s->host[3].size(), offset, static_cast<const uint8_t*>(src), bytes))
             s->wide.invalidate();
         std::memcpy(s->host[which].data() + offset, src, bytes);
     }

@@ -511,10 +511,14 @@ bool WideBvh::key_matches(const uint32_t* P) const {
     return std::memcmp(k, key, sizeof(k)) == 0;
 }
 
-bool WideBvh::reads_edit(const uint8_t* old_tables, uint64_t offset, const uint8_t* src, uint64_t bytes) const {
+bool WideBvh::reads_edit(const uint8_t* old_tables, uint64_t tables_bytes, uint64_t offset, const uint8_t* src,
+                         uint64_t bytes) const {
     if (!built || bytes == 0) return false;
-    const uint64_t t_inst = key[2], n_units = key[1], end = offset + bytes;
-    const uint64_t first = t_inst * 16, last = (t_inst + 10 * n_units) * 16;  // the unit records' bytes
+    const uint64_t t_inst = key[2], end = offset + bytes;
+    const uint64_t first = t_inst * 16;
+    if (first >= tables_bytes) return false;
+    const uint64_t n_units = std::min<uint64_t>(key[1], (tables_bytes - first) / 160);  // (records inside the copy)
+    const uint64_t last = first + 160 * n_units;  // the unit records' bytes
     if (end <= first || offset >= last) return false;
     const uint64_t r0 = (std::max(offset, first) - first) / 160, r1 = std::min(n_units, (end - first + 159) / 160);
     // A record's words the build reads: vec4 3's w (the mesh root), vec4 6's x (the first triangle), and of vec4 4's

@@ -136,7 +136,8 @@ struct WideBvh {
     bool key_matches(const uint32_t* params) const;
     // Whether writing src[0, bytes) at byte `offset` of the tables (old: the host copy before it) changes a word the
     // build read: a unit record's mesh root, first triangle or bits.
-    bool reads_edit(const uint8_t* old_tables, uint64_t offset, const uint8_t* src, uint64_t bytes) const;
+    bool reads_edit(const uint8_t* old_tables, uint64_t tables_bytes, uint64_t offset, const uint8_t* src,
+                    uint64_t bytes) const;
     void release();
     void invalidate() { built = false; }
 };
